@@ -1,0 +1,422 @@
+"""Benchmark: plain path tracing at scale (Mpaths/s) on one or more B200s.
+
+Workload (one step): the displaced-sphere scene - an icosphere subdivided to 1,997,120 triangles
+and displaced by fBm of amplitude 0.05 over a 2-triangle ground plane, per-object Disney
+parameters from seed 0, 4 quad lights and a constant environment of 0.1 - rendered at
+1920 x 1080 with 64 samples per pixel and path depth 16 in FP32 (132,710,400 paths), through
+wl_render in WL_MATH_FAST mode with the reference's TEA+LCG streams, uniform light selection,
+MIS and Russian roulette (after depth 5, p = 0.9). Synthetic data; the BVH is built once
+outside the timed region (Mpaths/s = W * H * spp / render time).
+
+Prints one JSON line (see the keys below). `--impl reference` times the reference's own device
+arithmetic (src/Frontend/Device/*.h compiled on the host, oracle/_ref/libwlref.so) inside a CPU
+restatement of PathTracing.cu's loop on all host cores, on a bounded sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W, H, SPP, DEPTH = 1920, 1080, 64, 16
+METRIC = "Mpaths/s"
+WORKLOAD = "plain PT at scale: displaced icosphere 1,997,120 tris + ground, 4 quad lights + env 0.1, 1920x1080, 64 spp, depth 16, FP32"
+
+
+def env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (SM clock, throttle reasons)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.flush()
+        rows = [l.split(",") for l in open(self.f.name).read().strip().splitlines() if l.strip()]
+        os.unlink(self.f.name)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for k, n in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+class CpuPT:
+    """The CPU path tracer on a bounded sample of the workload (pixel rows at 64 spp): the
+    reference's own device arithmetic (oracle/_ref/libwlref.so, kind "reference") when it was
+    built, else the project's CPU port (oracle/_build/liboracle.so, kind "port")."""
+
+    def __init__(self, scene, threads):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import ctypes as C
+        import pyoracle as po
+        self.C = C
+        self.threads = threads
+        if os.path.exists(po.LIB_REF):
+            self.lib, self.kind = po.RefLib(), "reference"
+        else:
+            self.lib, self.kind = po.Oracle(), "port"
+        self.cam = po.Camera()
+        for k in ("pos", "look_at", "up", "right"):
+            getattr(self.cam, k)[:] = [float(x) for x in scene.camera[k]]
+        self.p = po.RenderParams(width=W, height=H, spp=SPP, first_frame=0, max_depth=DEPTH,
+                                 rr_depth=5, rr_prob=0.9, eps=1e-3, strategy=2, rng=0, math=1,
+                                 lights=0, seed=0)
+        self.p.env[:] = list(scene.env)
+        self.keep, self.osc = po.make_or_scene(scene)
+        self.bvh = self.lib.lib.or_bvh_create(self.osc.V, self.osc.I, self.osc.nT)
+        self.film = np.zeros((H, W, 3), np.float32)
+        self.npx = None
+
+    def run(self, lo, hi):
+        C = self.C
+        t = time.perf_counter()
+        if self.kind == "reference":
+            self.lib.lib.ref_render(C.byref(self.osc), self.bvh, C.byref(self.cam), C.byref(self.p),
+                                    self.threads, self.film.ctypes.data, lo, hi)
+        else:
+            self.lib.lib.or_render(C.byref(self.osc), self.bvh, C.byref(self.cam), C.byref(self.p), 0,
+                                   self.threads, self.film.ctypes.data, None, lo, hi)
+        return time.perf_counter() - t
+
+    def calibrate(self, target_s):
+        mid = (H // 2) * W
+        dt = self.run(mid, mid + 4 * W)
+        rate = 4 * W / max(dt, 1e-6)
+        self.npx = int(min(max(rate * target_s, W), H * W // 2))
+
+    def sample(self):
+        """Returns (Mpaths/s, description) for one timed sample."""
+        lo = (H // 2) * W - self.npx // 2
+        dt = self.run(lo, lo + self.npx)
+        desc = (f"{self.npx} pixels ({self.npx / W:.1f} rows around the image centre) x {SPP} spp "
+                f"= {self.npx * SPP} paths in {dt:.1f} s")
+        return self.npx * SPP / dt / 1e6, desc
+
+    def close(self):
+        self.lib.lib.or_bvh_destroy(self.bvh)
+
+
+def reference_arm(args):
+    rank = env_int("RANK", 0)
+    if rank != 0:
+        return 0
+    from wayland_b200 import scenes
+    scene = scenes.displaced_sphere(W, H, SPP, DEPTH)
+    threads = os.cpu_count() or 1
+    cpu = CpuPT(scene, threads)
+    cpu.calibrate(args.ref_step_s)
+    vals, desc = [], ""
+    for step in range(args.warmup + args.steps):
+        v, desc = cpu.sample()
+        if step >= args.warmup:
+            vals.append(v)
+    cpu.close()
+    value = float(statistics.mean(vals))
+    line = {"metric": METRIC, "value": round(value, 4), "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(W * H * SPP / (value * 1e6) * 1e3, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "device": "host CPU", "threads": threads},
+            "cpu_baseline": {"value": round(value, 4), "unit": METRIC, "cores": threads,
+                             "kind": cpu.kind, "sample": desc},
+            "e2e": {"value": round(value, 4), "unit": METRIC, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    if cpu.kind != "reference":
+        line["note"] = "oracle/_ref/libwlref.so absent: the project's CPU port of the same loop was timed"
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def raycast_microbench(wl, torch, ctx, sc, scene, stream):
+    """2^24 coherent primary rays (4096 x 4096 view) and 2^24 cosine-distributed bounce rays from
+    the primary hit points; Mrays/s and traversal counts."""
+    n_side = 4096
+    dev = torch.device("cuda")
+    cam = {k: torch.tensor(np.asarray(scene.camera[k], np.float32), device=dev) for k in scene.camera}
+    # square view with the camera's vertical field of view
+    right = cam["right"] / torch.linalg.norm(cam["right"]) * torch.linalg.norm(cam["up"])
+    j, i = torch.meshgrid(torch.arange(n_side, device=dev), torch.arange(n_side, device=dev), indexing="ij")
+    u = (2.0 * (i.float() + 0.5) / n_side - 1.0).reshape(-1, 1)
+    v = (2.0 * (j.float() + 0.5) / n_side - 1.0).reshape(-1, 1)
+    d = cam["look_at"][None] + right[None] * u + cam["up"][None] * v
+    d = d / torch.linalg.norm(d, dim=1, keepdim=True)
+    n = d.shape[0]
+    rays = torch.zeros((n, 8), dtype=torch.float32, device=dev)
+    rays[:, 0:3] = cam["pos"][None]
+    rays[:, 3] = 1e-3
+    rays[:, 4:7] = d
+    rays[:, 7] = 1e30
+    hits = torch.empty((n, 4), dtype=torch.float32, device=dev)
+
+    def timed(rbuf, reps=5):
+        with torch.cuda.stream(stream):
+            sc.cast(rbuf.data_ptr(), hits.data_ptr(), n, wl.CAST_CLOSEST)
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                sc.cast(rbuf.data_ptr(), hits.data_ptr(), n, wl.CAST_CLOSEST)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    t_primary = timed(rays)
+    nodes_p, tris_p = sc.cast_stats(rays.data_ptr(), n)
+    # bounce rays from the primary hits
+    with torch.cuda.stream(stream):
+        sc.cast(rays.data_ptr(), hits.data_ptr(), n, wl.CAST_CLOSEST)
+    torch.cuda.synchronize()
+    prim = hits[:, 1].view(torch.int32)
+    ok = prim != -1
+    V = torch.from_numpy(scene.V).to(dev)
+    I = torch.from_numpy(scene.I.astype(np.int64)).to(dev)
+    p = torch.where(ok, prim, torch.zeros_like(prim)).long()
+    a, b, c = V[I[p, 0]], V[I[p, 1]], V[I[p, 2]]
+    ng = torch.cross(b - a, c - a, dim=1)
+    ng = ng / torch.linalg.norm(ng, dim=1, keepdim=True).clamp_min(1e-30)
+    ng = torch.where((ng * rays[:, 4:7]).sum(1, keepdim=True) > 0, -ng, ng)
+    g = torch.Generator(device=dev)
+    g.manual_seed(0)
+    r1 = torch.rand(n, device=dev, generator=g)
+    r2 = torch.rand(n, device=dev, generator=g)
+    phi = 2 * np.pi * r1
+    sx, sy, sz = torch.sqrt(r2) * torch.cos(phi), torch.sqrt(r2) * torch.sin(phi), torch.sqrt(1 - r2)
+    t1 = torch.where(ng[:, 0:1].abs() > 0.9, torch.tensor([[0.0, 1.0, 0.0]], device=dev),
+                     torch.tensor([[1.0, 0.0, 0.0]], device=dev))
+    tx = torch.cross(ng, t1, dim=1)
+    tx = tx / torch.linalg.norm(tx, dim=1, keepdim=True)
+    ty = torch.cross(ng, tx, dim=1)
+    bd = tx * sx[:, None] + ty * sy[:, None] + ng * sz[:, None]
+    brays = torch.zeros_like(rays)
+    brays[:, 0:3] = rays[:, 0:3] + rays[:, 4:7] * hits[:, 0:1]
+    brays[:, 3] = 1e-3
+    brays[:, 4:7] = bd
+    brays[:, 7] = 1e30
+    # rays whose primary missed become copies of primary rays (still 2^24 traced)
+    brays = torch.where(ok[:, None], brays, rays)
+    t_bounce = timed(brays)
+    nodes_b, tris_b = sc.cast_stats(brays.data_ptr(), n)
+    out = {}
+    for name, t, nn, tt in (("primary", t_primary, nodes_p, tris_p), ("bounce", t_bounce, nodes_b, tris_b)):
+        nodes_per, tris_per = nn / n, tt / n
+        bytes_per = 48 + 80 * nodes_per + 48 * tris_per
+        out[name] = {"rays": n, "ms": round(t, 3), "mrays_s": round(n / t / 1e3, 1),
+                     "nodes_per_ray": round(nodes_per, 2), "tris_per_ray": round(tris_per, 2),
+                     "algorithmic_gbs": round(n * bytes_per / (t * 1e-3) / 1e9, 1)}
+    out["primary_hit_fraction"] = round(float(ok.float().mean()), 4)
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ref-step-s", type=float, default=8.0, help="CPU seconds per reference step")
+    ap.add_argument("--cpu-sample-s", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-raycast", action="store_true")
+    ap.add_argument("--math", default="fast", choices=["fast", "strict"])
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+    import wayland_b200 as wl
+    from wayland_b200 import scenes
+
+    world = env_int("WORLD_SIZE", 1)
+    rank = env_int("RANK", 0)
+    local = env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    scene = scenes.displaced_sphere(W, H, SPP, DEPTH)
+    ctx = wl.Context(local)
+    sc = wl.Scene(ctx, scene)
+    info = sc.info()
+    film = wl.Film(ctx, W, H)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    cam = scene.camera_struct()
+    math_mode = wl.MATH_FAST if args.math == "fast" else wl.MATH_STRICT
+    # each rank renders its own 64 samples per pixel (frames rank*64 ...): weak scaling, no
+    # data-path collective
+    params = wl.render_params(W, H, SPP, max_depth=DEPTH, env=scene.env, math=math_mode,
+                              first_frame=rank * SPP)
+    paths = W * H * SPP
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        wl.render(ctx, sc, cam, params, film)
+    ctx.sync()
+    # untimed pass with traversal counters: segments per path, node visits and triangle tests
+    sp = wl.render_params(W, H, SPP, max_depth=DEPTH, env=scene.env, math=math_mode,
+                          first_frame=rank * SPP, flags=wl._abi.RENDER_TRAVERSAL_STATS)
+    wl.render(ctx, sc, cam, sp, film)
+    tstats = ctx.stats()
+
+    clocks = Clocks(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        wl.render(ctx, sc, cam, params, film)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    # per-kernel device times of the last timed render (CUDA events the library records around
+    # each launch on its stream)
+    st = ctx.stats()
+    ext_ms, shade_ms, shadow_ms, other_ms = st["ms_extend"], st["ms_shade"], st["ms_shadow"], st["ms_other"]
+    launches = st["kernel_launches"] * args.steps
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    ms_step = ms_max / args.steps
+    value = world * paths * args.steps / (ms_max * 1e-3) / 1e6
+
+    # end to end through the public API with host buffers: render + film download per step
+    host_film = np.empty((H, W, 3), np.float32)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        wl.render(ctx, sc, cam, params, film)
+        film.download(host_film)
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    et = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(et, op=dist.ReduceOp.MAX)
+    e2e_value = world * paths / float(et.item()) / 1e6
+
+    line = None
+    if rank == 0:
+        peak, peak_kind = peaks()
+        segs = tstats["segments"]
+        seg_per_path = segs / paths
+        nodes_per = tstats["extend_node_visits"] / max(segs, 1)
+        tris_per = tstats["extend_tri_tests"] / max(segs, 1)
+        b_ray = 48 + 80 * nodes_per + 48 * tris_per
+        achieved = segs * b_ray / (ext_ms * 1e-3) / 1e9
+        b_path = 96 + 364 * seg_per_path
+        traffic = None
+        tf = os.path.join(ROOT, "profiles", "extend_traffic.json")
+        if os.path.exists(tf):
+            traffic = json.load(open(tf)).get("dram_bytes_per_launch")
+        line = {
+            "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": SPP, "max_depth": DEPTH,
+                       "triangles": scene.num_tris, "math": args.math, "rng": "tea_lcg",
+                       "strategy": "mis", "parallelism": f"{world} independent sample sets (weak)",
+                       "l2": "working set larger than L2 (BVH %.0f MB + path queues), no flush" % (info["bytes"] / 1e6)},
+            "e2e": {"value": round(e2e_value, 2), "unit": METRIC,
+                    "h2d_bytes_per_step": 128, "d2h_bytes_per_step": W * H * 12},
+            "roofline": {"bound": "hbm", "kernel": "k_extend (closest-hit traversal)",
+                         "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "peak_kind": peak_kind,
+                         "bytes_per_ray": round(b_ray, 1),
+                         "note": "algorithmic bytes = rays x (48 + 80 N_node + 48 N_tri); BVH nodes are mostly L2 hits, so DRAM traffic is far below this"},
+            "roofline_path": {"bytes_per_path": round(b_path, 1),
+                              "achieved_gbs": round(b_path * value * 1e6 / world / 1e9, 1),
+                              "frac": round(b_path * value * 1e6 / world / 1e9 / peak, 4)},
+            "kernels_ms_per_step": {"extend": round(ext_ms, 2), "shade": round(shade_ms, 2),
+                                    "shadow": round(shadow_ms, 2), "other": round(other_ms, 2)},
+            "segments_per_path": round(seg_per_path, 3),
+            "shadow_rays_per_path": round(tstats["shadow_rays"] / paths, 3),
+            "extend_nodes_per_ray": round(nodes_per, 2), "extend_tris_per_ray": round(tris_per, 2),
+            "bvh": {"wide_nodes": info["wide_nodes"], "depth": info["wide_depth"],
+                    "build_ms": round(info["ms_build"], 1)},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        if not args.no_raycast:
+            line["raycast"] = raycast_microbench(wl, torch, ctx, sc, scene, stream)
+        if world == 1 and not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            cpu = CpuPT(scene, threads)
+            cpu.calibrate(args.cpu_sample_s)
+            v, desc = cpu.sample()
+            cpu.close()
+            line["cpu_baseline"] = {"value": round(v, 4), "unit": METRIC, "cores": threads,
+                                    "kind": cpu.kind, "sample": desc}
+    film.close()
+    sc.close()
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

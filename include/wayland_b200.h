@@ -1,0 +1,291 @@
+/*
+ * wayland_b200.h - C ABI of the B200-native renderer backend.
+ *
+ * This header replaces the OptiX-facing seam of EasyRender (Extra-Creativity/Wayland):
+ *   - src/Frontend/Core/DeviceManager.h:25-30   (SetupOptix / Launch / DownloadFrameBuffer /
+ *                                                GetTraversableHandle)
+ *   - src/Frontend/Core/ProgramManager.h:6-19   (Setup / Update / End / GetParamPtr /
+ *                                                GenerateSBT)
+ *   - src/Backend/Optix/Core/AccelStructure.cpp:133-162 (StaticAccelStructure = optixAccelBuild)
+ *   - src/Backend/Optix/Core/Launcher.cpp:12-20 (optixLaunch)
+ *   - src/Frontend/Programs/PathTracing/PathTracingLaunchParams.h:20-78 (LaunchParams / HitData)
+ *
+ * Conventions
+ *   - Every entry point returns int status (WL_OK == 0); no C++ exception crosses the ABI.
+ *     The reference only throws under ERROR_DEBUG (src/Backend/Optix/Utils/HostUtils/
+ *     ErrorCheck.h:9-59) and is silent otherwise; here every failure is reported.
+ *   - wl_last_error_string() returns a thread-local message for the last failure.
+ *   - The library owns all device memory behind opaque handles. Host arrays passed to
+ *     wl_scene_create are copied; nothing is retained.
+ *   - One wl_context = one device + one CUDA stream. Calls are stream ordered; the only
+ *     calls that synchronise are the *_download / *_host variants and wl_context_sync.
+ *   - Handles are not thread safe (the reference is single threaded: ContextManager.h:84-123).
+ */
+#ifndef WAYLAND_B200_H
+#define WAYLAND_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define WL_API __attribute__((visibility("default")))
+#else
+#define WL_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------ */
+enum {
+    WL_OK = 0,
+    WL_ERR_INVALID_ARG = 1,
+    WL_ERR_CUDA = 2,
+    WL_ERR_OOM = 3,
+    WL_ERR_QUEUE_OVERFLOW = 4,
+    WL_ERR_TIMEOUT = 5,
+    WL_ERR_NOT_BUILT = 6,
+    WL_ERR_UNSUPPORTED = 7
+};
+
+/* ---- enums ------------------------------------------------------------------------- */
+/* Integrator strategy: PathTracing.cu:21-29 (UPT = BSDF sampling only, NEE = light sampling
+ * only, MIS = both with the balance heuristic). */
+enum { WL_STRATEGY_UPT = 0, WL_STRATEGY_NEE = 1, WL_STRATEGY_MIS = 2 };
+
+/* Per-path random stream.
+ *  TEA_LCG: seed = tea<4>(pixelIndex, frameID), then LCG (Random.h:34-71), the reference's.
+ *  PCG32  : PCG-XSH-RR 64/32 (O'Neill 2014), one stream per pixel, state seeded by
+ *           (params.seed, frameID). */
+enum { WL_RNG_TEA_LCG = 0, WL_RNG_PCG32 = 1 };
+
+/* Arithmetic mode of the shading kernels.
+ *  FAST  : fast-math (hardware sin/cos/log, approximate div/sqrt, FMA contraction, FTZ),
+ *          like the reference's `nvcc --use_fast_math` (Module.h:23-31).
+ *  STRICT: IEEE single precision, no FMA contraction, the project's own sin/cos/log.
+ *          Bit-identical to the CPU oracle for the same inputs. */
+enum { WL_MATH_FAST = 0, WL_MATH_STRICT = 1 };
+
+/* Light selection for next-event estimation.
+ *  UNIFORM: uniform light, uniform triangle, uniform area (Sample.h:105-132), the reference's.
+ *  POWER  : one FP64 prefix-sum CDF over all emissive triangles, weighted by area x
+ *           luminance(L); pdf_A = weight / total / area. */
+enum { WL_LIGHTS_UNIFORM = 0, WL_LIGHTS_POWER = 1 };
+
+/* Film accumulation.
+ *  RUNNING_MEAN: FP32 storage, running mean last*f/(f+1) + x/(f+1) computed in double
+ *                (PathTracing.cu:145-154), the reference's.
+ *  FP64_SUM    : FP64 sum plus sample count (oracle film; mean = sum / count). */
+enum { WL_FILM_RUNNING_MEAN = 1u, WL_FILM_FP64_SUM = 2u };
+
+/* BVH builders. */
+enum { WL_BVH_LBVH = 0, WL_BVH_SAH = 1 };
+
+/* Ray cast modes for wl_cast_rays. */
+enum { WL_CAST_CLOSEST = 0, WL_CAST_ANY = 1 };
+
+/* ---- plain data ------------------------------------------------------------------- */
+/* Device::DisneyMaterial (src/Frontend/Device/Material.h:7-22), same field order, plus a
+ * texture index (Disney::textureId, Material.h:62; -1 = none). */
+typedef struct wl_disney {
+    float color[3];
+    float metallic;
+    float roughness;
+    float specular;
+    float specular_tint;
+    float eta;
+    float trans;
+    float subsurface;
+    float anisotropic;
+    float sheen;
+    float sheen_tint;
+    float clearcoat;
+    float clearcoat_gloss;
+    int32_t texture;
+} wl_disney;
+
+/* AreaLight (src/Frontend/Core/Light.h:8-14) + Device::DeviceAreaLight (Device/Light.h:9-17).
+ * The emitting mesh is the contiguous triangle range [first_tri, first_tri + tri_count) of
+ * the scene's index array (the reference binds one light to one mesh:
+ * SceneManager.cpp:236-246, DeviceManager.cpp:160-177). */
+typedef struct wl_area_light {
+    float L[3];
+    int32_t two_sided;
+    uint32_t first_tri;
+    uint32_t tri_count;
+} wl_area_light;
+
+/* Device::PinholeCamFrame (src/Frontend/Device/Camera.h:11-17). `up` is pre-scaled by
+ * tan(fov/2) and `right` by the aspect ratio, as PathTracingProgramManager.cpp:25-28 does. */
+typedef struct wl_camera {
+    float pos[3];
+    float look_at[3];
+    float up[3];
+    float right[3];
+} wl_camera;
+
+/* LaunchParams (PathTracingLaunchParams.h:45-58) + the integrator constants that the
+ * reference hard-codes (PathTracing.cu:19-29, 68, 130-138, 235). */
+typedef struct wl_render_params {
+    uint32_t width, height;
+    uint32_t spp;           /* samples per pixel rendered by this call (reference: 1 per frame) */
+    uint32_t first_frame;   /* frameID of the first sample (seeds and running mean) */
+    uint32_t max_depth;     /* a hit at this depth ends the path (reference: 25) */
+    uint32_t rr_depth;      /* Russian roulette when depth > rr_depth (reference: 5) */
+    float rr_prob;          /* continuation probability (reference: 0.9) */
+    float eps;              /* ray tmin and shadow shortening (reference: 1e-3) */
+    uint32_t strategy;      /* WL_STRATEGY_* (reference: MIS) */
+    uint32_t rng;           /* WL_RNG_* */
+    uint32_t math;          /* WL_MATH_* */
+    uint32_t lights;        /* WL_LIGHTS_* */
+    uint64_t seed;          /* PCG32 seed (ignored for TEA_LCG) */
+    float env[3];           /* constant radiance returned by a miss (reference: 0) */
+    uint32_t wave_paths;    /* paths in flight per wave; 0 = automatic */
+    uint32_t flags;         /* WL_RENDER_* bits */
+} wl_render_params;
+
+/* wl_render_params.flags: count BVH node visits and triangle tests of every traced ray into
+ * wl_render_stats (a slower instrumented traversal; for reporting, not for timing). */
+enum { WL_RENDER_TRAVERSAL_STATS = 1u };
+
+/* A ray as stored in the HBM ray queue: 32 bytes, two 16-byte vectors. */
+typedef struct wl_ray {
+    float org[3];
+    float tmin;
+    float dir[3];
+    float tmax;
+} wl_ray;
+
+/* A closest hit: 16 bytes. prim = UINT32_MAX on a miss; (u, v) are the barycentric weights of
+ * vertices 1 and 2 (optixGetTriangleBarycentrics convention). For WL_CAST_ANY, prim is 0 when
+ * the segment is occluded and UINT32_MAX when it is free. */
+typedef struct wl_hit {
+    float t;
+    uint32_t prim;
+    float u, v;
+} wl_hit;
+
+/* Counters of the last wl_render call. */
+typedef struct wl_render_stats {
+    uint64_t paths;             /* W*H*spp */
+    uint64_t segments;          /* closest-hit rays traced (extend) */
+    uint64_t shadow_rays;       /* any-hit rays traced */
+    uint32_t waves;
+    uint32_t kernel_launches;
+    float ms_total;             /* device time of the whole call (CUDA events) */
+    float ms_extend;            /* device time in closest-hit traversal kernels */
+    float ms_shade;
+    float ms_shadow;
+    float ms_other;
+    uint64_t extend_node_visits;   /* with WL_RENDER_TRAVERSAL_STATS */
+    uint64_t extend_tri_tests;
+    uint64_t shadow_node_visits;
+    uint64_t shadow_tri_tests;
+} wl_render_stats;
+
+/* BVH description for parity tests and reporting. */
+typedef struct wl_bvh_info {
+    uint32_t kind;
+    uint32_t num_tris;
+    uint32_t binary_nodes;      /* internal nodes of the binary tree (n - 1) */
+    uint32_t wide_nodes;        /* 8-wide compressed nodes */
+    uint32_t wide_depth;
+    uint32_t leaf_tris;         /* triangle records referenced by wide leaves (== num_tris) */
+    float ms_build;             /* device time of the build */
+    uint64_t bytes;             /* device bytes of nodes + triangle records */
+} wl_bvh_info;
+
+typedef struct wl_context wl_context;
+typedef struct wl_scene wl_scene;
+typedef struct wl_film wl_film;
+
+/* ---- context ---------------------------------------------------------------------- */
+/* ContextManager() (src/Backend/Optix/Core/ContextManager.cpp:99-157): one device, one
+ * stream. */
+WL_API int wl_context_create(int device, wl_context **out);
+WL_API int wl_context_destroy(wl_context *ctx);
+/* Make the context issue its work on an existing stream (e.g. the caller's); 0 = own. */
+WL_API int wl_context_set_stream(wl_context *ctx, void *cuda_stream);
+WL_API int wl_context_get_stream(wl_context *ctx, void **cuda_stream);
+WL_API int wl_context_sync(wl_context *ctx);
+WL_API const char *wl_last_error_string(void);
+WL_API const char *wl_version(void);
+
+/* ---- scene ------------------------------------------------------------------------ */
+/* DeviceManager::AllocDeviceBuffer + UploadDeviceBuffer (DeviceManager.cpp:77-181) over the
+ * flattened SceneManager fields (SceneManager.h:30-44).
+ *   V: 3*nV floats. N, UV: 3*nV / 2*nV floats or NULL. I: 3*nT vertex indices.
+ *   tri_material: nT material indices. tri_flags: nT flags or NULL (bit 0: use vertex normals,
+ *   default = N != NULL). lights: emitting triangle ranges (see wl_area_light). */
+WL_API int wl_scene_create(wl_context *ctx, const float *V, uint32_t nV, const float *N,
+                    const float *UV, const uint32_t *I, uint32_t nT,
+                    const uint32_t *tri_material, const uint32_t *tri_flags,
+                    const wl_disney *mats, uint32_t nMat, const wl_area_light *lights,
+                    uint32_t nLight, wl_scene **out);
+WL_API int wl_scene_destroy(wl_scene *scene);
+/* Add an RGBA8 texture (DeviceManager::UploadTextures, DeviceManager.cpp:183-229: bilinear,
+ * wrap, normalised float read). Returns its index through *index. */
+WL_API int wl_scene_add_texture(wl_scene *scene, const uint8_t *rgba8, uint32_t width,
+                         uint32_t height, int32_t *index);
+
+/* ---- acceleration structure -------------------------------------------------------- */
+/* StaticAccelStructure (AccelStructure.cpp:133-162): build the BVH of the scene on the GPU.
+ * WL_BVH_LBVH: 63-bit Morton codes -> radix tree (Karras 2012) -> bottom-up refit ->
+ *              8-wide compressed BVH. WL_BVH_SAH: binned-SAH top levels over the same. */
+WL_API int wl_bvh_build(wl_scene *scene, uint32_t kind);
+WL_API int wl_bvh_get_info(wl_scene *scene, wl_bvh_info *info);
+/* Parity exports (host arrays). Morton codes in the scene's triangle order; the binary radix
+ * tree as Karras' layout: internal nodes 0..n-2, leaves n-1..2n-2 in sorted order; child
+ * indices use that single index space. */
+WL_API int wl_bvh_export_morton(wl_scene *scene, uint64_t *codes, uint32_t n);
+WL_API int wl_bvh_export_binary(wl_scene *scene, uint32_t *sorted_prims, int32_t *left,
+                         int32_t *right, int32_t *parent, float *bounds /* 6*(2n-1) */,
+                         uint32_t n);
+
+/* optixTrace over a fixed batch (PathTracing.cu:72-75 closest, :92-102 any hit).
+ * Device pointers, stream ordered. */
+WL_API int wl_cast_rays(wl_scene *scene, const wl_ray *d_rays, wl_hit *d_hits, uint32_t n,
+                 uint32_t mode);
+/* Same with host buffers (copies in and out, synchronous). */
+WL_API int wl_cast_rays_host(wl_scene *scene, const wl_ray *rays, wl_hit *hits, uint32_t n,
+                      uint32_t mode);
+/* Traversal cost counters (node and triangle visits per ray) for the roofline figures. */
+WL_API int wl_cast_rays_stats(wl_scene *scene, const wl_ray *d_rays, uint32_t n, uint32_t mode,
+                       uint64_t *node_visits, uint64_t *tri_tests);
+
+/* ---- film and rendering ----------------------------------------------------------- */
+/* The radiance buffer of PathTracingProgramManager::Setup (PathTracingProgramManager.cpp:30-32)
+ * plus the u8 colour buffer (DeviceManager.cpp:80). flags: WL_FILM_* bits. */
+WL_API int wl_film_create(wl_context *ctx, uint32_t width, uint32_t height, uint32_t flags,
+                   wl_film **out);
+WL_API int wl_film_destroy(wl_film *film);
+WL_API int wl_film_clear(wl_film *film);
+/* Linear film to host: rgb (W*H*3 floats) and, when the film has WL_FILM_FP64_SUM, the FP64
+ * mean (W*H*3 doubles). Either may be NULL. Synchronous. */
+WL_API int wl_film_download(wl_film *film, float *rgb, double *rgb64);
+/* Tone-mapped film (AceApprox, Tonemap.h:34-43, times 255, truncated) to host RGBA8. */
+WL_API int wl_film_download_ldr(wl_film *film, uint8_t *rgba8);
+/* Device pointers of the film (for callers that keep the film on the GPU). */
+WL_API int wl_film_device_ptrs(wl_film *film, float **rgb, double **rgb64, uint8_t **ldr);
+
+/* __raygen__RenderFrame + __closesthit__radiance + misses (PathTracing.cu:40-288), as a
+ * wavefront: camera -> extend -> shade (Disney sample/eval/pdf, NEE light sample, MIS,
+ * Russian roulette) -> shadow -> film, for params->spp samples per pixel. Stream ordered. */
+WL_API int wl_render(wl_context *ctx, wl_scene *scene, const wl_camera *camera,
+              const wl_render_params *params, wl_film *film);
+WL_API int wl_render_get_stats(wl_context *ctx, wl_render_stats *stats);
+/* Fill params with the reference's constants (MIS, depth 25, RR after 5 with 0.9, eps 1e-3,
+ * TEA+LCG, uniform lights, no environment). */
+WL_API void wl_render_params_default(wl_render_params *params, uint32_t width, uint32_t height,
+                              uint32_t spp);
+
+/* Random streams for parity tests: the first `count` uniforms of the stream of each listed
+ * pixel at `frame` (count floats per pixel, pixel-major). Device pointers. */
+WL_API int wl_debug_rng(wl_context *ctx, uint32_t rng, uint64_t seed, const uint32_t *d_pixels,
+                 uint32_t npix, uint32_t frame, uint32_t count, float *d_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WAYLAND_B200_H */

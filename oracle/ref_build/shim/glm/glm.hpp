@@ -1,0 +1,86 @@
+// glm.hpp - project-written subset of glm 1.0.1 (MIT, g-truc/glm), restated for building the
+// reference's src/Frontend/Device/*.h as host C++. Test infrastructure only (oracle/_ref).
+// Semantics follow glm's published definitions: componentwise operators (vector / scalar
+// divides each component), dot(a, b) = (a.x*b.x + a.y*b.y) + a.z*b.z, length = sqrt(dot),
+// normalize(v) = v * (1 / sqrt(dot(v, v))), cross as in glm/detail/func_geometric.inl,
+// clamp(x, lo, hi) = min(max(x, lo), hi) with max(a, b) = a < b ? b : a, min(a, b) = b < a ? b : a.
+#pragma once
+#include <cmath>
+#include <cstdint>
+
+namespace glm {
+
+template <class T> struct tvec2 {
+    T x, y;
+    tvec2() : x(0), y(0) {}
+    tvec2(T a, T b) : x(a), y(b) {}
+    explicit tvec2(T s) : x(s), y(s) {}
+};
+template <class T> struct tvec4;
+template <class T> struct tvec3 {
+    T x, y, z;
+    tvec3() : x(0), y(0), z(0) {}
+    tvec3(T a, T b, T c) : x(a), y(b), z(c) {}
+    explicit tvec3(T s) : x(s), y(s), z(s) {}
+    template <class U> tvec3(const tvec4<U> &v) : x((T)v.x), y((T)v.y), z((T)v.z) {}
+    template <class U> explicit tvec3(const tvec3<U> &v) : x((T)v.x), y((T)v.y), z((T)v.z) {}
+    tvec3 &operator+=(const tvec3 &o) { x += o.x; y += o.y; z += o.z; return *this; }
+    tvec3 &operator-=(const tvec3 &o) { x -= o.x; y -= o.y; z -= o.z; return *this; }
+    tvec3 &operator*=(const tvec3 &o) { x *= o.x; y *= o.y; z *= o.z; return *this; }
+    tvec3 &operator*=(T s) { x *= s; y *= s; z *= s; return *this; }
+    tvec3 &operator/=(T s) { x /= s; y /= s; z /= s; return *this; }
+};
+template <class T> struct tvec4 {
+    T x, y, z, w;
+    tvec4() : x(0), y(0), z(0), w(0) {}
+    tvec4(T a, T b, T c, T d) : x(a), y(b), z(c), w(d) {}
+    explicit tvec4(T s) : x(s), y(s), z(s), w(s) {}
+    tvec4(const tvec3<T> &v, T d) : x(v.x), y(v.y), z(v.z), w(d) {}
+};
+
+template <class T> tvec3<T> operator+(const tvec3<T> &a, const tvec3<T> &b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class T> tvec3<T> operator-(const tvec3<T> &a, const tvec3<T> &b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class T> tvec3<T> operator*(const tvec3<T> &a, const tvec3<T> &b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+template <class T> tvec3<T> operator/(const tvec3<T> &a, const tvec3<T> &b) { return {a.x / b.x, a.y / b.y, a.z / b.z}; }
+template <class T> tvec3<T> operator-(const tvec3<T> &a) { return {-a.x, -a.y, -a.z}; }
+// scalar forms; the scalar type is taken from the vector (a double or int literal converts)
+template <class T> struct ident { typedef T type; };
+template <class T> tvec3<T> operator*(const tvec3<T> &a, typename ident<T>::type s) { return {a.x * s, a.y * s, a.z * s}; }
+template <class T> tvec3<T> operator*(typename ident<T>::type s, const tvec3<T> &a) { return {s * a.x, s * a.y, s * a.z}; }
+template <class T> tvec3<T> operator/(const tvec3<T> &a, typename ident<T>::type s) { return {a.x / s, a.y / s, a.z / s}; }
+template <class T> tvec3<T> operator/(typename ident<T>::type s, const tvec3<T> &a) { return {s / a.x, s / a.y, s / a.z}; }
+template <class T> tvec3<T> operator+(const tvec3<T> &a, typename ident<T>::type s) { return {a.x + s, a.y + s, a.z + s}; }
+template <class T> tvec3<T> operator+(typename ident<T>::type s, const tvec3<T> &a) { return {s + a.x, s + a.y, s + a.z}; }
+template <class T> tvec3<T> operator-(const tvec3<T> &a, typename ident<T>::type s) { return {a.x - s, a.y - s, a.z - s}; }
+template <class T> tvec3<T> operator-(typename ident<T>::type s, const tvec3<T> &a) { return {s - a.x, s - a.y, s - a.z}; }
+
+template <class T> tvec2<T> operator*(const tvec2<T> &a, typename ident<T>::type s) { return {a.x * s, a.y * s}; }
+
+template <class T> T dot(const tvec3<T> &a, const tvec3<T> &b) {
+    tvec3<T> t = a * b;
+    return t.x + t.y + t.z;
+}
+template <class T> tvec3<T> cross(const tvec3<T> &x, const tvec3<T> &y) {
+    return {x.y * y.z - y.y * x.z, x.z * y.x - y.z * x.x, x.x * y.y - y.x * x.y};
+}
+template <class T> T length(const tvec3<T> &v) { return std::sqrt(dot(v, v)); }
+template <class T> T inversesqrt(T x) { return static_cast<T>(1) / std::sqrt(x); }
+template <class T> tvec3<T> normalize(const tvec3<T> &v) { return v * inversesqrt(dot(v, v)); }
+template <class T> T gmax(T a, T b) { return a < b ? b : a; }
+template <class T> T gmin(T a, T b) { return b < a ? b : a; }
+template <class T> tvec3<T> clamp(const tvec3<T> &v, typename ident<T>::type lo, typename ident<T>::type hi) {
+    return {gmin(gmax(v.x, lo), hi), gmin(gmax(v.y, lo), hi), gmin(gmax(v.z, lo), hi)};
+}
+template <class T> tvec4<T> clamp(const tvec4<T> &v, typename ident<T>::type lo, typename ident<T>::type hi) {
+    return {gmin(gmax(v.x, lo), hi), gmin(gmax(v.y, lo), hi), gmin(gmax(v.z, lo), hi), gmin(gmax(v.w, lo), hi)};
+}
+
+typedef tvec2<float> vec2;
+typedef tvec3<float> vec3;
+typedef tvec4<float> vec4;
+typedef tvec4<double> dvec4;
+typedef tvec2<int> ivec2;
+typedef tvec3<int> ivec3;
+typedef tvec4<uint8_t> u8vec4;
+
+}  // namespace glm

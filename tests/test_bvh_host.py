@@ -1,0 +1,78 @@
+"""The BVH build and traversal logic of wayland_b200/csrc/wl_bvh.cuh, compiled for the CPU by the
+test harness, against the oracle: Morton codes and radix-tree topology bit-exact, closest hits
+(t, prim, u, v) bit-exact against brute force, any-hit occlusion identical."""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from helpers import axis_rays, geometries, random_rays
+
+GEOMS = geometries()
+
+
+def host_build(host_bvh, V, I):
+    V = np.ascontiguousarray(V, np.float32)
+    I = np.ascontiguousarray(I, np.uint32)
+    return host_bvh.hb_build(V.ctypes.data, I.ctypes.data, len(I)), V, I
+
+
+def host_cast(host_bvh, h, rays, mode):
+    hits = np.zeros(len(rays), po.HIT_DTYPE)
+    st = np.zeros(2, np.uint64)
+    host_bvh.hb_cast(h, rays.ctypes.data, len(rays), mode, hits.ctypes.data, st.ctypes.data)
+    return hits, st
+
+
+@pytest.mark.parametrize("name,V,I", GEOMS, ids=[g[0] for g in GEOMS])
+def test_topology(host_bvh, oracle, name, V, I):
+    import ctypes as C
+    h, V, I = host_build(host_bvh, V, I)
+    n = len(I)
+    mort = np.zeros(n, np.uint64)
+    sp = np.zeros(n, np.uint32)
+    L = np.zeros(max(n - 1, 1), np.int32)
+    R = np.zeros(max(n - 1, 1), np.int32)
+    host_bvh.hb_export(h, mort.ctypes.data, sp.ctypes.data, L.ctypes.data, R.ctypes.data)
+    assert np.array_equal(mort, oracle.morton63(V, I))
+    osp, ol, orr, _, _ = oracle.lbvh(V, I)
+    assert np.array_equal(sp, osp)
+    assert np.array_equal(L[:n - 1], ol) and np.array_equal(R[:n - 1], orr)
+    depth = C.c_uint32()
+    nodes = host_bvh.hb_info(h, C.byref(depth))
+    assert nodes >= 1 and depth.value <= 64
+    host_bvh.hb_destroy(h)
+
+
+@pytest.mark.parametrize("name,V,I", GEOMS, ids=[g[0] for g in GEOMS])
+def test_closest_hit_bitexact(host_bvh, oracle, name, V, I):
+    h, V, I = host_build(host_bvh, V, I)
+    rays = np.concatenate([random_rays(6000, 11), axis_rays(2000, 12)])
+    if name == "cornell":
+        rays["org"] = np.random.default_rng(2).uniform(0.01, 0.99, (len(rays), 3))
+    got, st = host_cast(host_bvh, h, rays, 0)
+    ref = oracle.cast_bruteforce(V, I, rays, 0)
+    assert np.array_equal(got.view(np.uint32).reshape(-1, 4), ref.view(np.uint32).reshape(-1, 4))
+    anyg, _ = host_cast(host_bvh, h, rays, 1)
+    anyr = oracle.cast_bruteforce(V, I, rays, 1)
+    assert np.array_equal(anyg["prim"] == po.np.uint32(0xFFFFFFFF), anyr["prim"] == 0xFFFFFFFF)
+    host_bvh.hb_destroy(h)
+
+
+def test_rays_from_surfaces(host_bvh, oracle):
+    """Secondary rays starting at hit points on the surface they left (the path tracer's
+    common case), in random directions."""
+    from wayland_b200 import scenes
+    sc = scenes.displaced_sphere(subdiv=24)
+    h, V, I = host_build(host_bvh, sc.V, sc.I)
+    prim = random_rays(6000, 7, -3.0, 3.0)
+    hit = oracle.cast_bruteforce(V, I, prim, 0)
+    ok = hit["prim"] != 0xFFFFFFFF
+    assert ok.sum() > 1000
+    rays = random_rays(int(ok.sum()), 8)
+    p = prim[ok]
+    rays["org"] = (p["org"] + p["dir"] * hit["t"][ok][:, None]).astype(np.float32)
+    got, _ = host_cast(host_bvh, h, rays, 0)
+    ref = oracle.cast_bruteforce(V, I, rays, 0)
+    assert np.array_equal(got.view(np.uint32).reshape(-1, 4), ref.view(np.uint32).reshape(-1, 4))
+    assert (ref["prim"] != 0xFFFFFFFF).mean() > 0.05
+    host_bvh.hb_destroy(h)

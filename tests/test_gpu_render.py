@@ -1,0 +1,175 @@
+"""The wavefront path tracer through the C ABI against the oracle.
+
+WL_MATH_STRICT renders are compared bit for bit: with the golden image made from the reference's
+own device code (TEA+LCG, Cornell box), and with the oracle's path tracer for both random streams,
+all three strategies, a scene with vertex normals, transmission, metallic lobes, an environment
+and four lights, multi-call accumulation and any wave size. WL_MATH_FAST (the benchmark mode)
+is compared with the FP64 oracle by relMSE at equal spp: tolerance 2e-3 (fast-math sin/cos/log
+and approximate division change a few paths; the statistics do not change)."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+import pyoracle as po
+import wayland_b200 as wl
+from wayland_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+FAST_RELMSE_TOL = 2e-3
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def ocam(sc):
+    c = po.Camera()
+    for k in ("pos", "look_at", "up", "right"):
+        getattr(c, k)[:] = [float(x) for x in sc.camera[k]]
+    return c
+
+
+def oparams(p):
+    q = po.RenderParams()
+    for k, _ in q._fields_:
+        if k == "env":
+            q.env[:] = list(p.env)
+        else:
+            setattr(q, k, getattr(p, k))
+    return q
+
+
+def gpu_render(ctx, scene_data, p, fp64=False, scene=None):
+    sc = scene or wl.Scene(ctx, scene_data)
+    film = wl.Film(ctx, p.width, p.height, fp64=fp64)
+    wl.render(ctx, sc, scene_data.camera_struct(), p, film)
+    img = film.download()
+    img64 = film.download64() if fp64 else None
+    return img, img64, film, sc
+
+
+def small_sphere(W=48, H=32):
+    return scenes.displaced_sphere(width=W, height=H, subdiv=24, seed=3)
+
+
+def test_golden_cornell_strict(ctx):
+    """GPU strict mode == the reference's device code (via oracle/_ref), bit for bit."""
+    g = dict(np.load(os.path.join(GOLD, "cornell_32x32_4spp.npz")))
+    sc = scenes.cornell_box(32, 32)
+    assert np.array_equal(sc.V, g["V"]) and np.array_equal(sc.I, g["I"])
+    p = wl.render_params(32, 32, 4, math=wl.MATH_STRICT)
+    img, _, film, s = gpu_render(ctx, sc, p)
+    assert np.array_equal(bits(img), bits(g["image"]))
+    assert ctx.stats()["segments"] == int(g["segments"])
+
+
+@pytest.mark.parametrize("rng", [wl.RNG_TEA_LCG, wl.RNG_PCG32])
+@pytest.mark.parametrize("strategy", [wl.STRATEGY_MIS, wl.STRATEGY_NEE, wl.STRATEGY_UPT])
+def test_cornell_strict_vs_oracle(ctx, oracle, rng, strategy):
+    sc = scenes.cornell_box(48, 40)
+    p = wl.render_params(48, 40, 3, math=wl.MATH_STRICT, rng=rng, strategy=strategy, seed=7,
+                         max_depth=8)
+    img, _, _, _ = gpu_render(ctx, sc, p)
+    ref, _, segs = oracle.render(sc, ocam(sc), oparams(p))
+    assert np.array_equal(bits(img), bits(ref))
+    assert ctx.stats()["segments"] == segs
+
+
+@pytest.mark.parametrize("rng", [wl.RNG_TEA_LCG, wl.RNG_PCG32])
+def test_sphere_strict_vs_oracle(ctx, oracle, rng):
+    """Vertex normals, random Disney (transmission, metallic), 4 lights, environment 0.1."""
+    sc = small_sphere()
+    p = wl.render_params(sc.width, sc.height, 2, math=wl.MATH_STRICT, rng=rng, max_depth=16,
+                         env=sc.env, seed=11)
+    img, _, _, _ = gpu_render(ctx, sc, p)
+    ref, _, segs = oracle.render(sc, ocam(sc), oparams(p))
+    assert np.array_equal(bits(img), bits(ref))
+    assert img.mean() > 0.01
+
+
+def test_accumulation_and_waves(ctx, oracle):
+    """Two calls (frames 0-1, 2-4) == one call of 5 frames == many small waves; FP64 film equals
+    the oracle's FP64 mean."""
+    sc = scenes.cornell_box(40, 24)
+    s = wl.Scene(ctx, sc)
+    cam = sc.camera_struct()
+    film = wl.Film(ctx, 40, 24, fp64=True)
+    wl.render(ctx, s, cam, wl.render_params(40, 24, 2, math=wl.MATH_STRICT), film)
+    wl.render(ctx, s, cam, wl.render_params(40, 24, 3, first_frame=2, math=wl.MATH_STRICT), film)
+    a = film.download()
+    p5 = wl.render_params(40, 24, 5, math=wl.MATH_STRICT)
+    one, one64, _, _ = gpu_render(ctx, sc, p5, fp64=True, scene=s)
+    small = wl.render_params(40, 24, 5, math=wl.MATH_STRICT, wave_paths=1000)
+    b, _, _, _ = gpu_render(ctx, sc, small, scene=s)
+    ref, ref64, _ = oracle.render(sc, ocam(sc), oparams(p5), want64=True)
+    assert np.array_equal(bits(a), bits(ref))
+    assert np.array_equal(bits(one), bits(ref))
+    assert np.array_equal(bits(b), bits(ref))
+    assert np.array_equal(one64.view(np.uint64), ref64.view(np.uint64))
+
+
+def test_fast_mode_relmse(ctx, oracle):
+    """Benchmark arithmetic vs the FP64 oracle at equal spp and the same random streams."""
+    sc = scenes.cornell_box(64, 64)
+    p = wl.render_params(64, 64, 16, math=wl.MATH_FAST, max_depth=8)
+    img, _, _, _ = gpu_render(ctx, sc, p)
+    _, ref64, _ = oracle.render(sc, ocam(sc), oparams(p), prec=1, want64=True)
+    rel = oracle.relmse(img, ref64)
+    assert rel < FAST_RELMSE_TOL, rel
+    sc2 = small_sphere()
+    p2 = wl.render_params(sc2.width, sc2.height, 8, math=wl.MATH_FAST, max_depth=16, env=sc2.env)
+    img2, _, _, _ = gpu_render(ctx, sc2, p2)
+    _, ref2, _ = oracle.render(sc2, ocam(sc2), oparams(p2), prec=1, want64=True)
+    assert oracle.relmse(img2, ref2) < 5 * FAST_RELMSE_TOL
+
+
+@pytest.mark.parametrize("rng", [wl.RNG_TEA_LCG, wl.RNG_PCG32])
+def test_rng_streams(ctx, oracle, rng):
+    pix = np.array([0, 1, 77, 65535, 1 << 20, 2073599], np.uint32)
+    d_pix = torch.from_numpy(pix.view(np.int32)).cuda()
+    out = torch.empty(len(pix) * 40, dtype=torch.float32, device="cuda")
+    ctx.debug_rng(rng, 12345, d_pix.data_ptr(), len(pix), 9, 40, out.data_ptr())
+    ctx.sync()
+    got = out.cpu().numpy().reshape(len(pix), 40)
+    for i, px in enumerate(pix):
+        assert np.array_equal(bits(got[i]), bits(oracle.rng_stream(rng, 12345, int(px), 9, 40)))
+
+
+def test_ldr_tonemap(ctx, oracle):
+    sc = scenes.cornell_box(32, 32)
+    p = wl.render_params(32, 32, 2, math=wl.MATH_STRICT)
+    img, _, film, _ = gpu_render(ctx, sc, p)
+    ldr = film.download_ldr()
+    rad = np.clip(img.reshape(-1, 3), 0, 1e30)
+    exp = (oracle.ace(rad) * np.float32(255.0)).astype(np.uint8).reshape(32, 32, 3)
+    assert np.array_equal(ldr[..., :3], exp) and (ldr[..., 3] == 255).all()
+
+
+def test_render_errors(ctx):
+    sc = scenes.cornell_box(16, 16)
+    s = wl.Scene(ctx, sc, build=False)
+    film = wl.Film(ctx, 16, 16)
+    with pytest.raises(wl.WlError, match="NOT_BUILT"):
+        wl.render(ctx, s, sc.camera_struct(), wl.render_params(16, 16, 1), film)
+    s.build_bvh()
+    with pytest.raises(wl.WlError, match="INVALID_ARG"):
+        wl.render(ctx, s, sc.camera_struct(), wl.render_params(16, 8, 1), film)
+    with pytest.raises(wl.WlError, match="INVALID_ARG"):
+        wl.render(ctx, s, sc.camera_struct(), wl.render_params(16, 16, 0), film)
+
+
+def test_path_tracer_program(ctx, oracle):
+    """PathTracingProgramManager-style use: Setup, Update per frame, End."""
+    sc = scenes.cornell_box(24, 24)
+    s = wl.Scene(ctx, sc)
+    pt = wl.PathTracer(ctx, s, sc.camera_struct(), 24, 24, math=wl.MATH_STRICT)
+    pt.Setup()
+    for _ in range(3):
+        pt.Update(1)
+    img = pt.film.download()
+    pt.End()
+    ref, _, _ = oracle.render(sc, ocam(sc), oparams(wl.render_params(24, 24, 3, math=wl.MATH_STRICT)))
+    assert np.array_equal(bits(img), bits(ref))

@@ -1,0 +1,99 @@
+"""The oracle against the golden vectors generated from the reference's own device code
+(tests/golden/make_golden.py). Bit-exact: every comparison is on the float bit patterns."""
+import os
+
+import numpy as np
+import pytest
+
+import pyoracle as po
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return dict(np.load(os.path.join(GOLD, "device_math.npz")))
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+def test_tea4(oracle, gold):
+    got = np.array([oracle.tea4(int(a), int(b)) for a, b in gold["tea_in"]], np.uint32)
+    assert np.array_equal(got, gold["tea_out"])
+
+
+def test_lcg_stream(oracle, gold):
+    for s, ref in zip(gold["rnd_seed"], gold["rnd_out"]):
+        assert np.array_equal(bits(oracle.lcg_stream(int(s), 64)), bits(ref))
+
+
+def test_disney_eval(oracle, gold):
+    g = gold
+    got = oracle.disney_eval(g["mats"], g["Ns"], g["Ng"], g["V"], g["L"], g["tex"])
+    assert np.array_equal(bits(got), bits(g["eval"]))
+    assert (np.abs(g["eval"]) > 0).any(axis=1).mean() > 0.2  # the cases exercise the lobes
+
+
+def test_disney_pdf(oracle, gold):
+    g = gold
+    got = oracle.disney_pdf(g["mats"], g["Ns"], g["Ng"], g["V"], g["L"])
+    assert np.array_equal(bits(got), bits(g["pdf"]))
+
+
+def test_disney_sample(oracle, gold):
+    g = gold
+    got, seeds = oracle.disney_sample(g["mats"], g["Ns"], g["Ng"], g["V"], g["sample_seed"])
+    assert np.array_equal(bits(got), bits(g["sample"]))
+    assert np.array_equal(seeds, g["sample_seed_out"])
+    # transmission, diffuse and specular branches are all present
+    refl = (np.einsum("ij,ij->i", g["sample"], g["Ns"]) * np.einsum("ij,ij->i", g["V"], g["Ns"]))
+    assert (refl < 0).sum() > 100 and (refl > 0).sum() > 100
+
+
+def test_camera(oracle, gold):
+    g = gold
+    cam = po.Camera()
+    for i, k in enumerate(("pos", "look_at", "up", "right")):
+        getattr(cam, k)[:] = [float(x) for x in g["cam"][i]]
+    d, s = oracle.camera_rays(cam, 256, 256, g["cam_px"], g["cam_py"], g["cam_seed"])
+    assert np.array_equal(bits(d), bits(g["cam_dir"]))
+    assert np.array_equal(s, g["cam_seed_out"])
+
+
+def test_ace(oracle, gold):
+    assert np.array_equal(bits(oracle.ace(gold["ace_in"])), bits(gold["ace_out"]))
+
+
+def test_cornell_image(oracle):
+    """The oracle's path tracer reproduces the reference-math render of the Cornell box."""
+    g = dict(np.load(os.path.join(GOLD, "cornell_32x32_4spp.npz")))
+
+    class S:
+        V, I, tri_material, mats, lights = g["V"], g["I"], g["tri_material"], g["mats"], g["lights"]
+        N = None
+        tri_flags = None
+
+    cam = po.Camera()
+    for i, k in enumerate(("pos", "look_at", "up", "right")):
+        getattr(cam, k)[:] = [float(x) for x in g["cam"][i]]
+    p = po.RenderParams(width=32, height=32, spp=4, first_frame=0, max_depth=25, rr_depth=5,
+                        rr_prob=0.9, eps=1e-3, strategy=2, rng=0, math=1, lights=0, seed=0)
+    img, _, segs = oracle.render(S(), cam, p)
+    assert np.array_equal(bits(img), bits(g["image"]))
+    assert segs == int(g["segments"])
+    assert img.mean() > 0.05
+
+
+def test_own_transcendentals(oracle):
+    """The project's sin/cos/log are within a few ulp of the double-precision values."""
+    xs = np.linspace(0, 2 * np.pi, 4001, dtype=np.float32)
+    s = np.array([oracle.sinf(x) for x in xs])
+    c = np.array([oracle.cosf(x) for x in xs])
+    assert np.abs(s - np.sin(xs.astype(np.float64))).max() < 2e-7
+    assert np.abs(c - np.cos(xs.astype(np.float64))).max() < 2e-7
+    ys = np.exp(np.linspace(-25, 10, 4001)).astype(np.float32)
+    lg = np.array([oracle.logf(y) for y in ys])
+    assert (np.abs(lg - np.log(ys.astype(np.float64))) / np.maximum(1.0, np.abs(np.log(ys)))).max() < 3e-7
+    assert np.isnan(oracle.logf(-1.0)) and np.isneginf(oracle.logf(0.0))

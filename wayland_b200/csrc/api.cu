@@ -1,0 +1,714 @@
+// api.cu - the C ABI of include/wayland_b200.h: context, scene upload, BVH build, ray casts,
+// film and the wavefront render loop. Host code; kernels live in bvh_build.cu, traverse.cu,
+// pt_fast.cu and pt_strict.cu.
+//
+// Reference counterparts: DeviceManager (src/Frontend/Core/DeviceManager.cpp:30-254),
+// PathTracingProgramManager (Programs/PathTracing/PathTracingProgramManager.cpp:11-55),
+// Launcher (src/Backend/Optix/Core/Launcher.cpp:12-20).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "wl_bvh.cuh"
+#include "wl_internal.h"
+
+using namespace wl;
+
+namespace {
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+}  // namespace
+
+#define CK(x)                                                                                 \
+    do {                                                                                      \
+        cudaError_t e_ = (x);                                                                 \
+        if (e_ != cudaSuccess) {                                                              \
+            return fail(e_ == cudaErrorMemoryAllocation ? WL_ERR_OOM : WL_ERR_CUDA,           \
+                        std::string(#x) + ": " + cudaGetErrorString(e_));                     \
+        }                                                                                     \
+    } while (0)
+#define ARG(cond, msg)                                 \
+    do {                                               \
+        if (!(cond)) return fail(WL_ERR_INVALID_ARG, msg); \
+    } while (0)
+
+struct TimedPair {
+    cudaEvent_t a, b;
+};
+
+struct wl_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    Queues q{};
+    void *q_block = nullptr;
+    uint32_t *d_misc = nullptr;               // [0] cast work counter
+    unsigned long long *d_cast_counts = nullptr;
+    wl_render_stats stats{};
+    // per-launch events of the last render: category 0 extend, 1 shade, 2 shadow, 3 other
+    std::vector<TimedPair> ev[4];
+    size_t ev_used[4] = {0, 0, 0, 0};
+    cudaEvent_t ev_total[2] = {nullptr, nullptr};
+    bool stats_pending = false;
+    int live_children = 0;  // scenes and films created on this context and not yet destroyed
+};
+
+struct wl_scene {
+    wl_context *ctx = nullptr;
+    uint32_t nV = 0, nT = 0, nMat = 0, nLight = 0;
+    float *d_V = nullptr, *d_N = nullptr, *d_UV = nullptr;
+    uint32_t *d_I = nullptr;
+    uint4 *d_tri = nullptr;
+    uint32_t *d_tri_light = nullptr;
+    wl_disney *d_mats = nullptr;
+    DevLight *d_lights = nullptr;
+    std::vector<cudaArray_t> tex_arrays;
+    std::vector<cudaTextureObject_t> tex_objs;
+    cudaTextureObject_t *d_tex = nullptr;
+    BvhBuild bvh{};
+    bool built = false;
+    wl_bvh_info info{};
+};
+
+struct wl_film {
+    wl_context *ctx = nullptr;
+    Film f{};
+};
+
+namespace {
+
+DevScene dev_scene(const wl_scene *s) {
+    DevScene d{};
+    d.nV = s->nV; d.nT = s->nT; d.nMat = s->nMat; d.nLight = s->nLight;
+    d.V = s->d_V; d.N = s->d_N; d.UV = s->d_UV;
+    d.tri = s->d_tri; d.tri_light = s->d_tri_light;
+    d.mats = s->d_mats; d.lights = s->d_lights;
+    d.nodes = s->bvh.nodes; d.tris = s->bvh.tris;
+    d.has_bvh = (s->built && s->nT > 0) ? 1u : 0u;
+    d.tex = s->d_tex;
+    d.nTex = (uint32_t)s->tex_objs.size();
+    return d;
+}
+
+template <class T> size_t al(size_t n) { return ((n * sizeof(T) + 255) / 256) * 256; }
+
+// Path-state and queue arrays for `cap` paths in one allocation.
+int ensure_queues(wl_context *c, uint32_t cap) {
+    if (c->q.capacity >= cap && c->q_block) return WL_OK;
+    if (c->q_block) {
+        cudaFree(c->q_block);
+        c->q_block = nullptr;
+    }
+    size_t f4 = al<float4>(cap), u32 = al<uint32_t>(cap), u2 = al<uint2>(cap);
+    size_t total = 4 * f4 + 2 * u32 + f4 + 3 * f4 + u2 + 3 * f4 + 256 + 256;
+    CK(cudaMalloc(&c->q_block, total));
+    char *p = (char *)c->q_block;
+    Queues &q = c->q;
+    q.capacity = cap;
+    q.ray_o[0] = (float4 *)p; p += f4;
+    q.ray_d[0] = (float4 *)p; p += f4;
+    q.ray_o[1] = (float4 *)p; p += f4;
+    q.ray_d[1] = (float4 *)p; p += f4;
+    q.ray_slot[0] = (uint32_t *)p; p += u32;
+    q.ray_slot[1] = (uint32_t *)p; p += u32;
+    q.hit = (float4 *)p; p += f4;
+    q.st_thr = (float4 *)p; p += f4;
+    q.st_term = (float4 *)p; p += f4;
+    q.st_rad = (float4 *)p; p += f4;
+    q.st_rng = (uint2 *)p; p += u2;
+    q.sh_o = (float4 *)p; p += f4;
+    q.sh_d = (float4 *)p; p += f4;
+    q.sh_l = (float4 *)p; p += f4;
+    q.counters = (uint32_t *)p; p += 256;
+    q.totals = (unsigned long long *)p; p += 256;
+    CK(cudaMemsetAsync(q.counters, 0, 512, c->stream));
+    return WL_OK;
+}
+
+void rec(wl_context *c, int cat, bool begin) {
+    auto &v = c->ev[cat];
+    size_t &u = c->ev_used[cat];
+    if (begin) {
+        if (u == v.size()) {
+            TimedPair tp;
+            cudaEventCreate(&tp.a);
+            cudaEventCreate(&tp.b);
+            v.push_back(tp);
+        }
+        cudaEventRecord(v[u].a, c->stream);
+    } else {
+        cudaEventRecord(v[u].b, c->stream);
+        u++;
+    }
+}
+
+int finish_stats(wl_context *c) {
+    if (!c->stats_pending) return WL_OK;
+    CK(cudaEventSynchronize(c->ev_total[1]));
+    float *dst[4] = {&c->stats.ms_extend, &c->stats.ms_shade, &c->stats.ms_shadow, &c->stats.ms_other};
+    for (int k = 0; k < 4; k++) {
+        float acc = 0.f;
+        for (size_t i = 0; i < c->ev_used[k]; i++) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, c->ev[k][i].a, c->ev[k][i].b));
+            acc += ms;
+        }
+        *dst[k] = acc;
+    }
+    CK(cudaEventElapsedTime(&c->stats.ms_total, c->ev_total[0], c->ev_total[1]));
+    unsigned long long tot[6];
+    CK(cudaMemcpy(tot, c->q.totals, sizeof(tot), cudaMemcpyDeviceToHost));
+    c->stats.segments = tot[0];
+    c->stats.shadow_rays = tot[1];
+    c->stats.extend_node_visits = tot[2];
+    c->stats.extend_tri_tests = tot[3];
+    c->stats.shadow_node_visits = tot[4];
+    c->stats.shadow_tri_tests = tot[5];
+    c->stats_pending = false;
+    return WL_OK;
+}
+
+bool finite3(const float *p) { return std::isfinite(p[0]) && std::isfinite(p[1]) && std::isfinite(p[2]); }
+
+}  // namespace
+
+extern "C" {
+
+const char *wl_last_error_string(void) { return g_err.c_str(); }
+const char *wl_version(void) { return "wayland_b200 0.1 (sm_100a)"; }
+
+int wl_context_create(int device, wl_context **out) {
+    ARG(out, "out is null");
+    int n = 0;
+    CK(cudaGetDeviceCount(&n));
+    ARG(device >= 0 && device < n, "no such device");
+    CK(cudaSetDevice(device));
+    wl_context *c = new wl_context();
+    c->device = device;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return fail(WL_ERR_CUDA, cudaGetErrorString(e));
+    }
+    c->own_stream = true;
+    if (cudaMalloc(&c->d_misc, 256) != cudaSuccess ||
+        cudaMalloc(&c->d_cast_counts, 2 * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaEventCreate(&c->ev_total[0]) != cudaSuccess ||
+        cudaEventCreate(&c->ev_total[1]) != cudaSuccess) {
+        wl_context_destroy(c);
+        return fail(WL_ERR_OOM, "context allocation failed");
+    }
+    *out = c;
+    return WL_OK;
+}
+
+int wl_context_destroy(wl_context *c) {
+    if (!c) return WL_OK;
+    if (c->live_children > 0)
+        return fail(WL_ERR_INVALID_ARG, "destroy the context's scenes and films first (" +
+                                            std::to_string(c->live_children) + " alive)");
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->q_block) cudaFree(c->q_block);
+    if (c->d_misc) cudaFree(c->d_misc);
+    if (c->d_cast_counts) cudaFree(c->d_cast_counts);
+    for (auto &v : c->ev)
+        for (auto &p : v) {
+            cudaEventDestroy(p.a);
+            cudaEventDestroy(p.b);
+        }
+    for (auto e : c->ev_total)
+        if (e) cudaEventDestroy(e);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return WL_OK;
+}
+
+int wl_context_set_stream(wl_context *c, void *stream) {
+    ARG(c, "null context");
+    CK(cudaSetDevice(c->device));
+    if (c->own_stream && c->stream) {
+        CK(cudaStreamSynchronize(c->stream));
+        CK(cudaStreamDestroy(c->stream));
+    }
+    if (stream) {
+        c->stream = (cudaStream_t)stream;
+        c->own_stream = false;
+    } else {
+        CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->own_stream = true;
+    }
+    return WL_OK;
+}
+
+int wl_context_get_stream(wl_context *c, void **stream) {
+    ARG(c && stream, "null argument");
+    *stream = (void *)c->stream;
+    return WL_OK;
+}
+
+int wl_context_sync(wl_context *c) {
+    ARG(c, "null context");
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    return WL_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+int wl_scene_create(wl_context *c, const float *V, uint32_t nV, const float *N, const float *UV,
+                    const uint32_t *I, uint32_t nT, const uint32_t *tri_material,
+                    const uint32_t *tri_flags, const wl_disney *mats, uint32_t nMat,
+                    const wl_area_light *lights, uint32_t nLight, wl_scene **out) {
+    ARG(c && out, "null argument");
+    ARG(nT == 0 || (V && I && tri_material), "V, I and tri_material are required");
+    ARG(nMat > 0 && mats, "at least one material is required");
+    ARG(nLight == 0 || lights, "lights is null");
+    for (uint64_t i = 0; i < 3ull * nT; i++) ARG(I[i] < nV, "vertex index out of range");
+    for (uint32_t i = 0; i < nT; i++) ARG(tri_material[i] < nMat, "material index out of range");
+    for (uint32_t i = 0; i < nV; i++) ARG(finite3(V + 3 * (size_t)i), "non-finite vertex");
+    if (N)
+        for (uint32_t i = 0; i < nV; i++) ARG(finite3(N + 3 * (size_t)i), "non-finite normal");
+    for (uint32_t l = 0; l < nLight; l++) {
+        ARG(lights[l].tri_count > 0, "light without triangles");
+        ARG((uint64_t)lights[l].first_tri + lights[l].tri_count <= nT, "light triangle range out of range");
+        ARG(finite3(lights[l].L), "non-finite light radiance");
+    }
+    std::vector<uint32_t> tri_light(nT, INVALID);
+    for (uint32_t l = 0; l < nLight; l++)
+        for (uint32_t t = 0; t < lights[l].tri_count; t++) {
+            uint32_t k = lights[l].first_tri + t;
+            ARG(tri_light[k] == INVALID, "a triangle belongs to two lights");
+            tri_light[k] = l;
+        }
+    CK(cudaSetDevice(c->device));
+    wl_scene *s = new wl_scene();
+    s->ctx = c;
+    s->nV = nV; s->nT = nT; s->nMat = nMat; s->nLight = nLight;
+    std::vector<uint4> tri(nT);
+    for (uint32_t i = 0; i < nT; i++) {
+        bool hn = N && (!tri_flags || (tri_flags[i] & 1u));
+        tri[i] = make_uint4(I[3 * (size_t)i], I[3 * (size_t)i + 1], I[3 * (size_t)i + 2],
+                            tri_material[i] | (hn ? 0x80000000u : 0u));
+    }
+    std::vector<DevLight> dl(nLight);
+    for (uint32_t l = 0; l < nLight; l++) {
+        for (int k = 0; k < 3; k++) dl[l].L[k] = lights[l].L[k];
+        dl[l].two_sided = lights[l].two_sided ? 1 : 0;
+        dl[l].first_tri = lights[l].first_tri;
+        dl[l].tri_count = lights[l].tri_count;
+        dl[l].has_normal = (N && (!tri_flags || (tri_flags[lights[l].first_tri] & 1u))) ? 1u : 0u;
+        dl[l].pad = 0;
+    }
+    auto up = [&](void **dst, const void *src, size_t bytes) -> cudaError_t {
+        if (!bytes) return cudaSuccess;
+        cudaError_t e = cudaMalloc(dst, bytes);
+        if (e != cudaSuccess) return e;
+        return cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
+    };
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = up((void **)&s->d_V, V, 3 * sizeof(float) * (size_t)nV);
+    if (e == cudaSuccess && N) e = up((void **)&s->d_N, N, 3 * sizeof(float) * (size_t)nV);
+    if (e == cudaSuccess && UV) e = up((void **)&s->d_UV, UV, 2 * sizeof(float) * (size_t)nV);
+    if (e == cudaSuccess) e = up((void **)&s->d_I, I, 3 * sizeof(uint32_t) * (size_t)nT);
+    if (e == cudaSuccess) e = up((void **)&s->d_tri, tri.data(), sizeof(uint4) * (size_t)nT);
+    if (e == cudaSuccess) e = up((void **)&s->d_tri_light, tri_light.data(), sizeof(uint32_t) * (size_t)nT);
+    if (e == cudaSuccess) e = up((void **)&s->d_mats, mats, sizeof(wl_disney) * (size_t)nMat);
+    if (e == cudaSuccess) e = up((void **)&s->d_lights, dl.data(), sizeof(DevLight) * (size_t)nLight);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        c->live_children++;
+        wl_scene_destroy(s);
+        return fail(e == cudaErrorMemoryAllocation ? WL_ERR_OOM : WL_ERR_CUDA, cudaGetErrorString(e));
+    }
+    c->live_children++;
+    *out = s;
+    return WL_OK;
+}
+
+int wl_scene_destroy(wl_scene *s) {
+    if (!s) return WL_OK;
+    s->ctx->live_children--;
+    cudaSetDevice(s->ctx->device);
+    cudaStreamSynchronize(s->ctx->stream);
+    void *ps[] = {s->d_V, s->d_N, s->d_UV, s->d_I, s->d_tri, s->d_tri_light, s->d_mats, s->d_lights, s->d_tex};
+    for (void *p : ps)
+        if (p) cudaFree(p);
+    for (auto t : s->tex_objs) cudaDestroyTextureObject(t);
+    for (auto a : s->tex_arrays) cudaFreeArray(a);
+    bvh_free(s->bvh);
+    delete s;
+    return WL_OK;
+}
+
+int wl_scene_add_texture(wl_scene *s, const uint8_t *rgba8, uint32_t w, uint32_t h, int32_t *index) {
+    ARG(s && rgba8 && index && w > 0 && h > 0, "invalid texture arguments");
+    CK(cudaSetDevice(s->ctx->device));
+    // DeviceManager::UploadTextures (DeviceManager.cpp:183-229)
+    cudaChannelFormatDesc cd = cudaCreateChannelDesc<uchar4>();
+    cudaArray_t arr;
+    CK(cudaMallocArray(&arr, &cd, w, h));
+    s->tex_arrays.push_back(arr);
+    CK(cudaMemcpy2DToArray(arr, 0, 0, rgba8, (size_t)w * 4, (size_t)w * 4, h, cudaMemcpyHostToDevice));
+    cudaResourceDesc rd{};
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = arr;
+    cudaTextureDesc td{};
+    td.addressMode[0] = cudaAddressModeWrap;
+    td.addressMode[1] = cudaAddressModeWrap;
+    td.filterMode = cudaFilterModeLinear;
+    td.readMode = cudaReadModeNormalizedFloat;
+    td.normalizedCoords = 1;
+    td.maxAnisotropy = 1;
+    td.maxMipmapLevelClamp = 99;
+    td.minMipmapLevelClamp = 0;
+    td.mipmapFilterMode = cudaFilterModePoint;
+    td.borderColor[0] = 1.0f;
+    cudaTextureObject_t t = 0;
+    CK(cudaCreateTextureObject(&t, &rd, &td, nullptr));
+    s->tex_objs.push_back(t);
+    if (s->d_tex) cudaFree(s->d_tex);
+    s->d_tex = nullptr;
+    CK(cudaMalloc(&s->d_tex, sizeof(cudaTextureObject_t) * s->tex_objs.size()));
+    CK(cudaMemcpy(s->d_tex, s->tex_objs.data(), sizeof(cudaTextureObject_t) * s->tex_objs.size(),
+                  cudaMemcpyHostToDevice));
+    *index = (int32_t)s->tex_objs.size() - 1;
+    return WL_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+int wl_bvh_build(wl_scene *s, uint32_t kind) {
+    ARG(s, "null scene");
+    ARG(kind == WL_BVH_LBVH, "only WL_BVH_LBVH is available");
+    CK(cudaSetDevice(s->ctx->device));
+    bvh_free(s->bvh);
+    s->built = false;
+    s->bvh.V = s->d_V;
+    s->bvh.I = s->d_I;
+    s->bvh.nT = s->nT;
+    std::string err;
+    int rc = bvh_build_lbvh(s->bvh, s->ctx->stream, err);
+    if (rc != WL_OK) {
+        bvh_free(s->bvh);
+        return fail(rc, "bvh build: " + err);
+    }
+    s->built = true;
+    wl_bvh_info &in = s->info;
+    in.kind = kind;
+    in.num_tris = s->nT;
+    in.binary_nodes = s->nT > 1 ? s->nT - 1 : 0;
+    in.wide_nodes = s->bvh.wide_nodes;
+    in.wide_depth = s->bvh.wide_depth;
+    in.leaf_tris = s->nT;
+    in.ms_build = s->bvh.ms;
+    in.bytes = (uint64_t)s->bvh.wide_nodes * 80 + (uint64_t)s->nT * 48;
+    return WL_OK;
+}
+
+int wl_bvh_get_info(wl_scene *s, wl_bvh_info *info) {
+    ARG(s && info, "null argument");
+    if (!s->built) return fail(WL_ERR_NOT_BUILT, "bvh not built");
+    *info = s->info;
+    return WL_OK;
+}
+
+int wl_bvh_export_morton(wl_scene *s, uint64_t *codes, uint32_t n) {
+    ARG(s && codes, "null argument");
+    if (!s->built) return fail(WL_ERR_NOT_BUILT, "bvh not built");
+    ARG(n == s->nT, "n must equal the triangle count");
+    if (n == 0) return WL_OK;
+    CK(cudaSetDevice(s->ctx->device));
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    CK(cudaMemcpy(codes, s->bvh.morton, sizeof(uint64_t) * n, cudaMemcpyDeviceToHost));
+    return WL_OK;
+}
+
+int wl_bvh_export_binary(wl_scene *s, uint32_t *sorted, int32_t *left, int32_t *right,
+                         int32_t *parent, float *bounds, uint32_t n) {
+    ARG(s, "null scene");
+    if (!s->built) return fail(WL_ERR_NOT_BUILT, "bvh not built");
+    ARG(n == s->nT, "n must equal the triangle count");
+    if (n == 0) return WL_OK;
+    CK(cudaSetDevice(s->ctx->device));
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    size_t total = 2 * (size_t)n - 1;
+    if (sorted) CK(cudaMemcpy(sorted, s->bvh.sorted, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
+    if (left && n > 1) CK(cudaMemcpy(left, s->bvh.left, sizeof(int) * (n - 1), cudaMemcpyDeviceToHost));
+    if (right && n > 1) CK(cudaMemcpy(right, s->bvh.right, sizeof(int) * (n - 1), cudaMemcpyDeviceToHost));
+    if (parent) CK(cudaMemcpy(parent, s->bvh.parent, sizeof(int) * total, cudaMemcpyDeviceToHost));
+    if (bounds) {
+        std::vector<float4> lo(total), hi(total);
+        CK(cudaMemcpy(lo.data(), s->bvh.blo, sizeof(float4) * total, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(hi.data(), s->bvh.bhi, sizeof(float4) * total, cudaMemcpyDeviceToHost));
+        for (size_t i = 0; i < total; i++) {
+            bounds[6 * i + 0] = lo[i].x; bounds[6 * i + 1] = lo[i].y; bounds[6 * i + 2] = lo[i].z;
+            bounds[6 * i + 3] = hi[i].x; bounds[6 * i + 4] = hi[i].y; bounds[6 * i + 5] = hi[i].z;
+        }
+    }
+    return WL_OK;
+}
+
+int wl_cast_rays(wl_scene *s, const wl_ray *d_rays, wl_hit *d_hits, uint32_t n, uint32_t mode) {
+    ARG(s, "null scene");
+    ARG(mode == WL_CAST_CLOSEST || mode == WL_CAST_ANY, "bad cast mode");
+    if (!s->built) return fail(WL_ERR_NOT_BUILT, "bvh not built");
+    if (n == 0) return WL_OK;
+    ARG(d_rays && d_hits, "null ray or hit buffer");
+    ARG(((uintptr_t)d_rays & 15) == 0 && ((uintptr_t)d_hits & 15) == 0, "buffers must be 16-byte aligned");
+    CK(cudaSetDevice(s->ctx->device));
+    launch_cast(dev_scene(s), d_rays, d_hits, n, mode, s->ctx->d_misc, s->ctx->stream);
+    CK(cudaGetLastError());
+    return WL_OK;
+}
+
+int wl_cast_rays_host(wl_scene *s, const wl_ray *rays, wl_hit *hits, uint32_t n, uint32_t mode) {
+    ARG(s, "null scene");
+    if (n == 0) return WL_OK;
+    ARG(rays && hits, "null ray or hit buffer");
+    CK(cudaSetDevice(s->ctx->device));
+    wl_ray *dr = nullptr;
+    wl_hit *dh = nullptr;
+    CK(cudaMallocAsync((void **)&dr, sizeof(wl_ray) * (size_t)n, s->ctx->stream));
+    cudaError_t e = cudaMallocAsync((void **)&dh, sizeof(wl_hit) * (size_t)n, s->ctx->stream);
+    int rc = WL_OK;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dr, rays, sizeof(wl_ray) * (size_t)n, cudaMemcpyHostToDevice, s->ctx->stream);
+    if (e == cudaSuccess) rc = wl_cast_rays(s, dr, dh, n, mode);
+    if (e == cudaSuccess && rc == WL_OK)
+        e = cudaMemcpyAsync(hits, dh, sizeof(wl_hit) * (size_t)n, cudaMemcpyDeviceToHost, s->ctx->stream);
+    if (dr) cudaFreeAsync(dr, s->ctx->stream);
+    if (dh) cudaFreeAsync(dh, s->ctx->stream);
+    cudaError_t e2 = cudaStreamSynchronize(s->ctx->stream);
+    if (rc != WL_OK) return rc;
+    CK(e);
+    CK(e2);
+    return WL_OK;
+}
+
+int wl_cast_rays_stats(wl_scene *s, const wl_ray *d_rays, uint32_t n, uint32_t mode,
+                       uint64_t *node_visits, uint64_t *tri_tests) {
+    ARG(s && node_visits && tri_tests, "null argument");
+    if (!s->built) return fail(WL_ERR_NOT_BUILT, "bvh not built");
+    CK(cudaSetDevice(s->ctx->device));
+    launch_cast_stats(dev_scene(s), d_rays, n, mode, s->ctx->d_cast_counts, s->ctx->d_misc,
+                      s->ctx->stream);
+    CK(cudaGetLastError());
+    unsigned long long h[2];
+    CK(cudaMemcpyAsync(h, s->ctx->d_cast_counts, sizeof(h), cudaMemcpyDeviceToHost, s->ctx->stream));
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    *node_visits = h[0];
+    *tri_tests = h[1];
+    return WL_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+int wl_film_create(wl_context *c, uint32_t w, uint32_t h, uint32_t flags, wl_film **out) {
+    ARG(c && out && w > 0 && h > 0, "invalid film arguments");
+    ARG((uint64_t)w * h <= 0xFFFFFFFFull, "film too large");
+    CK(cudaSetDevice(c->device));
+    wl_film *f = new wl_film();
+    f->ctx = c;
+    f->f.W = w;
+    f->f.H = h;
+    f->f.flags = flags | WL_FILM_RUNNING_MEAN;
+    size_t np = (size_t)w * h;
+    cudaError_t e = cudaMalloc(&f->f.rgb, 3 * sizeof(float) * np);
+    if (e == cudaSuccess) e = cudaMalloc(&f->f.ldr, 4 * np);
+    if (e == cudaSuccess && (flags & WL_FILM_FP64_SUM)) e = cudaMalloc(&f->f.sum64, 3 * sizeof(double) * np);
+    c->live_children++;
+    if (e != cudaSuccess) {
+        wl_film_destroy(f);
+        return fail(WL_ERR_OOM, cudaGetErrorString(e));
+    }
+    *out = f;
+    return wl_film_clear(f);
+}
+
+int wl_film_destroy(wl_film *f) {
+    if (!f) return WL_OK;
+    f->ctx->live_children--;
+    cudaSetDevice(f->ctx->device);
+    cudaStreamSynchronize(f->ctx->stream);
+    if (f->f.rgb) cudaFree(f->f.rgb);
+    if (f->f.sum64) cudaFree(f->f.sum64);
+    if (f->f.ldr) cudaFree(f->f.ldr);
+    delete f;
+    return WL_OK;
+}
+
+int wl_film_clear(wl_film *f) {
+    ARG(f, "null film");
+    CK(cudaSetDevice(f->ctx->device));
+    size_t np = (size_t)f->f.W * f->f.H;
+    CK(cudaMemsetAsync(f->f.rgb, 0, 3 * sizeof(float) * np, f->ctx->stream));
+    if (f->f.sum64) CK(cudaMemsetAsync(f->f.sum64, 0, 3 * sizeof(double) * np, f->ctx->stream));
+    f->f.frames64 = 0;
+    return WL_OK;
+}
+
+int wl_film_download(wl_film *f, float *rgb, double *rgb64) {
+    ARG(f, "null film");
+    CK(cudaSetDevice(f->ctx->device));
+    size_t np = (size_t)f->f.W * f->f.H;
+    if (rgb) CK(cudaMemcpyAsync(rgb, f->f.rgb, 3 * sizeof(float) * np, cudaMemcpyDeviceToHost, f->ctx->stream));
+    if (rgb64) {
+        ARG(f->f.sum64, "film has no FP64 accumulation");
+        std::vector<double> tmp(3 * np);
+        CK(cudaMemcpyAsync(tmp.data(), f->f.sum64, 3 * sizeof(double) * np, cudaMemcpyDeviceToHost, f->ctx->stream));
+        CK(cudaStreamSynchronize(f->ctx->stream));
+        double cnt = (double)f->f.frames64;
+        for (size_t i = 0; i < 3 * np; i++) rgb64[i] = f->f.frames64 ? tmp[i] / cnt : 0.0;
+    }
+    CK(cudaStreamSynchronize(f->ctx->stream));
+    return WL_OK;
+}
+
+int wl_film_download_ldr(wl_film *f, uint8_t *rgba8) {
+    ARG(f && rgba8, "null argument");
+    CK(cudaSetDevice(f->ctx->device));
+    strict::launch_tonemap(f->f, f->ctx->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(rgba8, f->f.ldr, 4 * (size_t)f->f.W * f->f.H, cudaMemcpyDeviceToHost, f->ctx->stream));
+    CK(cudaStreamSynchronize(f->ctx->stream));
+    return WL_OK;
+}
+
+int wl_film_device_ptrs(wl_film *f, float **rgb, double **rgb64, uint8_t **ldr) {
+    ARG(f, "null film");
+    if (rgb) *rgb = f->f.rgb;
+    if (rgb64) *rgb64 = f->f.sum64;
+    if (ldr) *ldr = f->f.ldr;
+    return WL_OK;
+}
+
+void wl_render_params_default(wl_render_params *p, uint32_t w, uint32_t h, uint32_t spp) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->width = w;
+    p->height = h;
+    p->spp = spp;
+    p->first_frame = 0;
+    p->max_depth = 25;     // PathTracing.cu:235
+    p->rr_depth = 5;       // PathTracing.cu:130
+    p->rr_prob = 0.9f;     // PathTracing.cu:68
+    p->eps = 1e-3f;        // PathTracing.cu:19
+    p->strategy = WL_STRATEGY_MIS;  // PathTracing.cu:29
+    p->rng = WL_RNG_TEA_LCG;
+    p->math = WL_MATH_FAST;
+    p->lights = WL_LIGHTS_UNIFORM;
+    p->seed = 0;
+    p->wave_paths = 0;
+}
+
+int wl_render(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_params *p, wl_film *f) {
+    ARG(c && s && cam && p && f, "null argument");
+    ARG(s->ctx == c && f->ctx == c, "scene and film must belong to the context");
+    if (!s->built) return fail(WL_ERR_NOT_BUILT, "bvh not built");
+    ARG(p->width == f->f.W && p->height == f->f.H, "film size differs from the render size");
+    ARG(p->spp > 0, "spp must be > 0");
+    ARG(p->max_depth > 0 && p->max_depth <= 1024, "max_depth out of range");
+    ARG(p->strategy <= WL_STRATEGY_MIS, "bad strategy");
+    ARG(p->rng <= WL_RNG_PCG32, "bad rng");
+    ARG(p->math <= WL_MATH_STRICT, "bad math mode");
+    ARG(p->lights == WL_LIGHTS_UNIFORM, "only uniform light selection is available");
+    ARG(p->rr_prob > 0.0f && p->rr_prob <= 1.0f, "rr_prob must be in (0, 1]");
+    ARG(finite3(cam->pos) && finite3(cam->look_at) && finite3(cam->up) && finite3(cam->right), "non-finite camera");
+    CK(cudaSetDevice(c->device));
+    c->stats_pending = false;  // counters of an earlier call that nobody read are discarded
+    const uint32_t npix = p->width * p->height;
+    const uint64_t total = (uint64_t)npix * p->spp;
+    uint64_t want = p->wave_paths ? p->wave_paths : (1ull << 23);
+    if (want < 1024) want = 1024;
+    if (want > (1ull << 26)) want = 1ull << 26;
+    uint32_t spp_per_wave = (uint32_t)(want / npix);
+    uint64_t wave = spp_per_wave >= 1 ? (uint64_t)spp_per_wave * npix : want;
+    if (wave > total) wave = total;
+    int rc = ensure_queues(c, (uint32_t)wave);
+    if (rc != WL_OK) return rc;
+
+    WaveParams wp{};
+    wp.W = p->width; wp.H = p->height; wp.npix = npix;
+    wp.first_frame = p->first_frame;
+    wp.max_depth = p->max_depth; wp.rr_depth = p->rr_depth;
+    wp.rr_prob = p->rr_prob; wp.eps = p->eps;
+    wp.strategy = p->strategy; wp.rng = p->rng; wp.lights = p->lights; wp.seed = p->seed;
+    for (int k = 0; k < 3; k++) {
+        wp.env[k] = p->env[k];
+        wp.cam_pos[k] = cam->pos[k]; wp.cam_look[k] = cam->look_at[k];
+        wp.cam_up[k] = cam->up[k]; wp.cam_right[k] = cam->right[k];
+    }
+    wp.has_env = (p->env[0] != 0.f || p->env[1] != 0.f || p->env[2] != 0.f) ? 1u : 0u;
+    DevScene sc = dev_scene(s);
+    cudaStream_t st = c->stream;
+    for (auto &u : c->ev_used) u = 0;
+    CK(cudaMemsetAsync(c->q.totals, 0, 6 * sizeof(unsigned long long), st));
+    const bool tstats = (p->flags & WL_RENDER_TRAVERSAL_STATS) != 0;
+    CK(cudaEventRecord(c->ev_total[0], st));
+    uint32_t launches = 0, waves = 0;
+    const bool strict_math = p->math == WL_MATH_STRICT;
+    for (uint64_t base = 0; base < total; base += wave) {
+        wp.base = base;
+        wp.count = (uint32_t)((total - base) < wave ? (total - base) : wave);
+        rec(c, 3, true);
+        if (strict_math) strict::launch_generate(wp, c->q, st);
+        else fast::launch_generate(wp, c->q, st);
+        rec(c, 3, false);
+        launches++;
+        int in = 0;
+        for (uint32_t b = 0; b < p->max_depth; b++) {
+            rec(c, 0, true);
+            launch_extend(sc, c->q, in, tstats, st);
+            rec(c, 0, false);
+            CK(cudaMemsetAsync(c->q.counters + (in ^ 1), 0, sizeof(uint32_t), st));
+            CK(cudaMemsetAsync(c->q.counters + 2, 0, sizeof(uint32_t), st));
+            rec(c, 1, true);
+            if (strict_math) strict::launch_shade(wp, sc, c->q, in, st);
+            else fast::launch_shade(wp, sc, c->q, in, st);
+            rec(c, 1, false);
+            rec(c, 2, true);
+            launch_shadow(sc, c->q, tstats, st);
+            rec(c, 2, false);
+            launches += 3;
+            in ^= 1;
+        }
+        rec(c, 3, true);
+        strict::launch_film(wp, c->q, f->f, st);
+        rec(c, 3, false);
+        launches++;
+        waves++;
+        CK(cudaGetLastError());
+    }
+    CK(cudaEventRecord(c->ev_total[1], st));
+    f->f.frames64 += p->spp;
+    c->stats = wl_render_stats{};
+    c->stats.paths = total;
+    c->stats.waves = waves;
+    c->stats.kernel_launches = launches;
+    c->stats_pending = true;
+    return WL_OK;
+}
+
+int wl_render_get_stats(wl_context *c, wl_render_stats *out) {
+    ARG(c && out, "null argument");
+    CK(cudaSetDevice(c->device));
+    int rc = finish_stats(c);
+    if (rc != WL_OK) return rc;
+    *out = c->stats;
+    return WL_OK;
+}
+
+int wl_debug_rng(wl_context *c, uint32_t rng, uint64_t seed, const uint32_t *d_pixels, uint32_t npix,
+                 uint32_t frame, uint32_t count, float *d_out) {
+    ARG(c && d_pixels && d_out, "null argument");
+    ARG(rng <= WL_RNG_PCG32, "bad rng");
+    CK(cudaSetDevice(c->device));
+    strict::launch_debug_rng(rng, seed, d_pixels, npix, frame, count, d_out, c->stream);
+    CK(cudaGetLastError());
+    return WL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,269 @@
+// pt_kernels.cuh - wavefront form of the reference's path tracer (PathTracing.cu:40-288).
+//
+// Included by pt_fast.cu (--use_fast_math) and pt_strict.cu (IEEE, no FMA contraction) with
+// WL_NS set to the namespace of the instantiation. One megakernel thread per pixel sample in the
+// reference becomes, per bounce:
+//   extend (traverse.cu)  closest hit of every ray in the queue
+//   shade  (here)         __closesthit__radiance + the NEE block of __raygen__RenderFrame:
+//                         emitter hit with MIS, Disney sample/pdf/eval, the light sample and its
+//                         MIS-weighted contribution (pushed with a shadow ray), Russian roulette,
+//                         the next ray (pushed, compacted by warp ballot + one atomic per warp)
+//   shadow (traverse.cu)  any hit; adds the light sample to the path radiance when unoccluded
+// and, once per wave, film: the running mean of PathTracing.cu:145-154 in path order.
+// The random stream of a path is consumed in the reference's order (camera 2, BSDF sample 7
+// (+2), light 4, roulette 1), so each path sees the same numbers as the reference's loop.
+#pragma once
+#include "wl_bvh.cuh"
+#include "wl_disney.cuh"
+#include "wl_internal.h"
+
+namespace wl {
+namespace WL_NS {
+
+constexpr int PT = 256;
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Warp-aggregated append: one atomic per warp, slots in lane order.
+__device__ __forceinline__ uint32_t warp_append(bool want, uint32_t *ctr) {
+    uint32_t mask = __ballot_sync(0xffffffffu, want);
+    uint32_t base = 0;
+    int leader = __ffs(mask) - 1;
+    if (mask && (int)(threadIdx.x & 31) == leader) base = atomicAdd(ctr, (uint32_t)__popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader < 0 ? 0 : leader);
+    return base + __popc(mask & lanemask_lt());
+}
+
+__global__ void __launch_bounds__(PT) k_generate(WaveParams wp, Queues q) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        q.counters[0] = wp.count;
+        q.counters[1] = 0;
+        q.counters[2] = 0;
+    }
+    if (i >= wp.count) return;
+    uint64_t g = wp.base + i;
+    uint32_t pixel = (uint32_t)(g % wp.npix);
+    uint32_t frame = wp.first_frame + (uint32_t)(g / wp.npix);
+    uint32_t px = pixel % wp.W, py = pixel / wp.W;
+    Rng rng = make_rng(wp.rng, wp.seed, pixel, frame);
+    // PinholeGenerateRay, Camera.h:28-35
+    float u = 2.f * ((float)px + rng.next()) / (float)wp.W - 1.f;
+    float v = 2.f * ((float)py + rng.next()) / (float)wp.H - 1.f;
+    v3 dir = normalize(ld3(wp.cam_look) + ld3(wp.cam_right) * u + ld3(wp.cam_up) * v);
+    q.ray_o[0][i] = make_float4(wp.cam_pos[0], wp.cam_pos[1], wp.cam_pos[2], wp.eps);
+    q.ray_d[0][i] = make_float4(dir.x, dir.y, dir.z, 1e30f);
+    q.ray_slot[0][i] = i;
+    q.st_thr[i] = make_float4(1.f, 1.f, 1.f, 1.f);
+    q.st_term[i] = make_float4(1.f, 1.f, 1.f, __uint_as_float(0u));
+    q.st_rad[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    q.st_rng[i] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
+}
+
+__device__ __forceinline__ v3 vtx(const float *V, uint32_t i) {
+    return v3(V[3 * (size_t)i], V[3 * (size_t)i + 1], V[3 * (size_t)i + 2]);
+}
+
+// GetTriangleArea, Common.h:59-62
+__device__ __forceinline__ float tri_area(const DevScene &sc, uint32_t t) {
+    uint4 ti = sc.tri[t];
+    v3 a = vtx(sc.V, ti.x), b = vtx(sc.V, ti.y), c = vtx(sc.V, ti.z);
+    return 0.5f * length(cross(b - a, c - a));
+}
+
+__global__ void __launch_bounds__(PT) k_shade(WaveParams wp, DevScene sc, Queues q, int in) {
+    const uint32_t n = q.counters[in];
+    const int out = in ^ 1;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        uint32_t i = base + threadIdx.x;
+        bool valid = i < n;
+        bool push_ray = false, push_shadow = false;
+        uint32_t slot = 0;
+        v3 new_o, new_d, sh_d, ld;
+        float sh_tmax = 0.f;
+        if (valid) {
+            slot = q.ray_slot[in][i];
+            float4 h = q.hit[i];
+            float4 ro = q.ray_o[in][i], rd = q.ray_d[in][i];
+            float4 thr4 = q.st_thr[slot], term4 = q.st_term[slot], rad4 = q.st_rad[slot];
+            uint2 rs = q.st_rng[slot];
+            v3 thr = f4xyz(thr4), term = f4xyz(term4), rad = f4xyz(rad4);
+            float last_pdf = thr4.w;
+            uint32_t depth = __float_as_uint(term4.w);
+            uint64_t g = wp.base + slot;
+            Rng rng;
+            rng.mode = wp.rng;
+            rng.pixel = (uint32_t)(g % wp.npix);
+            rng.state = (uint64_t)rs.x | ((uint64_t)rs.y << 32);
+            v3 pos = f4xyz(ro), dir = f4xyz(rd);
+            uint32_t prim = __float_as_uint(h.y);
+            bool alive = true;
+            if (prim == INVALID) {
+                // __miss__radiance (PathTracing.cu:163-171); a constant environment is weighted
+                // by the last BSDF term as well (the reference's background is 0)
+                if (wp.has_env) rad = rad + thr * term * ld3(wp.env);
+                alive = false;
+            } else {
+                // __closesthit__radiance (PathTracing.cu:181-288)
+                depth += 1;
+                float t = h.x;
+                uint4 ti = sc.tri[prim];
+                v3 a = vtx(sc.V, ti.x), b = vtx(sc.V, ti.y), c = vtx(sc.V, ti.z);
+                v3 Ng = normalize(cross(b - a, c - a));
+                v3 Ns;
+                if (ti.w >> 31) {
+                    float bu = h.z, bv = h.w;
+                    Ns = normalize(vtx(sc.N, ti.x) * (1.0f - bu - bv) + vtx(sc.N, ti.y) * bu +
+                                   vtx(sc.N, ti.z) * bv);
+                } else {
+                    Ns = Ng;
+                }
+                v3 hit_pos = pos + dir * t;
+                uint32_t lid = sc.tri_light[prim];
+                if (lid != INVALID) {
+                    const DevLight &lt = sc.lights[lid];
+                    if (depth == 1 || (wp.strategy != WL_STRATEGY_NEE &&
+                                       (lt.two_sided || dot(Ns, dir) < 0.0f))) {
+                        float nee_pdf = 0.0f;
+                        if (wp.strategy != WL_STRATEGY_UPT && depth > 1) {
+                            // PdfAreaLightPos, Pdf.h:28-39
+                            float lp = 1.0f / (float)sc.nLight;
+                            lp /= (float)lt.tri_count;
+                            lp /= tri_area(sc, prim);
+                            nee_pdf = lp * t * t / fabsf(dot(Ns, dir));
+                        }
+                        rad = rad + thr * ld3(lt.L) * term * (last_pdf / (last_pdf + nee_pdf));
+                    }
+                    alive = false;
+                } else if (depth >= wp.max_depth) {
+                    alive = false;
+                } else {
+                    Mat m = load_mat(sc.mats + (ti.w & 0x7fffffffu));
+                    if (m.trans < 0.1f) {
+                        if (dot(Ng, dir) > 0.0f) Ng = -Ng;
+                        if (dot(Ns, dir) > 0.0f) Ns = -Ns;
+                    }
+                    v3 V = -dir;
+                    v3 ndir = normalize(sample_disney(m, Ns, V, rng));
+                    float pdf = pdf_disney(m, Ns, V, ndir);
+                    if (pdf < 0.0f || isnan(pdf)) {
+                        alive = false;
+                    } else {
+                        v3 tex(1.0f);
+                        thr = thr * term;
+                        float cosw = dot(ndir, Ns);
+                        v3 bsdf = clampv(eval_disney(m, Ns, Ng, V, ndir, tex), 0.f, 1e30f);
+                        term = bsdf * fabsf(cosw) / pdf;
+                        last_pdf = pdf;
+                        // next-event estimation (PathTracing.cu:81-129) at this vertex
+                        if (wp.strategy != WL_STRATEGY_UPT && sc.nLight > 0) {
+                            // SampleAreaLightPos, Sample.h:105-132
+                            uint32_t li = (uint32_t)((float)sc.nLight * rng.next());
+                            if (li >= sc.nLight) li = sc.nLight - 1;
+                            const DevLight &lt = sc.lights[li];
+                            float lp = 1.0f / (float)sc.nLight;
+                            uint32_t tk = (uint32_t)(rng.next() * (float)lt.tri_count);
+                            if (tk >= lt.tri_count) tk = lt.tri_count - 1;
+                            lp = lp / (float)lt.tri_count;
+                            uint32_t lt_tri = lt.first_tri + tk;
+                            uint4 li4 = sc.tri[lt_tri];
+                            v3 v0 = vtx(sc.V, li4.x), v1 = vtx(sc.V, li4.y), v2 = vtx(sc.V, li4.z);
+                            float su = rng.next(), sv = rng.next();
+                            if (su + sv > 1.0f) { su = 1.0f - su; sv = 1.0f - sv; }
+                            float cx = 1.0f - su - sv, cy = su;
+                            v3 lpos = v0 + su * (v1 - v0) + sv * (v2 - v0);
+                            lp = lp / tri_area(sc, lt_tri);
+                            v3 lN;
+                            if (lt.has_normal) {
+                                lN = normalize(vtx(sc.N, li4.x) * (1.0f - cx - cy) + vtx(sc.N, li4.y) * cx +
+                                               vtx(sc.N, li4.z) * cy);
+                            } else {
+                                lN = normalize(cross(v1 - v0, v2 - v0));
+                            }
+                            v3 vis = lpos - hit_pos;
+                            float dist = length(vis);
+                            vis = vis / dist;
+                            float cos1 = dot(lN, vis);
+                            if (lt.two_sided || cos1 < 0.0f) {
+                                float cos2 = dot(Ns, vis);
+                                float nee_pdf = lp * dist * dist / fabsf(cos1);
+                                float upt_pdf = 0.0f;
+                                if (wp.strategy != WL_STRATEGY_NEE) {
+                                    upt_pdf = pdf_disney(m, Ns, V, vis);
+                                    if (upt_pdf < 0.0f || isnan(upt_pdf)) upt_pdf = 0.0f;
+                                }
+                                v3 bv = clampv(eval_disney(m, Ns, Ng, V, vis, tex), 0.f, 1e30f);
+                                ld = thr * bv * fabsf(cos2) * ld3(lt.L) / nee_pdf *
+                                     (1.0f - upt_pdf / (upt_pdf + nee_pdf));
+                                sh_d = vis;
+                                sh_tmax = dist * (1.0f - wp.eps);
+                                new_o = hit_pos;
+                                push_shadow = true;
+                            }
+                        }
+                        // Russian roulette (PathTracing.cu:130-138)
+                        if (depth > wp.rr_depth) {
+                            if (rng.next() > wp.rr_prob) alive = false;
+                            else thr = thr / wp.rr_prob;
+                        }
+                        if (alive) {
+                            push_ray = true;
+                            new_o = hit_pos;
+                            new_d = ndir;
+                        }
+                    }
+                }
+            }
+            (void)alive;
+            q.st_thr[slot] = make_float4(thr.x, thr.y, thr.z, last_pdf);
+            q.st_term[slot] = make_float4(term.x, term.y, term.z, __uint_as_float(depth));
+            q.st_rad[slot] = make_float4(rad.x, rad.y, rad.z, 0.f);
+            q.st_rng[slot] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
+        }
+        uint32_t rpos = warp_append(push_ray, &q.counters[out]);
+        if (push_ray) {
+            q.ray_o[out][rpos] = make_float4(new_o.x, new_o.y, new_o.z, wp.eps);
+            q.ray_d[out][rpos] = make_float4(new_d.x, new_d.y, new_d.z, 1e30f);
+            q.ray_slot[out][rpos] = slot;
+        }
+        uint32_t spos = warp_append(push_shadow, &q.counters[2]);
+        if (push_shadow) {
+            q.sh_o[spos] = make_float4(new_o.x, new_o.y, new_o.z, wp.eps);
+            q.sh_d[spos] = make_float4(sh_d.x, sh_d.y, sh_d.z, sh_tmax);
+            q.sh_l[spos] = make_float4(ld.x, ld.y, ld.z, __uint_as_float(slot));
+        }
+        // segment and shadow-ray totals (one atomic per warp)
+        uint32_t nv = __popc(__ballot_sync(0xffffffffu, valid));
+        uint32_t ns = __popc(__ballot_sync(0xffffffffu, push_shadow));
+        if ((threadIdx.x & 31) == 0) {
+            if (nv) atomicAdd(&q.totals[0], (unsigned long long)nv);
+            if (ns) atomicAdd(&q.totals[1], (unsigned long long)ns);
+        }
+    }
+}
+
+void launch_generate(const WaveParams &wp, const Queues &q, cudaStream_t s) {
+    uint32_t blocks = (wp.count + PT - 1) / PT;
+    if (blocks == 0) blocks = 1;
+    k_generate<<<blocks, PT, 0, s>>>(wp, q);
+}
+
+void launch_shade(const WaveParams &wp, const DevScene &sc, const Queues &q, int in, cudaStream_t s) {
+    static int grid = 0;
+    if (!grid) {
+        int dev = 0, sms = 0, per = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_shade, PT, 0);
+        grid = sms * (per > 0 ? per : 1);
+    }
+    k_shade<<<grid, PT, 0, s>>>(wp, sc, q, in);
+}
+
+}  // namespace WL_NS
+}  // namespace wl

@@ -1,0 +1,469 @@
+// wl_bvh.cuh - BVH formats, build steps and traversal (host + device).
+//
+// Replaces optixAccelBuild / optixTrace (src/Backend/Optix/Core/AccelStructure.cpp:133-162,
+// src/Frontend/Programs/PathTracing/PathTracing.cu:72-102). OptiX is closed, so these are the
+// project's own definitions:
+//   1. 63-bit Morton codes of triangle-AABB centres (21 bits per axis, x most significant);
+//   2. a radix tree over the (code, index)-sorted triangles after Karras 2012, "Maximizing
+//      Parallelism in the Construction of BVHs, Octrees, and k-d Trees" (internal nodes 0..n-2,
+//      leaves n-1..2n-2);
+//   3. bottom-up bounds (exact min/max, so the result is independent of thread order);
+//   4. collapse into an 8-wide compressed BVH in the spirit of Ylitie, Karras, Laine 2017
+//      ("Efficient Incoherent Ray Traversal on GPUs Through Compressed Wide BVHs"): 80-byte
+//      nodes with 8-bit quantised child boxes, leaves of up to 3 triangles, children placed in
+//      slots by ray octant so that visiting slots in order (slot XOR octant) is near-to-far;
+//   5. traversal with a stack of node groups and the watertight triangle test of wl_math.cuh.
+// Child boxes decode exactly (the grid origin is a multiple of the power-of-two scale) and the
+// slab test keeps a relative margin of 2^-20, so a box never rejects a triangle the triangle
+// test accepts: closest hits equal the brute-force definition bit for bit.
+#pragma once
+#include "wl_math.cuh"
+
+namespace wl {
+
+constexpr uint32_t INVALID = 0xFFFFFFFFu;
+constexpr int TRAV_STACK = 64;
+constexpr int LEAF_MAX = 3;
+
+// 80-byte node = 5 x 16 bytes:
+//  n0: p.x, p.y, p.z (float), e.x | e.y << 8 | e.z << 16 | imask << 24
+//  n1: child_base, tri_base, meta[0..3], meta[4..7]
+//  n2: qlo_x[8], qlo_y[8]   n3: qlo_z[8], qhi_x[8]   n4: qhi_y[8], qhi_z[8]
+// meta[s]: 0 = empty; internal child = 0x20 | (24 + s); leaf = unary(count) << 5 | offset.
+struct alignas(16) WideNode {
+    float4 n0, n1, n2, n3, n4;
+};
+static_assert(sizeof(WideNode) == 80, "wide node is 80 bytes");
+
+WL_HD uint8_t byte_of(uint32_t lo, uint32_t hi, int s) {
+    uint32_t w = s < 4 ? lo : hi;
+    return (uint8_t)((w >> (8 * (s & 3))) & 0xffu);
+}
+
+// ---------------------------------------------------------------------------------------
+// Morton codes
+WL_HD uint64_t expand21(uint32_t v) {
+    uint64_t x = v & 0x1fffffu;
+    x = (x | x << 32) & 0x1f00000000ffffULL;
+    x = (x | x << 16) & 0x1f0000ff0000ffULL;
+    x = (x | x << 8) & 0x100f00f00f00f00fULL;
+    x = (x | x << 4) & 0x10c30c30c30c30c3ULL;
+    x = (x | x << 2) & 0x1249249249249249ULL;
+    return x;
+}
+// centre of the triangle's AABB on one axis
+WL_HD float tri_centre(float p0, float p1, float p2) {
+    float mn = fminf(fminf(p0, p1), p2), mx = fmaxf(fmaxf(p0, p1), p2);
+    return XMUL(XADD(mn, mx), 0.5f);
+}
+WL_HD uint32_t morton_q(float c, float lo, float hi) {
+    float ext = XSUB(hi, lo);
+    float scale = ext > 0.0f ? XDIV(2097152.0f, ext) : 0.0f;
+    float f = XMUL(XSUB(c, lo), scale);
+    f = fminf(fmaxf(f, 0.0f), 2097151.0f);
+    return (uint32_t)f;
+}
+
+// ---------------------------------------------------------------------------------------
+// Karras 2012 radix tree node i over n sorted 63-bit keys (made unique by the index).
+WL_HD int clz64(uint64_t x) {
+#ifdef __CUDA_ARCH__
+    return __clzll((long long)x);
+#else
+    return x ? __builtin_clzll(x) : 64;
+#endif
+}
+WL_HD int clz32(uint32_t x) {
+#ifdef __CUDA_ARCH__
+    return __clz((int)x);
+#else
+    return x ? __builtin_clz(x) : 32;
+#endif
+}
+struct KarrasKeys {
+    const uint64_t *k;
+    int n;
+    WL_HD int delta(int i, int j) const {
+        if (j < 0 || j > n - 1) return -1;
+        uint64_t a = k[i], b = k[j];
+        if (a == b) return 64 + clz32((uint32_t)(i ^ j));
+        return clz64(a ^ b);
+    }
+    WL_HD void node(int i, int &left, int &right) const {
+        int d = (delta(i, i + 1) - delta(i, i - 1)) > 0 ? 1 : -1;
+        int dmin = delta(i, i - d);
+        int lmax = 2;
+        while (delta(i, i + lmax * d) > dmin) lmax <<= 1;
+        int l = 0;
+        for (int t = lmax >> 1; t >= 1; t >>= 1)
+            if (delta(i, i + (l + t) * d) > dmin) l += t;
+        int j = i + l * d;
+        int dnode = delta(i, j);
+        int s = 0, div = 2;
+        int t = (l + div - 1) / div;
+        while (true) {
+            if (delta(i, i + (s + t) * d) > dnode) s += t;
+            if (t <= 1) break;
+            div <<= 1;
+            t = (l + div - 1) / div;
+        }
+        int g = i + s * d + (d < 0 ? d : 0);
+        int lo = i < j ? i : j, hi = i < j ? j : i;
+        left = (lo == g) ? (n - 1 + g) : g;
+        right = (hi == g + 1) ? (n - 1 + g + 1) : (g + 1);
+    }
+};
+
+// ---------------------------------------------------------------------------------------
+// Binary tree as the collapse reads it: blo = (lo.xyz, half area), bhi = (hi.xyz, count bits).
+struct BinTree {
+    const int *left, *right;
+    const float4 *blo, *bhi;
+    const uint32_t *sorted_prims;
+    int n;
+    WL_HD bool leaf(int x) const { return x >= n - 1; }
+    WL_HD uint32_t count(int x) const { return leaf(x) ? 1u : as_uint(bhi[x].w); }
+    WL_HD float area(int x) const { return blo[x].w; }
+};
+WL_HD float half_area(float lx, float ly, float lz, float hx, float hy, float hz) {
+    float dx = hx - lx, dy = hy - ly, dz = hz - lz;
+    return dx * dy + dy * dz + dz * dx;
+}
+
+struct Entries {
+    int ent[8];
+    int slot[8];
+    int ne;
+};
+
+// Children of the wide node made from binary node b: open the largest-area internal entry
+// holding more than LEAF_MAX triangles until 8 entries exist; if slots remain, open further
+// internal entries by area. Ties keep the earlier entry (deterministic).
+WL_HD void select_entries(const BinTree &T, int b, Entries &E) {
+    E.ne = 0;
+    if (T.leaf(b)) {
+        E.ent[0] = b;
+        E.ne = 1;
+    } else {
+        E.ent[0] = T.left[b];
+        E.ent[1] = T.right[b];
+        E.ne = 2;
+    }
+    while (E.ne < 8) {
+        int best = -1;
+        float best_a = -1.0f;
+        for (int k = 0; k < E.ne; k++) {
+            int x = E.ent[k];
+            if (!T.leaf(x) && T.count(x) > (uint32_t)LEAF_MAX && T.area(x) > best_a) {
+                best = k;
+                best_a = T.area(x);
+            }
+        }
+        if (best < 0) {
+            for (int k = 0; k < E.ne; k++) {
+                int x = E.ent[k];
+                if (!T.leaf(x) && T.area(x) > best_a) {
+                    best = k;
+                    best_a = T.area(x);
+                }
+            }
+        }
+        if (best < 0) break;
+        int x = E.ent[best];
+        E.ent[best] = T.left[x];
+        E.ent[E.ne++] = T.right[x];
+    }
+}
+
+// Greedy octant assignment: slot s is the first child for rays whose direction has sign bits s
+// (bit a set = negative component a); the score of (entry, slot) is the offset of the entry's
+// centre from the parent's centre projected on (+-1, +-1, +-1) with + where bit a is set.
+WL_HD void assign_slots(const BinTree &T, int b, Entries &E) {
+    float4 plo = T.blo[b], phi = T.bhi[b];
+    float pcx = plo.x + phi.x, pcy = plo.y + phi.y, pcz = plo.z + phi.z;
+    float sc[8][8];
+    for (int e = 0; e < E.ne; e++) {
+        int x = E.ent[e];
+        float cx = T.blo[x].x + T.bhi[x].x - pcx;
+        float cy = T.blo[x].y + T.bhi[x].y - pcy;
+        float cz = T.blo[x].z + T.bhi[x].z - pcz;
+        for (int s = 0; s < 8; s++)
+            sc[e][s] = ((s & 1) ? cx : -cx) + ((s & 2) ? cy : -cy) + ((s & 4) ? cz : -cz);
+        E.slot[e] = -1;
+    }
+    uint32_t used = 0;
+    for (int it = 0; it < E.ne; it++) {
+        int be = -1, bs = -1;
+        float bv = 0.f;
+        for (int e = 0; e < E.ne; e++) {
+            if (E.slot[e] >= 0) continue;
+            for (int s = 0; s < 8; s++) {
+                if (used & (1u << s)) continue;
+                if (be < 0 || sc[e][s] > bv) {
+                    be = e; bs = s; bv = sc[e][s];
+                }
+            }
+        }
+        E.slot[be] = bs;
+        used |= 1u << bs;
+    }
+}
+
+// Number of internal wide children and of triangles referenced by leaf slots.
+WL_HD void entry_counts(const BinTree &T, const Entries &E, uint32_t &n_int, uint32_t &n_tri) {
+    n_int = 0;
+    n_tri = 0;
+    for (int e = 0; e < E.ne; e++) {
+        uint32_t c = T.count(E.ent[e]);
+        if (c > (uint32_t)LEAF_MAX) n_int++;
+        else n_tri += c;
+    }
+}
+
+// ceil(log2(x)) for x > 0 (double)
+WL_HD int ceil_log2(double x) {
+    int k;
+    double f = frexp(x, &k);  // x = f 2^k, f in [0.5, 1)
+    return f == 0.5 ? k - 1 : k;
+}
+
+// Quantisation grid of one axis: scale = 2^e with 254 scale >= extent and |bound| / scale < 2^22,
+// origin p = floor(lo / scale) * scale. Then p + q * scale is exact in float for q in [0, 255].
+WL_HD void quant_axis(float lo, float hi, int &e, float &p, double &scale) {
+    double ext = (double)hi - (double)lo;
+    double m = fmax(fabs((double)lo), fabs((double)hi));
+    int e1 = ext > 0.0 ? ceil_log2(ext / 254.0) : -126;
+    int e2 = m > 0.0 ? ceil_log2(m / 4194304.0) : -126;
+    e = e1 > e2 ? e1 : e2;
+    if (e < -126) e = -126;
+    if (e > 127) e = 127;
+    scale = ldexp(1.0, e);
+    p = (float)(floor((double)lo / scale) * scale);
+}
+
+// Gather the triangles below binary node x (leaves in left-to-right order) into out (<= 3).
+WL_HD int gather_leaf_prims(const BinTree &T, int x, uint32_t *out) {
+    int st[8], sp = 0, n = 0;
+    st[sp++] = x;
+    while (sp) {
+        int y = st[--sp];
+        if (T.leaf(y)) {
+            out[n++] = T.sorted_prims[y - (T.n - 1)];
+        } else {
+            st[sp++] = T.right[y];
+            st[sp++] = T.left[y];
+        }
+    }
+    return n;
+}
+
+// Write the wide node for binary node b. child_base / tri_base: its first internal child's wide
+// index and first triangle record. child_items receives the binary index of each internal
+// child in rank (slot) order. tris: triangle records (3 float4 each) starting at tri_base.
+WL_HD void emit_wide(const BinTree &T, int b, const Entries &E, uint32_t child_base,
+                     uint32_t tri_base, const float *V, const uint32_t *I, WideNode *node_out,
+                     float4 *tris, int *child_items) {
+    float4 plo = T.blo[b], phi = T.bhi[b];
+    int ex, ey, ez;
+    float px, py, pz;
+    double sx, sy, sz;
+    quant_axis(plo.x, phi.x, ex, px, sx);
+    quant_axis(plo.y, phi.y, ey, py, sy);
+    quant_axis(plo.z, phi.z, ez, pz, sz);
+    int by_slot[8];
+    for (int s = 0; s < 8; s++) by_slot[s] = -1;
+    for (int e = 0; e < E.ne; e++) by_slot[E.slot[e]] = e;
+    uint8_t meta[8], qlx[8], qly[8], qlz[8], qhx[8], qhy[8], qhz[8];
+    uint32_t imask = 0, rank = 0, toff = 0;
+    for (int s = 0; s < 8; s++) {
+        meta[s] = qlx[s] = qly[s] = qlz[s] = qhx[s] = qhy[s] = qhz[s] = 0;
+        int e = by_slot[s];
+        if (e < 0) continue;
+        int x = E.ent[e];
+        float4 clo = T.blo[x], chi = T.bhi[x];
+        auto ql = [](float c, float p, double sc) {
+            double q = floor(((double)c - (double)p) / sc);
+            return (uint8_t)(q < 0 ? 0 : (q > 255 ? 255 : q));
+        };
+        auto qh = [](float c, float p, double sc) {
+            double q = ceil(((double)c - (double)p) / sc);
+            return (uint8_t)(q < 0 ? 0 : (q > 255 ? 255 : q));
+        };
+        qlx[s] = ql(clo.x, px, sx); qly[s] = ql(clo.y, py, sy); qlz[s] = ql(clo.z, pz, sz);
+        qhx[s] = qh(chi.x, px, sx); qhy[s] = qh(chi.y, py, sy); qhz[s] = qh(chi.z, pz, sz);
+        uint32_t c = T.count(x);
+        if (c > (uint32_t)LEAF_MAX) {
+            imask |= 1u << s;
+            meta[s] = (uint8_t)(0x20 | (24 + s));
+            child_items[rank++] = x;
+        } else {
+            uint32_t prims[LEAF_MAX];
+            int np = gather_leaf_prims(T, x, prims);
+            uint32_t unary = (1u << np) - 1u;
+            meta[s] = (uint8_t)((unary << 5) | toff);
+            for (int k = 0; k < np; k++) {
+                uint32_t pr = prims[k];
+                float4 *r = tris + 3 * (size_t)(tri_base + toff + k);
+                const float *a = V + 3 * (size_t)I[3 * (size_t)pr];
+                const float *bb = V + 3 * (size_t)I[3 * (size_t)pr + 1];
+                const float *cc = V + 3 * (size_t)I[3 * (size_t)pr + 2];
+                r[0] = make_float4(a[0], a[1], a[2], as_float(pr));
+                r[1] = make_float4(bb[0], bb[1], bb[2], 0.f);
+                r[2] = make_float4(cc[0], cc[1], cc[2], 0.f);
+            }
+            toff += np;
+        }
+    }
+    auto pack4 = [](const uint8_t *q) {
+        return (uint32_t)q[0] | ((uint32_t)q[1] << 8) | ((uint32_t)q[2] << 16) | ((uint32_t)q[3] << 24);
+    };
+    WideNode w;
+    w.n0 = make_float4(px, py, pz,
+                       as_float((uint32_t)(ex + 127) | ((uint32_t)(ey + 127) << 8) |
+                                ((uint32_t)(ez + 127) << 16) | (imask << 24)));
+    w.n1 = make_float4(as_float(child_base), as_float(tri_base), as_float(pack4(meta)),
+                       as_float(pack4(meta + 4)));
+    w.n2 = make_float4(as_float(pack4(qlx)), as_float(pack4(qlx + 4)), as_float(pack4(qly)),
+                       as_float(pack4(qly + 4)));
+    w.n3 = make_float4(as_float(pack4(qlz)), as_float(pack4(qlz + 4)), as_float(pack4(qhx)),
+                       as_float(pack4(qhx + 4)));
+    w.n4 = make_float4(as_float(pack4(qhy)), as_float(pack4(qhy + 4)), as_float(pack4(qhz)),
+                       as_float(pack4(qhz + 4)));
+    *node_out = w;
+}
+
+// ---------------------------------------------------------------------------------------
+// Traversal
+WL_HD float safe_rcp(float d) {
+    return fabsf(d) < 1e-30f ? (d < 0.0f ? -1e30f : 1e30f) : XDIV(1.0f, d);
+}
+
+template <class Load>
+struct NodeView {
+    float4 n0, n1, n2, n3, n4;
+};
+
+#ifdef __CUDA_ARCH__
+__device__ __forceinline__ float4 ldg4(const float4 *p) { return __ldg(p); }
+#else
+inline float4 ldg4(const float4 *p) { return *p; }
+#endif
+
+struct TraceResult {
+    float t, u, v;
+    uint32_t prim;
+};
+
+// ANY: stop at the first hit (shadow rays). STATS: count node visits and triangle tests.
+// Returns false if the traversal stack overflowed (cannot happen when the tree depth is
+// <= TRAV_STACK, which the build checks).
+template <bool ANY, bool STATS>
+WL_HD bool traverse(const float4 *__restrict__ nodes, const float4 *__restrict__ tris, float ox,
+                    float oy, float oz, float dx, float dy, float dz, float tmin, float tmax,
+                    TraceResult &res, uint32_t *n_nodes, uint32_t *n_tris) {
+    res.t = tmax;
+    res.prim = INVALID;
+    res.u = res.v = 0.f;
+    RayPre pre = ray_pre(dx, dy, dz);
+    const float idx = safe_rcp(dx), idy = safe_rcp(dy), idz = safe_rcp(dz);
+    const uint32_t oct = (dx < 0.0f ? 1u : 0u) | (dy < 0.0f ? 2u : 0u) | (dz < 0.0f ? 4u : 0u);
+    const float grow = 1.0f + 0x1p-20f;
+    uint2 stack[TRAV_STACK];
+    int sp = 0;
+    uint2 ng = make_uint2(0u, (1u << (24 + oct)) | 1u);
+    uint2 tg = make_uint2(0u, 0u);
+    bool ok = true;
+    while (true) {
+        if (ng.y & 0xff000000u) {
+            uint32_t hits = ng.y >> 24;
+#ifdef __CUDA_ARCH__
+            int k = __ffs(hits) - 1;
+#else
+            int k = __builtin_ffs(hits) - 1;
+#endif
+            ng.y &= ~(1u << (24 + k));
+            uint32_t slot = (uint32_t)k ^ oct;
+            uint32_t below = ng.y & 0xffu & ((1u << slot) - 1u);
+#ifdef __CUDA_ARCH__
+            uint32_t node = ng.x + __popc(below);
+#else
+            uint32_t node = ng.x + __builtin_popcount(below);
+#endif
+            if (ng.y & 0xff000000u) {
+                if (sp < TRAV_STACK) stack[sp++] = ng;
+                else ok = false;
+            }
+            const float4 *np = nodes + 5 * (size_t)node;
+            float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3),
+                   n4 = ldg4(np + 4);
+            if (STATS) (*n_nodes)++;
+            uint32_t ew = as_uint(n0.w);
+            float scx = as_float((ew & 0xffu) << 23), scy = as_float(((ew >> 8) & 0xffu) << 23),
+                  scz = as_float(((ew >> 16) & 0xffu) << 23);
+            uint32_t imask = ew >> 24;
+            uint32_t m0 = as_uint(n1.z), m1 = as_uint(n1.w);
+            uint32_t qlx0 = as_uint(n2.x), qlx1 = as_uint(n2.y), qly0 = as_uint(n2.z), qly1 = as_uint(n2.w);
+            uint32_t qlz0 = as_uint(n3.x), qlz1 = as_uint(n3.y), qhx0 = as_uint(n3.z), qhx1 = as_uint(n3.w);
+            uint32_t qhy0 = as_uint(n4.x), qhy1 = as_uint(n4.y), qhz0 = as_uint(n4.z), qhz1 = as_uint(n4.w);
+            float tcur = res.t;
+            uint32_t ihits = 0, thits = 0;
+#pragma unroll
+            for (int s = 0; s < 8; s++) {
+                uint32_t meta = byte_of(m0, m1, s);
+                if (meta == 0) continue;
+                float lx = fmaf((float)byte_of(qlx0, qlx1, s), scx, n0.x);
+                float ly = fmaf((float)byte_of(qly0, qly1, s), scy, n0.y);
+                float lz = fmaf((float)byte_of(qlz0, qlz1, s), scz, n0.z);
+                float hx = fmaf((float)byte_of(qhx0, qhx1, s), scx, n0.x);
+                float hy = fmaf((float)byte_of(qhy0, qhy1, s), scy, n0.y);
+                float hz = fmaf((float)byte_of(qhz0, qhz1, s), scz, n0.z);
+                float t0x = XMUL(XSUB(lx, ox), idx), t1x = XMUL(XSUB(hx, ox), idx);
+                float t0y = XMUL(XSUB(ly, oy), idy), t1y = XMUL(XSUB(hy, oy), idy);
+                float t0z = XMUL(XSUB(lz, oz), idz), t1z = XMUL(XSUB(hz, oz), idz);
+                float tn = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), tmin));
+                float tf = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), tcur));
+                if (tn <= XMUL(tf, grow)) {
+                    if (imask & (1u << s)) ihits |= 1u << ((uint32_t)s ^ oct);
+                    else thits |= (meta >> 5) << (meta & 31u);
+                }
+            }
+            ng = make_uint2(as_uint(n1.x), (ihits << 24) | imask);
+            tg = make_uint2(as_uint(n1.y), thits);
+        }
+        while (tg.y) {
+#ifdef __CUDA_ARCH__
+            int k = __ffs(tg.y) - 1;
+#else
+            int k = __builtin_ffs(tg.y) - 1;
+#endif
+            tg.y &= tg.y - 1u;
+            const float4 *tp = tris + 3 * (size_t)(tg.x + (uint32_t)k);
+            float4 v0 = ldg4(tp), v1 = ldg4(tp + 1), v2 = ldg4(tp + 2);
+            if (STATS) (*n_tris)++;
+            float t, u, v;
+            if (tri_hit(pre, ox, oy, oz, v0, v1, v2, tmin, tmax, t, u, v)) {
+                uint32_t prim = as_uint(v0.w);
+                if (ANY) {
+                    res.t = t;
+                    res.prim = prim;
+                    res.u = u;
+                    res.v = v;
+                    return ok;
+                }
+                if (t < res.t || (t == res.t && prim < res.prim)) {
+                    res.t = t;
+                    res.prim = prim;
+                    res.u = u;
+                    res.v = v;
+                }
+            }
+        }
+        if (!(ng.y & 0xff000000u)) {
+            if (sp == 0) break;
+            ng = stack[--sp];
+        }
+    }
+    return ok;
+}
+
+}  // namespace wl

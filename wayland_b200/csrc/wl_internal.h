@@ -1,0 +1,131 @@
+// wl_internal.h - device data layout and the launch functions shared by the translation units
+// of libwayland_b200.so. Not part of the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/wayland_b200.h"
+
+namespace wl {
+
+// Light table entry on the device (Device::DeviceAreaLight, Device/Light.h:9-17, with the
+// emitting triangles as a range of the scene's index array): 32 bytes.
+struct DevLight {
+    float L[3];
+    int32_t two_sided;
+    uint32_t first_tri;
+    uint32_t tri_count;
+    uint32_t has_normal;
+    uint32_t pad;
+};
+
+// Everything a kernel needs to shade a hit (HitData of PathTracingLaunchParams.h:64-78, one
+// table for the whole scene instead of one SBT record per mesh).
+struct DevScene {
+    uint32_t nV, nT, nMat, nLight;
+    const float *V;          // 3 nV
+    const float *N;          // 3 nV or null
+    const float *UV;         // 2 nV or null
+    const uint4 *tri;        // (i0, i1, i2, material | has_normal << 31)
+    const uint32_t *tri_light;
+    const wl_disney *mats;
+    const DevLight *lights;
+    const float4 *nodes;     // 8-wide BVH, 5 float4 per node
+    const float4 *tris;      // triangle records in leaf order, 3 float4 each
+    uint32_t has_bvh;
+    // power-proportional light selection: FP64 CDF over emissive triangles
+    const double *emit_cdf;  // nEmit, inclusive prefix sums / total
+    const uint32_t *emit_tri;
+    uint32_t nEmit;
+    const cudaTextureObject_t *tex;
+    uint32_t nTex;
+};
+
+// Path-state arrays of one wave (structure of arrays in HBM, indexed by path slot).
+struct Queues {
+    uint32_t capacity;
+    // ray queues A/B: 32-byte rays as two float4, plus the path slot of each entry
+    float4 *ray_o[2], *ray_d[2];
+    uint32_t *ray_slot[2];
+    float4 *hit;             // (t, prim, u, v) for the current queue
+    // per path slot
+    float4 *st_thr;          // throughput.xyz, last bsdf pdf
+    float4 *st_term;         // last trace term (bsdf |cos| / pdf).xyz, depth (bits)
+    float4 *st_rad;          // radiance.xyz
+    uint2 *st_rng;           // random stream state
+    // shadow queue: origin/tmin, dir/tmax, (Ld.xyz, slot)
+    float4 *sh_o, *sh_d, *sh_l;
+    // counters: [0], [1] ray queue sizes, [2] shadow queue size, [3] segments, [4] shadow rays,
+    // [5] error flags
+    uint32_t *counters;
+    // 64-bit sums over a render: [0] segments, [1] shadow rays, [2..3] extend node visits and
+    // triangle tests, [4..5] the same for shadow rays
+    unsigned long long *totals;
+};
+
+// Film (the radiance buffer of PathTracingProgramManager.cpp:30-32 + colour buffer)
+struct Film {
+    uint32_t W, H, flags;
+    float *rgb;      // running mean, 3 W H
+    double *sum64;   // FP64 sum, 3 W H (flags & WL_FILM_FP64_SUM)
+    uint8_t *ldr;    // RGBA8
+    uint64_t frames64;  // samples in sum64
+};
+
+struct WaveParams {
+    uint32_t W, H, npix;
+    uint32_t first_frame;
+    uint64_t base;            // global path index of the wave's first slot
+    uint32_t count;           // paths in this wave
+    uint32_t max_depth, rr_depth;
+    float rr_prob, eps;
+    uint32_t strategy, rng, lights;
+    uint64_t seed;
+    float env[3];
+    uint32_t has_env;
+    float cam_pos[3], cam_look[3], cam_up[3], cam_right[3];
+};
+
+// launch functions (pt_kernels.cuh instantiated in pt_fast.cu / pt_strict.cu)
+namespace fast {
+void launch_generate(const WaveParams &wp, const Queues &q, cudaStream_t s);
+void launch_shade(const WaveParams &wp, const DevScene &sc, const Queues &q, int in, cudaStream_t s);
+}
+namespace strict {
+void launch_generate(const WaveParams &wp, const Queues &q, cudaStream_t s);
+void launch_shade(const WaveParams &wp, const DevScene &sc, const Queues &q, int in, cudaStream_t s);
+void launch_film(const WaveParams &wp, const Queues &q, const Film &f, cudaStream_t s);
+void launch_tonemap(const Film &f, cudaStream_t s);
+void launch_debug_rng(uint32_t rng, uint64_t seed, const uint32_t *pixels, uint32_t npix,
+                      uint32_t frame, uint32_t count, float *out, cudaStream_t s);
+}
+// traverse.cu
+void launch_extend(const DevScene &sc, const Queues &q, int in, bool stats, cudaStream_t s);
+void launch_shadow(const DevScene &sc, const Queues &q, bool stats, cudaStream_t s);
+void launch_cast(const DevScene &sc, const wl_ray *rays, wl_hit *hits, uint32_t n, uint32_t mode,
+                 uint32_t *fetch, cudaStream_t s);
+void launch_cast_stats(const DevScene &sc, const wl_ray *rays, uint32_t n, uint32_t mode,
+                       unsigned long long *counts, uint32_t *fetch, cudaStream_t s);
+
+// bvh_build.cu
+struct BvhBuild {
+    // inputs
+    const float *V;
+    const uint32_t *I;  // 3 nT (device copy of the caller's index array)
+    uint32_t nT;
+    // outputs (device, owned by the caller after the build)
+    uint64_t *morton;      // nT, scene order
+    uint32_t *sorted;      // nT
+    int *left, *right, *parent;
+    float4 *blo, *bhi;     // 2 nT - 1
+    float4 *nodes;         // 5 per wide node
+    float4 *tris;          // 3 per triangle
+    uint32_t wide_nodes, wide_depth;
+    float ms;
+};
+int bvh_build_lbvh(BvhBuild &b, cudaStream_t s, std::string &err);
+void bvh_free(BvhBuild &b);
+
+}  // namespace wl

@@ -1,0 +1,303 @@
+"""Procedural scenes for the benchmark configurations (seeded, synthetic).
+
+The reference renders pbrt scenes (scene/*.pbrt via SceneManager, src/Frontend/Core/
+SceneManager.cpp:14-49); the configurations measured here are procedural stand-ins with the
+shapes, sizes and value distributions the benchmark names:
+
+  cornell_box()        Plain PT, procedural Cornell box: unit-cube room of 5 quads, two
+                       axis-aligned boxes of height 0.3 and 0.6, one 0.25 x 0.25 ceiling light
+                       of radiance (17, 12, 4), matte albedos white 0.73, red (0.65, 0.05, 0.05),
+                       green (0.12, 0.45, 0.15); 256 x 256, 16 spp, depth 8.
+  displaced_sphere()   Plain PT at scale: icosphere subdivided to about 2M triangles displaced by
+                       fBm of amplitude 0.05, on a 2-triangle ground plane; Disney parameters per
+                       object from the seed; 4 quad lights and a constant environment of 0.1;
+                       1920 x 1080, 64 spp, depth 16.
+
+Matte surfaces use the reference's matte -> Disney mapping (Material.cpp:51-67: roughness 0.5,
+specular 0, sheenTint 0.5, eta 1.5), since the renderer's only surface model is that BSDF.
+"""
+from dataclasses import dataclass, field
+import math
+
+import numpy as np
+
+from . import _abi
+
+DISNEY = _abi.DISNEY_DTYPE
+LIGHT = _abi.LIGHT_DTYPE
+
+
+@dataclass
+class Scene:
+    """Flattened scene: the SceneManager fields (SceneManager.h:30-44) as the C ABI takes them."""
+    name: str
+    V: np.ndarray                      # (nV, 3) float32
+    I: np.ndarray                      # (nT, 3) uint32
+    tri_material: np.ndarray           # (nT,) uint32
+    mats: np.ndarray                   # (nMat,) DISNEY
+    lights: np.ndarray                 # (nLight,) LIGHT
+    N: np.ndarray = None               # (nV, 3) float32 or None
+    tri_flags: np.ndarray = None       # (nT,) uint32 or None
+    camera: dict = field(default_factory=dict)   # pos, look_at, up, right (wl_camera)
+    width: int = 256
+    height: int = 256
+    spp: int = 16
+    max_depth: int = 8
+    env: tuple = (0.0, 0.0, 0.0)
+
+    @property
+    def num_tris(self):
+        return int(self.I.shape[0])
+
+    def camera_struct(self):
+        c = _abi.Camera()
+        for k in ("pos", "look_at", "up", "right"):
+            getattr(c, k)[:] = [float(x) for x in self.camera[k]]
+        return c
+
+
+def disney(color, metallic=0.0, roughness=0.5, specular=0.0, specular_tint=0.0, eta=1.5,
+           trans=0.0, subsurface=0.0, anisotropic=0.0, sheen=0.0, sheen_tint=0.5,
+           clearcoat=0.0, clearcoat_gloss=1.0, texture=-1):
+    m = np.zeros((), DISNEY)
+    m["color"] = color
+    for k, v in dict(metallic=metallic, roughness=roughness, specular=specular,
+                     specular_tint=specular_tint, eta=eta, trans=trans, subsurface=subsurface,
+                     anisotropic=anisotropic, sheen=sheen, sheen_tint=sheen_tint,
+                     clearcoat=clearcoat, clearcoat_gloss=clearcoat_gloss, texture=texture).items():
+        m[k] = v
+    return m
+
+
+def matte(color):
+    """Disney(minipbrt::MatteMaterial*), Material.cpp:51-67."""
+    return disney(color, metallic=0.0, roughness=0.5, specular=0.0, specular_tint=0.0, eta=1.5,
+                  trans=0.0, sheen=0.0, sheen_tint=0.5, clearcoat=0.0, clearcoat_gloss=1.0)
+
+
+def pinhole(pos, target, up, fov_deg, width, height):
+    """PinholeCamera (Camera.cpp:15-28) + the aspect scaling of PathTracingProgramManager.cpp:28:
+    lookAt = normalize(target - pos), up scaled by tan(fov/2), right = cross(lookAt, up) * W/H."""
+    pos = np.asarray(pos, np.float64)
+    look = np.asarray(target, np.float64) - pos
+    look /= np.linalg.norm(look)
+    up = np.asarray(up, np.float64)
+    up = up - look * np.dot(up, look)
+    up /= np.linalg.norm(up)
+    up = up * math.tan(math.radians(fov_deg) / 2)
+    right = np.cross(look, up) * (width / height)
+    return dict(pos=pos.astype(np.float32), look_at=look.astype(np.float32),
+                up=up.astype(np.float32), right=right.astype(np.float32))
+
+
+def _quad(p0, p1, p2, p3):
+    """Two triangles (p0, p1, p2), (p0, p2, p3); normal = cross(p1 - p0, p2 - p0)."""
+    V = np.array([p0, p1, p2, p3], np.float32)
+    I = np.array([[0, 1, 2], [0, 2, 3]], np.uint32)
+    return V, I
+
+
+def _box(lo, hi):
+    x0, y0, z0 = lo
+    x1, y1, z1 = hi
+    faces = [
+        ((x0, y0, z0), (x1, y0, z0), (x1, y0, z1), (x0, y0, z1)),  # bottom
+        ((x0, y1, z0), (x0, y1, z1), (x1, y1, z1), (x1, y1, z0)),  # top
+        ((x0, y0, z0), (x0, y1, z0), (x1, y1, z0), (x1, y0, z0)),  # z0
+        ((x0, y0, z1), (x1, y0, z1), (x1, y1, z1), (x0, y1, z1)),  # z1
+        ((x0, y0, z0), (x0, y0, z1), (x0, y1, z1), (x0, y1, z0)),  # x0
+        ((x1, y0, z0), (x1, y1, z0), (x1, y1, z1), (x1, y0, z1)),  # x1
+    ]
+    return [_quad(*f) for f in faces]
+
+
+class _Builder:
+    def __init__(self):
+        self.V, self.I, self.M = [], [], []
+        self.nv = 0
+
+    def add(self, parts, mat):
+        first = sum(len(i) for i in self.I)
+        for V, I in parts:
+            self.V.append(V)
+            self.I.append(I + self.nv)
+            self.M.append(np.full(len(I), mat, np.uint32))
+            self.nv += len(V)
+        return first, sum(len(i) for i in self.I) - first
+
+    def arrays(self):
+        return (np.concatenate(self.V).astype(np.float32), np.concatenate(self.I).astype(np.uint32),
+                np.concatenate(self.M).astype(np.uint32))
+
+
+def cornell_box(width=256, height=256, spp=16, max_depth=8):
+    """Config 1: 10 room triangles + 24 box triangles + 2 light triangles = 36."""
+    b = _Builder()
+    white, red, green = 0, 1, 2
+    mats = np.array([matte((0.73, 0.73, 0.73)), matte((0.65, 0.05, 0.05)),
+                     matte((0.12, 0.45, 0.15))])
+    # room: x, y, z in [0, 1], open towards +z where the camera is
+    b.add([_quad((0, 0, 0), (1, 0, 0), (1, 0, 1), (0, 0, 1))], white)   # floor
+    b.add([_quad((0, 1, 0), (0, 1, 1), (1, 1, 1), (1, 1, 0))], white)   # ceiling
+    b.add([_quad((0, 0, 0), (0, 1, 0), (1, 1, 0), (1, 0, 0))], white)   # back wall
+    b.add([_quad((0, 0, 0), (0, 0, 1), (0, 1, 1), (0, 1, 0))], red)     # left wall
+    b.add([_quad((1, 0, 0), (1, 1, 0), (1, 1, 1), (1, 0, 1))], green)   # right wall
+    b.add(_box((0.13, 0.0, 0.53), (0.43, 0.3, 0.83)), white)            # short box
+    b.add(_box((0.53, 0.0, 0.17), (0.83, 0.6, 0.47)), white)            # tall box
+    # ceiling light, facing down: cross(p1 - p0, p2 - p0) = -y
+    y = 0.999
+    first, count = b.add([_quad((0.375, y, 0.375), (0.625, y, 0.375), (0.625, y, 0.625),
+                                (0.375, y, 0.625))], white)
+    V, I, M = b.arrays()
+    lights = np.zeros(1, LIGHT)
+    lights[0]["L"] = (17.0, 12.0, 4.0)
+    lights[0]["two_sided"] = 0
+    lights[0]["first_tri"] = first
+    lights[0]["tri_count"] = count
+    cam = pinhole((0.5, 0.5, 2.4), (0.5, 0.5, 0.0), (0, 1, 0), 39.3, width, height)
+    return Scene("cornell_box", V, I, M, mats, lights, camera=cam, width=width, height=height,
+                 spp=spp, max_depth=max_depth)
+
+
+# ---- config 2 ------------------------------------------------------------------------------
+def _icosahedron():
+    t = (1.0 + 5 ** 0.5) / 2.0
+    V = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t],
+                  [0, -1, -t], [0, 1, -t], [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]],
+                 np.float64)
+    V /= np.linalg.norm(V, axis=1, keepdims=True)
+    F = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9],
+                  [5, 11, 4], [11, 10, 2], [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2],
+                  [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5], [2, 4, 11], [6, 2, 10],
+                  [8, 6, 7], [9, 8, 1]], np.int64)
+    return V, F
+
+
+def subdivided_icosphere(n):
+    """Each icosahedron face split into n^2 triangles (20 n^2 in total), vertices welded."""
+    V0, F = _icosahedron()
+    ii, jj = np.meshgrid(np.arange(n + 1), np.arange(n + 1), indexing="ij")
+    keep = (ii + jj) <= n
+    ii, jj = ii[keep], jj[keep]
+    local = -np.ones((n + 1, n + 1), np.int64)
+    local[ii, jj] = np.arange(len(ii))
+    # triangles of one face in (i, j) lattice coordinates
+    a_i, a_j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    up = (a_i + a_j) <= n - 1
+    ui, uj = a_i[up], a_j[up]
+    t_up = np.stack([local[ui, uj], local[ui + 1, uj], local[ui, uj + 1]], 1)
+    dn = (a_i + a_j) <= n - 2
+    di, dj = a_i[dn], a_j[dn]
+    t_dn = np.stack([local[di + 1, dj], local[di + 1, dj + 1], local[di, dj + 1]], 1)
+    tri_local = np.concatenate([t_up, t_dn])
+    P, T = [], []
+    for f, (a, b, c) in enumerate(F):
+        A, B, Cc = V0[a], V0[b], V0[c]
+        pts = A[None] + (B - A)[None] * (ii[:, None] / n) + (Cc - A)[None] * (jj[:, None] / n)
+        P.append(pts)
+        T.append(tri_local + f * len(ii))
+    P = np.concatenate(P)
+    T = np.concatenate(T)
+    P /= np.linalg.norm(P, axis=1, keepdims=True)
+    key = np.round(P * 1e7).astype(np.int64)
+    _, first, inv = np.unique(key, axis=0, return_index=True, return_inverse=True)
+    return P[first], inv.reshape(-1)[T]
+
+
+def _value_noise(p, seed):
+    """Smoothstep-interpolated lattice value noise in [-1, 1] (hashed integer lattice)."""
+    pi = np.floor(p).astype(np.int64)
+    f = p - pi
+    w = f * f * (3.0 - 2.0 * f)
+
+    def h(ix, iy, iz):
+        x = (ix * 73856093) ^ (iy * 19349663) ^ (iz * 83492791) ^ (seed * 2654435761)
+        x = (x ^ (x >> 13)) * 1274126177
+        x = x ^ (x >> 16)
+        return (x & 0xFFFF).astype(np.float64) / 32767.5 - 1.0
+
+    out = 0.0
+    for dx in (0, 1):
+        for dy in (0, 1):
+            for dz in (0, 1):
+                wx = w[:, 0] if dx else 1 - w[:, 0]
+                wy = w[:, 1] if dy else 1 - w[:, 1]
+                wz = w[:, 2] if dz else 1 - w[:, 2]
+                out = out + wx * wy * wz * h(pi[:, 0] + dx, pi[:, 1] + dy, pi[:, 2] + dz)
+    return out
+
+
+def fbm(p, seed, octaves=5, base=2.0):
+    acc, amp, freq, norm = 0.0, 1.0, base, 0.0
+    for o in range(octaves):
+        acc = acc + amp * _value_noise(p * freq, seed + o)
+        norm += amp
+        amp *= 0.5
+        freq *= 2.0
+    return acc / norm
+
+
+def vertex_normals(V, I):
+    V = V.astype(np.float64)
+    fn = np.cross(V[I[:, 1]] - V[I[:, 0]], V[I[:, 2]] - V[I[:, 0]])
+    N = np.zeros_like(V)
+    for k in range(3):
+        np.add.at(N, I[:, k], fn)
+    N /= np.maximum(np.linalg.norm(N, axis=1, keepdims=True), 1e-30)
+    return N.astype(np.float32)
+
+
+def random_disney(rng):
+    """Per-object Disney parameters from the seed: metallic, specTrans ~ U[0,1],
+    roughness ~ U[0.05, 1]."""
+    return disney(tuple(rng.uniform(0.2, 0.9, 3)), metallic=rng.uniform(0, 1),
+                  roughness=rng.uniform(0.05, 1.0), specular=0.5, trans=rng.uniform(0, 1),
+                  eta=1.5, sheen_tint=0.5)
+
+
+def displaced_sphere(width=1920, height=1080, spp=64, max_depth=16, subdiv=316, seed=0,
+                     amplitude=0.05):
+    """Config 2: 20*subdiv^2 sphere triangles (1,997,120 at subdiv 316) + 2 ground + 8 light."""
+    rng = np.random.default_rng(seed)
+    P, T = subdivided_icosphere(subdiv)
+    r = 1.0 + amplitude * fbm(P * 1.5, seed)
+    Vs = (P * r[:, None]).astype(np.float32)
+    Is = T.astype(np.uint32)
+    Ns = vertex_normals(Vs, Is)
+    mats = np.array([random_disney(rng), random_disney(rng), matte((0.8, 0.8, 0.8))])
+    y = -1.0 - 1.5 * amplitude
+    Vg, Ig = _quad((-12, y, -12), (-12, y, 12), (12, y, 12), (12, y, -12))
+    Vl, Il = [], []
+    lights = np.zeros(4, LIGHT)
+    centers = [(-2.5, 3.0, -2.0), (2.5, 3.0, -2.0), (-2.5, 3.0, 2.5), (2.5, 3.0, 2.5)]
+    for k, (cx, cy, cz) in enumerate(centers):
+        h = 0.5
+        v, i = _quad((cx - h, cy, cz - h), (cx + h, cy, cz - h), (cx + h, cy, cz + h),
+                     (cx - h, cy, cz + h))
+        Vl.append(v)
+        Il.append(i + 4 * k)
+        lights[k]["L"] = tuple(rng.uniform(4.0, 8.0, 3))
+        lights[k]["two_sided"] = 0
+    nS = len(Vs)
+    V = np.concatenate([Vs, Vg, *Vl]).astype(np.float32)
+    I = np.concatenate([Is, Ig + nS, *(i + nS + 4 for i in Il)]).astype(np.uint32)
+    N = np.concatenate([Ns, np.tile([[0, 1, 0]], (4, 1)), np.tile([[0, -1, 0]], (16, 1))]).astype(np.float32)
+    M = np.concatenate([np.zeros(len(Is), np.uint32), np.ones(2, np.uint32),
+                        np.full(8, 2, np.uint32)])
+    flags = np.concatenate([np.ones(len(Is), np.uint32), np.zeros(10, np.uint32)])
+    first = len(Is) + 2
+    for k in range(4):
+        lights[k]["first_tri"] = first + 2 * k
+        lights[k]["tri_count"] = 2
+    cam = pinhole((0.0, 0.6, 4.2), (0.0, -0.2, 0.0), (0, 1, 0), 40.0, width, height)
+    return Scene("displaced_sphere", V, I, M, mats, lights, N=N, tri_flags=flags, camera=cam,
+                 width=width, height=height, spp=spp, max_depth=max_depth, env=(0.1, 0.1, 0.1))
+
+
+def random_triangles(n, seed=0, spread=1.0, size=0.1):
+    """Random triangle soup in [-spread, spread]^3 for traversal parity tests."""
+    rng = np.random.default_rng(seed)
+    c = rng.uniform(-spread, spread, (n, 1, 3))
+    V = (c + rng.normal(0, size, (n, 3, 3))).reshape(-1, 3).astype(np.float32)
+    I = np.arange(3 * n, dtype=np.uint32).reshape(-1, 3)
+    return V, I
