@@ -285,6 +285,26 @@ WL_API void wl_render_params_default(wl_render_params *params, uint32_t width, u
 WL_API int wl_debug_rng(wl_context *ctx, uint32_t rng, uint64_t seed, const uint32_t *d_pixels,
                  uint32_t npix, uint32_t frame, uint32_t count, float *d_out);
 
+/* ---- rendering without device allocation ------------------------------------------- */
+/* No counterpart in the reference. Same result as wl_render, but the call allocates no device
+ * memory: its path queues live in one static device array of WL_NOALLOC_SCRATCH_BYTES
+ * (about 12 MiB), which every GPU that loads this library holds until the process exits.
+ * It serves callers that must not call cudaMalloc once they are running. Examples are a host
+ * that reserves its whole device-memory budget up front, and a real-time frame loop where an
+ * allocation's implicit device synchronisation would stall the frame.
+ *  - At most WL_NOALLOC_MAX_PATHS paths are in flight per wave; larger renders run in more
+ *    waves. params->wave_paths above that limit is rejected with WL_ERR_INVALID_ARG.
+ *  - The first call on a device looks up the array's device address (cudaGetSymbolAddress);
+ *    make that first call before any stream capture.
+ *  - All calls on a device share the one array and its contents persist between calls. Calls
+ *    whose work overlaps on the GPU (other streams, other threads) race on it and must not
+ *    overlap.
+ *  - No render statistics are recorded (wl_render_get_stats keeps the last wl_render's). */
+#define WL_NOALLOC_MAX_PATHS 65536u
+#define WL_NOALLOC_SCRATCH_BYTES (192u * WL_NOALLOC_MAX_PATHS + 512u)
+WL_API int wl_render_noalloc(wl_context *ctx, wl_scene *scene, const wl_camera *camera,
+                             const wl_render_params *params, wl_film *film);
+
 #ifdef __cplusplus
 }
 #endif

@@ -118,7 +118,9 @@ SIGNATURES = {
     "wl_render_get_stats": (C.c_int, [_P, C.POINTER(RenderStats)]),
     "wl_render_params_default": (None, [C.POINTER(RenderParams), _U32, _U32, _U32]),
     "wl_debug_rng": (C.c_int, [_P, _U32, C.c_uint64, _P, _U32, _U32, _U32, _P]),
+    "wl_render_noalloc": (C.c_int, [_P, _P, C.POINTER(Camera), C.POINTER(RenderParams), _P]),
 }
+NOALLOC_MAX_PATHS = 65536
 
 
 class WlError(RuntimeError):

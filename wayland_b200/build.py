@@ -25,6 +25,7 @@ UNITS = {
     "traverse.cu": [],
     "pt_fast.cu": ["--use_fast_math"],
     "pt_strict.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
+    "noalloc.cu": [],
 }
 
 

@@ -712,3 +712,31 @@ int wl_debug_rng(wl_context *c, uint32_t rng, uint64_t seed, const uint32_t *d_p
 }
 
 }  // extern "C"
+
+namespace wl {
+// Resolves the handles of a render call for wl_render_noalloc (noalloc.cu): the same argument
+// checks as wl_render, then the device scene, the film and the stream. Allocates nothing.
+int noalloc_render_inputs(wl_context *c, wl_scene *s, const wl_camera *cam,
+                          const wl_render_params *p, wl_film *f, DevScene *sc, Film **film,
+                          cudaStream_t *stream, int *device) {
+    ARG(c && s && cam && p && f && sc && film && stream && device, "null argument");
+    ARG(s->ctx == c && f->ctx == c, "scene and film must belong to the context");
+    if (!s->built) return fail(WL_ERR_NOT_BUILT, "bvh not built");
+    ARG(p->width == f->f.W && p->height == f->f.H, "film size differs from the render size");
+    ARG(p->spp > 0, "spp must be > 0");
+    ARG(p->max_depth > 0 && p->max_depth <= 1024, "max_depth out of range");
+    ARG(p->strategy <= WL_STRATEGY_MIS, "bad strategy");
+    ARG(p->rng <= WL_RNG_PCG32, "bad rng");
+    ARG(p->math <= WL_MATH_STRICT, "bad math mode");
+    ARG(p->lights == WL_LIGHTS_UNIFORM, "only uniform light selection is available");
+    ARG(p->rr_prob > 0.0f && p->rr_prob <= 1.0f, "rr_prob must be in (0, 1]");
+    ARG(finite3(cam->pos) && finite3(cam->look_at) && finite3(cam->up) && finite3(cam->right),
+        "non-finite camera");
+    *sc = dev_scene(s);
+    *film = &f->f;
+    *stream = c->stream;
+    *device = c->device;
+    return WL_OK;
+}
+void noalloc_fail(const std::string &msg) { g_err = msg; }
+}  // namespace wl

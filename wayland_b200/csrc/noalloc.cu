@@ -1,0 +1,156 @@
+// noalloc.cu - wl_render_noalloc: the wavefront render of wl_render with its path queues in a
+// file-scope static device array instead of cudaMalloc'd memory, for callers that must not
+// allocate device memory after start-up (a host that owns the whole device-memory budget, or
+// a real-time loop that cannot absorb an allocation's implicit synchronisation). The kernels
+// are the same as wl_render's (pt_fast.cu / pt_strict.cu / traverse.cu); only where the
+// queues live differs, so the images are identical.
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "wl_internal.h"
+
+namespace wl {
+int noalloc_render_inputs(wl_context *c, wl_scene *s, const wl_camera *cam,
+                          const wl_render_params *p, wl_film *f, DevScene *sc, Film **film,
+                          cudaStream_t *stream, int *device);
+void noalloc_fail(const std::string &msg);
+}  // namespace wl
+
+using namespace wl;
+
+namespace {
+
+constexpr uint32_t MAX_PATHS = WL_NOALLOC_MAX_PATHS;
+constexpr size_t PER_PATH = 192;  // bytes of queues and path state per path slot
+static_assert(PER_PATH * MAX_PATHS + 512 == WL_NOALLOC_SCRATCH_BYTES, "scratch layout size");
+
+// The scratch: every GPU that loads this library holds it until the process exits.
+static __device__ __align__(256) unsigned char g_wave_scratch[WL_NOALLOC_SCRATCH_BYTES];
+
+constexpr int MAX_DEVICES = 64;
+std::mutex g_mu;
+void *g_addr[MAX_DEVICES] = {};
+
+// Host code cannot use g_wave_scratch's name as a device address: look the address up once per
+// device, with that device current.
+int scratch_address(int device, void **out) {
+    if (device < 0 || device >= MAX_DEVICES) {
+        noalloc_fail("wl_render_noalloc: device index out of range");
+        return WL_ERR_INVALID_ARG;
+    }
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_addr[device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_wave_scratch);
+        if (e != cudaSuccess || !p) {
+            noalloc_fail(std::string("wl_render_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            return WL_ERR_CUDA;
+        }
+        g_addr[device] = p;
+    }
+    *out = g_addr[device];
+    return WL_OK;
+}
+
+// Same arrays as the allocated queues, carved out of the static scratch for MAX_PATHS slots.
+Queues carve(void *base) {
+    const size_t f4 = sizeof(float4) * (size_t)MAX_PATHS, u32 = sizeof(uint32_t) * (size_t)MAX_PATHS,
+                 u2 = sizeof(uint2) * (size_t)MAX_PATHS;
+    char *p = (char *)base;
+    Queues q{};
+    q.capacity = MAX_PATHS;
+    q.ray_o[0] = (float4 *)p; p += f4;
+    q.ray_d[0] = (float4 *)p; p += f4;
+    q.ray_o[1] = (float4 *)p; p += f4;
+    q.ray_d[1] = (float4 *)p; p += f4;
+    q.ray_slot[0] = (uint32_t *)p; p += u32;
+    q.ray_slot[1] = (uint32_t *)p; p += u32;
+    q.hit = (float4 *)p; p += f4;
+    q.st_thr = (float4 *)p; p += f4;
+    q.st_term = (float4 *)p; p += f4;
+    q.st_rad = (float4 *)p; p += f4;
+    q.st_rng = (uint2 *)p; p += u2;
+    q.sh_o = (float4 *)p; p += f4;
+    q.sh_d = (float4 *)p; p += f4;
+    q.sh_l = (float4 *)p; p += f4;
+    q.counters = (uint32_t *)p; p += 256;
+    q.totals = (unsigned long long *)p; p += 256;
+    return q;
+}
+
+}  // namespace
+
+extern "C" int wl_render_noalloc(wl_context *ctx, wl_scene *scene, const wl_camera *cam,
+                                 const wl_render_params *p, wl_film *film) {
+    DevScene sc;
+    Film *f = nullptr;
+    cudaStream_t st = nullptr;
+    int device = 0;
+    int rc = noalloc_render_inputs(ctx, scene, cam, p, film, &sc, &f, &st, &device);
+    if (rc != WL_OK) return rc;
+    if (p->wave_paths > MAX_PATHS) {
+        noalloc_fail("wl_render_noalloc: wave_paths " + std::to_string(p->wave_paths) +
+                     " exceeds the static scratch limit of " + std::to_string(MAX_PATHS) + " paths");
+        return WL_ERR_INVALID_ARG;
+    }
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        noalloc_fail(std::string("wl_render_noalloc: ") + cudaGetErrorString(e));
+        return WL_ERR_CUDA;
+    }
+    void *base = nullptr;
+    rc = scratch_address(device, &base);
+    if (rc != WL_OK) return rc;
+    Queues q = carve(base);
+    // the array keeps the previous call's contents: zero the counters and sums
+    e = cudaMemsetAsync(q.counters, 0, 512, st);
+    if (e != cudaSuccess) {
+        noalloc_fail(std::string("wl_render_noalloc: ") + cudaGetErrorString(e));
+        return WL_ERR_CUDA;
+    }
+    const uint32_t npix = p->width * p->height;
+    const uint64_t total = (uint64_t)npix * p->spp;
+    uint64_t want = p->wave_paths ? p->wave_paths : MAX_PATHS;
+    uint32_t spp_per_wave = (uint32_t)(want / npix);
+    uint64_t wave = spp_per_wave >= 1 ? (uint64_t)spp_per_wave * npix : want;
+    if (wave > total) wave = total;
+
+    WaveParams wp{};
+    wp.W = p->width; wp.H = p->height; wp.npix = npix;
+    wp.first_frame = p->first_frame;
+    wp.max_depth = p->max_depth; wp.rr_depth = p->rr_depth;
+    wp.rr_prob = p->rr_prob; wp.eps = p->eps;
+    wp.strategy = p->strategy; wp.rng = p->rng; wp.lights = p->lights; wp.seed = p->seed;
+    for (int k = 0; k < 3; k++) {
+        wp.env[k] = p->env[k];
+        wp.cam_pos[k] = cam->pos[k]; wp.cam_look[k] = cam->look_at[k];
+        wp.cam_up[k] = cam->up[k]; wp.cam_right[k] = cam->right[k];
+    }
+    wp.has_env = (p->env[0] != 0.f || p->env[1] != 0.f || p->env[2] != 0.f) ? 1u : 0u;
+    const bool strict_math = p->math == WL_MATH_STRICT;
+    for (uint64_t b0 = 0; b0 < total; b0 += wave) {
+        wp.base = b0;
+        wp.count = (uint32_t)((total - b0) < wave ? (total - b0) : wave);
+        if (strict_math) strict::launch_generate(wp, q, st);
+        else fast::launch_generate(wp, q, st);
+        int in = 0;
+        for (uint32_t b = 0; b < p->max_depth; b++) {
+            launch_extend(sc, q, in, false, st);
+            cudaMemsetAsync(q.counters + (in ^ 1), 0, sizeof(uint32_t), st);
+            cudaMemsetAsync(q.counters + 2, 0, sizeof(uint32_t), st);
+            if (strict_math) strict::launch_shade(wp, sc, q, in, st);
+            else fast::launch_shade(wp, sc, q, in, st);
+            launch_shadow(sc, q, false, st);
+            in ^= 1;
+        }
+        strict::launch_film(wp, q, *f, st);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) {
+            noalloc_fail(std::string("wl_render_noalloc: ") + cudaGetErrorString(e));
+            return WL_ERR_CUDA;
+        }
+    }
+    f->frames64 += p->spp;
+    return WL_OK;
+}
