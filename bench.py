@@ -269,10 +269,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-raycast", action="store_true")
     ap.add_argument("--math", default="fast", choices=["fast", "strict"])
+    ap.add_argument("--case", default="full", choices=["full", "small"],
+                    help="small: the same 2M-triangle scene at 960x540 x 4 spp (for ncu captures)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return reference_arm(args)
+    global W, H, SPP
+    if args.case == "small":
+        W, H, SPP = 960, 540, 4
 
     import torch
     import torch.distributed as dist
@@ -288,6 +293,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
     scene = scenes.displaced_sphere(W, H, SPP, DEPTH)
+    if args.case == "small":
+        scene.camera = scenes.pinhole((0.0, 0.6, 4.2), (0.0, -0.2, 0.0), (0, 1, 0), 40.0, W, H)
     ctx = wl.Context(local)
     sc = wl.Scene(ctx, scene)
     info = sc.info()
@@ -372,7 +379,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 2),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "width": W, "height": H, "spp": SPP, "max_depth": DEPTH,
+            "config": {"workload": WORKLOAD if args.case == "full" else "profiling case: " + WORKLOAD.replace("1920x1080, 64 spp", f"{W}x{H}, {SPP} spp"), "width": W, "height": H, "spp": SPP, "max_depth": DEPTH,
                        "triangles": scene.num_tris, "math": args.math, "rng": "tea_lcg",
                        "strategy": "mis", "parallelism": f"{world} independent sample sets (weak)",
                        "l2": "working set larger than L2 (BVH %.0f MB + path queues), no flush" % (info["bytes"] / 1e6)},

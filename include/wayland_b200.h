@@ -280,6 +280,31 @@ WL_API int wl_render_get_stats(wl_context *ctx, wl_render_stats *stats);
 WL_API void wl_render_params_default(wl_render_params *params, uint32_t width, uint32_t height,
                               uint32_t spp);
 
+/* Ambient occlusion (src/Frontend/Programs/AO/AO.cu:21-130): per pixel and frame,
+ * camera_samples jittered camera rays; at each hit, ao_rays cosine-distributed occlusion rays
+ * of length radius from the hit point around the normal turned towards the viewer; each
+ * unoccluded ray adds cos/pi/ao_rays/pdf. The frame value (mean over camera samples, in double)
+ * goes into the film's running mean like wl_render's. A camera ray that misses adds 0. Camera
+ * sample k of a pixel continues the pixel's random stream after k * (2 + 2 * ao_rays) numbers,
+ * as the reference's sequential loop does. Reference values: 4 camera samples, 32 rays,
+ * radius 1. Arithmetic is IEEE single precision (bit-identical to the oracle). */
+typedef struct wl_ao_params {
+    uint32_t width, height;
+    uint32_t spp;             /* frames rendered by this call */
+    uint32_t first_frame;
+    uint32_t camera_samples;  /* reference: 4 */
+    uint32_t ao_rays;         /* reference: 32 */
+    float radius;             /* reference: 1.0 */
+    float eps;                /* reference: 1e-3 */
+    uint32_t rng;             /* WL_RNG_* */
+    uint32_t wave_paths;      /* camera samples in flight per wave; 0 = automatic */
+    uint64_t seed;
+} wl_ao_params;
+WL_API void wl_ao_params_default(wl_ao_params *params, uint32_t width, uint32_t height,
+                                 uint32_t spp);
+WL_API int wl_render_ao(wl_context *ctx, wl_scene *scene, const wl_camera *camera,
+                        const wl_ao_params *params, wl_film *film);
+
 /* Random streams for parity tests: the first `count` uniforms of the stream of each listed
  * pixel at `frame` (count floats per pixel, pixel-major). Device pointers. */
 WL_API int wl_debug_rng(wl_context *ctx, uint32_t rng, uint64_t seed, const uint32_t *d_pixels,

@@ -69,6 +69,13 @@ class RenderParams(C.Structure):
                 ("flags", C.c_uint32)]
 
 
+class AoParams(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32),
+                ("first_frame", C.c_uint32), ("camera_samples", C.c_uint32),
+                ("ao_rays", C.c_uint32), ("radius", C.c_float), ("eps", C.c_float),
+                ("rng", C.c_uint32), ("wave_paths", C.c_uint32), ("seed", C.c_uint64)]
+
+
 class OrScene(C.Structure):
     _fields_ = [("V", C.c_void_p), ("nV", C.c_uint32), ("N", C.c_void_p), ("I", C.c_void_p),
                 ("nT", C.c_uint32), ("tri_material", C.c_void_p), ("tri_flags", C.c_void_p),
@@ -258,6 +265,19 @@ class Oracle:
         del keep
         return film, f64, segs
 
+    def render_ao(self, scene, cam, params, threads=0, want64=False):
+        """Ambient occlusion (AO.cu:21-130); returns (film[H,W,3] f32, film64 or None, rays)."""
+        W, H = params.width, params.height
+        film = np.zeros((H, W, 3), np.float32)
+        f64 = np.zeros((H, W, 3), np.float64) if want64 else None
+        b = self.bvh_for(scene)
+        keep, osc = make_or_scene(scene)
+        self.lib.or_render_ao.restype = C.c_uint64
+        rays = self.lib.or_render_ao(C.byref(osc), b.handle, C.byref(cam), C.byref(params), threads,
+                                     ptr(film), ptr(f64))
+        del keep
+        return film, f64, rays
+
     def bvh_for(self, scene):
         key = id(scene)
         c = self.__dict__.setdefault("_bvh_cache", {})
@@ -354,6 +374,19 @@ class RefLib:
         out = np.empty_like(rgb)
         self.lib.ref_ace(C.c_uint32(len(rgb)), ptr(rgb), ptr(out))
         return out
+
+    def render_ao(self, scene, cam, params, threads=0):
+        W, H = params.width, params.height
+        film = np.zeros((H, W, 3), np.float32)
+        keep, osc = make_or_scene(scene)
+        h = self.lib.or_bvh_create(osc.V, osc.I, osc.nT)
+        self.lib.ref_render_ao.restype = C.c_uint64
+        try:
+            rays = self.lib.ref_render_ao(C.byref(osc), C.c_void_p(h), C.byref(cam), C.byref(params),
+                                          threads, ptr(film))
+        finally:
+            self.lib.or_bvh_destroy(h)
+        return film, rays
 
     def render(self, scene, cam, params, threads=0, film=None, pixel_range=None):
         W, H = params.width, params.height

@@ -272,4 +272,69 @@ uint64_t ref_render(const or_scene *scene, void *bvh, const wl_camera *camc,
     return segs;
 }
 
+// AO.cu:21-130 written over the reference's own SampleCosineHemisphere / PinholeGenerateRay /
+// GetGeometry normal arithmetic; a camera ray that misses adds 0 (the reference would trace
+// from the previous sample's hit point) and skips its 2 * ao_rays random numbers.
+uint64_t ref_render_ao(const or_scene *scene, void *bvh, const wl_camera *camc,
+                       const wl_ao_params *p, int threads, float *film_rgb) {
+    PinholeCamFrame cam;
+    cam.pos = g3(camc->pos); cam.lookAt = g3(camc->look_at); cam.up = g3(camc->up); cam.right = g3(camc->right);
+    const or_scene *s = scene;
+    uint32_t npix = p->width * p->height;
+    uint64_t rays = 0;
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#endif
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : rays)
+    for (int64_t pix = 0; pix < (int64_t)npix; pix++) {
+        uint32_t ix = (uint32_t)(pix % p->width), iy = (uint32_t)(pix / p->width);
+        float acc = film_rgb[3 * pix];
+        for (uint32_t fs = 0; fs < p->spp; fs++) {
+            uint32_t frameID = p->first_frame + fs;
+            uint32_t seed = tea<4>((uint32_t)pix, frameID);
+            double thisFrame = 0.0;
+            for (uint32_t i = 0; i < p->camera_samples; ++i) {
+                glm::vec3 radiance(0.f, 0.f, 0.f);
+                glm::vec3 rayDir = PinholeGenerateRay(glm::ivec2((int)ix, (int)iy),
+                                                      glm::ivec2((int)p->width, (int)p->height), cam, seed);
+                wl_ray ray = {{cam.pos.x, cam.pos.y, cam.pos.z}, p->eps, {rayDir.x, rayDir.y, rayDir.z}, 1e30f};
+                wl_hit hit;
+                or_cast_bvh(bvh, &ray, 1, WL_CAST_CLOSEST, &hit);
+                rays++;
+                if (hit.prim != INVALID_INDEX) {
+                    glm::ivec3 ind((int)s->I[3 * hit.prim], (int)s->I[3 * hit.prim + 1], (int)s->I[3 * hit.prim + 2]);
+                    glm::vec3 N;
+                    if (ref_tri_has_normal(s, hit.prim)) {
+                        float2 bc = {hit.u, hit.v};
+                        N = BarycentricByIndices((glm::vec3 *)s->N, ind, bc);
+                    } else {
+                        glm::vec3 *Vv = (glm::vec3 *)s->V;
+                        N = glm::cross(Vv[ind.y] - Vv[ind.x], Vv[ind.z] - Vv[ind.x]);
+                    }
+                    N = glm::normalize(N);
+                    if (glm::dot(N, rayDir) > 0) N = -N;
+                    glm::vec3 hitPos = cam.pos + rayDir * hit.t;
+                    for (uint32_t j = 0; j < p->ao_rays; ++j) {
+                        float pdf;
+                        glm::vec3 d = SampleCosineHemisphere(N, pdf, seed);
+                        wl_ray sr = {{hitPos.x, hitPos.y, hitPos.z}, p->eps, {d.x, d.y, d.z}, p->radius};
+                        wl_hit sh;
+                        or_cast_bvh(bvh, &sr, 1, WL_CAST_ANY, &sh);
+                        rays++;
+                        if (sh.prim == INVALID_INDEX)
+                            radiance += glm::dot(d, N) / PI / (float)p->ao_rays / pdf;
+                    }
+                } else {
+                    for (uint32_t j = 0; j < 2 * p->ao_rays; ++j) rnd(seed);
+                }
+                thisFrame += radiance.x / (float)p->camera_samples;
+            }
+            if (frameID == 0) acc = (float)thisFrame;
+            else acc = (float)((double)acc * double(frameID / (frameID + 1.0f)) + thisFrame * double(1.0f / (frameID + 1.0f)));
+        }
+        for (int c = 0; c < 3; c++) film_rgb[3 * pix + c] = acc;
+    }
+    return rays;
+}
+
 }  // extern "C"

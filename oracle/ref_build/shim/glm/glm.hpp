@@ -28,6 +28,8 @@ template <class T> struct tvec3 {
     tvec3 &operator-=(const tvec3 &o) { x -= o.x; y -= o.y; z -= o.z; return *this; }
     tvec3 &operator*=(const tvec3 &o) { x *= o.x; y *= o.y; z *= o.z; return *this; }
     tvec3 &operator*=(T s) { x *= s; y *= s; z *= s; return *this; }
+    tvec3 &operator+=(T s) { x += s; y += s; z += s; return *this; }
+    tvec3 &operator-=(T s) { x -= s; y -= s; z -= s; return *this; }
     tvec3 &operator/=(T s) { x /= s; y /= s; z /= s; return *this; }
 };
 template <class T> struct tvec4 {

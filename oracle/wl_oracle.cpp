@@ -1093,6 +1093,65 @@ PathOut<T> trace_path(const SceneView &sv, const wl_camera &cam, const wl_render
     return out;
 }
 
+// Ambient occlusion, AO.cu:21-130: camera_samples camera rays per pixel; at a hit, ao_rays
+// cosine-hemisphere rays (SampleCosineHemisphere with pdf, Sample.h:55-66) of length radius;
+// each unoccluded ray adds dot(dir, N) / PI / ao_rays / pdf. A camera ray that misses adds 0
+// (the reference would trace from the previous sample's hit point).
+double ao_frame(const SceneView &sv, const wl_camera &cam, const wl_ao_params &P, uint32_t px,
+               uint32_t py, uint32_t frame, uint64_t &rays) {
+    const or_scene *s = sv.s;
+    uint32_t pixel = P.width * py + px;
+    Rng rng = make_rng(P.rng, P.seed, pixel, frame);
+    double acc = 0.0;
+    V3<float> lookat(cam.look_at[0], cam.look_at[1], cam.look_at[2]);
+    V3<float> right(cam.right[0], cam.right[1], cam.right[2]), up(cam.up[0], cam.up[1], cam.up[2]);
+    for (uint32_t k = 0; k < P.camera_samples; k++) {
+        float rad = 0.0f;
+        float cu = 2.f * ((float)px + rng.next()) / (float)P.width - 1.f;
+        float cv = 2.f * ((float)py + rng.next()) / (float)P.height - 1.f;
+        V3<float> dir = normalize(lookat + right * cu + up * cv);
+        wl_ray ray = {{cam.pos[0], cam.pos[1], cam.pos[2]}, P.eps, {dir.x, dir.y, dir.z}, 1e30f};
+        wl_hit hit;
+        obvh_cast_one(*sv.bvh, ray, WL_CAST_CLOSEST, hit);
+        rays++;
+        if (hit.prim != INVALID) {
+            uint32_t prim = hit.prim;
+            V3<float> N;
+            if (tri_has_normal(s, prim)) {
+                float bu = hit.u, bv = hit.v;
+                N = vload<float>(s->N, s->I[3 * prim]) * (1.0f - bu - bv) +
+                    vload<float>(s->N, s->I[3 * prim + 1]) * bu + vload<float>(s->N, s->I[3 * prim + 2]) * bv;
+            } else {
+                V3<float> a = vload<float>(s->V, s->I[3 * prim]), b = vload<float>(s->V, s->I[3 * prim + 1]),
+                          c = vload<float>(s->V, s->I[3 * prim + 2]);
+                N = cross(b - a, c - a);
+            }
+            N = normalize(N);
+            if (dot(N, dir) > 0.0f) N = -N;
+            V3<float> pos = V3<float>(cam.pos[0], cam.pos[1], cam.pos[2]) + dir * hit.t;
+            for (uint32_t j = 0; j < P.ao_rays; j++) {
+                V3<float> x, y;
+                onb(N, x, y);
+                float r = std::sqrt(rng.next());
+                float theta = rng.next() * C<float>::two_pi();
+                float dx = r * m_cos(theta), dy = r * m_sin(theta);
+                float z = std::sqrt(1.0f - dx * dx - dy * dy);
+                float pdf = z / C<float>::pi();
+                V3<float> od = x * dx + y * dy + N * z;
+                wl_ray sr = {{pos.x, pos.y, pos.z}, P.eps, {od.x, od.y, od.z}, P.radius};
+                wl_hit sh;
+                obvh_cast_one(*sv.bvh, sr, WL_CAST_ANY, sh);
+                rays++;
+                if (sh.prim == INVALID) rad += dot(od, N) / C<float>::pi() / (float)P.ao_rays / pdf;
+            }
+        } else {
+            for (uint32_t j = 0; j < 2 * P.ao_rays; j++) rng.next();
+        }
+        acc += (double)(rad / (float)P.camera_samples);
+    }
+    return acc;  // AO.cu keeps the frame value in double (glm::dvec4 thisFrame)
+}
+
 }  // namespace
 
 // ========================================================================================
@@ -1245,6 +1304,35 @@ uint64_t or_render(const or_scene *scene, void *bvh, const wl_camera *cam,
         if (film64) for (int c = 0; c < 3; c++) film64[3 * pix + c] = sum[c] / (double)p->spp;
     }
     return segs;
+}
+
+uint64_t or_render_ao(const or_scene *scene, void *bvh, const wl_camera *cam,
+                      const wl_ao_params *p, int threads, float *film_rgb, double *film64) {
+    SceneView sv;
+    sv.s = scene;
+    sv.bvh = (const OBvh *)bvh;
+    uint32_t npix = p->width * p->height;
+    uint64_t rays = 0;
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#endif
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : rays)
+    for (int64_t pix = 0; pix < (int64_t)npix; pix++) {
+        uint32_t px = (uint32_t)(pix % p->width), py = (uint32_t)(pix / p->width);
+        float acc = film_rgb[3 * pix];
+        double sum = 0.0;
+        for (uint32_t s = 0; s < p->spp; s++) {
+            uint32_t f = p->first_frame + s;
+            double v = ao_frame(sv, *cam, *p, px, py, f, rays);
+            if (f == 0) acc = (float)v;
+            else acc = (float)((double)acc * (double)((float)f / ((float)f + 1.0f)) +
+                               v * (double)(1.0f / ((float)f + 1.0f)));
+            sum += v;
+        }
+        for (int c = 0; c < 3; c++) film_rgb[3 * pix + c] = acc;
+        if (film64) for (int c = 0; c < 3; c++) film64[3 * pix + c] = sum / (double)p->spp;
+    }
+    return rays;
 }
 
 double or_relmse(const float *img, const double *ref, uint64_t n, double eps) {

@@ -77,6 +77,11 @@ uint64_t or_render(const or_scene *scene, void *bvh, const wl_camera *cam,
                    const wl_render_params *p, int prec, int threads, float *film_rgb,
                    double *film64, uint32_t pixel_begin, uint32_t pixel_end);
 
+/* Ambient occlusion (AO.cu:21-130); film_rgb: running mean (grey in all 3 channels), film64: FP64
+ * mean (nullable). Returns rays traced. */
+uint64_t or_render_ao(const or_scene *scene, void *bvh, const wl_camera *cam,
+                      const wl_ao_params *p, int threads, float *film_rgb, double *film64);
+
 /* relMSE = mean over pixels and channels of (I - R)^2 / (R^2 + eps) */
 double or_relmse(const float *img, const double *ref, uint64_t n, double eps);
 

@@ -98,6 +98,20 @@ def main():
     np.savez_compressed(os.path.join(HERE, "cornell_32x32_4spp.npz"), image=img,
                         segments=np.uint64(segs), V=sc.V, I=sc.I, tri_material=sc.tri_material,
                         mats=sc.mats, lights=sc.lights, cam=out["cam"])
+
+    # ambient occlusion (AO.cu) of the displaced sphere through the reference's arithmetic
+    sph = scenes.displaced_sphere(40, 24, subdiv=12, seed=5)
+    scam = po.Camera()
+    for k in ("pos", "look_at", "up", "right"):
+        getattr(scam, k)[:] = [float(x) for x in sph.camera[k]]
+    ap = po.AoParams(width=40, height=24, spp=2, first_frame=0, camera_samples=4, ao_rays=32,
+                     radius=1.0, eps=1e-3, rng=0, wave_paths=0, seed=0)
+    ao_img, ao_rays = ref.render_ao(sph, scam, ap)
+    np.savez_compressed(os.path.join(HERE, "ao_sphere_40x24.npz"), image=ao_img,
+                        rays=np.uint64(ao_rays), V=sph.V, N=sph.N, I=sph.I,
+                        tri_flags=sph.tri_flags,
+                        cam=np.array([list(scam.pos), list(scam.look_at), list(scam.up),
+                                      list(scam.right)], np.float32))
     print("golden vectors written to", HERE)
 
 

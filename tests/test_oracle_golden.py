@@ -97,3 +97,25 @@ def test_own_transcendentals(oracle):
     lg = np.array([oracle.logf(y) for y in ys])
     assert (np.abs(lg - np.log(ys.astype(np.float64))) / np.maximum(1.0, np.abs(np.log(ys)))).max() < 3e-7
     assert np.isnan(oracle.logf(-1.0)) and np.isneginf(oracle.logf(0.0))
+
+
+class _GoldScene:
+    def __init__(self, g):
+        self.V, self.I, self.N = g["V"], g["I"], g.get("N")
+        self.tri_flags = g.get("tri_flags")
+        self.tri_material = np.zeros(len(self.I), np.uint32)
+        self.mats = np.zeros(1, po.DISNEY_DTYPE)
+        self.lights = np.zeros(0, po.LIGHT_DTYPE)
+
+
+def test_ao_image(oracle):
+    """The oracle's ambient occlusion reproduces AO.cu's loop over the reference's arithmetic."""
+    g = dict(np.load(os.path.join(GOLD, "ao_sphere_40x24.npz")))
+    cam = po.Camera()
+    for i, k in enumerate(("pos", "look_at", "up", "right")):
+        getattr(cam, k)[:] = [float(x) for x in g["cam"][i]]
+    p = po.AoParams(width=40, height=24, spp=2, first_frame=0, camera_samples=4, ao_rays=32,
+                    radius=1.0, eps=1e-3, rng=0, wave_paths=0, seed=0)
+    img, _, rays = oracle.render_ao(_GoldScene(g), cam, p)
+    assert np.array_equal(bits(img), bits(g["image"]))
+    assert rays == int(g["rays"])

@@ -217,6 +217,21 @@ def render_params(width, height, spp, **kw):
     return p
 
 
+def ao_params(width, height, spp, **kw):
+    """wl_ao_params with the reference's constants (4 camera samples, 32 rays, radius 1)."""
+    p = _abi.AoParams()
+    _abi.load().wl_ao_params_default(C.byref(p), width, height, spp)
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def render_ao(ctx, scene, camera, params, film):
+    """Ambient occlusion (AO.cu) into the film's running mean."""
+    _abi.check("wl_render_ao", ctx.lib.wl_render_ao(ctx.handle, scene.handle, C.byref(camera),
+                                                    C.byref(params), film.handle))
+
+
 def render(ctx, scene, camera, params, film):
     _abi.check("wl_render", ctx.lib.wl_render(ctx.handle, scene.handle, C.byref(camera),
                                               C.byref(params), film.handle))

@@ -53,6 +53,13 @@ class RenderParams(C.Structure):
                 ("flags", C.c_uint32)]
 
 
+class AoParams(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32),
+                ("first_frame", C.c_uint32), ("camera_samples", C.c_uint32),
+                ("ao_rays", C.c_uint32), ("radius", C.c_float), ("eps", C.c_float),
+                ("rng", C.c_uint32), ("wave_paths", C.c_uint32), ("seed", C.c_uint64)]
+
+
 class RenderStats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("segments", C.c_uint64), ("shadow_rays", C.c_uint64),
                 ("waves", C.c_uint32), ("kernel_launches", C.c_uint32), ("ms_total", C.c_float),
@@ -119,6 +126,8 @@ SIGNATURES = {
     "wl_render_params_default": (None, [C.POINTER(RenderParams), _U32, _U32, _U32]),
     "wl_debug_rng": (C.c_int, [_P, _U32, C.c_uint64, _P, _U32, _U32, _U32, _P]),
     "wl_render_noalloc": (C.c_int, [_P, _P, C.POINTER(Camera), C.POINTER(RenderParams), _P]),
+    "wl_ao_params_default": (None, [C.POINTER(AoParams), _U32, _U32, _U32]),
+    "wl_render_ao": (C.c_int, [_P, _P, C.POINTER(Camera), C.POINTER(AoParams), _P]),
 }
 NOALLOC_MAX_PATHS = 65536
 

@@ -26,6 +26,7 @@ UNITS = {
     "pt_fast.cu": ["--use_fast_math"],
     "pt_strict.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
     "noalloc.cu": [],
+    "ao.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
 }
 
 

@@ -701,6 +701,59 @@ int wl_render_get_stats(wl_context *c, wl_render_stats *out) {
     return WL_OK;
 }
 
+void wl_ao_params_default(wl_ao_params *p, uint32_t w, uint32_t h, uint32_t spp) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->width = w;
+    p->height = h;
+    p->spp = spp;
+    p->camera_samples = 4;   // AO.cu:35
+    p->ao_rays = 32;         // AO.cu:46
+    p->radius = 1.0f;        // AO.cu:47
+    p->eps = 1e-3f;          // AO.cu:16
+    p->rng = WL_RNG_TEA_LCG;
+}
+
+int wl_render_ao(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_ao_params *p, wl_film *f) {
+    ARG(c && s && cam && p && f, "null argument");
+    ARG(s->ctx == c && f->ctx == c, "scene and film must belong to the context");
+    if (!s->built) return fail(WL_ERR_NOT_BUILT, "bvh not built");
+    ARG(p->width == f->f.W && p->height == f->f.H, "film size differs from the render size");
+    ARG(p->spp > 0 && p->camera_samples > 0 && p->ao_rays > 0, "spp, camera_samples and ao_rays must be > 0");
+    ARG(p->camera_samples <= 4096 && p->ao_rays <= 65536, "camera_samples or ao_rays too large");
+    ARG(p->rng <= WL_RNG_PCG32, "bad rng");
+    ARG(std::isfinite(p->radius) && p->radius > 0.0f, "radius must be > 0");
+    ARG(finite3(cam->pos) && finite3(cam->look_at) && finite3(cam->up) && finite3(cam->right), "non-finite camera");
+    CK(cudaSetDevice(c->device));
+    c->stats_pending = false;
+    const uint32_t npix = p->width * p->height;
+    const uint64_t groups = (uint64_t)npix * p->spp;
+    uint64_t want = p->wave_paths ? p->wave_paths : (1ull << 22);
+    uint64_t wave_groups = want / p->camera_samples;
+    if (wave_groups < 1) wave_groups = 1;
+    if (wave_groups > npix) wave_groups = npix;  // at most one group per pixel in a wave
+    int rc = ensure_queues(c, (uint32_t)(wave_groups * p->camera_samples));
+    if (rc != WL_OK) return rc;
+    AoWave w{};
+    w.W = p->width; w.H = p->height; w.npix = npix; w.first_frame = p->first_frame;
+    w.cs = p->camera_samples; w.ao_rays = p->ao_rays; w.rng = p->rng;
+    w.radius = p->radius; w.eps = p->eps; w.seed = p->seed;
+    for (int k = 0; k < 3; k++) {
+        w.cam_pos[k] = cam->pos[k]; w.cam_look[k] = cam->look_at[k];
+        w.cam_up[k] = cam->up[k]; w.cam_right[k] = cam->right[k];
+    }
+    DevScene sc = dev_scene(s);
+    for (uint64_t g0 = 0; g0 < groups; g0 += wave_groups) {
+        uint64_t ng = groups - g0 < wave_groups ? groups - g0 : wave_groups;
+        w.base = g0 * p->camera_samples;
+        w.count = (uint32_t)(ng * p->camera_samples);
+        launch_ao(w, sc, c->q, f->f, c->stream);
+        CK(cudaGetLastError());
+    }
+    f->f.frames64 += p->spp;
+    return WL_OK;
+}
+
 int wl_debug_rng(wl_context *c, uint32_t rng, uint64_t seed, const uint32_t *d_pixels, uint32_t npix,
                  uint32_t frame, uint32_t count, float *d_out) {
     ARG(c && d_pixels && d_out, "null argument");

@@ -33,41 +33,58 @@ __device__ __forceinline__ void add_stats(unsigned long long *totals, uint32_t a
     }
 }
 
-template <bool STATS>
-__global__ void __launch_bounds__(TT) k_extend(DevScene sc, Queues q, int in, uint32_t *fetch) {
-    const uint32_t n = q.counters[in];
-    const float4 *ro = q.ray_o[in], *rd = q.ray_d[in];
-    while (true) {
-        uint32_t base = warp_fetch(fetch);
-        if (base >= n) break;
-        uint32_t i = base + (threadIdx.x & 31);
-        uint32_t cn = 0, ct = 0;
-        if (i < n) {
-            float4 o = ro[i], d = rd[i];
-            TraceResult r;
-            traverse<false, STATS>(sc.nodes, sc.tris, o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w, r,
-                                   &cn, &ct);
-            q.hit[i] = make_float4(r.t, __uint_as_float(r.prim), r.u, r.v);
-        }
-        if (STATS) add_stats(q.totals + 2, cn, ct);
-    }
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
 }
 
-template <bool STATS>
-__global__ void __launch_bounds__(TT) k_shadow(DevScene sc, Queues q, uint32_t *fetch) {
-    const uint32_t n = q.counters[2];
+// Refill threshold: a warp fetches new rays for its idle lanes once this many are idle (or
+// when none is busy), so that long rays no longer hold the whole warp (Aila & Laine 2009,
+// persistent threads with dynamic fetch).
+constexpr int REFILL = 12;
+
+// Persistent traversal over a queue of n rays. MODE 0: closest hit of ray queue `in`, hit
+// written to q.hit. MODE 1: any hit of the shadow queue; an unoccluded ray adds its light
+// sample to the path radiance.
+template <int MODE, bool STATS>
+__global__ void __launch_bounds__(TT) k_trace(DevScene sc, Queues q, int in, uint32_t *fetch) {
+    constexpr bool ANY = MODE == 1;
+    const uint32_t n = MODE == 0 ? q.counters[in] : q.counters[2];
+    const float4 *ro = MODE == 0 ? q.ray_o[in] : q.sh_o;
+    const float4 *rd = MODE == 0 ? q.ray_d[in] : q.sh_d;
+    const uint32_t lane = threadIdx.x & 31;
+    TravState st;
+    uint2 stack[TRAV_STACK];
+    uint32_t my = 0, cn = 0, ct = 0;
+    bool active = false, exhausted = false;
     while (true) {
-        uint32_t base = warp_fetch(fetch);
-        if (base >= n) break;
-        uint32_t i = base + (threadIdx.x & 31);
-        uint32_t cn = 0, ct = 0;
-        if (i < n) {
-            float4 o = q.sh_o[i], d = q.sh_d[i];
-            TraceResult r;
-            traverse<true, STATS>(sc.nodes, sc.tris, o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w, r,
-                                  &cn, &ct);
-            if (r.prim == INVALID) {
-                float4 l = q.sh_l[i];
+        uint32_t idle = __ballot_sync(0xffffffffu, !active && !exhausted);
+        uint32_t busy = __ballot_sync(0xffffffffu, active);
+        if (idle && (__popc(idle) >= REFILL || busy == 0)) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(fetch, (uint32_t)__popc(idle));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (!active && !exhausted) {
+                uint32_t r = base + __popc(idle & lanemask_lt());
+                if (r < n) {
+                    float4 o = ro[r], d = rd[r];
+                    trav_init(st, o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w);
+                    my = r;
+                    active = true;
+                } else {
+                    exhausted = true;
+                }
+            }
+            busy = __ballot_sync(0xffffffffu, active);
+        }
+        if (busy == 0) break;
+        if (active && trav_step<ANY, STATS>(st, stack, sc.nodes, sc.tris, &cn, &ct)) {
+            active = false;
+            if (MODE == 0) {
+                q.hit[my] = make_float4(st.res.t, __uint_as_float(st.res.prim), st.res.u, st.res.v);
+            } else if (st.res.prim == INVALID) {
+                float4 l = q.sh_l[my];
                 uint32_t slot = __float_as_uint(l.w);
                 float4 rad = q.st_rad[slot];
                 rad.x = rad.x + l.x;
@@ -76,34 +93,53 @@ __global__ void __launch_bounds__(TT) k_shadow(DevScene sc, Queues q, uint32_t *
                 q.st_rad[slot] = rad;
             }
         }
-        if (STATS) add_stats(q.totals + 4, cn, ct);
+    }
+    if (STATS) add_stats(q.totals + (MODE == 0 ? 2 : 4), cn, ct);
+}
+
+// wl_cast_rays: the same persistent traversal over an array of 32-byte wl_ray records.
+template <bool ANY>
+__global__ void __launch_bounds__(TT) k_cast(DevScene sc, const float4 *rays, float4 *hits,
+                                              uint32_t n, uint32_t *fetch) {
+    const uint32_t lane = threadIdx.x & 31;
+    TravState st;
+    uint2 stack[TRAV_STACK];
+    uint32_t my = 0;
+    bool active = false, exhausted = false;
+    while (true) {
+        uint32_t idle = __ballot_sync(0xffffffffu, !active && !exhausted);
+        uint32_t busy = __ballot_sync(0xffffffffu, active);
+        if (idle && (__popc(idle) >= REFILL || busy == 0)) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(fetch, (uint32_t)__popc(idle));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (!active && !exhausted) {
+                uint32_t r = base + __popc(idle & lanemask_lt());
+                if (r < n) {
+                    float4 o = rays[2 * (size_t)r], d = rays[2 * (size_t)r + 1];
+                    trav_init(st, o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w);
+                    my = r;
+                    active = true;
+                } else {
+                    exhausted = true;
+                }
+            }
+            busy = __ballot_sync(0xffffffffu, active);
+        }
+        if (busy == 0) break;
+        if (active && trav_step<ANY, false>(st, stack, sc.nodes, sc.tris, nullptr, nullptr)) {
+            active = false;
+            uint32_t prim = st.res.prim;
+            if (ANY && prim != INVALID) prim = 0;
+            hits[my] = make_float4(st.res.t, __uint_as_float(prim), st.res.u, st.res.v);
+        }
     }
 }
 
-__global__ void __launch_bounds__(TT) k_cast(DevScene sc, const wl_ray *rays, wl_hit *hits,
-                                              uint32_t n, uint32_t mode, uint32_t *fetch) {
-    while (true) {
-        uint32_t base = warp_fetch(fetch);
-        if (base >= n) break;
-        uint32_t i = base + (threadIdx.x & 31);
-        if (i < n) {
-            const float4 *rp = reinterpret_cast<const float4 *>(rays + i);
-            float4 o = rp[0], d = rp[1];
-            TraceResult r;
-            if (sc.has_bvh) {
-                if (mode == WL_CAST_ANY)
-                    traverse<true, false>(sc.nodes, sc.tris, o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w,
-                                          r, nullptr, nullptr);
-                else
-                    traverse<false, false>(sc.nodes, sc.tris, o.x, o.y, o.z, d.x, d.y, d.z, o.w,
-                                           d.w, r, nullptr, nullptr);
-            } else {
-                r.t = d.w; r.prim = INVALID; r.u = r.v = 0.f;
-            }
-            if (mode == WL_CAST_ANY && r.prim != INVALID) r.prim = 0;
-            reinterpret_cast<float4 *>(hits)[i] = make_float4(r.t, __uint_as_float(r.prim), r.u, r.v);
-        }
-    }
+// rays of an empty scene miss
+__global__ void k_cast_empty(const float4 *rays, float4 *hits, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) hits[i] = make_float4(rays[2 * (size_t)i + 1].w, __uint_as_float(INVALID), 0.f, 0.f);
 }
 
 __global__ void __launch_bounds__(TT) k_cast_stats(DevScene sc, const wl_ray *rays, uint32_t n,
@@ -153,24 +189,31 @@ int grid_for(const void *kernel) {
 
 // Work counters live in the queues' counter block: [6] extend, [7] shadow, [8] cast.
 void launch_extend(const DevScene &sc, const Queues &q, int in, bool stats, cudaStream_t s) {
-    static int grid = grid_for((const void *)k_extend<false>);
+    static int grid = grid_for((const void *)k_trace<0, false>);
     cudaMemsetAsync(q.counters + 6, 0, sizeof(uint32_t), s);
-    if (stats) k_extend<true><<<grid, TT, 0, s>>>(sc, q, in, q.counters + 6);
-    else k_extend<false><<<grid, TT, 0, s>>>(sc, q, in, q.counters + 6);
+    if (stats) k_trace<0, true><<<grid, TT, 0, s>>>(sc, q, in, q.counters + 6);
+    else k_trace<0, false><<<grid, TT, 0, s>>>(sc, q, in, q.counters + 6);
 }
 
 void launch_shadow(const DevScene &sc, const Queues &q, bool stats, cudaStream_t s) {
-    static int grid = grid_for((const void *)k_shadow<false>);
+    static int grid = grid_for((const void *)k_trace<1, false>);
     cudaMemsetAsync(q.counters + 7, 0, sizeof(uint32_t), s);
-    if (stats) k_shadow<true><<<grid, TT, 0, s>>>(sc, q, q.counters + 7);
-    else k_shadow<false><<<grid, TT, 0, s>>>(sc, q, q.counters + 7);
+    if (stats) k_trace<1, true><<<grid, TT, 0, s>>>(sc, q, 0, q.counters + 7);
+    else k_trace<1, false><<<grid, TT, 0, s>>>(sc, q, 0, q.counters + 7);
 }
 
 void launch_cast(const DevScene &sc, const wl_ray *rays, wl_hit *hits, uint32_t n, uint32_t mode,
                  uint32_t *fetch, cudaStream_t s) {
-    static int grid = grid_for((const void *)k_cast);
+    static int grid = grid_for((const void *)k_cast<false>);
+    const float4 *r = reinterpret_cast<const float4 *>(rays);
+    float4 *h = reinterpret_cast<float4 *>(hits);
+    if (!sc.has_bvh) {
+        k_cast_empty<<<(n + 255) / 256, 256, 0, s>>>(r, h, n);
+        return;
+    }
     cudaMemsetAsync(fetch, 0, sizeof(uint32_t), s);
-    k_cast<<<grid, TT, 0, s>>>(sc, rays, hits, n, mode, fetch);
+    if (mode == WL_CAST_ANY) k_cast<true><<<grid, TT, 0, s>>>(sc, r, h, n, fetch);
+    else k_cast<false><<<grid, TT, 0, s>>>(sc, r, h, n, fetch);
 }
 
 void launch_cast_stats(const DevScene &sc, const wl_ray *rays, uint32_t n, uint32_t mode,

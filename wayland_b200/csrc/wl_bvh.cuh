@@ -334,15 +334,6 @@ WL_HD void emit_wide(const BinTree &T, int b, const Entries &E, uint32_t child_b
 
 // ---------------------------------------------------------------------------------------
 // Traversal
-WL_HD float safe_rcp(float d) {
-    return fabsf(d) < 1e-30f ? (d < 0.0f ? -1e30f : 1e30f) : XDIV(1.0f, d);
-}
-
-template <class Load>
-struct NodeView {
-    float4 n0, n1, n2, n3, n4;
-};
-
 #ifdef __CUDA_ARCH__
 __device__ __forceinline__ float4 ldg4(const float4 *p) { return __ldg(p); }
 #else
@@ -354,6 +345,141 @@ struct TraceResult {
     uint32_t prim;
 };
 
+WL_HD int lowest_bit(uint32_t x) {
+#ifdef __CUDA_ARCH__
+    return __ffs(x) - 1;
+#else
+    return __builtin_ffs(x) - 1;
+#endif
+}
+WL_HD uint32_t popcount(uint32_t x) {
+#ifdef __CUDA_ARCH__
+    return __popc(x);
+#else
+    return (uint32_t)__builtin_popcount(x);
+#endif
+}
+
+// Traversal state of one ray: the ray and its precomputed terms, the best hit so far, the
+// current node group (child base, internal hit bits in [24, 32) ordered by slot XOR octant,
+// imask in [0, 8)), the current triangle group (base, hit bits) and the stack depth.
+struct TravState {
+    float ox, oy, oz, dx, dy, dz, idx, idy, idz, tmin, tmax;
+    RayPre pre;
+    uint32_t oct;
+    TraceResult res;
+    uint2 ng, tg;
+    int sp;
+    bool ok;
+};
+
+WL_HD float safe_rcp(float d) {
+    return fabsf(d) < 1e-30f ? (d < 0.0f ? -1e30f : 1e30f) : XDIV(1.0f, d);
+}
+
+WL_HD void trav_init(TravState &s, float ox, float oy, float oz, float dx, float dy, float dz,
+                     float tmin, float tmax) {
+    s.ox = ox; s.oy = oy; s.oz = oz;
+    s.dx = dx; s.dy = dy; s.dz = dz;
+    s.tmin = tmin; s.tmax = tmax;
+    s.pre = ray_pre(dx, dy, dz);
+    s.idx = safe_rcp(dx); s.idy = safe_rcp(dy); s.idz = safe_rcp(dz);
+    s.oct = (dx < 0.0f ? 1u : 0u) | (dy < 0.0f ? 2u : 0u) | (dz < 0.0f ? 4u : 0u);
+    s.res.t = tmax;
+    s.res.prim = INVALID;
+    s.res.u = s.res.v = 0.f;
+    s.ng = make_uint2(0u, (1u << (24 + s.oct)) | 1u);  // the root as the only child of a group
+    s.tg = make_uint2(0u, 0u);
+    s.sp = 0;
+    s.ok = true;
+}
+
+// One step: visit the nearest pending child node (if the current group has one), test the
+// triangles of its hit leaves, and pop the stack when the group is exhausted. Returns true when
+// the ray is finished (stack empty, or an any-hit found). The box test decodes child bounds
+// exactly (grid origin = multiple of the power-of-two scale) and keeps a relative margin of
+// 2^-20, so it never rejects a triangle the triangle test accepts.
+template <bool ANY, bool STATS>
+WL_HD bool trav_step(TravState &s, uint2 *stack, const float4 *__restrict__ nodes,
+                     const float4 *__restrict__ tris, uint32_t *n_nodes, uint32_t *n_tris) {
+    const float grow = 1.0f + 0x1p-20f;
+    if (s.ng.y & 0xff000000u) {
+        int k = lowest_bit(s.ng.y >> 24);
+        s.ng.y &= ~(1u << (24 + k));
+        uint32_t slot = (uint32_t)k ^ s.oct;
+        uint32_t node = s.ng.x + popcount(s.ng.y & 0xffu & ((1u << slot) - 1u));
+        if (s.ng.y & 0xff000000u) {
+            if (s.sp < TRAV_STACK) stack[s.sp++] = s.ng;
+            else s.ok = false;
+        }
+        const float4 *np = nodes + 5 * (size_t)node;
+        float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3),
+               n4 = ldg4(np + 4);
+        if (STATS) (*n_nodes)++;
+        uint32_t ew = as_uint(n0.w);
+        float scx = as_float((ew & 0xffu) << 23), scy = as_float(((ew >> 8) & 0xffu) << 23),
+              scz = as_float(((ew >> 16) & 0xffu) << 23);
+        uint32_t imask = ew >> 24;
+        uint32_t m0 = as_uint(n1.z), m1 = as_uint(n1.w);
+        uint32_t qlx0 = as_uint(n2.x), qlx1 = as_uint(n2.y), qly0 = as_uint(n2.z), qly1 = as_uint(n2.w);
+        uint32_t qlz0 = as_uint(n3.x), qlz1 = as_uint(n3.y), qhx0 = as_uint(n3.z), qhx1 = as_uint(n3.w);
+        uint32_t qhy0 = as_uint(n4.x), qhy1 = as_uint(n4.y), qhz0 = as_uint(n4.z), qhz1 = as_uint(n4.w);
+        const float tcur = s.res.t;
+        uint32_t ihits = 0, thits = 0;
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            uint32_t meta = byte_of(m0, m1, c);
+            if (meta == 0) continue;
+            float lx = fmaf((float)byte_of(qlx0, qlx1, c), scx, n0.x);
+            float ly = fmaf((float)byte_of(qly0, qly1, c), scy, n0.y);
+            float lz = fmaf((float)byte_of(qlz0, qlz1, c), scz, n0.z);
+            float hx = fmaf((float)byte_of(qhx0, qhx1, c), scx, n0.x);
+            float hy = fmaf((float)byte_of(qhy0, qhy1, c), scy, n0.y);
+            float hz = fmaf((float)byte_of(qhz0, qhz1, c), scz, n0.z);
+            float t0x = XMUL(XSUB(lx, s.ox), s.idx), t1x = XMUL(XSUB(hx, s.ox), s.idx);
+            float t0y = XMUL(XSUB(ly, s.oy), s.idy), t1y = XMUL(XSUB(hy, s.oy), s.idy);
+            float t0z = XMUL(XSUB(lz, s.oz), s.idz), t1z = XMUL(XSUB(hz, s.oz), s.idz);
+            float tn = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), s.tmin));
+            float tf = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), tcur));
+            if (tn <= XMUL(tf, grow)) {
+                if (imask & (1u << c)) ihits |= 1u << ((uint32_t)c ^ s.oct);
+                else thits |= (meta >> 5) << (meta & 31u);
+            }
+        }
+        s.ng = make_uint2(as_uint(n1.x), (ihits << 24) | imask);
+        s.tg = make_uint2(as_uint(n1.y), thits);
+    }
+    while (s.tg.y) {
+        int k = lowest_bit(s.tg.y);
+        s.tg.y &= s.tg.y - 1u;
+        const float4 *tp = tris + 3 * (size_t)(s.tg.x + (uint32_t)k);
+        float4 v0 = ldg4(tp), v1 = ldg4(tp + 1), v2 = ldg4(tp + 2);
+        if (STATS) (*n_tris)++;
+        float t, u, v;
+        if (tri_hit(s.pre, s.ox, s.oy, s.oz, v0, v1, v2, s.tmin, s.tmax, t, u, v)) {
+            uint32_t prim = as_uint(v0.w);
+            if (ANY) {
+                s.res.t = t;
+                s.res.prim = prim;
+                s.res.u = u;
+                s.res.v = v;
+                return true;
+            }
+            if (t < s.res.t || (t == s.res.t && prim < s.res.prim)) {
+                s.res.t = t;
+                s.res.prim = prim;
+                s.res.u = u;
+                s.res.v = v;
+            }
+        }
+    }
+    if (!(s.ng.y & 0xff000000u)) {
+        if (s.sp == 0) return true;
+        s.ng = stack[--s.sp];
+    }
+    return false;
+}
+
 // ANY: stop at the first hit (shadow rays). STATS: count node visits and triangle tests.
 // Returns false if the traversal stack overflowed (cannot happen when the tree depth is
 // <= TRAV_STACK, which the build checks).
@@ -361,109 +487,13 @@ template <bool ANY, bool STATS>
 WL_HD bool traverse(const float4 *__restrict__ nodes, const float4 *__restrict__ tris, float ox,
                     float oy, float oz, float dx, float dy, float dz, float tmin, float tmax,
                     TraceResult &res, uint32_t *n_nodes, uint32_t *n_tris) {
-    res.t = tmax;
-    res.prim = INVALID;
-    res.u = res.v = 0.f;
-    RayPre pre = ray_pre(dx, dy, dz);
-    const float idx = safe_rcp(dx), idy = safe_rcp(dy), idz = safe_rcp(dz);
-    const uint32_t oct = (dx < 0.0f ? 1u : 0u) | (dy < 0.0f ? 2u : 0u) | (dz < 0.0f ? 4u : 0u);
-    const float grow = 1.0f + 0x1p-20f;
+    TravState s;
     uint2 stack[TRAV_STACK];
-    int sp = 0;
-    uint2 ng = make_uint2(0u, (1u << (24 + oct)) | 1u);
-    uint2 tg = make_uint2(0u, 0u);
-    bool ok = true;
-    while (true) {
-        if (ng.y & 0xff000000u) {
-            uint32_t hits = ng.y >> 24;
-#ifdef __CUDA_ARCH__
-            int k = __ffs(hits) - 1;
-#else
-            int k = __builtin_ffs(hits) - 1;
-#endif
-            ng.y &= ~(1u << (24 + k));
-            uint32_t slot = (uint32_t)k ^ oct;
-            uint32_t below = ng.y & 0xffu & ((1u << slot) - 1u);
-#ifdef __CUDA_ARCH__
-            uint32_t node = ng.x + __popc(below);
-#else
-            uint32_t node = ng.x + __builtin_popcount(below);
-#endif
-            if (ng.y & 0xff000000u) {
-                if (sp < TRAV_STACK) stack[sp++] = ng;
-                else ok = false;
-            }
-            const float4 *np = nodes + 5 * (size_t)node;
-            float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3),
-                   n4 = ldg4(np + 4);
-            if (STATS) (*n_nodes)++;
-            uint32_t ew = as_uint(n0.w);
-            float scx = as_float((ew & 0xffu) << 23), scy = as_float(((ew >> 8) & 0xffu) << 23),
-                  scz = as_float(((ew >> 16) & 0xffu) << 23);
-            uint32_t imask = ew >> 24;
-            uint32_t m0 = as_uint(n1.z), m1 = as_uint(n1.w);
-            uint32_t qlx0 = as_uint(n2.x), qlx1 = as_uint(n2.y), qly0 = as_uint(n2.z), qly1 = as_uint(n2.w);
-            uint32_t qlz0 = as_uint(n3.x), qlz1 = as_uint(n3.y), qhx0 = as_uint(n3.z), qhx1 = as_uint(n3.w);
-            uint32_t qhy0 = as_uint(n4.x), qhy1 = as_uint(n4.y), qhz0 = as_uint(n4.z), qhz1 = as_uint(n4.w);
-            float tcur = res.t;
-            uint32_t ihits = 0, thits = 0;
-#pragma unroll
-            for (int s = 0; s < 8; s++) {
-                uint32_t meta = byte_of(m0, m1, s);
-                if (meta == 0) continue;
-                float lx = fmaf((float)byte_of(qlx0, qlx1, s), scx, n0.x);
-                float ly = fmaf((float)byte_of(qly0, qly1, s), scy, n0.y);
-                float lz = fmaf((float)byte_of(qlz0, qlz1, s), scz, n0.z);
-                float hx = fmaf((float)byte_of(qhx0, qhx1, s), scx, n0.x);
-                float hy = fmaf((float)byte_of(qhy0, qhy1, s), scy, n0.y);
-                float hz = fmaf((float)byte_of(qhz0, qhz1, s), scz, n0.z);
-                float t0x = XMUL(XSUB(lx, ox), idx), t1x = XMUL(XSUB(hx, ox), idx);
-                float t0y = XMUL(XSUB(ly, oy), idy), t1y = XMUL(XSUB(hy, oy), idy);
-                float t0z = XMUL(XSUB(lz, oz), idz), t1z = XMUL(XSUB(hz, oz), idz);
-                float tn = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), tmin));
-                float tf = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), tcur));
-                if (tn <= XMUL(tf, grow)) {
-                    if (imask & (1u << s)) ihits |= 1u << ((uint32_t)s ^ oct);
-                    else thits |= (meta >> 5) << (meta & 31u);
-                }
-            }
-            ng = make_uint2(as_uint(n1.x), (ihits << 24) | imask);
-            tg = make_uint2(as_uint(n1.y), thits);
-        }
-        while (tg.y) {
-#ifdef __CUDA_ARCH__
-            int k = __ffs(tg.y) - 1;
-#else
-            int k = __builtin_ffs(tg.y) - 1;
-#endif
-            tg.y &= tg.y - 1u;
-            const float4 *tp = tris + 3 * (size_t)(tg.x + (uint32_t)k);
-            float4 v0 = ldg4(tp), v1 = ldg4(tp + 1), v2 = ldg4(tp + 2);
-            if (STATS) (*n_tris)++;
-            float t, u, v;
-            if (tri_hit(pre, ox, oy, oz, v0, v1, v2, tmin, tmax, t, u, v)) {
-                uint32_t prim = as_uint(v0.w);
-                if (ANY) {
-                    res.t = t;
-                    res.prim = prim;
-                    res.u = u;
-                    res.v = v;
-                    return ok;
-                }
-                if (t < res.t || (t == res.t && prim < res.prim)) {
-                    res.t = t;
-                    res.prim = prim;
-                    res.u = u;
-                    res.v = v;
-                }
-            }
-        }
-        if (!(ng.y & 0xff000000u)) {
-            if (sp == 0) break;
-            ng = stack[--sp];
-        }
+    trav_init(s, ox, oy, oz, dx, dy, dz, tmin, tmax);
+    while (!trav_step<ANY, STATS>(s, stack, nodes, tris, n_nodes, n_tris)) {
     }
-    return ok;
+    res = s.res;
+    return s.ok;
 }
 
 }  // namespace wl

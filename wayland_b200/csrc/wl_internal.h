@@ -88,6 +88,18 @@ struct WaveParams {
     float cam_pos[3], cam_look[3], cam_up[3], cam_right[3];
 };
 
+// One wave of ambient-occlusion camera samples (ao.cu): slot i is camera sample
+// (base + i) % cs of pixel-frame group (base + i) / cs; a wave holds at most one group per pixel.
+struct AoWave {
+    uint32_t W, H, npix, first_frame;
+    uint64_t base;
+    uint32_t count, cs, ao_rays, rng;
+    float radius, eps;
+    uint64_t seed;
+    float cam_pos[3], cam_look[3], cam_up[3], cam_right[3];
+};
+void launch_ao(const AoWave &w, const DevScene &sc, const Queues &q, const Film &f, cudaStream_t s);
+
 // launch functions (pt_kernels.cuh instantiated in pt_fast.cu / pt_strict.cu)
 namespace fast {
 void launch_generate(const WaveParams &wp, const Queues &q, cudaStream_t s);

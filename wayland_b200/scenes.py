@@ -12,6 +12,9 @@ shapes, sizes and value distributions the benchmark names:
                        fBm of amplitude 0.05, on a 2-triangle ground plane; Disney parameters per
                        object from the seed; 4 quad lights and a constant environment of 0.1;
                        1920 x 1080, 64 spp, depth 16.
+  door_slit_room()     Radiance-cache PT: a ~500K-triangle room lit only through a 0.05-wide
+                       door slit by an area light outside (mostly indirect light), glossy Disney
+                       walls with roughness U[0.1, 0.4].
 
 Matte surfaces use the reference's matte -> Disney mapping (Material.cpp:51-67: roughness 0.5,
 specular 0, sheenTint 0.5, eta 1.5), since the renderer's only surface model is that BSDF.
@@ -292,6 +295,75 @@ def displaced_sphere(width=1920, height=1080, spp=64, max_depth=16, subdiv=316, 
     cam = pinhole((0.0, 0.6, 4.2), (0.0, -0.2, 0.0), (0, 1, 0), 40.0, width, height)
     return Scene("displaced_sphere", V, I, M, mats, lights, N=N, tri_flags=flags, camera=cam,
                  width=width, height=height, spp=spp, max_depth=max_depth, env=(0.1, 0.1, 0.1))
+
+
+def _grid(p0, du, dv, nu, nv):
+    """Quad p0 + [0,1] du + [0,1] dv tessellated into nu x nv cells (2 nu nv triangles);
+    normal = cross(du, dv)."""
+    u = np.linspace(0.0, 1.0, nu + 1)
+    v = np.linspace(0.0, 1.0, nv + 1)
+    uu, vv = np.meshgrid(u, v, indexing="ij")
+    P = (np.asarray(p0, np.float64)[None] + uu.reshape(-1, 1) * np.asarray(du, np.float64)[None]
+         + vv.reshape(-1, 1) * np.asarray(dv, np.float64)[None])
+    i, j = np.meshgrid(np.arange(nu), np.arange(nv), indexing="ij")
+    a = (i * (nv + 1) + j).reshape(-1)
+    b = ((i + 1) * (nv + 1) + j).reshape(-1)
+    c = ((i + 1) * (nv + 1) + j + 1).reshape(-1)
+    d = (i * (nv + 1) + j + 1).reshape(-1)
+    I = np.concatenate([np.stack([a, b, c], 1), np.stack([a, c, d], 1)])
+    return P.astype(np.float32), I.astype(np.uint32)
+
+
+def door_slit_room(width=1920, height=1080, spp=1, max_depth=16, seed=0, cells=200,
+                   slit=0.05):
+    """Radiance-cache configuration: a closed room 4 x 3 x 5 whose walls are tessellated into
+    about 500K triangles (cells x cells quads per wall), lit only by an area light outside,
+    through a vertical slit of width `slit` in the +x wall, so most of the light is indirect.
+    Glossy Disney walls (roughness ~ U[0.1, 0.4]); four boxes and a displaced sphere inside."""
+    rng = np.random.default_rng(seed)
+    X, Y, Z = 4.0, 3.0, 5.0
+    b = _Builder()
+    mats = []
+
+    def glossy():
+        mats.append(disney(tuple(rng.uniform(0.35, 0.85, 3)), metallic=0.0,
+                           roughness=rng.uniform(0.1, 0.4), specular=0.5, sheen_tint=0.5))
+        return len(mats) - 1
+
+    n = cells
+    # floor, ceiling, walls x = 0, z = 0, z = Z
+    b.add([_grid((0, 0, 0), (0, 0, Z), (X, 0, 0), n, n)], glossy())
+    b.add([_grid((0, Y, 0), (X, 0, 0), (0, 0, Z), n, n)], glossy())
+    b.add([_grid((0, 0, 0), (0, Y, 0), (0, 0, Z), n, n)], glossy())
+    b.add([_grid((0, 0, 0), (X, 0, 0), (0, Y, 0), n, n)], glossy())
+    b.add([_grid((0, 0, Z), (0, Y, 0), (X, 0, 0), n, n)], glossy())
+    # +x wall with the slit: z in [zc - slit/2, zc + slit/2], y in [0, yt]
+    zc, yt = 2.5, 2.2
+    z0, z1 = zc - slit / 2, zc + slit / 2
+    b.add([_grid((X, 0, 0), (0, 0, z0), (0, Y, 0), n // 2, n),
+           _grid((X, 0, z1), (0, 0, Z - z1), (0, Y, 0), n // 2, n),
+           _grid((X, yt, z0), (0, 0, z1 - z0), (0, Y - yt, 0), 1, 4)], glossy())
+    for k in range(4):
+        lo = np.array([rng.uniform(0.3, 3.0), 0.0, rng.uniform(0.3, 4.0)])
+        size = np.array([rng.uniform(0.3, 0.8), rng.uniform(0.3, 1.2), rng.uniform(0.3, 0.8)])
+        b.add(_box(tuple(lo), tuple(np.minimum(lo + size, [X - 0.4, Y - 0.2, Z - 0.2]))), glossy())
+    P, T = subdivided_icosphere(40)
+    r = 1.0 + 0.05 * fbm(P * 1.5, seed)
+    Vs = (P * r[:, None] * 0.6 + np.array([1.2, 0.7, 3.4])).astype(np.float32)
+    b.add([(Vs, T.astype(np.uint32))], glossy())
+    # the light: a 1.2 x 2.0 quad at x = X + 1.5 facing -x (towards the slit), radiance ~60
+    lx = X + 1.5
+    first, count = b.add([_quad((lx, 0.1, zc - 0.6), (lx, 0.1, zc + 0.6), (lx, 2.1, zc + 0.6),
+                                (lx, 2.1, zc - 0.6))], 0)
+    V, I, M = b.arrays()
+    lights = np.zeros(1, LIGHT)
+    lights[0]["L"] = (60.0, 55.0, 45.0)
+    lights[0]["two_sided"] = 0
+    lights[0]["first_tri"] = first
+    lights[0]["tri_count"] = count
+    cam = pinhole((0.6, 1.6, 0.5), (3.0, 1.0, 4.2), (0, 1, 0), 60.0, width, height)
+    return Scene("door_slit_room", V, I, M, np.array(mats), lights, camera=cam, width=width,
+                 height=height, spp=spp, max_depth=max_depth)
 
 
 def random_triangles(n, seed=0, spread=1.0, size=0.1):
