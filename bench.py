@@ -258,6 +258,77 @@ def raycast_microbench(wl, torch, ctx, sc, scene, stream):
     return out
 
 
+def nrc_convergence(wl, torch, ctx, res=(480, 270), oracle_spp=16384, target=1e-2,
+                    budget_s=60.0, chunk=4):
+    """Time to relMSE <= target against an FP64-accumulated high-spp render, for the plain path
+    tracer and for the radiance-cache path tracer, on the door-slit room (about 500K triangles,
+    mostly indirect light). relMSE = mean over pixels and channels of (I - R)^2 / (R^2 + 1e-2).
+    Times are device time of the render calls (CUDA events on the library's stream)."""
+    from wayland_b200 import scenes
+    W_, H_ = res
+    sc = scenes.door_slit_room(W_, H_)
+    scene = wl.Scene(ctx, sc)
+    cam = sc.camera_struct()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    # oracle: FP64 film, plain path tracer, fast math
+    ref_film = wl.Film(ctx, W_, H_, fp64=True)
+    t0 = time.perf_counter()
+    done = 0
+    while done < oracle_spp:
+        k = min(1024, oracle_spp - done)
+        wl.render(ctx, scene, cam, wl.render_params(W_, H_, k, first_frame=1000000 + done,
+                                                    max_depth=16), ref_film)
+        done += k
+    ref = torch.from_numpy(ref_film.download64()).cuda()
+    oracle_s = time.perf_counter() - t0
+
+    def relmse(img):
+        x = torch.from_numpy(img).cuda().double()
+        return float(((x - ref) ** 2 / (ref * ref + 1e-2)).mean())
+
+    def run(kind):
+        film = wl.Film(ctx, W_, H_)
+        cache = wl.RadianceCache(ctx, scene) if kind == "nrc" else None
+        t_dev = 0.0
+        spp = 0
+        curve = []
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        while True:
+            n = chunk
+            p = wl.render_params(W_, H_, n, first_frame=spp, max_depth=16)
+            e0.record(stream)
+            if cache is None:
+                wl.render(ctx, scene, cam, p, film)
+            else:
+                wl.render_nrc(ctx, scene, cam, p, cache, film)
+            e1.record(stream)
+            e1.synchronize()
+            t_dev += e0.elapsed_time(e1) * 1e-3
+            spp += n
+            err = relmse(film.download())
+            curve.append((spp, round(t_dev, 4), err))
+            if err <= target or t_dev > budget_s:
+                break
+        if cache is not None:
+            cache.close()
+        film.close()
+        reached = curve[-1][2] <= target
+        return {"reached": reached, "seconds": curve[-1][1] if reached else None, "spp": curve[-1][0],
+                "final_relmse": curve[-1][2], "curve": curve[:: max(1, len(curve) // 12)]}
+
+    plain = run("plain")
+    nrc = run("nrc")
+    ref_film.close()
+    scene.close()
+    out = {"scene": f"door-slit room {sc.num_tris} tris, {W_}x{H_}, depth 16, fast math",
+           "oracle": f"{oracle_spp} spp, FP64 film, plain path tracer ({oracle_s:.1f} s)",
+           "target_relmse": target, "plain": plain, "nrc": nrc}
+    if plain["seconds"] and nrc["seconds"]:
+        out["nrc_time_fraction"] = round(nrc["seconds"] / plain["seconds"], 4)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -269,6 +340,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-raycast", action="store_true")
     ap.add_argument("--math", default="fast", choices=["fast", "strict"])
+    ap.add_argument("--nrc-only", action="store_true",
+                    help="only the radiance-cache convergence comparison (prints its JSON)")
+    ap.add_argument("--no-nrc", action="store_true")
     ap.add_argument("--case", default="full", choices=["full", "small"],
                     help="small: the same 2M-triangle scene at 960x540 x 4 spp (for ncu captures)")
     args = ap.parse_args()
@@ -288,6 +362,11 @@ def main():
     rank = env_int("RANK", 0)
     local = env_int("LOCAL_RANK", 0)
     torch.cuda.set_device(local)
+    if args.nrc_only:
+        ctx = wl.Context(local)
+        print(json.dumps(nrc_convergence(wl, torch, ctx)), flush=True)
+        ctx.close()
+        return 0
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))

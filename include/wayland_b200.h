@@ -305,6 +305,45 @@ WL_API void wl_ao_params_default(wl_ao_params *params, uint32_t width, uint32_t 
 WL_API int wl_render_ao(wl_context *ctx, wl_scene *scene, const wl_camera *camera,
                         const wl_ao_params *params, wl_film *film);
 
+/* ---- neural radiance cache ---------------------------------------------------------- */
+/* No counterpart in the reference: a multiresolution hash-grid encoding
+ * (after Mueller et al. 2022) feeding an MLP that predicts the radiance reflected at a surface
+ * point, trained online on the path tracer's own estimates (after Mueller et al. 2021,
+ * "Real-time Neural Radiance Caching"). Paths that are not training paths stop at
+ * query_depth and add throughput x cache prediction; training paths are traced unbiased to
+ * max_depth and give one training sample per surface vertex. */
+typedef struct wl_nrc_params {
+    uint32_t levels;            /* hash-grid levels (16) */
+    uint32_t log2_table;        /* entries per level = 2^log2_table (19) */
+    uint32_t base_resolution;   /* coarsest grid resolution (16) */
+    float per_level_scale;      /* resolution growth per level (1.38) */
+    uint32_t train_paths;       /* training paths per frame (2^14; ~2^16 samples) */
+    uint32_t query_depth;       /* surface vertex where other paths query the cache (2) */
+    float learning_rate;        /* Adam step size (1e-2) */
+    uint32_t seed;              /* initialisation */
+} wl_nrc_params;
+typedef struct wl_nrc wl_nrc;
+#define WL_NRC_WEIGHTS 17408u   /* 4 x 64 x 64 + 16 x 64 */
+WL_API void wl_nrc_params_default(wl_nrc_params *params);
+WL_API int wl_nrc_create(wl_context *ctx, wl_scene *scene, const wl_nrc_params *params,
+                         wl_nrc **out);
+WL_API int wl_nrc_destroy(wl_nrc *nrc);
+/* Render params->spp frames with the cache (query, then train on the frame's samples). */
+WL_API int wl_render_nrc(wl_context *ctx, wl_scene *scene, const wl_camera *camera,
+                         const wl_render_params *params, wl_nrc *nrc, wl_film *film);
+/* Network access for tests: inputs are n x 64 feature rows (FP32, device), outputs n x 4. */
+WL_API int wl_nrc_mlp_forward(wl_nrc *nrc, const float *d_in, float *d_out, uint32_t n);
+/* One training step on n (input, target) rows; returns the batch loss (relative L2). */
+WL_API int wl_nrc_train_step(wl_nrc *nrc, const float *d_in, const float *d_target, uint32_t n,
+                             float *loss);
+/* Weight gradients of the loss on n rows without applying them (17408 floats, host). */
+WL_API int wl_nrc_mlp_gradients(wl_nrc *nrc, const float *d_in, const float *d_target,
+                                uint32_t n, float *grad);
+/* MLP weights as FP32 (17408 floats: W0..W3 64x64 then W4 16x64, row = output), host. */
+WL_API int wl_nrc_get_weights(wl_nrc *nrc, float *w);
+WL_API int wl_nrc_set_weights(wl_nrc *nrc, const float *w);
+WL_API int wl_nrc_stats(wl_nrc *nrc, uint32_t *train_samples, uint32_t *queries, float *loss);
+
 /* Random streams for parity tests: the first `count` uniforms of the stream of each listed
  * pixel at `frame` (count floats per pixel, pixel-major). Device pointers. */
 WL_API int wl_debug_rng(wl_context *ctx, uint32_t rng, uint64_t seed, const uint32_t *d_pixels,

@@ -232,6 +232,70 @@ def render_ao(ctx, scene, camera, params, film):
                                                     C.byref(params), film.handle))
 
 
+class RadianceCache:
+    """The neural radiance cache (hash grid + MLP) of a scene; wl_nrc_* in the C ABI."""
+
+    def __init__(self, ctx, scene, **kw):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        p = _abi.NrcParams()
+        self.lib.wl_nrc_params_default(C.byref(p))
+        for k, v in kw.items():
+            setattr(p, k, v)
+        self.params = p
+        h = C.c_void_p()
+        _abi.check("wl_nrc_create", self.lib.wl_nrc_create(ctx.handle, scene.handle, C.byref(p), C.byref(h)))
+        self.handle = h
+        ctx._children.add(self)
+
+    def forward(self, d_in, d_out, n):
+        _abi.check("wl_nrc_mlp_forward", self.lib.wl_nrc_mlp_forward(self.handle, C.c_void_p(d_in),
+                                                                     C.c_void_p(d_out), n))
+
+    def train_step(self, d_in, d_target, n):
+        loss = C.c_float()
+        _abi.check("wl_nrc_train_step", self.lib.wl_nrc_train_step(
+            self.handle, C.c_void_p(d_in), C.c_void_p(d_target), n, C.byref(loss)))
+        return loss.value
+
+    def gradients(self, d_in, d_target, n):
+        g = np.empty(_abi.NRC_WEIGHTS, np.float32)
+        _abi.check("wl_nrc_mlp_gradients", self.lib.wl_nrc_mlp_gradients(
+            self.handle, C.c_void_p(d_in), C.c_void_p(d_target), n, _p(g)))
+        return g
+
+    def weights(self):
+        w = np.empty(_abi.NRC_WEIGHTS, np.float32)
+        _abi.check("wl_nrc_get_weights", self.lib.wl_nrc_get_weights(self.handle, _p(w)))
+        return w
+
+    def set_weights(self, w):
+        w = np.ascontiguousarray(w, np.float32)
+        _abi.check("wl_nrc_set_weights", self.lib.wl_nrc_set_weights(self.handle, _p(w)))
+
+    def stats(self):
+        a, b, l = C.c_uint32(), C.c_uint32(), C.c_float()
+        _abi.check("wl_nrc_stats", self.lib.wl_nrc_stats(self.handle, C.byref(a), C.byref(b), C.byref(l)))
+        return {"train_samples": a.value, "queries": b.value, "loss": l.value}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.wl_nrc_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def render_nrc(ctx, scene, camera, params, cache, film):
+    """params.spp frames with the radiance cache: query, then one training step per frame."""
+    _abi.check("wl_render_nrc", ctx.lib.wl_render_nrc(ctx.handle, scene.handle, C.byref(camera),
+                                                      C.byref(params), cache.handle, film.handle))
+
+
 def render(ctx, scene, camera, params, film):
     _abi.check("wl_render", ctx.lib.wl_render(ctx.handle, scene.handle, C.byref(camera),
                                               C.byref(params), film.handle))

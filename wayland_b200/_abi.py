@@ -60,6 +60,15 @@ class AoParams(C.Structure):
                 ("rng", C.c_uint32), ("wave_paths", C.c_uint32), ("seed", C.c_uint64)]
 
 
+class NrcParams(C.Structure):
+    _fields_ = [("levels", C.c_uint32), ("log2_table", C.c_uint32), ("base_resolution", C.c_uint32),
+                ("per_level_scale", C.c_float), ("train_paths", C.c_uint32),
+                ("query_depth", C.c_uint32), ("learning_rate", C.c_float), ("seed", C.c_uint32)]
+
+
+NRC_WEIGHTS = 17408
+
+
 class RenderStats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("segments", C.c_uint64), ("shadow_rays", C.c_uint64),
                 ("waves", C.c_uint32), ("kernel_launches", C.c_uint32), ("ms_total", C.c_float),
@@ -127,6 +136,16 @@ SIGNATURES = {
     "wl_debug_rng": (C.c_int, [_P, _U32, C.c_uint64, _P, _U32, _U32, _U32, _P]),
     "wl_render_noalloc": (C.c_int, [_P, _P, C.POINTER(Camera), C.POINTER(RenderParams), _P]),
     "wl_ao_params_default": (None, [C.POINTER(AoParams), _U32, _U32, _U32]),
+    "wl_nrc_params_default": (None, [C.POINTER(NrcParams)]),
+    "wl_nrc_create": (C.c_int, [_P, _P, C.POINTER(NrcParams), C.POINTER(_P)]),
+    "wl_nrc_destroy": (C.c_int, [_P]),
+    "wl_render_nrc": (C.c_int, [_P, _P, C.POINTER(Camera), C.POINTER(RenderParams), _P, _P]),
+    "wl_nrc_mlp_forward": (C.c_int, [_P, _P, _P, _U32]),
+    "wl_nrc_train_step": (C.c_int, [_P, _P, _P, _U32, C.POINTER(C.c_float)]),
+    "wl_nrc_mlp_gradients": (C.c_int, [_P, _P, _P, _U32, _P]),
+    "wl_nrc_get_weights": (C.c_int, [_P, _P]),
+    "wl_nrc_set_weights": (C.c_int, [_P, _P]),
+    "wl_nrc_stats": (C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_float)]),
     "wl_render_ao": (C.c_int, [_P, _P, C.POINTER(Camera), C.POINTER(AoParams), _P]),
 }
 NOALLOC_MAX_PATHS = 65536

@@ -27,6 +27,7 @@ UNITS = {
     "pt_strict.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
     "noalloc.cu": [],
     "ao.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
+    "nrc.cu": [],
 }
 
 

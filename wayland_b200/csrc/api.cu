@@ -81,6 +81,22 @@ struct wl_film {
     Film f{};
 };
 
+struct wl_nrc {
+    wl_context *ctx = nullptr;
+    wl_scene *scene = nullptr;
+    NrcNet *net = nullptr;
+    wl_nrc_params p{};
+    // per-wave buffers
+    uint32_t q_cap = 0, t_cap = 0, depth_cap = 0;
+    NrcVertex *queries = nullptr;
+    uint32_t *n_queries = nullptr;
+    NrcVertex *rec_v = nullptr;
+    float4 *rec_tr = nullptr, *rec_rb = nullptr;
+    uint32_t *rec_count = nullptr, *rec_slot = nullptr;
+    uint32_t last_samples = 0, last_queries = 0;
+    float last_loss = 0.f;
+};
+
 namespace {
 
 DevScene dev_scene(const wl_scene *s) {
@@ -748,6 +764,237 @@ int wl_render_ao(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_ao_p
         w.base = g0 * p->camera_samples;
         w.count = (uint32_t)(ng * p->camera_samples);
         launch_ao(w, sc, c->q, f->f, c->stream);
+        CK(cudaGetLastError());
+    }
+    f->f.frames64 += p->spp;
+    return WL_OK;
+}
+
+void wl_nrc_params_default(wl_nrc_params *p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->levels = 16;
+    p->log2_table = 19;
+    p->base_resolution = 16;
+    p->per_level_scale = 1.38f;
+    p->train_paths = 1u << 14;
+    p->query_depth = 2;
+    p->learning_rate = 1e-2f;
+    p->seed = 1337;
+}
+
+static void nrc_free_buffers(wl_nrc *n) {
+    void *ps[] = {n->queries, n->n_queries, n->rec_v, n->rec_tr, n->rec_rb, n->rec_count, n->rec_slot};
+    for (void *p : ps)
+        if (p) cudaFree(p);
+    n->queries = nullptr; n->n_queries = nullptr; n->rec_v = nullptr; n->rec_tr = nullptr;
+    n->rec_rb = nullptr; n->rec_count = nullptr; n->rec_slot = nullptr;
+    n->q_cap = n->t_cap = n->depth_cap = 0;
+}
+
+int wl_nrc_create(wl_context *c, wl_scene *s, const wl_nrc_params *p, wl_nrc **out) {
+    ARG(c && s && p && out, "null argument");
+    ARG(s->ctx == c, "scene must belong to the context");
+    ARG(p->levels >= 1 && p->levels <= 16, "levels must be in [1, 16]");
+    ARG(p->log2_table >= 8 && p->log2_table <= 24, "log2_table must be in [8, 24]");
+    ARG(p->base_resolution >= 2 && p->per_level_scale >= 1.0f && p->per_level_scale <= 4.0f, "bad grid resolution");
+    ARG(p->train_paths >= 1 && p->query_depth >= 1 && p->learning_rate > 0.f, "bad training parameters");
+    CK(cudaSetDevice(c->device));
+    std::vector<float> V(3 * (size_t)s->nV);
+    float lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+    if (s->nV) {
+        CK(cudaMemcpy(V.data(), s->d_V, V.size() * 4, cudaMemcpyDeviceToHost));
+        for (int k = 0; k < 3; k++) { lo[k] = INFINITY; hi[k] = -INFINITY; }
+        for (size_t i = 0; i < s->nV; i++)
+            for (int k = 0; k < 3; k++) {
+                lo[k] = std::fmin(lo[k], V[3 * i + k]);
+                hi[k] = std::fmax(hi[k], V[3 * i + k]);
+            }
+    }
+    wl_nrc *n = new wl_nrc();
+    n->ctx = c;
+    n->scene = s;
+    n->p = *p;
+    std::string err;
+    uint32_t max_samples = 1u << 17;
+    int rc = nrc_create(*p, lo, hi, max_samples, c->stream, &n->net, err);
+    if (rc != WL_OK) {
+        delete n;
+        return fail(rc, err);
+    }
+    c->live_children++;
+    *out = n;
+    return WL_OK;
+}
+
+int wl_nrc_destroy(wl_nrc *n) {
+    if (!n) return WL_OK;
+    cudaSetDevice(n->ctx->device);
+    cudaStreamSynchronize(n->ctx->stream);
+    nrc_free_buffers(n);
+    nrc_free(n->net);
+    n->ctx->live_children--;
+    delete n;
+    return WL_OK;
+}
+
+int wl_nrc_mlp_forward(wl_nrc *n, const float *d_in, float *d_out, uint32_t count) {
+    ARG(n && d_in && d_out, "null argument");
+    CK(cudaSetDevice(n->ctx->device));
+    nrc_forward_raw(n->net, d_in, d_out, count, n->ctx->stream);
+    CK(cudaGetLastError());
+    return WL_OK;
+}
+
+int wl_nrc_train_step(wl_nrc *n, const float *d_in, const float *d_target, uint32_t count, float *loss) {
+    ARG(n && d_in && d_target, "null argument");
+    ARG(count > 0 && count <= nrc_max_samples(n->net), "count out of range");
+    CK(cudaSetDevice(n->ctx->device));
+    nrc_train_raw(n->net, d_in, d_target, count, n->ctx->stream);
+    CK(cudaGetLastError());
+    if (loss) {
+        CK(cudaMemcpyAsync(loss, nrc_loss_ptr(n->net), 4, cudaMemcpyDeviceToHost, n->ctx->stream));
+        CK(cudaStreamSynchronize(n->ctx->stream));
+    }
+    return WL_OK;
+}
+
+int wl_nrc_mlp_gradients(wl_nrc *n, const float *d_in, const float *d_target, uint32_t count, float *grad) {
+    ARG(n && d_in && d_target && grad, "null argument");
+    ARG(count > 0 && count <= nrc_max_samples(n->net), "count out of range");
+    CK(cudaSetDevice(n->ctx->device));
+    nrc_gradients_raw(n->net, d_in, d_target, count, n->ctx->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(grad, nrc_weight_grad(n->net), WL_NRC_WEIGHTS * 4, cudaMemcpyDeviceToHost, n->ctx->stream));
+    CK(cudaStreamSynchronize(n->ctx->stream));
+    return WL_OK;
+}
+
+int wl_nrc_get_weights(wl_nrc *n, float *w) {
+    ARG(n && w, "null argument");
+    CK(cudaSetDevice(n->ctx->device));
+    CK(cudaMemcpyAsync(w, nrc_weights(n->net), WL_NRC_WEIGHTS * 4, cudaMemcpyDeviceToHost, n->ctx->stream));
+    CK(cudaStreamSynchronize(n->ctx->stream));
+    return WL_OK;
+}
+
+int wl_nrc_set_weights(wl_nrc *n, const float *w) {
+    ARG(n && w, "null argument");
+    CK(cudaSetDevice(n->ctx->device));
+    CK(cudaMemcpyAsync(nrc_weights(n->net), w, WL_NRC_WEIGHTS * 4, cudaMemcpyHostToDevice, n->ctx->stream));
+    CK(cudaStreamSynchronize(n->ctx->stream));
+    return WL_OK;
+}
+
+int wl_nrc_stats(wl_nrc *n, uint32_t *samples, uint32_t *queries, float *loss) {
+    ARG(n, "null argument");
+    CK(cudaSetDevice(n->ctx->device));
+    uint32_t cnt[2] = {0, 0}, q = 0;
+    float l = 0.f;
+    CK(cudaMemcpyAsync(cnt, nrc_counters(n->net), 8, cudaMemcpyDeviceToHost, n->ctx->stream));
+    CK(cudaMemcpyAsync(&l, nrc_loss_ptr(n->net), 4, cudaMemcpyDeviceToHost, n->ctx->stream));
+    if (n->n_queries) CK(cudaMemcpyAsync(&q, n->n_queries, 4, cudaMemcpyDeviceToHost, n->ctx->stream));
+    CK(cudaStreamSynchronize(n->ctx->stream));
+    if (samples) *samples = cnt[0] < nrc_max_samples(n->net) ? cnt[0] : nrc_max_samples(n->net);
+    if (queries) *queries = q;
+    if (loss) *loss = l;
+    return WL_OK;
+}
+
+int wl_render_nrc(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_params *p,
+                  wl_nrc *n, wl_film *f) {
+    ARG(c && s && cam && p && n && f, "null argument");
+    ARG(s->ctx == c && f->ctx == c && n->ctx == c && n->scene == s, "objects must belong together");
+    if (!s->built) return fail(WL_ERR_NOT_BUILT, "bvh not built");
+    ARG(p->width == f->f.W && p->height == f->f.H, "film size differs from the render size");
+    ARG(p->spp > 0 && p->max_depth > 0 && p->max_depth <= 1024, "bad spp or max_depth");
+    ARG(p->strategy <= WL_STRATEGY_MIS && p->rng <= WL_RNG_PCG32 && p->math <= WL_MATH_STRICT, "bad params");
+    ARG(p->lights == WL_LIGHTS_UNIFORM, "only uniform light selection is available");
+    ARG(finite3(cam->pos) && finite3(cam->look_at) && finite3(cam->up) && finite3(cam->right), "non-finite camera");
+    CK(cudaSetDevice(c->device));
+    c->stats_pending = false;
+    const uint32_t npix = p->width * p->height;
+    uint64_t want = p->wave_paths ? p->wave_paths : (1ull << 23);
+    uint64_t wave = want < npix ? want : npix;  // one frame at a time
+    int rc = ensure_queues(c, (uint32_t)wave);
+    if (rc != WL_OK) return rc;
+    uint32_t stride = npix / (n->p.train_paths ? n->p.train_paths : 1);
+    if (stride < 1) stride = 1;
+    uint32_t t_cap = (uint32_t)(wave / stride + 2);
+    if (n->q_cap < wave || n->t_cap < t_cap || n->depth_cap < p->max_depth) {
+        nrc_free_buffers(n);
+        cudaError_t e = cudaMalloc(&n->queries, sizeof(NrcVertex) * wave);
+        if (e == cudaSuccess) e = cudaMalloc(&n->n_queries, 256);
+        size_t nr = (size_t)t_cap * p->max_depth;
+        if (e == cudaSuccess) e = cudaMalloc(&n->rec_v, sizeof(NrcVertex) * nr);
+        if (e == cudaSuccess) e = cudaMalloc(&n->rec_tr, sizeof(float4) * nr);
+        if (e == cudaSuccess) e = cudaMalloc(&n->rec_rb, sizeof(float4) * nr);
+        if (e == cudaSuccess) e = cudaMalloc(&n->rec_count, sizeof(uint32_t) * t_cap);
+        if (e == cudaSuccess) e = cudaMalloc(&n->rec_slot, sizeof(uint32_t) * t_cap);
+        if (e != cudaSuccess) {
+            nrc_free_buffers(n);
+            return fail(WL_ERR_OOM, cudaGetErrorString(e));
+        }
+        n->q_cap = (uint32_t)wave;
+        n->t_cap = t_cap;
+        n->depth_cap = p->max_depth;
+    }
+    WaveParams wp{};
+    wp.W = p->width; wp.H = p->height; wp.npix = npix;
+    wp.max_depth = p->max_depth; wp.rr_depth = p->rr_depth;
+    wp.rr_prob = p->rr_prob; wp.eps = p->eps;
+    wp.strategy = p->strategy; wp.rng = p->rng; wp.lights = p->lights; wp.seed = p->seed;
+    for (int k = 0; k < 3; k++) {
+        wp.env[k] = p->env[k];
+        wp.cam_pos[k] = cam->pos[k]; wp.cam_look[k] = cam->look_at[k];
+        wp.cam_up[k] = cam->up[k]; wp.cam_right[k] = cam->right[k];
+    }
+    wp.has_env = (p->env[0] != 0.f || p->env[1] != 0.f || p->env[2] != 0.f) ? 1u : 0u;
+    DevScene sc = dev_scene(s);
+    cudaStream_t st = c->stream;
+    const bool strict_math = p->math == WL_MATH_STRICT;
+    uint32_t *ncnt = nrc_counters(n->net);
+    for (uint32_t fr = 0; fr < p->spp; fr++) {
+        uint32_t frame = p->first_frame + fr;
+        wp.first_frame = frame;
+        // training paths of this frame: pixel indices congruent to an offset that moves each frame
+        uint32_t offset = (uint32_t)(splitmix64(frame * 0x9E3779B97F4A7C15ULL + n->p.seed) % stride);
+        CK(cudaMemsetAsync(ncnt, 0, 8, st));
+        for (uint64_t base = 0; base < npix; base += wave) {
+            wp.base = base;
+            wp.count = (uint32_t)((npix - base) < wave ? (npix - base) : wave);
+            uint64_t first_g = base + ((offset + stride - (base % stride)) % stride);
+            uint32_t tcount = first_g < base + wp.count ? (uint32_t)((base + wp.count - 1 - first_g) / stride + 1) : 0;
+            NrcWaveBuffers nb{};
+            nb.query_depth = n->p.query_depth;
+            nb.train_stride = stride;
+            nb.first_g = first_g;
+            nb.max_depth = p->max_depth;
+            nb.queries = n->queries;
+            nb.n_queries = n->n_queries;
+            nb.rec_v = n->rec_v; nb.rec_tr = n->rec_tr; nb.rec_rb = n->rec_rb;
+            nb.rec_count = n->rec_count; nb.rec_slot = n->rec_slot;
+            CK(cudaMemsetAsync(n->n_queries, 0, 4, st));
+            if (tcount) CK(cudaMemsetAsync(n->rec_count, 0, sizeof(uint32_t) * tcount, st));
+            if (strict_math) strict::launch_generate(wp, c->q, st);
+            else fast::launch_generate(wp, c->q, st);
+            int in = 0;
+            for (uint32_t b = 0; b < p->max_depth; b++) {
+                launch_extend(sc, c->q, in, false, st);
+                CK(cudaMemsetAsync(c->q.counters + (in ^ 1), 0, sizeof(uint32_t), st));
+                CK(cudaMemsetAsync(c->q.counters + 2, 0, sizeof(uint32_t), st));
+                if (strict_math) strict::launch_shade_nrc(wp, sc, c->q, in, nb, st);
+                else fast::launch_shade_nrc(wp, sc, c->q, in, nb, st);
+                launch_shadow(sc, c->q, false, st);
+                in ^= 1;
+            }
+            nrc_query(n->net, s->d_mats, n->queries, n->n_queries, c->q.st_rad, wp.count, st);
+            nrc_collect(n->net, nb, c->q, tcount, st);
+            strict::launch_film(wp, c->q, f->f, st);
+            CK(cudaGetLastError());
+        }
+        // clamp the sample count to the buffer and train one step on the frame's samples
+        nrc_train_collected(n->net, s->d_mats, st);
         CK(cudaGetLastError());
     }
     f->f.frames64 += p->spp;

@@ -75,7 +75,9 @@ __device__ __forceinline__ float tri_area(const DevScene &sc, uint32_t t) {
     return 0.5f * length(cross(b - a, c - a));
 }
 
-__global__ void __launch_bounds__(PT) k_shade(WaveParams wp, DevScene sc, Queues q, int in) {
+template <bool NRC>
+__global__ void __launch_bounds__(PT) k_shade(WaveParams wp, DevScene sc, Queues q, int in,
+                                              NrcWaveBuffers nb) {
     const uint32_t n = q.counters[in];
     const int out = in ^ 1;
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -149,9 +151,37 @@ __global__ void __launch_bounds__(PT) k_shade(WaveParams wp, DevScene sc, Queues
                         if (dot(Ns, dir) > 0.0f) Ns = -Ns;
                     }
                     v3 V = -dir;
-                    v3 ndir = normalize(sample_disney(m, Ns, V, rng));
-                    float pdf = pdf_disney(m, Ns, V, ndir);
-                    if (pdf < 0.0f || isnan(pdf)) {
+                    bool query = false;
+                    if (NRC) {
+                        // radiance cache: training paths record this vertex; other paths stop at
+                        // query_depth and take the cache's prediction of the reflected radiance
+                        bool train = (g % nb.train_stride) == (nb.first_g % nb.train_stride);
+                        v3 T = thr * term;
+                        NrcVertex rv;
+                        rv.pos_mat = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, __uint_as_float(ti.w & 0x7fffffffu));
+                        rv.wo = make_float4(V.x, V.y, V.z, 0.f);
+                        rv.n = make_float4(Ns.x, Ns.y, Ns.z, 0.f);
+                        if (train) {
+                            uint32_t tl = (uint32_t)((g - nb.first_g) / nb.train_stride);
+                            size_t r = (size_t)tl * nb.max_depth + (depth - 1);
+                            rv.extra = make_float4(0.f, 0.f, 0.f, 0.f);
+                            nb.rec_v[r] = rv;
+                            nb.rec_tr[r] = make_float4(T.x, T.y, T.z, 0.f);
+                            nb.rec_rb[r] = make_float4(rad.x, rad.y, rad.z, 0.f);
+                            nb.rec_count[tl] = depth;
+                            nb.rec_slot[tl] = slot;
+                        } else if (depth == nb.query_depth) {
+                            rv.extra = make_float4(T.x, T.y, T.z, __uint_as_float(slot));
+                            uint32_t qi = atomicAdd(nb.n_queries, 1u);
+                            nb.queries[qi] = rv;
+                            query = true;
+                            alive = false;
+                        }
+                    }
+                    v3 ndir = query ? v3(0.f, 0.f, 1.f) : normalize(sample_disney(m, Ns, V, rng));
+                    float pdf = query ? 0.0f : pdf_disney(m, Ns, V, ndir);
+                    if (query) {
+                    } else if (pdf < 0.0f || isnan(pdf)) {
                         alive = false;
                     } else {
                         v3 tex(1.0f);
@@ -253,16 +283,23 @@ void launch_generate(const WaveParams &wp, const Queues &q, cudaStream_t s) {
     k_generate<<<blocks, PT, 0, s>>>(wp, q);
 }
 
+static int shade_grid(const void *k) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, PT, 0);
+    return sms * (per > 0 ? per : 1);
+}
+
 void launch_shade(const WaveParams &wp, const DevScene &sc, const Queues &q, int in, cudaStream_t s) {
-    static int grid = 0;
-    if (!grid) {
-        int dev = 0, sms = 0, per = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_shade, PT, 0);
-        grid = sms * (per > 0 ? per : 1);
-    }
-    k_shade<<<grid, PT, 0, s>>>(wp, sc, q, in);
+    static int grid = shade_grid((const void *)k_shade<false>);
+    k_shade<false><<<grid, PT, 0, s>>>(wp, sc, q, in, NrcWaveBuffers{});
+}
+
+void launch_shade_nrc(const WaveParams &wp, const DevScene &sc, const Queues &q, int in,
+                      const NrcWaveBuffers &nb, cudaStream_t s) {
+    static int grid = shade_grid((const void *)k_shade<true>);
+    k_shade<true><<<grid, PT, 0, s>>>(wp, sc, q, in, nb);
 }
 
 }  // namespace WL_NS

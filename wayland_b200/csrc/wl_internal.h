@@ -88,6 +88,33 @@ struct WaveParams {
     float cam_pos[3], cam_look[3], cam_up[3], cam_right[3];
 };
 
+// Neural radiance cache records (nrc.cu, wl_nrc.cuh): position + material, outgoing direction,
+// shading normal, and either throughput + slot (query) or target radiance (training sample).
+struct NrcVertex {
+    float4 pos_mat;
+    float4 wo;
+    float4 n;
+    float4 extra;
+};
+
+// Cache buffers of one wave of wl_render_nrc. Training paths are the paths whose global index g
+// satisfies g % train_stride == train_offset; local index (g - first_g) / train_stride.
+struct NrcWaveBuffers {
+    uint32_t query_depth, train_stride;
+    uint64_t first_g;
+    uint32_t max_depth;
+    NrcVertex *queries;
+    uint32_t *n_queries;
+    NrcVertex *rec_v;       // [training path][vertex]
+    float4 *rec_tr;         // throughput reaching the vertex
+    float4 *rec_rb;         // path radiance before the vertex's own contributions
+    uint32_t *rec_count;    // vertices recorded per training path
+    uint32_t *rec_slot;     // path slot of the training path
+    NrcVertex *samples;     // training samples of the frame (set by nrc_collect)
+    uint32_t *n_samples;
+    uint32_t max_samples;
+};
+
 // One wave of ambient-occlusion camera samples (ao.cu): slot i is camera sample
 // (base + i) % cs of pixel-frame group (base + i) / cs; a wave holds at most one group per pixel.
 struct AoWave {
@@ -104,10 +131,14 @@ void launch_ao(const AoWave &w, const DevScene &sc, const Queues &q, const Film 
 namespace fast {
 void launch_generate(const WaveParams &wp, const Queues &q, cudaStream_t s);
 void launch_shade(const WaveParams &wp, const DevScene &sc, const Queues &q, int in, cudaStream_t s);
+void launch_shade_nrc(const WaveParams &wp, const DevScene &sc, const Queues &q, int in,
+                      const NrcWaveBuffers &nb, cudaStream_t s);
 }
 namespace strict {
 void launch_generate(const WaveParams &wp, const Queues &q, cudaStream_t s);
 void launch_shade(const WaveParams &wp, const DevScene &sc, const Queues &q, int in, cudaStream_t s);
+void launch_shade_nrc(const WaveParams &wp, const DevScene &sc, const Queues &q, int in,
+                      const NrcWaveBuffers &nb, cudaStream_t s);
 void launch_film(const WaveParams &wp, const Queues &q, const Film &f, cudaStream_t s);
 void launch_tonemap(const Film &f, cudaStream_t s);
 void launch_debug_rng(uint32_t rng, uint64_t seed, const uint32_t *pixels, uint32_t npix,
@@ -139,5 +170,24 @@ struct BvhBuild {
 };
 int bvh_build_lbvh(BvhBuild &b, cudaStream_t s, std::string &err);
 void bvh_free(BvhBuild &b);
+
+// nrc.cu
+struct NrcNet;
+int nrc_create(const wl_nrc_params &p, const float *bbox_lo, const float *bbox_hi,
+               uint32_t max_samples, cudaStream_t s, NrcNet **out, std::string &err);
+void nrc_free(NrcNet *n);
+void nrc_forward_raw(NrcNet *n, const float *in, float *out, uint32_t count, cudaStream_t s);
+void nrc_train_raw(NrcNet *n, const float *in, const float *target, uint32_t count, cudaStream_t s);
+void nrc_gradients_raw(NrcNet *n, const float *in, const float *target, uint32_t count,
+                       cudaStream_t s);
+void nrc_train_collected(NrcNet *n, const wl_disney *mats, cudaStream_t s);
+void nrc_query(NrcNet *n, const wl_disney *mats, const NrcVertex *q, const uint32_t *nq,
+               float4 *rad, uint32_t max_q, cudaStream_t s);
+void nrc_collect(NrcNet *n, NrcWaveBuffers b, const Queues &q, uint32_t tcount, cudaStream_t s);
+float *nrc_weights(NrcNet *n);
+float *nrc_weight_grad(NrcNet *n);
+float *nrc_loss_ptr(NrcNet *n);
+uint32_t *nrc_counters(NrcNet *n);
+uint32_t nrc_max_samples(NrcNet *n);
 
 }  // namespace wl
