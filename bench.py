@@ -28,6 +28,7 @@ sys.path.insert(0, ROOT)
 
 W, H, SPP, DEPTH = 1920, 1080, 64, 16
 METRIC = "Mpaths/s"
+EXTEND_DRAM_BYTES_PER_LAUNCH = 221.2e6
 WORKLOAD = "plain PT at scale: displaced icosphere 1,997,120 tris + ground, 4 quad lights + env 0.1, 1920x1080, 64 spp, depth 16, FP32"
 
 
@@ -343,6 +344,9 @@ def main():
     ap.add_argument("--nrc-only", action="store_true",
                     help="only the radiance-cache convergence comparison (prints its JSON)")
     ap.add_argument("--no-nrc", action="store_true")
+    ap.add_argument("--nrc-res", default="480x270", help="resolution of the radiance-cache comparison")
+    ap.add_argument("--nrc-oracle-spp", type=int, default=16384)
+    ap.add_argument("--nrc-budget-s", type=float, default=60.0)
     ap.add_argument("--case", default="full", choices=["full", "small"],
                     help="small: the same 2M-triangle scene at 960x540 x 4 spp (for ncu captures)")
     args = ap.parse_args()
@@ -364,7 +368,9 @@ def main():
     torch.cuda.set_device(local)
     if args.nrc_only:
         ctx = wl.Context(local)
-        print(json.dumps(nrc_convergence(wl, torch, ctx)), flush=True)
+        w_, h_ = (int(v) for v in args.nrc_res.split("x"))
+        print(json.dumps(nrc_convergence(wl, torch, ctx, res=(w_, h_), oracle_spp=args.nrc_oracle_spp,
+                                         budget_s=args.nrc_budget_s)), flush=True)
         ctx.close()
         return 0
     if world > 1:
@@ -449,10 +455,9 @@ def main():
         b_ray = 48 + 80 * nodes_per + 48 * tris_per
         achieved = segs * b_ray / (ext_ms * 1e-3) / 1e9
         b_path = 96 + 364 * seg_per_path
-        traffic = None
-        tf = os.path.join(ROOT, "profiles", "extend_traffic.json")
-        if os.path.exists(tf):
-            traffic = json.load(open(tf)).get("dram_bytes_per_launch")
+        # DRAM bytes (read + write) per extend launch of this workload, from the ncu launch list
+        # in profiles/launches_plain_pt_displaced_sphere_1920x1080x64spp.md
+        traffic = EXTEND_DRAM_BYTES_PER_LAUNCH if args.case == "full" else None
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 2),

@@ -28,6 +28,7 @@ UNITS = {
     "noalloc.cu": [],
     "ao.cu": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
     "nrc.cu": [],
+    "nrc_tc.cu": [],
 }
 
 

@@ -889,15 +889,16 @@ int wl_nrc_set_weights(wl_nrc *n, const float *w) {
 int wl_nrc_stats(wl_nrc *n, uint32_t *samples, uint32_t *queries, float *loss) {
     ARG(n, "null argument");
     CK(cudaSetDevice(n->ctx->device));
-    uint32_t cnt[2] = {0, 0}, q = 0;
+    uint32_t cnt[3] = {0, 0, 0}, q = 0;
     float l = 0.f;
-    CK(cudaMemcpyAsync(cnt, nrc_counters(n->net), 8, cudaMemcpyDeviceToHost, n->ctx->stream));
+    CK(cudaMemcpyAsync(cnt, nrc_counters(n->net), 12, cudaMemcpyDeviceToHost, n->ctx->stream));
     CK(cudaMemcpyAsync(&l, nrc_loss_ptr(n->net), 4, cudaMemcpyDeviceToHost, n->ctx->stream));
     if (n->n_queries) CK(cudaMemcpyAsync(&q, n->n_queries, 4, cudaMemcpyDeviceToHost, n->ctx->stream));
     CK(cudaStreamSynchronize(n->ctx->stream));
     if (samples) *samples = cnt[0] < nrc_max_samples(n->net) ? cnt[0] : nrc_max_samples(n->net);
     if (queries) *queries = q;
     if (loss) *loss = l;
+    if (cnt[2]) return fail(WL_ERR_TIMEOUT, "radiance-cache tensor-core wait timed out");
     return WL_OK;
 }
 

@@ -63,19 +63,6 @@ __device__ __forceinline__ void load_weights(const float *w, float *sW) {
     __syncthreads();
 }
 
-// raw inputs -> outputs (test entry point)
-__global__ void __launch_bounds__(FT) k_mlp_forward_raw(const float *w, const float *in, float *out,
-                                                         uint32_t n) {
-    extern __shared__ float sW[];
-    load_weights(w, sW);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        float a0[NRC_IN], o[NRC_OUT];
-        for (int k = 0; k < NRC_IN; k++) a0[k] = bf16r(in[(size_t)i * NRC_IN + k]);
-        mlp_forward(sW, a0, nullptr, o);
-        for (int k = 0; k < 4; k++) out[(size_t)i * 4 + k] = o[k];
-    }
-}
-
 // Training forward: activations acts[s][5][64] (layer 0 = input), dL/dout[s][16], loss.
 template <bool ENC>
 __global__ void __launch_bounds__(FT) k_train_fwd(const float *w, NrcGrid g, const wl_disney *mats,
@@ -161,29 +148,50 @@ __global__ void __launch_bounds__(FT) k_train_bwd(const float *w, NrcGrid g, con
 }
 
 // Partial weight gradients over a chunk of samples: layer l < 4 uses deltas[s][l] and acts[s][l];
-// the output layer uses dout and acts[s][4]. Thread t owns output row t / 4 and 16 inputs.
+// the output layer uses dout and acts[s][4]. Sub-tiles of 32 samples are staged in shared
+// memory; thread t owns output row t / 4 and 16 consecutive inputs.
 __global__ void __launch_bounds__(256) k_dw_partial(const uint32_t *n_ptr, uint32_t n_fixed,
                                                     const float *acts, const float *deltas,
                                                     const float *dout, float *partial) {
+    constexpr int SUB = 32;
+    __shared__ float sa[SUB][NRC_HID];
+    __shared__ float sd[SUB][NRC_HID];
     const uint32_t n = n_ptr ? min(*n_ptr, n_fixed) : n_fixed;
     const int layer = blockIdx.y;
     const uint32_t s0 = blockIdx.x * DW_CHUNK;
     const int rows = layer < NRC_HIDDEN_MATS ? NRC_HID : NRC_OUT;
     float *P = partial + (size_t)blockIdx.x * NRC_WEIGHTS + layer * NRC_HID * NRC_HID;
-    for (int task = threadIdx.x; task < rows * 4; task += blockDim.x) {
-        int o = task / 4, i0 = (task % 4) * 16;
-        float acc[16];
-        for (int k = 0; k < 16; k++) acc[k] = 0.0f;
-        for (uint32_t s = s0; s < s0 + DW_CHUNK && s < n; s++) {
-            float d = layer < NRC_HIDDEN_MATS ? deltas[((size_t)s * NRC_HIDDEN_MATS + layer) * NRC_HID + o]
-                                              : dout[(size_t)s * NRC_OUT + o];
-            if (d == 0.0f) continue;
-            const float *a = acts + ((size_t)s * 5 + layer) * NRC_HID + i0;
+    const int t = threadIdx.x;
+    const int o = t / 4, i0 = (t % 4) * 16;
+    const bool own = t < rows * 4;
+    float acc[16];
 #pragma unroll
-            for (int k = 0; k < 16; k++) acc[k] = fmaf(d, a[k], acc[k]);
+    for (int k = 0; k < 16; k++) acc[k] = 0.0f;
+    const uint32_t s_end = min(s0 + DW_CHUNK, n);
+    for (uint32_t sub = s0; sub < s_end; sub += SUB) {
+        for (int k = t; k < SUB * NRC_HID; k += blockDim.x) {
+            uint32_t s = sub + k / NRC_HID;
+            int c = k % NRC_HID;
+            sa[k / NRC_HID][c] = s < s_end ? acts[((size_t)s * 5 + layer) * NRC_HID + c] : 0.0f;
+            float d = 0.0f;
+            if (s < s_end && c < rows)
+                d = layer < NRC_HIDDEN_MATS ? deltas[((size_t)s * NRC_HIDDEN_MATS + layer) * NRC_HID + c]
+                                            : dout[(size_t)s * NRC_OUT + c];
+            sd[k / NRC_HID][c] = d;
         }
-        for (int k = 0; k < 16; k++) P[o * NRC_HID + i0 + k] = acc[k];
+        __syncthreads();
+        if (own) {
+#pragma unroll 4
+            for (int j = 0; j < SUB; j++) {
+                float d = sd[j][o];
+#pragma unroll
+                for (int k = 0; k < 16; k++) acc[k] = fmaf(d, sa[j][i0 + k], acc[k]);
+            }
+        }
+        __syncthreads();
     }
+    if (own)
+        for (int k = 0; k < 16; k++) P[o * NRC_HID + i0 + k] = acc[k];
 }
 
 __global__ void k_dw_reduce(const float *partial, uint32_t chunks, float *grad) {
@@ -206,27 +214,6 @@ __global__ void k_adam(float *p, float *g, float *m, float *v, size_t count, flo
         v[i] = vi;
         p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
         if (zero) g[i] = 0.0f;
-    }
-}
-
-// Cache queries of the render loop: radiance[slot] += throughput * max(prediction, 0).
-__global__ void __launch_bounds__(FT) k_nrc_query(const float *w, NrcGrid g, const wl_disney *mats,
-                                                   const NrcVertex *q, const uint32_t *nq,
-                                                   float4 *rad) {
-    extern __shared__ float sW[];
-    load_weights(w, sW);
-    const uint32_t n = *nq;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        NrcVertex v = q[i];
-        float a0[NRC_IN], o[NRC_OUT];
-        nrc_encode(g, mats, v, a0);
-        mlp_forward(sW, a0, nullptr, o);
-        uint32_t slot = __float_as_uint(v.extra.w);
-        float4 r = rad[slot];
-        r.x += v.extra.x * fmaxf(o[0], 0.0f);
-        r.y += v.extra.y * fmaxf(o[1], 0.0f);
-        r.z += v.extra.z * fmaxf(o[2], 0.0f);
-        rad[slot] = r;
     }
 }
 
@@ -364,12 +351,10 @@ int nrc_create(const wl_nrc_params &p, const float *bbox_lo, const float *bbox_h
     static bool attr = false;
     if (!attr) {
         size_t sm = NRC_WEIGHTS * sizeof(float);
-        cudaFuncSetAttribute(k_mlp_forward_raw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         cudaFuncSetAttribute(k_train_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         cudaFuncSetAttribute(k_train_fwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         cudaFuncSetAttribute(k_train_bwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         cudaFuncSetAttribute(k_train_bwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        cudaFuncSetAttribute(k_nrc_query, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         attr = true;
     }
     *out = n;
@@ -379,10 +364,7 @@ int nrc_create(const wl_nrc_params &p, const float *bbox_lo, const float *bbox_h
 static const size_t WSMEM = NRC_WEIGHTS * sizeof(float);
 
 void nrc_forward_raw(NrcNet *n, const float *in, float *out, uint32_t count, cudaStream_t s) {
-    uint32_t blocks = (count + FT - 1) / FT;
-    if (blocks > (uint32_t)n->grid_blocks) blocks = n->grid_blocks;
-    if (blocks == 0) blocks = 1;
-    k_mlp_forward_raw<<<blocks, FT, WSMEM, s>>>(n->w, in, out, count);
+    nrc_tc_forward_raw(n->w, in, out, count, n->counters + 2, s);
 }
 
 // Forward + backward + weight gradients for `count` rows (raw inputs) or for the samples
@@ -442,10 +424,7 @@ void nrc_train_collected(NrcNet *n, const wl_disney *mats, cudaStream_t s) {
 
 void nrc_query(NrcNet *n, const wl_disney *mats, const NrcVertex *q, const uint32_t *nq,
                float4 *rad, uint32_t max_q, cudaStream_t s) {
-    uint32_t blocks = (max_q + FT - 1) / FT;
-    if (blocks > (uint32_t)n->grid_blocks) blocks = n->grid_blocks;
-    if (blocks == 0) blocks = 1;
-    k_nrc_query<<<blocks, FT, WSMEM, s>>>(n->w, n->grid, mats, q, nq, rad);
+    nrc_tc_query(n->w, n->grid, mats, q, nq, rad, max_q, n->counters + 2, s);
 }
 
 void nrc_collect(NrcNet *n, NrcWaveBuffers b, const Queues &q, uint32_t tcount, cudaStream_t s) {

@@ -1,0 +1,266 @@
+// nrc_tc.cu - radiance-cache MLP inference on the 5th-generation tensor cores (sm_100a).
+//
+// One CTA of 128 threads (4 warps) processes tiles of 128 rows. The bfloat16 weights and the
+// current activation tile live in shared memory in the canonical K-major layout without
+// swizzle (8-row x 16-byte core matrices; adjacent K core matrices 128 B apart, adjacent 8-row
+// groups 1024 B apart). Per layer, one thread issues four tcgen05.mma (M=128, N=64 or 16,
+// K=16, bf16 x bf16 -> fp32) accumulating in tensor memory and commits them to an mbarrier;
+// every warp then reads its 32 rows back with tcgen05.ld (thread t owns row t), applies ReLU,
+// rounds to bfloat16 and writes the next layer's input tile. Waits on the mbarrier are bounded:
+// a timeout sets the error word, waits once more, frees the tensor memory and returns.
+#include <cuda_bf16.h>
+
+#include "wl_internal.h"
+#include "wl_nrc.cuh"
+
+namespace wl {
+
+namespace {
+
+constexpr int TC_THREADS = 128;
+constexpr uint32_t TMEM_COLS = 64;
+constexpr uint32_t WAIT_LIMIT = 1u << 22;
+// shared-memory layout (bytes)
+constexpr uint32_t SM_W = 0;                        // W0..W3, 8 KB each
+constexpr uint32_t SM_W4 = 4 * 8192;                // W4 (16 x 64), 2 KB
+constexpr uint32_t SM_A = SM_W4 + 2048;             // activation tile 128 x 64, 16 KB
+constexpr uint32_t SM_BAR = SM_A + 16384;           // mbarrier
+constexpr uint32_t SM_TMEM = SM_BAR + 8;            // tensor-memory address
+constexpr uint32_t SM_BYTES = SM_TMEM + 8;
+
+// byte offset of element (r, k) in a K-major tile with 64 columns
+__device__ __forceinline__ uint32_t kmaj(uint32_t r, uint32_t k) {
+    return (r >> 3) * 1024u + (k >> 3) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
+}
+
+// shared-memory matrix descriptor: start address, leading (K) byte offset 128, stride (8-row
+// group) byte offset 1024, descriptor version 1, no swizzle
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) |
+           ((uint64_t)(1024u >> 4) << 32) | (1ull << 46);
+}
+
+// instruction descriptor: F32 accumulate, A and B bfloat16, both K-major, N and M
+__host__ __device__ constexpr uint32_t idesc(uint32_t n, uint32_t m) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((m >> 4) << 24);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t id,
+                                         uint32_t accumulate) {
+    uint32_t z = 0;
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
+        "}\n" ::"r"(d_tmem),
+        "l"(a), "l"(b), "r"(id), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+    for (uint32_t it = 0; it < WAIT_LIMIT; it++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t"
+            ".reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t"
+            "}\n"
+            : "=r"(ok)
+            : "r"(bar), "r"(phase)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+          "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// write row r (64 values, rounded to bfloat16) of a K-major tile
+__device__ __forceinline__ void store_row(uint8_t *tile, uint32_t r, const float *x) {
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        __nv_bfloat162 p0 = __floats2bfloat162_rn(x[8 * c + 0], x[8 * c + 1]);
+        __nv_bfloat162 p1 = __floats2bfloat162_rn(x[8 * c + 2], x[8 * c + 3]);
+        __nv_bfloat162 p2 = __floats2bfloat162_rn(x[8 * c + 4], x[8 * c + 5]);
+        __nv_bfloat162 p3 = __floats2bfloat162_rn(x[8 * c + 6], x[8 * c + 7]);
+        uint4 u;
+        u.x = *reinterpret_cast<uint32_t *>(&p0);
+        u.y = *reinterpret_cast<uint32_t *>(&p1);
+        u.z = *reinterpret_cast<uint32_t *>(&p2);
+        u.w = *reinterpret_cast<uint32_t *>(&p3);
+        *reinterpret_cast<uint4 *>(tile + kmaj(r, 8 * c)) = u;
+    }
+}
+
+// MODE 0: raw rows in[n][64] -> out[n][4]. MODE 1: cache queries of the render loop.
+template <int MODE>
+__global__ void __launch_bounds__(TC_THREADS) k_mlp_tc(const float *w, NrcGrid g, const wl_disney *mats,
+                                                        const NrcVertex *q, const uint32_t *nq,
+                                                        float4 *rad, const float *in, float *out,
+                                                        uint32_t n_raw, uint32_t *err) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t bar = smem_u32(smem + SM_BAR);
+    // weights -> bfloat16 K-major tiles
+    for (uint32_t i = tid; i < (uint32_t)NRC_WEIGHTS; i += TC_THREADS) {
+        uint32_t l = i / 4096u, rem = i % 4096u;
+        uint32_t r = rem / 64u, k = rem % 64u;
+        uint8_t *base = l < 4 ? smem + SM_W + l * 8192u : smem + SM_W4;
+        *reinterpret_cast<__nv_bfloat16 *>(base + kmaj(r, k)) = __float2bfloat16_rn(w[i]);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(smem + SM_TMEM)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    fence_async_smem();
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t *>(smem + SM_TMEM);
+    const uint32_t lane_base = (warp * 32u) << 16;
+    const uint32_t n = MODE == 0 ? n_raw : *nq;
+    const uint32_t aA = smem_u32(smem + SM_A);
+    uint32_t phase = 0;
+    bool ok = true;
+    for (uint32_t tile = blockIdx.x * TC_THREADS; tile < n && ok; tile += gridDim.x * TC_THREADS) {
+        const uint32_t i = tile + tid;
+        const bool valid = i < n;
+        float x[NRC_IN];
+        NrcVertex v;
+        if (valid) {
+            if (MODE == 0) {
+                for (int k = 0; k < NRC_IN; k++) x[k] = in[(size_t)i * NRC_IN + k];
+            } else {
+                v = q[i];
+                nrc_encode(g, mats, v, x);
+            }
+        } else {
+            for (int k = 0; k < NRC_IN; k++) x[k] = 0.0f;
+        }
+        store_row(smem + SM_A, tid, x);
+        fence_async_smem();
+        tc_before_sync();
+        __syncthreads();
+        tc_after_sync();
+        for (int layer = 0; layer < 5 && ok; layer++) {
+            const uint32_t wB = smem_u32(smem + (layer < 4 ? SM_W + layer * 8192u : SM_W4));
+            const uint32_t id = layer < 4 ? idesc(64, 128) : idesc(16, 128);
+            if (tid == 0) {
+#pragma unroll
+                for (uint32_t ks = 0; ks < 4; ks++)
+                    mma_bf16(tmem, sdesc(aA + ks * 256u), sdesc(wB + ks * 256u), id, ks > 0 ? 1u : 0u);
+                mma_commit(bar);
+            }
+            bool got = mbar_wait(bar, phase);
+            phase ^= 1u;
+            ok = __syncthreads_and(got) != 0;
+            tc_after_sync();
+            if (!ok) break;
+            if (layer < 4) {
+                float h[NRC_HID];
+#pragma unroll
+                for (int c = 0; c < 4; c++) tmem_ld16(tmem + lane_base + 16u * c, h + 16 * c);
+                tmem_wait_ld();
+#pragma unroll
+                for (int k = 0; k < NRC_HID; k++) h[k] = fmaxf(h[k], 0.0f);
+                store_row(smem + SM_A, tid, h);
+                fence_async_smem();
+            } else {
+                float o[16];
+                tmem_ld16(tmem + lane_base, o);
+                tmem_wait_ld();
+                if (valid) {
+                    if (MODE == 0) {
+                        for (int c = 0; c < 4; c++) out[(size_t)i * 4 + c] = o[c];
+                    } else {
+                        uint32_t slot = __float_as_uint(v.extra.w);
+                        float4 r = rad[slot];
+                        r.x += v.extra.x * fmaxf(o[0], 0.0f);
+                        r.y += v.extra.y * fmaxf(o[1], 0.0f);
+                        r.z += v.extra.z * fmaxf(o[2], 0.0f);
+                        rad[slot] = r;
+                    }
+                }
+            }
+            tc_before_sync();
+            __syncthreads();
+            tc_after_sync();
+        }
+    }
+    if (!ok) {
+        if (tid == 0) atomicExch(err, 1u);
+        // let the tensor-core work still in flight (the phase that timed out) finish before the
+        // memory is released
+        mbar_wait(bar, phase ^ 1u);
+    }
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+}
+
+int tc_grid(const void *k) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BYTES);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, TC_THREADS, SM_BYTES);
+    if (per < 1) per = 1;
+    if (per > 4) per = 4;  // 4 x 64 tensor-memory columns per SM
+    return sms * per;
+}
+
+}  // namespace
+
+void nrc_tc_forward_raw(const float *w, const float *in, float *out, uint32_t n, uint32_t *err,
+                        cudaStream_t s) {
+    static int grid = tc_grid((const void *)k_mlp_tc<0>);
+    uint32_t tiles = (n + TC_THREADS - 1) / TC_THREADS;
+    uint32_t blocks = tiles < (uint32_t)grid ? tiles : (uint32_t)grid;
+    if (blocks == 0) return;
+    k_mlp_tc<0><<<blocks, TC_THREADS, SM_BYTES, s>>>(w, NrcGrid{}, nullptr, nullptr, nullptr, nullptr,
+                                                      in, out, n, err);
+}
+
+void nrc_tc_query(const float *w, const NrcGrid &g, const wl_disney *mats, const NrcVertex *q,
+                  const uint32_t *nq, float4 *rad, uint32_t max_q, uint32_t *err, cudaStream_t s) {
+    static int grid = tc_grid((const void *)k_mlp_tc<1>);
+    uint32_t tiles = (max_q + TC_THREADS - 1) / TC_THREADS;
+    uint32_t blocks = tiles < (uint32_t)grid ? tiles : (uint32_t)grid;
+    if (blocks == 0) blocks = 1;
+    k_mlp_tc<1><<<blocks, TC_THREADS, SM_BYTES, s>>>(w, g, mats, q, nq, rad, nullptr, nullptr, 0, err);
+}
+
+}  // namespace wl

@@ -189,5 +189,11 @@ float *nrc_weight_grad(NrcNet *n);
 float *nrc_loss_ptr(NrcNet *n);
 uint32_t *nrc_counters(NrcNet *n);
 uint32_t nrc_max_samples(NrcNet *n);
+// nrc_tc.cu (tensor-core inference)
+struct NrcGrid;
+void nrc_tc_forward_raw(const float *w, const float *in, float *out, uint32_t n, uint32_t *err,
+                        cudaStream_t s);
+void nrc_tc_query(const float *w, const NrcGrid &g, const wl_disney *mats, const NrcVertex *q,
+                  const uint32_t *nq, float4 *rad, uint32_t max_q, uint32_t *err, cudaStream_t s);
 
 }  // namespace wl
