@@ -51,8 +51,14 @@ enum {
 
 /* ---- enums ------------------------------------------------------------------------- */
 /* Integrator strategy: PathTracing.cu:21-29 (UPT = BSDF sampling only, NEE = light sampling
- * only, MIS = both with the balance heuristic). */
-enum { WL_STRATEGY_UPT = 0, WL_STRATEGY_NEE = 1, WL_STRATEGY_MIS = 2 };
+ * only, MIS = both with the balance heuristic). BDPT selects the bidirectional program
+ * (Programs/BDPT/BDPT.cu:42-567): an eye subpath and a light subpath of at most max_depth
+ * vertices each (the reference's 10; at most WL_BDPT_MAX_VERTICES), every eye vertex connected
+ * to every light vertex with a visibility ray, balance-heuristic MIS over all strategies
+ * (BDPT.cu:19-29: USE_UPT, balance heuristic). rr_depth, rr_prob and env do not apply to it,
+ * and its film keeps the reference's FP32 running mean (BDPT.cu:548-556). */
+enum { WL_STRATEGY_UPT = 0, WL_STRATEGY_NEE = 1, WL_STRATEGY_MIS = 2, WL_STRATEGY_BDPT = 3 };
+#define WL_BDPT_MAX_VERTICES 10u
 
 /* Per-path random stream.
  *  TEA_LCG: seed = tea<4>(pixelIndex, frameID), then LCG (Random.h:34-71), the reference's.

@@ -278,6 +278,20 @@ class Oracle:
         del keep
         return film, f64, rays
 
+    def render_bdpt(self, scene, cam, params, prec=0, threads=0, film=None, want64=False):
+        """Bidirectional path tracer (BDPT.cu:42-567); returns (film_rgb[H,W,3] f32, film64 or
+        None, rays)."""
+        W, H = params.width, params.height
+        film = np.zeros((H, W, 3), np.float32) if film is None else film
+        f64 = np.zeros((H, W, 3), np.float64) if want64 else None
+        b = self.bvh_for(scene)
+        keep, osc = make_or_scene(scene)
+        self.lib.or_render_bdpt.restype = C.c_uint64
+        rays = self.lib.or_render_bdpt(C.byref(osc), b.handle, C.byref(cam), C.byref(params), prec,
+                                       threads, ptr(film), ptr(f64))
+        del keep
+        return film, f64, rays
+
     def bvh_for(self, scene):
         key = id(scene)
         c = self.__dict__.setdefault("_bvh_cache", {})
@@ -400,3 +414,20 @@ class RefLib:
         finally:
             self.lib.or_bvh_destroy(h)
         return film, segs
+
+    def render_bdpt(self, scene, cam, W, H, spp, first_frame=0, threads=0, radiance=None):
+        """The reference's BDPT program (Programs/BDPT/BDPT.cu, run over the OptiX host emulation).
+        Returns the reference's radiance buffer [H, W, 4] (FP32 running mean)."""
+        rad = np.zeros((H, W, 4), np.float32) if radiance is None else radiance
+        keep, osc = make_or_scene(scene)
+        h = self.lib.or_bvh_create(osc.V, osc.I, osc.nT)
+        L = self.lib
+        L.ref_render_bdpt.restype = C.c_uint64
+        L.ref_render_bdpt.argtypes = [C.POINTER(OrScene), C.c_void_p, C.POINTER(Camera), C.c_uint32,
+                                      C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_void_p]
+        try:
+            L.ref_render_bdpt(C.byref(osc), h, C.byref(cam), W, H, spp, first_frame, threads, ptr(rad))
+        finally:
+            self.lib.or_bvh_destroy(h)
+        del keep
+        return rad

@@ -8,6 +8,8 @@
 #define __device__
 #define __forceinline__ inline
 #define __inline__ inline
+#define __global__
+#define __constant__
 struct float2 { float x, y; };
 struct float3 { float x, y, z; };
 struct float4 { float x, y, z, w; };

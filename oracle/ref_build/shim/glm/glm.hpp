@@ -38,6 +38,7 @@ template <class T> struct tvec4 {
     tvec4(T a, T b, T c, T d) : x(a), y(b), z(c), w(d) {}
     explicit tvec4(T s) : x(s), y(s), z(s), w(s) {}
     tvec4(const tvec3<T> &v, T d) : x(v.x), y(v.y), z(v.z), w(d) {}
+    template <class U> tvec4(const tvec4<U> &v) : x((T)v.x), y((T)v.y), z((T)v.z), w((T)v.w) {}
 };
 
 template <class T> tvec3<T> operator+(const tvec3<T> &a, const tvec3<T> &b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
@@ -57,6 +58,9 @@ template <class T> tvec3<T> operator-(const tvec3<T> &a, typename ident<T>::type
 template <class T> tvec3<T> operator-(typename ident<T>::type s, const tvec3<T> &a) { return {s - a.x, s - a.y, s - a.z}; }
 
 template <class T> tvec2<T> operator*(const tvec2<T> &a, typename ident<T>::type s) { return {a.x * s, a.y * s}; }
+template <class T> tvec2<T> operator+(const tvec2<T> &a, const tvec2<T> &b) { return {a.x + b.x, a.y + b.y}; }
+template <class T> tvec4<T> operator*(const tvec4<T> &a, typename ident<T>::type s) { return {a.x * s, a.y * s, a.z * s, a.w * s}; }
+template <class T> tvec4<T> operator+(const tvec4<T> &a, const tvec4<T> &b) { return {a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w}; }
 
 template <class T> T dot(const tvec3<T> &a, const tvec3<T> &b) {
     tvec3<T> t = a * b;

@@ -1152,6 +1152,351 @@ double ao_frame(const SceneView &sv, const wl_camera &cam, const wl_ao_params &P
     return acc;  // AO.cu keeps the frame value in double (glm::dvec4 thisFrame)
 }
 
+// ---------------------------------------------------------------------------------------
+// Bidirectional path tracer: Programs/BDPT/BDPT.cu:42-567 restated over the flattened scene.
+// A subpath vertex (BDPT.h BDPTVertex without the texture colour, which is 1 for every triangle
+// of a flattened scene): the light vertex of the light subpath has mat == nullptr and light >= 0.
+template <class T> struct BdVertex {
+    V3<T> pos, ns, ng, wi, tput;
+    const wl_disney *mat;
+    int32_t light;
+    T pdf, pdf_inv, pdf_light;
+};
+
+// ComputePdfForward (BDPT.cu:42-50): area-measure pdf of reaching `next` from `mid` by BSDF
+// sampling with incoming direction wi.
+template <class T> T bd_pdf_forward(V3<T> wi, const BdVertex<T> &mid, const BdVertex<T> &next) {
+    V3<T> d = next.pos - mid.pos;
+    T dist = length(d);
+    d = d / dist;
+    T p = pdf_disney(to_mat<T>(*mid.mat), mid.ns, mid.ng, wi, d);
+    return clampf(p, K(1e-30), K(1e30)) * std::fabs(dot(next.ns, d)) / (dist * dist);
+}
+
+// ComputePdfLightDir (BDPT.cu:52-58): cosine emission from light vertex l towards e, area measure.
+template <class T> T bd_pdf_light_dir(const BdVertex<T> &l, const BdVertex<T> &e) {
+    V3<T> d = e.pos - l.pos;
+    T dist = length(d);
+    d = d / dist;
+    return dot(d, l.ns) * C<T>::recip_pi() * std::fabs(dot(d, e.ns)) / (dist * dist);
+}
+
+// MISweight (BDPT.cu:61-217) with the reference's settings: USE_UPT, not PT_MODE, balance
+// heuristic. lightEnd == -1 is the eye path that reached a light (E[eyeEnd] is the light
+// vertex, Lp points at it).
+template <class T>
+T bd_mis_weight(const BdVertex<T> *E, const BdVertex<T> *Lp, int eyeEnd, int lightEnd) {
+    const int strategies = eyeEnd + lightEnd + 1 + 1;
+    T fwd[2 * WL_BDPT_MAX_VERTICES], inv[2 * WL_BDPT_MAX_VERTICES];
+    int nf = 0, ni = 0;
+    if (lightEnd == -1) {
+        for (int i = 1; i <= eyeEnd; ++i) {
+            fwd[nf++] = E[i].pdf;
+            inv[ni++] = E[i].pdf_inv;
+        }
+    } else if (eyeEnd == 0 && lightEnd == 0) {
+        const BdVertex<T> &e = E[0], &l = Lp[0];
+        fwd[nf++] = bd_pdf_forward(e.wi, e, l);
+        inv[ni++] = bd_pdf_light_dir(l, e);
+    } else if (eyeEnd == 0) {
+        const BdVertex<T> &e = E[0], &l = Lp[lightEnd], &ll = Lp[lightEnd - 1];
+        V3<T> d = normalize(l.pos - e.pos);
+        T p_el = bd_pdf_forward(e.wi, e, l);
+        T p_le = bd_pdf_forward(l.wi, l, e);
+        T p_ll = bd_pdf_forward(-d, l, ll);
+        fwd[nf++] = p_el;
+        inv[ni++] = p_le;
+        fwd[nf++] = p_ll;
+        inv[ni++] = ll.pdf_inv;
+        for (int i = lightEnd - 2; i >= 0; --i) {
+            fwd[nf++] = Lp[i].pdf;
+            inv[ni++] = Lp[i].pdf_inv;
+        }
+    } else if (lightEnd == 0) {
+        const BdVertex<T> &ee = E[eyeEnd - 1], &e = E[eyeEnd], &l = Lp[0];
+        V3<T> d = normalize(l.pos - e.pos);
+        T p_ee = bd_pdf_forward(d, e, ee);
+        T p_el = bd_pdf_forward(e.wi, e, l);
+        T p_le = bd_pdf_light_dir(l, e);
+        for (int i = 1; i < eyeEnd; ++i) {
+            fwd[nf++] = E[i].pdf;
+            inv[ni++] = E[i].pdf_inv;
+        }
+        fwd[nf++] = e.pdf;
+        inv[ni++] = p_ee;
+        fwd[nf++] = p_el;
+        inv[ni++] = p_le;
+    } else {
+        const BdVertex<T> &ee = E[eyeEnd - 1], &e = E[eyeEnd];
+        const BdVertex<T> &l = Lp[lightEnd], &ll = Lp[lightEnd - 1];
+        V3<T> d = normalize(l.pos - e.pos);
+        T p_ee = bd_pdf_forward(d, e, ee);
+        T p_el = bd_pdf_forward(e.wi, e, l);
+        T p_le = bd_pdf_forward(l.wi, l, e);
+        T p_ll = bd_pdf_forward(-d, l, ll);
+        for (int i = 1; i < eyeEnd; ++i) {
+            fwd[nf++] = E[i].pdf;
+            inv[ni++] = E[i].pdf_inv;
+        }
+        fwd[nf++] = e.pdf;
+        inv[ni++] = p_ee;
+        fwd[nf++] = p_el;
+        inv[ni++] = p_le;
+        fwd[nf++] = p_ll;
+        inv[ni++] = ll.pdf_inv;
+        for (int i = lightEnd - 2; i >= 0; --i) {
+            fwd[nf++] = Lp[i].pdf;
+            inv[ni++] = Lp[i].pdf_inv;
+        }
+    }
+    inv[ni++] = Lp[0].pdf_light;
+    T den = T(1), tmp = T(1);
+    for (int i = eyeEnd - 1; i >= 0; --i) {
+        tmp *= inv[i + 1] / fwd[i];
+        den += tmp;
+    }
+    tmp = T(1);
+    for (int i = eyeEnd + 1; i < strategies; ++i) {
+        tmp *= fwd[i - 1] / inv[i];
+        den += tmp;
+    }
+    T w = T(1) / den;
+    if (w < T(0) || std::isnan(w) || std::isinf(w)) return T(0);
+    return w;
+}
+
+// Surface record of a closest hit (__closesthit__radiance, BDPT.cu:581-640): geometric and
+// shading normals, flipped towards the ray unless the triangle is an emitter or transmissive.
+template <class T> struct BdHit {
+    V3<T> pos, ns, ng;
+    int32_t light;
+    const wl_disney *mat;
+};
+template <class T>
+BdHit<T> bd_surface(const SceneView &sv, const wl_hit &hit, V3<T> org, V3<T> dir) {
+    const or_scene *s = sv.s;
+    uint32_t prim = hit.prim;
+    V3<T> a = vload<T>(s->V, s->I[3 * prim]), b = vload<T>(s->V, s->I[3 * prim + 1]),
+          c = vload<T>(s->V, s->I[3 * prim + 2]);
+    BdHit<T> h;
+    h.ng = normalize(cross(b - a, c - a));
+    if (tri_has_normal(s, prim)) {
+        T bu = T(hit.u), bv = T(hit.v);
+        h.ns = normalize(vload<T>(s->N, s->I[3 * prim]) * (T(1) - bu - bv) +
+                         vload<T>(s->N, s->I[3 * prim + 1]) * bu + vload<T>(s->N, s->I[3 * prim + 2]) * bv);
+    } else {
+        h.ns = h.ng;
+    }
+    h.pos = org + dir * T(hit.t);
+    uint32_t lid = sv.tri_light[prim];
+    h.light = lid == INVALID ? -1 : (int32_t)lid;
+    h.mat = &s->mats[s->tri_material[prim]];
+    if (h.light < 0 && to_mat<T>(*h.mat).trans < K(0.1)) {
+        if (dot(h.ng, dir) > T(0)) h.ng = -h.ng;
+        if (dot(h.ns, dir) > T(0)) h.ns = -h.ns;
+    }
+    return h;
+}
+
+template <class T> bool bd_cast(const SceneView &sv, V3<T> o, V3<T> d, float tmin, float tmax,
+                                uint32_t mode, wl_hit &hit) {
+    wl_ray r;
+    r.org[0] = (float)o.x; r.org[1] = (float)o.y; r.org[2] = (float)o.z;
+    r.dir[0] = (float)d.x; r.dir[1] = (float)d.y; r.dir[2] = (float)d.z;
+    r.tmin = tmin;
+    r.tmax = tmax;
+    obvh_cast_one(*sv.bvh, r, mode, hit);
+    return hit.prim != INVALID;
+}
+
+// TraceEyeSubpath (BDPT.cu:219-336). Returns the number of stored eye vertices; `radiance`
+// receives the light reached by the eye path itself (MIS-weighted after the first bounce).
+template <class T>
+uint32_t bd_eye(const SceneView &sv, const wl_camera &cam, const wl_render_params &P, uint32_t px,
+                uint32_t py, Rng &rng, BdVertex<T> *E, V3<T> &radiance, uint64_t &rays) {
+    const or_scene *s = sv.s;
+    V3<T> org(cam.pos[0], cam.pos[1], cam.pos[2]);
+    V3<T> lookat(cam.look_at[0], cam.look_at[1], cam.look_at[2]);
+    V3<T> right(cam.right[0], cam.right[1], cam.right[2]), up(cam.up[0], cam.up[1], cam.up[2]);
+    T cu = T(2) * (T(px) + T(rng.next())) / T(P.width) - T(1);
+    T cv = T(2) * (T(py) + T(rng.next())) / T(P.height) - T(1);
+    V3<T> dir = normalize(lookat + right * cu + up * cv);
+    uint32_t depth = 0;
+    bool hit_light = false;
+    T rr_k = T(1);
+    while (depth < P.max_depth) {
+        wl_hit hit;
+        rays++;
+        if (!bd_cast(sv, org, dir, P.eps, 1e30f, WL_CAST_CLOSEST, hit)) break;
+        depth += 1;
+        BdHit<T> h = bd_surface(sv, hit, org, dir);
+        hit_light = h.light >= 0;
+        const uint32_t v = depth - 1;
+        BdVertex<T> &e = E[v];
+        e.pos = h.pos; e.ns = h.ns; e.ng = h.ng; e.wi = -dir;
+        e.mat = h.mat; e.light = h.light;
+        e.pdf = T(0); e.pdf_light = T(0); e.pdf_inv = T(0);
+        if (v == 0) {
+            e.tput = V3<T>(T(1));
+            e.pdf = T(1);
+        } else {
+            const BdVertex<T> &le = E[v - 1];
+            Mat<T> lm = to_mat<T>(*le.mat);
+            V3<T> f = eval_disney(lm, le.ns, le.ng, le.wi, dir, V3<T>(T(1)));
+            T cosw = dot(dir, le.ns);
+            T pdf = clampf(pdf_disney(lm, le.ns, le.ng, le.wi, dir), K(1e-30), K(1e30));
+            e.tput = le.tput * clampv(f, T(0), K(1e30)) * std::fabs(cosw) / pdf * rr_k;
+            V3<T> d = e.pos - le.pos;
+            e.pdf = pdf * std::fabs(dot(e.wi, e.ns)) / dot(d, d);
+        }
+        if (v >= 2) E[v - 1].pdf_inv = bd_pdf_forward(-e.wi, E[v - 1], E[v - 2]);
+        if (hit_light) {
+            const wl_area_light &lt = s->lights[h.light];
+            if (!lt.two_sided && dot(e.ns, dir) > T(0)) break;
+            V3<T> L(lt.L[0], lt.L[1], lt.L[2]);
+            if (v == 0) {
+                radiance = L;
+            } else {
+                e.pdf_inv = bd_pdf_light_dir(e, E[v - 1]);
+                // PdfAreaLightPos (Pdf.h:18-26) of the hit triangle
+                T lp = T(1) / T(s->nLight);
+                lp /= T(lt.tri_count);
+                lp /= tri_area<T>(s, hit.prim);
+                e.pdf_light = lp;
+                radiance = L * e.tput * bd_mis_weight(E, &e, (int)v, -1);
+            }
+            break;
+        }
+        // Russian roulette (BDPT.cu:315-325); never reached with at most 10 vertices
+        T rr_rate = clampf(K(1.2) - T(depth) * K(0.5), K(0.1), T(1));
+        rr_k = T(1);
+        if (depth > 10) {
+            if (T(rng.next()) > rr_rate) break;
+            rr_k = T(1) / rr_rate;
+        }
+        dir = normalize(sample_disney(to_mat<T>(*e.mat), e.ns, e.ng, e.wi, rng));
+        org = e.pos;
+    }
+    return hit_light ? depth - 1 : depth;
+}
+
+// TraceLightSubpath (BDPT.cu:338-452). Returns the number of light-subpath vertices (the
+// light vertex included).
+template <class T>
+uint32_t bd_light(const SceneView &sv, const wl_render_params &P, Rng &rng, BdVertex<T> *Lp,
+                  uint64_t &rays) {
+    const or_scene *s = sv.s;
+    V3<T> lpos, lN;
+    T lpdf;
+    uint32_t lid;
+    sample_light(sv, rng, lpos, lN, lpdf, lid);
+    // SampleCosineHemisphere with pdf (Sample.h:55-66) around the light normal
+    V3<T> x, y;
+    onb(lN, x, y);
+    T r = std::sqrt(T(rng.next()));
+    T theta = T(rng.next()) * C<T>::two_pi();
+    T dx = r * m_cos(theta), dy = r * m_sin(theta);
+    T z = std::sqrt(T(1) - dx * dx - dy * dy);
+    T dir_pdf = z / C<T>::pi();
+    V3<T> dir = x * dx + y * dy + lN * z;
+    BdVertex<T> &l = Lp[0];
+    l.pos = lpos; l.ns = lN; l.ng = lN;
+    l.mat = nullptr;
+    l.pdf = T(0); l.pdf_inv = T(0); l.pdf_light = lpdf;
+    l.light = (int32_t)lid;
+    l.wi = V3<T>(T(0));
+    const wl_area_light &lt = s->lights[lid];
+    l.tput = V3<T>(lt.L[0], lt.L[1], lt.L[2]) / lpdf;
+    uint32_t depth = 1;
+    bool hit_light = false;
+    T rr_k = T(1);
+    V3<T> org = lpos;
+    while (depth < P.max_depth) {
+        wl_hit hit;
+        rays++;
+        if (!bd_cast(sv, org, dir, P.eps, 1e30f, WL_CAST_CLOSEST, hit)) break;
+        depth += 1;
+        BdHit<T> h = bd_surface(sv, hit, org, dir);
+        if (h.light >= 0) {
+            hit_light = true;
+            break;
+        }
+        const uint32_t vi = depth - 1;
+        BdVertex<T> &v = Lp[vi];
+        v.pos = h.pos; v.ns = h.ns; v.ng = h.ng; v.wi = -dir;
+        v.mat = h.mat; v.light = -1;
+        v.pdf = T(0); v.pdf_light = T(0); v.pdf_inv = T(0);
+        BdVertex<T> &lv = Lp[vi - 1];
+        if (vi == 1) {
+            V3<T> d = v.pos - lv.pos;
+            T dist = length(d);
+            d = d / dist;
+            v.tput = Lp[0].tput * std::fabs(dot(d, lv.ns)) / dir_pdf * rr_k;
+            lv.pdf_inv = dir_pdf * std::fabs(dot(dir, v.ns)) / (dist * dist);
+        } else {
+            Mat<T> lm = to_mat<T>(*lv.mat);
+            V3<T> f = eval_disney(lm, lv.ns, lv.ng, lv.wi, dir, V3<T>(T(1)));
+            T cosw = dot(dir, lv.ns);
+            T pdf = clampf(pdf_disney(lm, lv.ns, lv.ng, lv.wi, dir), K(1e-30), K(1e30));
+            v.tput = lv.tput * clampv(f, T(0), K(1e30)) * std::fabs(cosw) / pdf * rr_k;
+            V3<T> d = v.pos - lv.pos;
+            lv.pdf_inv = pdf * std::fabs(dot(v.wi, v.ns)) / dot(d, d);
+            Lp[vi - 2].pdf = bd_pdf_forward(-v.wi, lv, Lp[vi - 2]);
+        }
+        T rr_rate = clampf(K(1.2) - T(depth) * K(0.5), K(0.1), T(1));
+        rr_k = T(1);
+        if (depth > 10) {
+            if (T(rng.next()) > rr_rate) break;
+            rr_k = T(1) / rr_rate;
+        }
+        dir = normalize(sample_disney(to_mat<T>(*v.mat), v.ns, v.ng, v.wi, rng));
+        org = v.pos;
+    }
+    return hit_light ? depth - 1 : depth;
+}
+
+// EvalContri (BDPT.cu:455-489) without its visibility ray, which the caller casts.
+template <class T> V3<T> bd_contribution(const SceneView &sv, const BdVertex<T> &e,
+                                          const BdVertex<T> &l, V3<T> vis, T dist) {
+    if (l.light >= 0 && !sv.s->lights[l.light].two_sided && dot(l.ns, vis) > T(0)) return V3<T>(T(0));
+    V3<T> fe = eval_disney(to_mat<T>(*e.mat), e.ns, e.ng, e.wi, vis, V3<T>(T(1)));
+    V3<T> c = e.tput * fe * std::fabs(dot(e.ns, vis)) * std::fabs(dot(l.ns, vis)) * l.tput /
+              (dist * dist);
+    if (l.light < 0) c = c * eval_disney(to_mat<T>(*l.mat), l.ns, l.ng, -vis, l.wi, V3<T>(T(1)));
+    return c;
+}
+
+// One sample of __raygen__RenderFrame (BDPT.cu:522-560): the value added to the film.
+template <class T>
+V3<T> bd_sample(const SceneView &sv, const wl_camera &cam, const wl_render_params &P, uint32_t px,
+                uint32_t py, uint32_t frame, uint64_t &rays) {
+    uint32_t pixel = P.width * py + px;
+    Rng rng = make_rng(P.rng, P.seed, pixel, frame);
+    BdVertex<T> E[WL_BDPT_MAX_VERTICES], Lp[WL_BDPT_MAX_VERTICES];
+    V3<T> radiance(T(0));
+    uint32_t ne = bd_eye(sv, cam, P, px, py, rng, E, radiance, rays);
+    V3<T> out = V3<T>(T(0)) + radiance;
+    if (ne == 0 || sv.s->nLight == 0) return out;
+    uint32_t nl = bd_light(sv, P, rng, Lp, rays);
+    V3<T> conn(T(0));
+    for (uint32_t i = 0; i < ne; ++i) {
+        for (uint32_t j = 0; j < nl; ++j) {
+            const BdVertex<T> &e = E[i], &l = Lp[j];
+            V3<T> vis = l.pos - e.pos;
+            T dist = length(vis);
+            vis = vis / dist;
+            wl_hit sh;
+            rays++;
+            const float eps = P.eps;
+            if (bd_cast(sv, e.pos, vis, eps, (float)(dist * (T(1) - T(eps))), WL_CAST_ANY, sh)) continue;
+            V3<T> c = bd_contribution(sv, e, l, vis, dist);
+            if (!(c.x + c.y + c.z > K(1e-10))) continue;
+            conn = conn + c * bd_mis_weight(E, Lp, (int)i, (int)j);
+        }
+    }
+    return out + conn;
+}
+
 }  // namespace
 
 // ========================================================================================
@@ -1331,6 +1676,54 @@ uint64_t or_render_ao(const or_scene *scene, void *bvh, const wl_camera *cam,
         }
         for (int c = 0; c < 3; c++) film_rgb[3 * pix + c] = acc;
         if (film64) for (int c = 0; c < 3; c++) film64[3 * pix + c] = sum / (double)p->spp;
+    }
+    return rays;
+}
+
+uint64_t or_render_bdpt(const or_scene *scene, void *bvh, const wl_camera *cam,
+                        const wl_render_params *p, int prec, int threads, float *film_rgb,
+                        double *film64) {
+    SceneView sv;
+    sv.s = scene;
+    sv.bvh = (const OBvh *)bvh;
+    sv.tri_light.assign(scene->nT, INVALID);
+    for (uint32_t l = 0; l < scene->nLight; l++)
+        for (uint32_t t = 0; t < scene->lights[l].tri_count; t++)
+            sv.tri_light[scene->lights[l].first_tri + t] = l;
+    uint32_t npix = p->width * p->height;
+    uint64_t rays = 0;
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#endif
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : rays)
+    for (int64_t pix = 0; pix < (int64_t)npix; pix++) {
+        uint32_t px = (uint32_t)(pix % p->width), py = (uint32_t)(pix / p->width);
+        float acc[3] = {0, 0, 0};
+        double sum[3] = {0, 0, 0};
+        if (film_rgb) for (int c = 0; c < 3; c++) acc[c] = film_rgb[3 * pix + c];
+        for (uint32_t s = 0; s < p->spp; s++) {
+            uint32_t f = p->first_frame + s;
+            double r[3];
+            if (prec == 0) {
+                V3<float> o = bd_sample<float>(sv, *cam, *p, px, py, f, rays);
+                r[0] = o.x; r[1] = o.y; r[2] = o.z;
+            } else {
+                V3<double> o = bd_sample<double>(sv, *cam, *p, px, py, f, rays);
+                r[0] = o.x; r[1] = o.y; r[2] = o.z;
+            }
+            // a sample that is not finite contributes 0 (the reference would keep a NaN in its
+            // running mean for the rest of the run)
+            if (!(std::isfinite(r[0]) && std::isfinite(r[1]) && std::isfinite(r[2]))) r[0] = r[1] = r[2] = 0;
+            // FP32 running mean with FP32 weights (BDPT.cu:548-556)
+            for (int c = 0; c < 3; c++) {
+                float thisf = (float)r[c];
+                if (f == 0) acc[c] = thisf;
+                else acc[c] = acc[c] * ((float)f / ((float)f + 1.0f)) + thisf * (1.0f / ((float)f + 1.0f));
+                sum[c] += r[c];
+            }
+        }
+        if (film_rgb) for (int c = 0; c < 3; c++) film_rgb[3 * pix + c] = acc[c];
+        if (film64) for (int c = 0; c < 3; c++) film64[3 * pix + c] = sum[c] / (double)p->spp;
     }
     return rays;
 }

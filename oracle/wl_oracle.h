@@ -82,6 +82,14 @@ uint64_t or_render(const or_scene *scene, void *bvh, const wl_camera *cam,
 uint64_t or_render_ao(const or_scene *scene, void *bvh, const wl_camera *cam,
                       const wl_ao_params *p, int threads, float *film_rgb, double *film64);
 
+/* Bidirectional path tracer (Programs/BDPT/BDPT.cu:42-567) with p->strategy ignored and
+ * p->max_depth the subpath vertex cap (the reference's 10, at most WL_BDPT_MAX_VERTICES);
+ * film_rgb: the reference's FP32 running mean with FP32 weights; film64 (nullable): FP64 mean.
+ * Returns rays traced (subpath segments + connection rays). */
+uint64_t or_render_bdpt(const or_scene *scene, void *bvh, const wl_camera *cam,
+                        const wl_render_params *p, int prec, int threads, float *film_rgb,
+                        double *film64);
+
 /* relMSE = mean over pixels and channels of (I - R)^2 / (R^2 + eps) */
 double or_relmse(const float *img, const double *ref, uint64_t n, double eps);
 

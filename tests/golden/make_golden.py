@@ -4,7 +4,9 @@ The reference (Extra-Creativity/Wayland) has no tests and no golden vectors of i
 fixtures are the outputs of its src/Frontend/Device/*.h functions (tea<4>, rnd, PinholeGenerateRay,
 SampleDisneyBSDF, EvalDisneyBSDF, PdfDisneyBSDF, AceApprox) compiled on the host from the
 reference tree by oracle/ref_build (-> oracle/_ref/libwlref.so), plus a small image rendered by
-the path loop of PathTracing.cu:40-288 written over those functions. sin/cos/log inside the
+the path loop of PathTracing.cu:40-288 written over those functions, and two images rendered
+by the reference's BDPT program itself (Programs/BDPT/BDPT.cu compiled on the host with its
+OptiX calls emulated over the oracle's CPU BVH, oracle/ref_build/ref_bdpt.cpp). sin/cos/log inside the
 reference functions are routed to the project's own single-precision versions (see
 oracle/ref_build/shim/wl_ref_math.h), so the vectors pin the oracle bit for bit.
 
@@ -112,6 +114,18 @@ def main():
                         tri_flags=sph.tri_flags,
                         cam=np.array([list(scam.pos), list(scam.look_at), list(scam.up),
                                       list(scam.right)], np.float32))
+    # the reference's own bidirectional program (Programs/BDPT/BDPT.cu, run over the host
+    # emulation of its OptiX calls): the Cornell box and a small glass sphere
+    for name, bsc in (("bdpt_cornell_32x32_4spp.npz", scenes.cornell_box(32, 32)),
+                      ("bdpt_glass_40x40_4spp.npz", scenes.glass_sphere(40, 40, subdiv=12))):
+        bcam = po.Camera()
+        for k in ("pos", "look_at", "up", "right"):
+            getattr(bcam, k)[:] = [float(x) for x in bsc.camera[k]]
+        rad = ref.render_bdpt(bsc, bcam, bsc.width, bsc.height, 4)
+        np.savez_compressed(os.path.join(HERE, name), image=rad[..., :3].copy(), V=bsc.V, I=bsc.I,
+                            N=bsc.N if bsc.N is not None else np.zeros(0, np.float32),
+                            cam=np.array([list(bcam.pos), list(bcam.look_at), list(bcam.up),
+                                          list(bcam.right)], np.float32))
     print("golden vectors written to", HERE)
 
 

@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 
 import pyoracle as po
+from wayland_b200 import scenes
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
@@ -119,3 +120,24 @@ def test_ao_image(oracle):
     img, _, rays = oracle.render_ao(_GoldScene(g), cam, p)
     assert np.array_equal(bits(img), bits(g["image"]))
     assert rays == int(g["rays"])
+
+
+@pytest.mark.parametrize("name,make", [
+    ("bdpt_cornell_32x32_4spp.npz", lambda: scenes.cornell_box(32, 32)),
+    ("bdpt_glass_40x40_4spp.npz", lambda: scenes.glass_sphere(40, 40, subdiv=12)),
+])
+def test_bdpt_image(oracle, name, make):
+    """The oracle's bidirectional path tracer reproduces the reference's BDPT program
+    (Programs/BDPT/BDPT.cu run over the OptiX host emulation) bit for bit."""
+    g = dict(np.load(os.path.join(GOLD, name)))
+    sc = make()
+    assert np.array_equal(sc.V, g["V"]) and np.array_equal(sc.I, g["I"])
+    cam = po.Camera()
+    for i, k in enumerate(("pos", "look_at", "up", "right")):
+        getattr(cam, k)[:] = [float(x) for x in g["cam"][i]]
+    p = po.RenderParams(width=sc.width, height=sc.height, spp=4, first_frame=0, max_depth=10,
+                        rr_depth=5, rr_prob=0.9, eps=1e-3, strategy=3, rng=0, math=1, lights=0,
+                        seed=0)
+    img, _, rays = oracle.render_bdpt(sc, cam, p)
+    assert np.isfinite(g["image"]).all() and g["image"].max() > 0
+    assert np.array_equal(bits(img), bits(g["image"]))

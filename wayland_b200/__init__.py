@@ -20,7 +20,8 @@ import numpy as np
 from . import _abi
 from ._abi import (BVH_LBVH, BVH_SAH, CAST_ANY, CAST_CLOSEST, FILM_FP64_SUM, INVALID,
                    LIGHTS_POWER, LIGHTS_UNIFORM, MATH_FAST, MATH_STRICT, RNG_PCG32, RNG_TEA_LCG,
-                   STRATEGY_MIS, STRATEGY_NEE, STRATEGY_UPT, HIT_DTYPE, RAY_DTYPE, WlError)
+                   STRATEGY_BDPT, STRATEGY_MIS, STRATEGY_NEE, STRATEGY_UPT, BDPT_MAX_VERTICES,
+                   HIT_DTYPE, RAY_DTYPE, WlError)
 
 __all__ = ["Context", "Scene", "Film", "PathTracer", "render_params", "WlError", "RAY_DTYPE",
            "HIT_DTYPE"]

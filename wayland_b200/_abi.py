@@ -15,7 +15,8 @@ WL_OK = 0
 ERR_NAMES = {0: "WL_OK", 1: "WL_ERR_INVALID_ARG", 2: "WL_ERR_CUDA", 3: "WL_ERR_OOM",
              4: "WL_ERR_QUEUE_OVERFLOW", 5: "WL_ERR_TIMEOUT", 6: "WL_ERR_NOT_BUILT",
              7: "WL_ERR_UNSUPPORTED"}
-STRATEGY_UPT, STRATEGY_NEE, STRATEGY_MIS = 0, 1, 2
+STRATEGY_UPT, STRATEGY_NEE, STRATEGY_MIS, STRATEGY_BDPT = 0, 1, 2, 3
+BDPT_MAX_VERTICES = 10
 RNG_TEA_LCG, RNG_PCG32 = 0, 1
 MATH_FAST, MATH_STRICT = 0, 1
 LIGHTS_UNIFORM, LIGHTS_POWER = 0, 1

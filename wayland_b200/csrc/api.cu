@@ -57,6 +57,8 @@ struct wl_context {
     cudaEvent_t ev_total[2] = {nullptr, nullptr};
     bool stats_pending = false;
     int live_children = 0;  // scenes and films created on this context and not yet destroyed
+    BdptWave bd{};          // bidirectional wave buffers (allocated by the first BDPT render)
+    void *bd_block = nullptr;
 };
 
 struct wl_scene {
@@ -147,6 +149,50 @@ int ensure_queues(wl_context *c, uint32_t cap) {
     return WL_OK;
 }
 
+// Bidirectional wave buffers for `cap` slots of subpaths of at most `maxv` vertices: 2 maxv
+// vertices of 80 bytes per slot, and the worst case of maxv^2 connections per slot (68 bytes
+// each: slot 4, value 16, connection ray 48).
+int ensure_bdpt(wl_context *c, uint32_t cap, uint32_t maxv) {
+    BdptWave &b = c->bd;
+    if (c->bd_block && b.cap >= cap && b.maxv >= maxv) {
+        b.maxv = maxv;  // the vertex arrays keep their allocated stride (cap)
+        return WL_OK;
+    }
+    if (c->bd_block) {
+        cudaFree(c->bd_block);
+        c->bd_block = nullptr;
+    }
+    const uint64_t conn = (uint64_t)cap * maxv * maxv;
+    if (conn >= (1ull << 32)) return fail(WL_ERR_INVALID_ARG, "bidirectional wave too large");
+    size_t vtx = al<float4>((size_t)cap * maxv);
+    size_t u32 = al<uint32_t>(cap), u32p = al<uint32_t>((size_t)cap + 1);
+    size_t cslot = al<uint32_t>(conn), cf4 = al<float4>(conn);
+    size_t scan = al<char>(strict::bdpt_scan_bytes(cap) + 256);
+    size_t total = 10 * vtx + 3 * u32 + u32p + cslot + 4 * cf4 + scan + 256;
+    CK(cudaMalloc(&c->bd_block, total));
+    char *p = (char *)c->bd_block;
+    b = BdptWave{};
+    b.cap = cap;
+    b.maxv = maxv;
+    float4 **vs[10] = {&b.eye.a, &b.eye.b, &b.eye.c, &b.eye.d, &b.eye.e,
+                       &b.lit.a, &b.lit.b, &b.lit.c, &b.lit.d, &b.lit.e};
+    for (auto v : vs) { *v = (float4 *)p; p += vtx; }
+    b.n_eye = (uint32_t *)p; p += u32;
+    b.n_light = (uint32_t *)p; p += u32;
+    b.conn_count = (uint32_t *)p; p += u32;
+    b.conn_first = (uint32_t *)p; p += u32p;
+    b.conn_slot = (uint32_t *)p; p += cslot;
+    b.conn_val = (float4 *)p; p += cf4;
+    b.cs_o = (float4 *)p; p += cf4;
+    b.cs_d = (float4 *)p; p += cf4;
+    b.cs_l = (float4 *)p; p += cf4;
+    b.conn_cap = (uint32_t)conn;
+    b.scan_tmp = p; b.scan_bytes = scan; p += scan;
+    b.counters = (uint32_t *)p; p += 256;
+    CK(cudaMemsetAsync(b.counters, 0, 256, c->stream));
+    return WL_OK;
+}
+
 void rec(wl_context *c, int cat, bool begin) {
     auto &v = c->ev[cat];
     size_t &u = c->ev_used[cat];
@@ -232,6 +278,7 @@ int wl_context_destroy(wl_context *c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->q_block) cudaFree(c->q_block);
+    if (c->bd_block) cudaFree(c->bd_block);
     if (c->d_misc) cudaFree(c->d_misc);
     if (c->d_cast_counts) cudaFree(c->d_cast_counts);
     for (auto &v : c->ev)
@@ -620,6 +667,70 @@ void wl_render_params_default(wl_render_params *p, uint32_t w, uint32_t h, uint3
     p->wave_paths = 0;
 }
 
+// One wave of the bidirectional path tracer (BDPT.cu:522-560 for wp.count samples): eye
+// subpaths, light subpaths, connections, connection rays, film. Returns the launches issued.
+// Event categories: 0 closest-hit passes, 1 vertex and connection kernels, 2 connection rays,
+// 3 the rest.
+static uint32_t bdpt_wave(wl_context *c, const WaveParams &wp, const DevScene &sc, const Film &film,
+                          bool strict_math, bool tstats) {
+    cudaStream_t st = c->stream;
+    BdptWave &bw = c->bd;
+    uint32_t launches = 0;
+    rec(c, 3, true);
+    if (strict_math) strict::launch_bdpt_eye_gen(wp, c->q, bw, st);
+    else fast::launch_bdpt_eye_gen(wp, c->q, bw, st);
+    rec(c, 3, false);
+    launches++;
+    int in = 0;
+    for (uint32_t d = 1; d <= bw.maxv; d++) {
+        rec(c, 0, true);
+        launch_extend(sc, c->q, in, tstats, st);
+        rec(c, 0, false);
+        cudaMemsetAsync(c->q.counters + (in ^ 1), 0, sizeof(uint32_t), st);
+        rec(c, 1, true);
+        if (strict_math) strict::launch_bdpt_eye(wp, sc, c->q, bw, in, d, st);
+        else fast::launch_bdpt_eye(wp, sc, c->q, bw, in, d, st);
+        rec(c, 1, false);
+        launches += 2;
+        in ^= 1;
+    }
+    cudaMemsetAsync(c->q.counters, 0, sizeof(uint32_t), st);
+    rec(c, 1, true);
+    if (strict_math) strict::launch_bdpt_light_gen(wp, sc, c->q, bw, st);
+    else fast::launch_bdpt_light_gen(wp, sc, c->q, bw, st);
+    rec(c, 1, false);
+    launches++;
+    in = 0;
+    for (uint32_t d = 2; d <= bw.maxv; d++) {
+        rec(c, 0, true);
+        launch_extend(sc, c->q, in, tstats, st);
+        rec(c, 0, false);
+        cudaMemsetAsync(c->q.counters + (in ^ 1), 0, sizeof(uint32_t), st);
+        rec(c, 1, true);
+        if (strict_math) strict::launch_bdpt_light(wp, sc, c->q, bw, in, d, st);
+        else fast::launch_bdpt_light(wp, sc, c->q, bw, in, d, st);
+        rec(c, 1, false);
+        launches += 2;
+        in ^= 1;
+    }
+    rec(c, 3, true);
+    strict::launch_bdpt_connections(wp, bw, st);
+    rec(c, 3, false);
+    launches += 4;
+    rec(c, 1, true);
+    if (strict_math) strict::launch_bdpt_connect(wp, sc, c->q, bw, st);
+    else fast::launch_bdpt_connect(wp, sc, c->q, bw, st);
+    rec(c, 1, false);
+    rec(c, 2, true);
+    launch_connection_rays(sc, c->q, bw, tstats, st);
+    rec(c, 2, false);
+    rec(c, 3, true);
+    strict::launch_bdpt_film(wp, sc, c->q, bw, film, st);
+    rec(c, 3, false);
+    launches += 3;
+    return launches;
+}
+
 int wl_render(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_params *p, wl_film *f) {
     ARG(c && s && cam && p && f, "null argument");
     ARG(s->ctx == c && f->ctx == c, "scene and film must belong to the context");
@@ -627,7 +738,9 @@ int wl_render(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_
     ARG(p->width == f->f.W && p->height == f->f.H, "film size differs from the render size");
     ARG(p->spp > 0, "spp must be > 0");
     ARG(p->max_depth > 0 && p->max_depth <= 1024, "max_depth out of range");
-    ARG(p->strategy <= WL_STRATEGY_MIS, "bad strategy");
+    ARG(p->strategy <= WL_STRATEGY_BDPT, "bad strategy");
+    ARG(p->strategy != WL_STRATEGY_BDPT || p->max_depth <= WL_BDPT_MAX_VERTICES,
+        "bidirectional subpaths hold at most WL_BDPT_MAX_VERTICES vertices (max_depth)");
     ARG(p->rng <= WL_RNG_PCG32, "bad rng");
     ARG(p->math <= WL_MATH_STRICT, "bad math mode");
     ARG(p->lights == WL_LIGHTS_UNIFORM, "only uniform light selection is available");
@@ -637,14 +750,21 @@ int wl_render(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_
     c->stats_pending = false;  // counters of an earlier call that nobody read are discarded
     const uint32_t npix = p->width * p->height;
     const uint64_t total = (uint64_t)npix * p->spp;
-    uint64_t want = p->wave_paths ? p->wave_paths : (1ull << 23);
+    const bool bdpt = p->strategy == WL_STRATEGY_BDPT;
+    const uint64_t maxv2 = (uint64_t)p->max_depth * p->max_depth;
+    uint64_t want = p->wave_paths ? p->wave_paths : (bdpt ? (1ull << 25) / maxv2 : (1ull << 23));
     if (want < 1024) want = 1024;
     if (want > (1ull << 26)) want = 1ull << 26;
+    if (bdpt && want > (1ull << 26) / maxv2) want = (1ull << 26) / maxv2;
     uint32_t spp_per_wave = (uint32_t)(want / npix);
     uint64_t wave = spp_per_wave >= 1 ? (uint64_t)spp_per_wave * npix : want;
     if (wave > total) wave = total;
     int rc = ensure_queues(c, (uint32_t)wave);
     if (rc != WL_OK) return rc;
+    if (bdpt) {
+        rc = ensure_bdpt(c, (uint32_t)wave, p->max_depth);
+        if (rc != WL_OK) return rc;
+    }
 
     WaveParams wp{};
     wp.W = p->width; wp.H = p->height; wp.npix = npix;
@@ -666,7 +786,14 @@ int wl_render(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_
     CK(cudaEventRecord(c->ev_total[0], st));
     uint32_t launches = 0, waves = 0;
     const bool strict_math = p->math == WL_MATH_STRICT;
-    for (uint64_t base = 0; base < total; base += wave) {
+    for (uint64_t base = 0; base < total && bdpt; base += wave) {
+        wp.base = base;
+        wp.count = (uint32_t)((total - base) < wave ? (total - base) : wave);
+        launches += bdpt_wave(c, wp, sc, f->f, strict_math, tstats);
+        waves++;
+        CK(cudaGetLastError());
+    }
+    for (uint64_t base = 0; base < total && !bdpt; base += wave) {
         wp.base = base;
         wp.count = (uint32_t)((total - base) < wave ? (total - base) : wave);
         rec(c, 3, true);

@@ -1,10 +1,13 @@
-// pt_strict.cu - wavefront path-tracing kernels in WL_MATH_STRICT mode. Built with -fmad=false
+// pt_strict.cu - wavefront path-tracing and bidirectional kernels in WL_MATH_STRICT mode. Built with -fmad=false
 // -prec-div=true -prec-sqrt=true -ftz=false and the project's own sin/cos/log, so every path
 // is bit-identical to the CPU oracle for the same inputs. Also holds the film, tone-map and
 // random-stream kernels, which are exact in both modes.
 #define WL_STRICT_MATH 1
 #define WL_NS strict
+#include <cub/device/device_scan.cuh>
+
 #include "pt_kernels.cuh"
+#include "bdpt_kernels.cuh"
 
 namespace wl {
 namespace strict {
@@ -43,6 +46,88 @@ __global__ void k_film(WaveParams wp, Queues q, Film f) {
         for (int c = 0; c < 3; c++) f.rgb[3 * (size_t)pixel + c] = acc[c];
     if (f.sum64)
         for (int c = 0; c < 3; c++) f.sum64[3 * (size_t)pixel + c] += sum[c];
+}
+
+// Connections of a bidirectional wave: n_eye * n_light per slot, numbered by an exclusive scan in
+// slot order (conn_first), and each connection tagged with its slot.
+__global__ void k_bd_count(uint32_t count, BdptWave bw) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) bw.conn_count[i] = bw.n_eye[i] * bw.n_light[i];
+}
+__global__ void k_bd_expand(uint32_t count, BdptWave bw) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+        uint32_t f = bw.conn_first[i], n = bw.conn_count[i];
+        for (uint32_t k = 0; k < n; k++) bw.conn_slot[f + k] = i;
+        if (i == count - 1) {
+            bw.counters[0] = f + n;
+            bw.counters[2] = 0;
+        }
+    }
+}
+
+size_t bdpt_scan_bytes(uint32_t cap) {
+    size_t bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, bytes, (uint32_t *)nullptr, (uint32_t *)nullptr, (int)cap);
+    return bytes;
+}
+
+void launch_bdpt_connections(const WaveParams &wp, const BdptWave &bw, cudaStream_t s) {
+    uint32_t blocks = (wp.count + 255) / 256;
+    k_bd_count<<<blocks ? blocks : 1, 256, 0, s>>>(wp.count, bw);
+    size_t bytes = bw.scan_bytes;
+    cub::DeviceScan::ExclusiveSum(bw.scan_tmp, bytes, bw.conn_count, bw.conn_first, (int)wp.count, s);
+    k_bd_expand<<<blocks ? blocks : 1, 256, 0, s>>>(wp.count, bw);
+}
+
+// Film update of a bidirectional wave (BDPT.cu:534-556): per pixel, the samples of this wave in
+// increasing frame; the sample is (0 + eye-path emission) + (0 + connection values in the
+// reference's order), the running mean is FP32 arithmetic with FP32 weights. A sample that is
+// not finite adds 0 (the reference would keep the NaN). The FP64 film sums the same values.
+__global__ void k_bd_film(WaveParams wp, uint32_t nlight, Queues q, BdptWave bw, Film f) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t lim = wp.count < wp.npix ? wp.count : wp.npix;
+    if (j >= lim) return;
+    uint64_t g0 = wp.base + j;
+    uint32_t pixel = (uint32_t)(g0 % wp.npix);
+    float acc[3];
+    double sum[3] = {0.0, 0.0, 0.0};
+    if (f.rgb)
+        for (int c = 0; c < 3; c++) acc[c] = f.rgb[3 * (size_t)pixel + c];
+    for (uint64_t g = g0; g < wp.base + wp.count; g += wp.npix) {
+        uint32_t slot = (uint32_t)(g - wp.base);
+        uint32_t frame = wp.first_frame + (uint32_t)(g / wp.npix);
+        v3 r = v3(0.f) + f4xyz(q.st_rad[slot]);
+        uint32_t n = bw.conn_count[slot];
+        if (n > 0 && nlight > 0) {
+            v3 conn(0.f);
+            uint32_t first = bw.conn_first[slot];
+            for (uint32_t t = 0; t < n; t++) conn = conn + f4xyz(bw.conn_val[first + t]);
+            r = r + conn;
+        }
+        float rc[3] = {r.x, r.y, r.z};
+        if (!(isfinite(rc[0]) && isfinite(rc[1]) && isfinite(rc[2]))) rc[0] = rc[1] = rc[2] = 0.f;
+        for (int c = 0; c < 3; c++) {
+            if (frame == 0) {
+                acc[c] = rc[c];
+            } else {
+                float w0 = (float)frame / ((float)frame + 1.0f);
+                float w1 = 1.0f / ((float)frame + 1.0f);
+                acc[c] = acc[c] * w0 + rc[c] * w1;
+            }
+            sum[c] += (double)rc[c];
+        }
+    }
+    if (f.rgb)
+        for (int c = 0; c < 3; c++) f.rgb[3 * (size_t)pixel + c] = acc[c];
+    if (f.sum64)
+        for (int c = 0; c < 3; c++) f.sum64[3 * (size_t)pixel + c] += sum[c];
+}
+
+void launch_bdpt_film(const WaveParams &wp, const DevScene &sc, const Queues &q, const BdptWave &bw,
+                      const Film &f, cudaStream_t s) {
+    uint32_t lim = wp.count < wp.npix ? wp.count : wp.npix;
+    k_bd_film<<<(lim + 255) / 256, 256, 0, s>>>(wp, sc.nLight, q, bw, f);
 }
 
 // colorBuffer = u8vec4(vec4(AceApprox(clamp(radiance, 0, 1e30)), 1) * 255) (PathTracing.cu:157-158)

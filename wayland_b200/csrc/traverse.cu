@@ -46,10 +46,12 @@ constexpr int REFILL = 12;
 
 // Persistent traversal over a queue of n rays. MODE 0: closest hit of ray queue `in`, hit
 // written to q.hit. MODE 1: any hit of the shadow queue; an unoccluded ray adds its light
-// sample to the path radiance.
+// sample to the path radiance. MODE 2: any hit of the bidirectional connection rays (passed as
+// the shadow queue); an unoccluded ray stores its value as the result of its connection
+// (EvalContri's visibility ray, BDPT.cu:460-467).
 template <int MODE, bool STATS>
 __global__ void __launch_bounds__(TT) k_trace(DevScene sc, Queues q, int in, uint32_t *fetch) {
-    constexpr bool ANY = MODE == 1;
+    constexpr bool ANY = MODE != 0;
     const uint32_t n = MODE == 0 ? q.counters[in] : q.counters[2];
     const float4 *ro = MODE == 0 ? q.ray_o[in] : q.sh_o;
     const float4 *rd = MODE == 0 ? q.ray_d[in] : q.sh_d;
@@ -83,7 +85,10 @@ __global__ void __launch_bounds__(TT) k_trace(DevScene sc, Queues q, int in, uin
             active = false;
             if (MODE == 0) {
                 q.hit[my] = make_float4(st.res.t, __uint_as_float(st.res.prim), st.res.u, st.res.v);
-            } else if (st.res.prim == INVALID) {
+            } else if (MODE == 2 && st.res.prim == INVALID) {
+                float4 l = q.sh_l[my];
+                q.conn_val[__float_as_uint(l.w)] = make_float4(l.x, l.y, l.z, 0.f);
+            } else if (MODE == 1 && st.res.prim == INVALID) {
                 float4 l = q.sh_l[my];
                 uint32_t slot = __float_as_uint(l.w);
                 float4 rad = q.st_rad[slot];
@@ -200,6 +205,22 @@ void launch_shadow(const DevScene &sc, const Queues &q, bool stats, cudaStream_t
     cudaMemsetAsync(q.counters + 7, 0, sizeof(uint32_t), s);
     if (stats) k_trace<1, true><<<grid, TT, 0, s>>>(sc, q, 0, q.counters + 7);
     else k_trace<1, false><<<grid, TT, 0, s>>>(sc, q, 0, q.counters + 7);
+}
+
+// Connection rays of a bidirectional wave: the shadow-queue fields of q are pointed at the
+// wave's connection-ray queue and counters ([2] queue size, [7] work counter).
+void launch_connection_rays(const DevScene &sc, const Queues &q, const BdptWave &bw, bool stats,
+                            cudaStream_t s) {
+    static int grid = grid_for((const void *)k_trace<2, false>);
+    Queues cq = q;
+    cq.sh_o = bw.cs_o;
+    cq.sh_d = bw.cs_d;
+    cq.sh_l = bw.cs_l;
+    cq.counters = bw.counters;
+    cq.conn_val = bw.conn_val;
+    cudaMemsetAsync(bw.counters + 7, 0, sizeof(uint32_t), s);
+    if (stats) k_trace<2, true><<<grid, TT, 0, s>>>(sc, cq, 0, bw.counters + 7);
+    else k_trace<2, false><<<grid, TT, 0, s>>>(sc, cq, 0, bw.counters + 7);
 }
 
 void launch_cast(const DevScene &sc, const wl_ray *rays, wl_hit *hits, uint32_t n, uint32_t mode,

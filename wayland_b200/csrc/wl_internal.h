@@ -63,6 +63,38 @@ struct Queues {
     // 64-bit sums over a render: [0] segments, [1] shadow rays, [2..3] extend node visits and
     // triangle tests, [4..5] the same for shadow rays
     unsigned long long *totals;
+    // bidirectional connections: result of each connection (set when its ray is unoccluded)
+    float4 *conn_val;
+};
+
+// Bidirectional subpath vertices (BDPT.h BDPTVertex; the texture colour of a flattened scene
+// is 1): structure of arrays indexed [vertex k * cap + slot], 80 bytes a vertex:
+//   a = (position, id)  id = material index, or BD_LIGHT | light index for a light vertex
+//   b = (shading normal, pdf)   c = (geometric normal, pdf_inv)
+//   d = (direction to the previous vertex Wi, pdf_light)   e = (throughput, light-vertex
+//   direction pdf of the light subpath)
+constexpr uint32_t BD_LIGHT = 0x80000000u;
+struct BdVerts {
+    float4 *a, *b, *c, *d, *e;
+};
+// One wave of bidirectional samples: slot i is sample (base + i) like the path tracer's waves.
+// Connections are numbered in slot order and, within a slot, in the reference's loop order
+// (eye vertex i outer, light vertex j inner): connection t of slot s is conn_first[s] + i nl + j.
+struct BdptWave {
+    uint32_t cap;        // slots
+    uint32_t maxv;       // subpath vertex cap
+    BdVerts eye, lit;    // [maxv][cap] each
+    uint32_t *n_eye, *n_light;  // stored vertices per slot
+    uint32_t *conn_count;       // n_eye * n_light per slot
+    uint32_t *conn_first;       // exclusive prefix sum of conn_count (cap + 1 entries)
+    uint32_t *conn_slot;        // slot of each connection
+    float4 *conn_val;           // value of each connection (0 unless unoccluded)
+    float4 *cs_o, *cs_d, *cs_l; // connection-ray queue: origin/tmin, dir/tmax, (value, connection)
+    uint32_t conn_cap;
+    // [0] connections in the wave, [2] connection-ray queue size, [7] traversal work counter
+    uint32_t *counters;
+    void *scan_tmp;
+    size_t scan_bytes;
 };
 
 // Film (the radiance buffer of PathTracingProgramManager.cpp:30-32 + colour buffer)
@@ -129,17 +161,39 @@ void launch_ao(const AoWave &w, const DevScene &sc, const Queues &q, const Film 
 
 // launch functions (pt_kernels.cuh instantiated in pt_fast.cu / pt_strict.cu)
 namespace fast {
+void launch_bdpt_eye_gen(const WaveParams &wp, const Queues &q, const BdptWave &bw, cudaStream_t s);
+void launch_bdpt_eye(const WaveParams &wp, const DevScene &sc, const Queues &q, const BdptWave &bw,
+                     int in, uint32_t depth, cudaStream_t s);
+void launch_bdpt_light_gen(const WaveParams &wp, const DevScene &sc, const Queues &q,
+                           const BdptWave &bw, cudaStream_t s);
+void launch_bdpt_light(const WaveParams &wp, const DevScene &sc, const Queues &q, const BdptWave &bw,
+                       int in, uint32_t depth, cudaStream_t s);
+void launch_bdpt_connect(const WaveParams &wp, const DevScene &sc, const Queues &q,
+                         const BdptWave &bw, cudaStream_t s);
 void launch_generate(const WaveParams &wp, const Queues &q, cudaStream_t s);
 void launch_shade(const WaveParams &wp, const DevScene &sc, const Queues &q, int in, cudaStream_t s);
 void launch_shade_nrc(const WaveParams &wp, const DevScene &sc, const Queues &q, int in,
                       const NrcWaveBuffers &nb, cudaStream_t s);
 }
 namespace strict {
+void launch_bdpt_eye_gen(const WaveParams &wp, const Queues &q, const BdptWave &bw, cudaStream_t s);
+void launch_bdpt_eye(const WaveParams &wp, const DevScene &sc, const Queues &q, const BdptWave &bw,
+                     int in, uint32_t depth, cudaStream_t s);
+void launch_bdpt_light_gen(const WaveParams &wp, const DevScene &sc, const Queues &q,
+                           const BdptWave &bw, cudaStream_t s);
+void launch_bdpt_light(const WaveParams &wp, const DevScene &sc, const Queues &q, const BdptWave &bw,
+                       int in, uint32_t depth, cudaStream_t s);
+void launch_bdpt_connect(const WaveParams &wp, const DevScene &sc, const Queues &q,
+                         const BdptWave &bw, cudaStream_t s);
 void launch_generate(const WaveParams &wp, const Queues &q, cudaStream_t s);
 void launch_shade(const WaveParams &wp, const DevScene &sc, const Queues &q, int in, cudaStream_t s);
 void launch_shade_nrc(const WaveParams &wp, const DevScene &sc, const Queues &q, int in,
                       const NrcWaveBuffers &nb, cudaStream_t s);
 void launch_film(const WaveParams &wp, const Queues &q, const Film &f, cudaStream_t s);
+void launch_bdpt_connections(const WaveParams &wp, const BdptWave &bw, cudaStream_t s);
+void launch_bdpt_film(const WaveParams &wp, const DevScene &sc, const Queues &q, const BdptWave &bw,
+                      const Film &f, cudaStream_t s);
+size_t bdpt_scan_bytes(uint32_t cap);
 void launch_tonemap(const Film &f, cudaStream_t s);
 void launch_debug_rng(uint32_t rng, uint64_t seed, const uint32_t *pixels, uint32_t npix,
                       uint32_t frame, uint32_t count, float *out, cudaStream_t s);
@@ -147,6 +201,8 @@ void launch_debug_rng(uint32_t rng, uint64_t seed, const uint32_t *pixels, uint3
 // traverse.cu
 void launch_extend(const DevScene &sc, const Queues &q, int in, bool stats, cudaStream_t s);
 void launch_shadow(const DevScene &sc, const Queues &q, bool stats, cudaStream_t s);
+void launch_connection_rays(const DevScene &sc, const Queues &q, const BdptWave &bw, bool stats,
+                            cudaStream_t s);
 void launch_cast(const DevScene &sc, const wl_ray *rays, wl_hit *hits, uint32_t n, uint32_t mode,
                  uint32_t *fetch, cudaStream_t s);
 void launch_cast_stats(const DevScene &sc, const wl_ray *rays, uint32_t n, uint32_t mode,

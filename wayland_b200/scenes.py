@@ -297,6 +297,45 @@ def displaced_sphere(width=1920, height=1080, spp=64, max_depth=16, subdiv=316, 
                  width=width, height=height, spp=spp, max_depth=max_depth, env=(0.1, 0.1, 0.1))
 
 
+def glass_sphere(width=1024, height=1024, spp=256, max_depth=10, subdiv=89, light_size=0.05,
+                 light_L=(4000.0, 3600.0, 3000.0), roughness=0.05):
+    """Bidirectional configuration: a smooth glass sphere (20 subdiv^2 triangles, 158,420 at
+    subdiv 89; specular transmission 1, IOR 1.5) resting on a 2-triangle diffuse plane, lit
+    only by a small one-sided quad light (light_size wide) above it, so most of the plane
+    under the sphere is lit by caustics that camera paths find only by connection. The glass
+    roughness is 0.05: at roughness 0 the reference's Disney lobes (GTR2 with alpha 0.001 and
+    pdfs clamped to [1e-30, 1e30]) give single samples of 1e16 and more, and no estimator of
+    the image converges."""
+    P, T = subdivided_icosphere(subdiv)
+    Vs = P.astype(np.float32)
+    Is = T.astype(np.uint32)
+    Ns = vertex_normals(Vs, Is)
+    glass = disney((1.0, 1.0, 1.0), metallic=0.0, roughness=roughness, specular=0.5, eta=1.5,
+                   trans=1.0)
+    mats = np.array([glass, matte((0.7, 0.7, 0.7)), matte((0.8, 0.8, 0.8))])
+    y = -1.0
+    Vg, Ig = _quad((-8, y, -8), (-8, y, 8), (8, y, 8), (8, y, -8))
+    h = 0.5 * light_size
+    ly = 2.5
+    # facing down: cross(p1 - p0, p2 - p0) = -y
+    Vl, Il = _quad((-0.6 - h, ly, 0.4 - h), (-0.6 + h, ly, 0.4 - h), (-0.6 + h, ly, 0.4 + h),
+                   (-0.6 - h, ly, 0.4 + h))
+    nS = len(Vs)
+    V = np.concatenate([Vs, Vg, Vl]).astype(np.float32)
+    I = np.concatenate([Is, Ig + nS, Il + nS + 4]).astype(np.uint32)
+    N = np.concatenate([Ns, np.tile([[0, 1, 0]], (4, 1)), np.tile([[0, -1, 0]], (4, 1))]).astype(np.float32)
+    M = np.concatenate([np.zeros(len(Is), np.uint32), np.ones(2, np.uint32), np.full(2, 2, np.uint32)])
+    flags = np.concatenate([np.ones(len(Is), np.uint32), np.zeros(4, np.uint32)])
+    lights = np.zeros(1, LIGHT)
+    lights[0]["L"] = light_L
+    lights[0]["two_sided"] = 0
+    lights[0]["first_tri"] = len(Is) + 2
+    lights[0]["tri_count"] = 2
+    cam = pinhole((0.0, 1.2, 4.5), (0.0, -0.4, 0.0), (0, 1, 0), 38.0, width, height)
+    return Scene("glass_sphere", V, I, M, mats, lights, N=N, tri_flags=flags, camera=cam,
+                 width=width, height=height, spp=spp, max_depth=max_depth)
+
+
 def _grid(p0, du, dv, nu, nv):
     """Quad p0 + [0,1] du + [0,1] dv tessellated into nu x nv cells (2 nu nv triangles);
     normal = cross(du, dv)."""
