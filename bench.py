@@ -8,9 +8,9 @@ wl_render in WL_MATH_FAST mode with the reference's TEA+LCG streams, uniform lig
 MIS and Russian roulette (after depth 5, p = 0.9). Synthetic data; the BVH is built once
 outside the timed region (Mpaths/s = W * H * spp / render time).
 
-Prints one JSON line (see the keys below). `--impl reference` times the reference's own device
-arithmetic (src/Frontend/Device/*.h compiled on the host, oracle/_ref/libwlref.so) inside a CPU
-restatement of PathTracing.cu's loop on all host cores, on a bounded sample of the same workload.
+Prints one JSON line (see the keys below). `--impl reference` times the reference's own
+PathTracing.cu program compiled on the host (oracle/_ref/libwlref.so, its OptiX calls emulated
+over the oracle's CPU BVH) on all host cores, on a bounded sample of the same workload.
 """
 import argparse
 import json
@@ -92,8 +92,10 @@ class Clocks:
 
 class CpuPT:
     """The CPU path tracer on a bounded sample of the workload (pixel rows at 64 spp): the
-    reference's own device arithmetic (oracle/_ref/libwlref.so, kind "reference") when it was
-    built, else the project's CPU port (oracle/_build/liboracle.so, kind "port")."""
+    reference's own PathTracing.cu program run on the host cores over an emulation of its OptiX
+    calls (oracle/_ref/libwlref.so, kind "reference") when it was built, else the project's CPU
+    port of the same loop (oracle/_build/liboracle.so, kind "port"). Traversal in both is the
+    oracle's CPU BVH (OptiX is closed); the program's background is 0 instead of 0.1."""
 
     def __init__(self, scene, threads):
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -115,14 +117,21 @@ class CpuPT:
         self.keep, self.osc = po.make_or_scene(scene)
         self.bvh = self.lib.lib.or_bvh_create(self.osc.V, self.osc.I, self.osc.nT)
         self.film = np.zeros((H, W, 3), np.float32)
+        self.film4 = np.zeros((H, W, 4), np.float32)
+        if self.kind == "reference":
+            f = self.lib.lib.ref_program_pt
+            f.restype = C.c_uint64
+            f.argtypes = [C.POINTER(po.OrScene), C.c_void_p, C.POINTER(po.Camera), C.c_uint32,
+                          C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_void_p, C.c_uint32,
+                          C.c_uint32]
         self.npx = None
 
     def run(self, lo, hi):
         C = self.C
         t = time.perf_counter()
         if self.kind == "reference":
-            self.lib.lib.ref_render(C.byref(self.osc), self.bvh, C.byref(self.cam), C.byref(self.p),
-                                    self.threads, self.film.ctypes.data, lo, hi)
+            self.lib.lib.ref_program_pt(C.byref(self.osc), self.bvh, C.byref(self.cam), W, H, SPP, 0,
+                                        self.threads, self.film4.ctypes.data, lo, hi)
         else:
             self.lib.lib.or_render(C.byref(self.osc), self.bvh, C.byref(self.cam), C.byref(self.p), 0,
                                    self.threads, self.film.ctypes.data, None, lo, hi)
@@ -140,6 +149,8 @@ class CpuPT:
         dt = self.run(lo, lo + self.npx)
         desc = (f"{self.npx} pixels ({self.npx / W:.1f} rows around the image centre) x {SPP} spp "
                 f"= {self.npx * SPP} paths in {dt:.1f} s")
+        if self.kind == "reference":
+            desc += " (PathTracing.cu as compiled: depth cap 25, background 0)"
         return self.npx * SPP / dt / 1e6, desc
 
     def close(self):

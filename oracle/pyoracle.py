@@ -431,3 +431,30 @@ class RefLib:
             self.lib.or_bvh_destroy(h)
         del keep
         return rad
+
+    def _program(self, fn, scene, cam, W, H, spp, first_frame, threads, radiance, extra=()):
+        rad = np.zeros((H, W, 4), np.float32) if radiance is None else radiance
+        keep, osc = make_or_scene(scene)
+        h = self.lib.or_bvh_create(osc.V, osc.I, osc.nT)
+        f = getattr(self.lib, fn)
+        f.restype = C.c_uint64
+        f.argtypes = [C.POINTER(OrScene), C.c_void_p, C.POINTER(Camera), C.c_uint32, C.c_uint32,
+                      C.c_uint32, C.c_uint32, C.c_int, C.c_void_p] + [C.c_uint32] * len(extra)
+        try:
+            f(C.byref(osc), h, C.byref(cam), W, H, spp, first_frame, threads, ptr(rad), *extra)
+        finally:
+            self.lib.or_bvh_destroy(h)
+        del keep
+        return rad
+
+    def program_pt(self, scene, cam, W, H, spp, first_frame=0, threads=0, radiance=None,
+                   pixel_range=None):
+        """The reference's PathTracing.cu program itself (OptiX host emulation); returns its
+        radiance buffer [H, W, 4]."""
+        lo, hi = pixel_range or (0, W * H)
+        return self._program("ref_program_pt", scene, cam, W, H, spp, first_frame, threads, radiance,
+                             (lo, hi))
+
+    def program_ao(self, scene, cam, W, H, spp, first_frame=0, threads=0, radiance=None):
+        """The reference's AO.cu program itself (views where every camera ray hits)."""
+        return self._program("ref_program_ao", scene, cam, W, H, spp, first_frame, threads, radiance)

@@ -110,6 +110,9 @@ uint64_t ref_render_bdpt(const or_scene *s, void *bvh, const wl_camera *cam, uin
     for (uint32_t k = 0; k < s->nT; k++) record_of_prim[k] = &records[mesh_of[k]];
     g_emu_scene.record_of_prim = record_of_prim.data();
     g_emu_scene.mesh_first = mesh_first.data();
+    EasyRender::Programs::BDPT::MissData miss{};
+    miss.bg_color = glm::vec3(0.f, 0.f, 0.f);  // BDPTProgramManager.cpp:69
+    g_emu_scene.miss_record = &miss;
     g_emu_programs.closest_hit[0] = __closesthit__radiance;
     g_emu_programs.closest_hit[1] = __closesthit__radiance;
     g_emu_programs.miss[0] = __miss__radiance;

@@ -8,7 +8,8 @@
 //                  SBToffset, with the payload registers passed in and copied back afterwards
 //   optixGet*      launch index/dimensions, payload registers, hit triangle (index relative to
 //                  its mesh), barycentrics, world ray and t of the current hit
-//   optixGetSbtDataPointer  the hit record of the mesh that holds the hit triangle
+//   optixGetSbtDataPointer  the hit record of the mesh that holds the hit triangle, or the miss
+//                  record inside a miss program
 // The calling translation unit fills g_emu_scene and g_emu_programs before the first launch.
 #pragma once
 #include <cstdint>
@@ -25,6 +26,7 @@ typedef unsigned long long CUdeviceptr;
 struct EmuScene {
     const void *const *record_of_prim;  // hit record (SBT data) of the mesh holding each triangle
     const uint32_t *mesh_first;         // first triangle of that mesh
+    const void *miss_record;            // SBT data of the miss programs
 };
 struct EmuPrograms {
     void (*closest_hit[2])();
@@ -39,6 +41,7 @@ struct EmuThread {
     uint32_t prim;
     float u, v, t;
     float3 org, dir;
+    bool in_miss;
 };
 inline thread_local EmuThread g_emu;
 
@@ -54,6 +57,7 @@ inline float3 optixGetWorldRayOrigin() { return g_emu.org; }
 inline float3 optixGetWorldRayDirection() { return g_emu.dir; }
 inline float optixGetRayTmax() { return g_emu.t; }
 inline CUdeviceptr optixGetSbtDataPointer() {
+    if (g_emu.in_miss) return (CUdeviceptr)(uintptr_t)g_emu_scene.miss_record;
     return (CUdeviceptr)(uintptr_t)g_emu_scene.record_of_prim[g_emu.prim];
 }
 
@@ -75,6 +79,7 @@ inline void optixTrace(OptixTraversableHandle handle, float3 org, float3 dir, fl
     const bool first = (flags & OPTIX_RAY_FLAG_TERMINATE_ON_FIRST_HIT) != 0;
     or_cast_bvh((void *)(uintptr_t)handle, &r, 1, first ? WL_CAST_ANY : WL_CAST_CLOSEST, &h);
     if (h.prim == 0xFFFFFFFFu) {
+        g_emu.in_miss = true;
         g_emu_programs.miss[miss_index]();
     } else if (!(flags & OPTIX_RAY_FLAG_DISABLE_CLOSESTHIT)) {
         g_emu.prim = h.prim;
@@ -83,6 +88,7 @@ inline void optixTrace(OptixTraversableHandle handle, float3 org, float3 dir, fl
         g_emu.t = h.t;
         g_emu.org = org;
         g_emu.dir = dir;
+        g_emu.in_miss = false;
         g_emu_programs.closest_hit[sbt_offset]();
     }
     k = 0;

@@ -4,9 +4,9 @@ The reference (Extra-Creativity/Wayland) has no tests and no golden vectors of i
 fixtures are the outputs of its src/Frontend/Device/*.h functions (tea<4>, rnd, PinholeGenerateRay,
 SampleDisneyBSDF, EvalDisneyBSDF, PdfDisneyBSDF, AceApprox) compiled on the host from the
 reference tree by oracle/ref_build (-> oracle/_ref/libwlref.so), plus a small image rendered by
-the path loop of PathTracing.cu:40-288 written over those functions, and two images rendered
-by the reference's BDPT program itself (Programs/BDPT/BDPT.cu compiled on the host with its
-OptiX calls emulated over the oracle's CPU BVH, oracle/ref_build/ref_bdpt.cpp). sin/cos/log inside the
+the path loop of PathTracing.cu:40-288 written over those functions, and images rendered by
+the reference's PathTracing.cu, AO.cu and BDPT.cu programs themselves (compiled on the host with their OptiX
+calls emulated over the oracle's CPU BVH, oracle/ref_build/ref_programs.cpp and ref_bdpt.cpp). sin/cos/log inside the
 reference functions are routed to the project's own single-precision versions (see
 oracle/ref_build/shim/wl_ref_math.h), so the vectors pin the oracle bit for bit.
 
@@ -126,6 +126,24 @@ def main():
                             N=bsc.N if bsc.N is not None else np.zeros(0, np.float32),
                             cam=np.array([list(bcam.pos), list(bcam.look_at), list(bcam.up),
                                           list(bcam.right)], np.float32))
+    # the reference's own PathTracing.cu and AO.cu programs over the OptiX host emulation
+    # (oracle/ref_build/ref_programs.cpp): the displaced sphere with vertex normals and four
+    # lights (the programs' background is 0), and ambient occlusion in a closed room (AO.cu
+    # needs every camera ray to hit: after a miss it traces from the payload's stale hit point)
+    sph2 = scenes.displaced_sphere(48, 32, subdiv=24, seed=3)
+    c2 = po.Camera()
+    for k in ("pos", "look_at", "up", "right"):
+        getattr(c2, k)[:] = [float(x) for x in sph2.camera[k]]
+    rad = ref.program_pt(sph2, c2, 48, 32, 4)
+    np.savez_compressed(os.path.join(HERE, "program_pt_sphere_48x32_4spp.npz"), image=rad[..., :3].copy(),
+                        V=sph2.V, I=sph2.I)
+    room = scenes.door_slit_room(32, 24, cells=8, slit=0.0)
+    c3 = po.Camera()
+    for k in ("pos", "look_at", "up", "right"):
+        getattr(c3, k)[:] = [float(x) for x in room.camera[k]]
+    rad = ref.program_ao(room, c3, 32, 24, 2)
+    np.savez_compressed(os.path.join(HERE, "program_ao_room_32x24_2spp.npz"), image=rad[..., :3].copy(),
+                        V=room.V, I=room.I)
     print("golden vectors written to", HERE)
 
 

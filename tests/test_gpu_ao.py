@@ -60,3 +60,16 @@ def test_ao_vs_oracle(ctx, oracle, rng):
     wl.render_ao(ctx, s, sc.camera_struct(), wl.ao_params(48, 40, 1, first_frame=2, rng=rng, seed=5,
                                                           radius=0.1, ao_rays=8, camera_samples=3), f2)
     assert np.array_equal(bits(f2.download()), bits(ref))
+
+
+def test_ao_program_golden(ctx):
+    """GPU strict AO == the reference's AO.cu program itself, closed room, bit for bit."""
+    g = dict(np.load(os.path.join(GOLD, "program_ao_room_32x24_2spp.npz")))
+    sc = scenes.door_slit_room(32, 24, cells=8, slit=0.0)
+    assert np.array_equal(sc.V, g["V"]) and np.array_equal(sc.I, g["I"])
+    s = wl.Scene(ctx, sc)
+    film = wl.Film(ctx, 32, 24)
+    wl.render_ao(ctx, s, sc.camera_struct(), wl.ao_params(32, 24, 2), film)
+    assert np.array_equal(bits(film.download()), bits(g["image"]))
+    film.close()
+    s.close()

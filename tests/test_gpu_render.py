@@ -173,3 +173,14 @@ def test_path_tracer_program(ctx, oracle):
     pt.End()
     ref, _, _ = oracle.render(sc, ocam(sc), oparams(wl.render_params(24, 24, 3, math=wl.MATH_STRICT)))
     assert np.array_equal(bits(img), bits(ref))
+
+
+def test_program_pt_golden_strict(ctx):
+    """GPU strict mode == the reference's PathTracing.cu program itself (vertex normals, Disney
+    lobes, four lights; the program's background is 0), bit for bit."""
+    g = dict(np.load(os.path.join(GOLD, "program_pt_sphere_48x32_4spp.npz")))
+    sc = small_sphere(48, 32)
+    assert np.array_equal(sc.V, g["V"]) and np.array_equal(sc.I, g["I"])
+    p = wl.render_params(48, 32, 4, math=wl.MATH_STRICT, env=(0.0, 0.0, 0.0))
+    img, _, _, _ = gpu_render(ctx, sc, p)
+    assert np.array_equal(bits(img), bits(g["image"]))

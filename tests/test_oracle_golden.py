@@ -141,3 +141,34 @@ def test_bdpt_image(oracle, name, make):
     img, _, rays = oracle.render_bdpt(sc, cam, p)
     assert np.isfinite(g["image"]).all() and g["image"].max() > 0
     assert np.array_equal(bits(img), bits(g["image"]))
+
+
+def test_program_pt_image(oracle):
+    """The oracle's path tracer reproduces the reference's PathTracing.cu program itself (run
+    over the OptiX host emulation) bit for bit: vertex normals, Disney lobes, four lights."""
+    g = dict(np.load(os.path.join(GOLD, "program_pt_sphere_48x32_4spp.npz")))
+    sc = scenes.displaced_sphere(48, 32, subdiv=24, seed=3)
+    assert np.array_equal(sc.V, g["V"]) and np.array_equal(sc.I, g["I"])
+    cam = po.Camera()
+    for k in ("pos", "look_at", "up", "right"):
+        getattr(cam, k)[:] = [float(x) for x in sc.camera[k]]
+    p = po.RenderParams(width=48, height=32, spp=4, first_frame=0, max_depth=25, rr_depth=5,
+                        rr_prob=0.9, eps=1e-3, strategy=2, rng=0, math=1, lights=0, seed=0)
+    img, _, _ = oracle.render(sc, cam, p)
+    assert g["image"].max() > 0
+    assert np.array_equal(bits(img), bits(g["image"]))
+
+
+def test_program_ao_image(oracle):
+    """The oracle's ambient occlusion reproduces the reference's AO.cu program itself in a
+    closed room (every camera ray hits)."""
+    g = dict(np.load(os.path.join(GOLD, "program_ao_room_32x24_2spp.npz")))
+    sc = scenes.door_slit_room(32, 24, cells=8, slit=0.0)
+    assert np.array_equal(sc.V, g["V"]) and np.array_equal(sc.I, g["I"])
+    cam = po.Camera()
+    for k in ("pos", "look_at", "up", "right"):
+        getattr(cam, k)[:] = [float(x) for x in sc.camera[k]]
+    p = po.AoParams(width=32, height=24, spp=2, first_frame=0, camera_samples=4, ao_rays=32,
+                    radius=1.0, eps=1e-3, rng=0, wave_paths=0, seed=0)
+    img, _, _ = oracle.render_ao(sc, cam, p)
+    assert np.array_equal(bits(img), bits(g["image"]))
