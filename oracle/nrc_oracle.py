@@ -1,9 +1,11 @@
 """FP64 CPU oracle of the radiance-cache MLP (test infrastructure only).
 
-Restates the network of wayland_b200/csrc/wl_nrc.cuh and nrc.cu in numpy float64: inputs,
+Restates the network of wayland_b200/csrc/wl_nrc.cuh and nrc_tc.cu in numpy float64: inputs,
 weights and hidden activations rounded to bfloat16 (round to nearest even) as the device does,
 products and sums in float64; relative L2 loss sum_{s,c<3} (o - t)^2 / (o^2 + 0.01) / (3 n) and
-its exact gradient with respect to the 17408 weights (W0..W3 64x64, W4 16x64, row = output).
+its gradient with respect to the 17408 weights (W0..W3 64x64, W4 16x64, row = output), with the
+loss gradient dY and the pre-activation gradients dZ_l rounded to bfloat16 where the device's
+tensor-core backward pass rounds them (they are MMA operands there).
 """
 import numpy as np
 
@@ -37,8 +39,9 @@ def forward(w, x):
     return a @ Ws[MATS].T, acts
 
 
-def gradients(w, x, t):
+def gradients(w, x, t, bf16_deltas=True):
     """Loss and dLoss/dW (float64, length 17408)."""
+    rd = bf16r if bf16_deltas else (lambda a: a)
     Ws = split(w)
     o, acts = forward(w, x)
     n = len(x)
@@ -47,11 +50,12 @@ def gradients(w, x, t):
     loss = float(((o3 - t[:, :3]) ** 2 / den).sum() / (3 * n))
     d = np.zeros_like(o)
     d[:, :3] = 2.0 * (o3 - t[:, :3]) / den / (3 * n)
+    d = rd(d)
     grads = [None] * (MATS + 1)
     grads[MATS] = d.T @ acts[MATS]
     g = d @ Ws[MATS]
     for l in range(MATS - 1, -1, -1):
-        dl = g * (acts[l + 1] > 0)
+        dl = rd(g * (acts[l + 1] > 0))
         grads[l] = dl.T @ acts[l]
         g = dl @ Ws[l]
     return loss, np.concatenate([gr.reshape(-1) for gr in grads])

@@ -231,6 +231,286 @@ __global__ void __launch_bounds__(TC_THREADS) k_mlp_tc(const float *w, NrcGrid g
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
 }
 
+// ---------------------------------------------------------------------------------------
+// Training step on the tensor cores: forward, relative-L2 loss, backward and weight gradients
+// of 128 samples per tile, fused in one persistent kernel (one CTA of 256 threads per SM).
+// Thread t owns sample row r = t % 128 and column half h = t / 128 of every 64-wide tile (warp
+// w reads tensor-memory lanes 32 (w % 4) .. + 31). Operands are bfloat16 with FP32
+// accumulation: activations (as in inference), the loss gradient dY and the pre-activation
+// gradients dZ are rounded to bfloat16 where they become MMA operands.
+//   forward   A_{l+1} = relu(A_l W_l^T), out = A_4 W_4^T            (M=128, K=64, N=64 / 16)
+//   backward  dA_4 = dY W_4, dZ_l = dA_{l+1} * [A_{l+1} > 0], dA_l = dZ_l W_l
+//   weights   dW_l += dZ_l^T A_l over the tile's 128 samples (K = 128), accumulated in tensor
+//             memory across all tiles of the CTA (M = 128 with the rows past the 64 (16) outputs
+//             unused), added to the global gradient once at the end
+//   grid      dA_0[:, 0:32] scattered into the hash grid's gradient
+// Tensor memory: columns 0-63 forward D, 64-127 backward D, 128 + 64 l the dW_l accumulators.
+constexpr int TR_THREADS = 256;
+constexpr uint32_t TR_TMEM_COLS = 512;
+constexpr uint32_t TS_DYT = 0;                  // dY^T, 16 x 128 (its M=128 read spans 32 KB)
+constexpr uint32_t TS_DY = 4096;                // dY, 128 x 16
+constexpr uint32_t TS_W = 8192;                 // W_0..W_3 (row = output), 8 KB each
+constexpr uint32_t TS_W4 = TS_W + 4 * 8192;     // W_4, 16 x 64
+constexpr uint32_t TS_WT = TS_W4 + 2048;        // W_0^T..W_3^T (row = input)
+constexpr uint32_t TS_W4T = TS_WT + 4 * 8192;   // W_4^T, 64 x 16
+constexpr uint32_t TS_T0 = TS_W4T + 2048;       // A_0, A_2, A_4
+constexpr uint32_t TS_T1 = TS_T0 + 16384;       // A_1, A_3, then dZ
+constexpr uint32_t TS_DZT = TS_T1 + 16384;      // dZ^T, 64 x 128 (its M=128 read spans 32 KB)
+constexpr uint32_t TS_AT = TS_DZT + 16384;      // A_0^T..A_4^T, 64 x 128 each
+constexpr uint32_t TS_BAR = TS_AT + 5 * 16384;
+constexpr uint32_t TS_TMEM = TS_BAR + 8;
+constexpr uint32_t TS_BYTES = TS_TMEM + 8;
+
+// K-major tiles with 16 and 128 columns (core matrices 8 rows x 16 bytes)
+__device__ __forceinline__ uint32_t kmaj16(uint32_t r, uint32_t k) {
+    return (r >> 3) * 256u + (k >> 3) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
+}
+__device__ __forceinline__ uint32_t kmaj128(uint32_t r, uint32_t k) {
+    return (r >> 3) * 2048u + (k >> 3) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
+}
+__device__ __forceinline__ uint64_t sdesc_s(uint32_t saddr, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) |
+           ((uint64_t)(sbo >> 4) << 32) | (1ull << 46);
+}
+
+// 8 consecutive values (k0 multiple of 8) of row r of a 64-wide K-major tile, as bfloat16
+__device__ __forceinline__ void store8(uint8_t *tile, uint32_t r, uint32_t k0, const float *x) {
+    __nv_bfloat162 p0 = __floats2bfloat162_rn(x[0], x[1]);
+    __nv_bfloat162 p1 = __floats2bfloat162_rn(x[2], x[3]);
+    __nv_bfloat162 p2 = __floats2bfloat162_rn(x[4], x[5]);
+    __nv_bfloat162 p3 = __floats2bfloat162_rn(x[6], x[7]);
+    uint4 u;
+    u.x = *reinterpret_cast<uint32_t *>(&p0);
+    u.y = *reinterpret_cast<uint32_t *>(&p1);
+    u.z = *reinterpret_cast<uint32_t *>(&p2);
+    u.w = *reinterpret_cast<uint32_t *>(&p3);
+    *reinterpret_cast<uint4 *>(tile + kmaj(r, k0)) = u;
+}
+// column k of a transposed 128-column tile (row = feature, column = sample r)
+__device__ __forceinline__ void store_t(uint8_t *tile, uint32_t k, uint32_t r, float x) {
+    *reinterpret_cast<__nv_bfloat16 *>(tile + kmaj128(k, r)) = __float2bfloat16_rn(x);
+}
+
+__device__ __forceinline__ bool tc_step(uint32_t bar, uint32_t &phase) {
+    bool got = mbar_wait(bar, phase);
+    phase ^= 1u;
+    bool ok = __syncthreads_and(got) != 0;
+    tc_after_sync();
+    return ok;
+}
+__device__ __forceinline__ void smem_to_tc() {
+    fence_async_smem();
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+}
+
+// MODE 0: raw rows in[n][64], targets target[n][4]. MODE 1: the collected training samples
+// (count on the device), encoded here; the input gradient goes to the hash grid.
+template <int MODE>
+__global__ void __launch_bounds__(TR_THREADS, 1)
+    k_train_tc(const float *w, NrcGrid g, const wl_disney *mats, const NrcVertex *samples,
+               const uint32_t *n_ptr, uint32_t n_fixed, const float *in, const float *target,
+               float *w_grad, float *loss, uint32_t *err) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    const uint32_t r = tid & 127u, h = tid >> 7;
+    const uint32_t bar = smem_u32(smem + TS_BAR);
+    for (uint32_t i = tid; i < (uint32_t)NRC_WEIGHTS; i += TR_THREADS) {
+        uint32_t l = i / 4096u, rem = i % 4096u;
+        uint32_t o = rem / 64u, k = rem % 64u;
+        __nv_bfloat16 b = __float2bfloat16_rn(w[i]);
+        if (l < 4) {
+            *reinterpret_cast<__nv_bfloat16 *>(smem + TS_W + l * 8192u + kmaj(o, k)) = b;
+            *reinterpret_cast<__nv_bfloat16 *>(smem + TS_WT + l * 8192u + kmaj(k, o)) = b;
+        } else {
+            *reinterpret_cast<__nv_bfloat16 *>(smem + TS_W4 + kmaj(o, k)) = b;
+            *reinterpret_cast<__nv_bfloat16 *>(smem + TS_W4T + kmaj16(k, o)) = b;
+        }
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(smem + TS_TMEM)),
+                     "r"(TR_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    smem_to_tc();
+    const uint32_t tmem = *reinterpret_cast<volatile uint32_t *>(smem + TS_TMEM);
+    const uint32_t lane = ((warp & 3u) * 32u) << 16;
+    const uint32_t n = MODE == 1 ? min(*n_ptr, n_fixed) : n_fixed;
+    const float inv = n ? 1.0f / (3.0f * (float)n) : 0.0f;
+    const uint32_t ID64 = idesc(64, 128), ID16 = idesc(16, 128);
+    const uint32_t sT0 = smem_u32(smem + TS_T0), sT1 = smem_u32(smem + TS_T1);
+    const uint32_t sAT = smem_u32(smem + TS_AT), sDZT = smem_u32(smem + TS_DZT);
+    const uint32_t sW = smem_u32(smem + TS_W), sWT = smem_u32(smem + TS_WT);
+    uint32_t phase = 0;
+    bool ok = true, any = false;
+    float lsum = 0.0f;
+    for (uint32_t tile = blockIdx.x * 128u; tile < n && ok; tile += gridDim.x * 128u) {
+        const uint32_t i = tile + r;
+        const bool valid = i < n;
+        // ---- inputs: columns [16h, 16h + 16) and [32 + 16h, 32 + 16h + 16)
+        float x[32], t3[3] = {0.f, 0.f, 0.f};
+        NrcVertex v{};
+        if (valid) {
+            if (MODE == 1) {
+                v = samples[i];
+                float3 pn = grid_normalise(g, v.pos_mat);
+                nrc_grid_features(g, pn, 8u * h, x);
+                if (h == 0) nrc_dir_features(v, x + 16);
+                else nrc_aux_features(mats, v, x + 16);
+                t3[0] = v.extra.x; t3[1] = v.extra.y; t3[2] = v.extra.z;
+            } else {
+                for (int k = 0; k < 16; k++) {
+                    x[k] = in[(size_t)i * NRC_IN + 16 * h + k];
+                    x[16 + k] = in[(size_t)i * NRC_IN + 32 + 16 * h + k];
+                }
+                for (int c = 0; c < 3; c++) t3[c] = target[(size_t)i * 4 + c];
+            }
+        } else {
+            for (int k = 0; k < 32; k++) x[k] = 0.0f;
+        }
+        store8(smem + TS_T0, r, 16 * h, x);
+        store8(smem + TS_T0, r, 16 * h + 8, x + 8);
+        store8(smem + TS_T0, r, 32 + 16 * h, x + 16);
+        store8(smem + TS_T0, r, 32 + 16 * h + 8, x + 24);
+        for (int k = 0; k < 16; k++) {
+            store_t(smem + TS_AT, 16 * h + k, r, x[k]);
+            store_t(smem + TS_AT, 32 + 16 * h + k, r, x[16 + k]);
+        }
+        smem_to_tc();
+        // ---- forward
+        uint32_t mask[4];
+        for (uint32_t l = 0; l < 5 && ok; l++) {
+            const uint32_t sA = (l & 1u) ? sT1 : sT0;
+            const uint32_t sB = l < 4 ? sW + l * 8192u : smem_u32(smem + TS_W4);
+            if (tid == 0) {
+#pragma unroll
+                for (uint32_t ks = 0; ks < 4; ks++)
+                    mma_bf16(tmem, sdesc(sA + ks * 256u), sdesc(sB + ks * 256u), l < 4 ? ID64 : ID16,
+                             ks > 0 ? 1u : 0u);
+                mma_commit(bar);
+            }
+            ok = tc_step(bar, phase);
+            if (!ok) break;
+            if (l < 4) {
+                float a[32];
+                tmem_ld16(tmem + lane + 32u * h, a);
+                tmem_ld16(tmem + lane + 32u * h + 16u, a + 16);
+                tmem_wait_ld();
+                uint32_t m = 0;
+#pragma unroll
+                for (int k = 0; k < 32; k++) {
+                    a[k] = bf16r(fmaxf(a[k], 0.0f));
+                    m |= (a[k] > 0.0f ? 1u : 0u) << k;
+                }
+                mask[l] = m;
+                uint8_t *next = smem + ((l & 1u) ? TS_T0 : TS_T1);
+#pragma unroll
+                for (int c = 0; c < 4; c++) store8(next, r, 32 * h + 8 * c, a + 8 * c);
+                uint8_t *at = smem + TS_AT + (l + 1) * 16384u;
+                for (int k = 0; k < 32; k++) store_t(at, 32 * h + k, r, a[k]);
+            } else if (h == 0) {
+                float o[16], d[16];
+                tmem_ld16(tmem + lane, o);
+                tmem_wait_ld();
+#pragma unroll
+                for (int c = 0; c < 16; c++) d[c] = 0.0f;
+                if (valid) {
+                    for (int c = 0; c < 3; c++) {
+                        float den = o[c] * o[c] + 0.01f;
+                        float e = o[c] - t3[c];
+                        lsum += e * e / den * inv;
+                        d[c] = 2.0f * e / den * inv;
+                    }
+                }
+                __nv_bfloat16 *dy = reinterpret_cast<__nv_bfloat16 *>(smem + TS_DY);
+                for (int c = 0; c < 16; c++) {
+                    dy[kmaj16(r, c) / 2] = __float2bfloat16_rn(d[c]);
+                    store_t(smem + TS_DYT, c, r, d[c]);
+                }
+            }
+            smem_to_tc();
+        }
+        if (!ok) break;
+        // ---- backward, output layer: dA_4 = dY W_4, dW_4 += dY^T A_4
+        if (tid == 0) {
+            mma_bf16(tmem + 64u, sdesc_s(smem_u32(smem + TS_DY), 256u),
+                     sdesc_s(smem_u32(smem + TS_W4T), 256u), ID64, 0u);
+#pragma unroll
+            for (uint32_t ks = 0; ks < 8; ks++)
+                mma_bf16(tmem + 128u + 4u * 64u, sdesc_s(smem_u32(smem + TS_DYT) + ks * 256u, 2048u),
+                         sdesc_s(sAT + 4u * 16384u + ks * 256u, 2048u), ID64, (any || ks > 0) ? 1u : 0u);
+            mma_commit(bar);
+        }
+        ok = tc_step(bar, phase);
+        for (int l = 3; l >= 0 && ok; l--) {
+            // dZ_l = dA_{l+1} masked by the activation of layer l
+            float d[32];
+            tmem_ld16(tmem + lane + 64u + 32u * h, d);
+            tmem_ld16(tmem + lane + 64u + 32u * h + 16u, d + 16);
+            tmem_wait_ld();
+#pragma unroll
+            for (int k = 0; k < 32; k++)
+                if (!((mask[l] >> k) & 1u)) d[k] = 0.0f;
+#pragma unroll
+            for (int c = 0; c < 4; c++) store8(smem + TS_T1, r, 32 * h + 8 * c, d + 8 * c);
+            for (int k = 0; k < 32; k++) store_t(smem + TS_DZT, 32 * h + k, r, d[k]);
+            smem_to_tc();
+            if (tid == 0) {
+#pragma unroll
+                for (uint32_t ks = 0; ks < 4; ks++)
+                    mma_bf16(tmem + 64u, sdesc(sT1 + ks * 256u), sdesc(sWT + l * 8192u + ks * 256u), ID64,
+                             ks > 0 ? 1u : 0u);
+#pragma unroll
+                for (uint32_t ks = 0; ks < 8; ks++)
+                    mma_bf16(tmem + 128u + 64u * l, sdesc_s(sDZT + ks * 256u, 2048u),
+                             sdesc_s(sAT + l * 16384u + ks * 256u, 2048u), ID64, (any || ks > 0) ? 1u : 0u);
+                mma_commit(bar);
+            }
+            ok = tc_step(bar, phase);
+        }
+        if (!ok) break;
+        // ---- input gradient of the grid features: levels [8h, 8h + 8)
+        {
+            float gin[16];
+            tmem_ld16(tmem + lane + 64u + 16u * h, gin);
+            tmem_wait_ld();
+            if (MODE == 1 && valid) nrc_grid_backward(g, v, gin, 8u * h, 8u * h + 8u);
+        }
+        any = true;
+        tc_before_sync();
+        __syncthreads();
+        tc_after_sync();
+    }
+    if (ok && any && r < 64u) {
+        // dW_l rows (outputs) r, columns [32h, 32h + 32)
+        for (uint32_t l = 0; l < 5; l++) {
+            float a[32];
+            tmem_ld16(tmem + lane + 128u + 64u * l + 32u * h, a);
+            tmem_ld16(tmem + lane + 128u + 64u * l + 32u * h + 16u, a + 16);
+            tmem_wait_ld();
+            const uint32_t rows = l < 4 ? 64u : 16u;
+            if (r < rows)
+                for (int k = 0; k < 32; k++) atomicAdd(w_grad + l * 4096u + r * 64u + 32u * h + k, a[k]);
+        }
+    }
+    for (int off = 16; off > 0; off >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, off);
+    if ((tid & 31u) == 0 && lsum != 0.0f) atomicAdd(loss, lsum);
+    if (!ok) {
+        if (tid == 0) atomicExch(err, 1u);
+        mbar_wait(bar, phase ^ 1u);
+    }
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TR_TMEM_COLS));
+}
+
 int tc_grid(const void *k) {
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
@@ -261,6 +541,32 @@ void nrc_tc_query(const float *w, const NrcGrid &g, const wl_disney *mats, const
     uint32_t blocks = tiles < (uint32_t)grid ? tiles : (uint32_t)grid;
     if (blocks == 0) blocks = 1;
     k_mlp_tc<1><<<blocks, TC_THREADS, SM_BYTES, s>>>(w, g, mats, q, nq, rad, nullptr, nullptr, 0, err);
+}
+
+// Gradients of one training step into w_grad (zeroed here) and the grid gradient; loss (zeroed
+// here) receives the mean relative L2 loss. Raw rows when samples is null.
+void nrc_tc_train(const float *w, const NrcGrid &g, const wl_disney *mats, const NrcVertex *samples,
+                  const uint32_t *n_ptr, uint32_t n_max, const float *in, const float *target,
+                  float *w_grad, float *loss, uint32_t *err, cudaStream_t s) {
+    static int sms = [] {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        cudaFuncSetAttribute(k_train_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS_BYTES);
+        cudaFuncSetAttribute(k_train_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS_BYTES);
+        return v;
+    }();
+    cudaMemsetAsync(w_grad, 0, NRC_WEIGHTS * sizeof(float), s);
+    cudaMemsetAsync(loss, 0, sizeof(float), s);
+    uint32_t tiles = (n_max + 127u) / 128u;
+    uint32_t blocks = tiles < (uint32_t)sms ? tiles : (uint32_t)sms;
+    if (blocks == 0) return;
+    if (samples)
+        k_train_tc<1><<<blocks, TR_THREADS, TS_BYTES, s>>>(w, g, mats, samples, n_ptr, n_max, nullptr,
+                                                           nullptr, w_grad, loss, err);
+    else
+        k_train_tc<0><<<blocks, TR_THREADS, TS_BYTES, s>>>(w, g, mats, nullptr, nullptr, n_max, in,
+                                                           target, w_grad, loss, err);
 }
 
 }  // namespace wl

@@ -100,12 +100,11 @@ __device__ __forceinline__ void sh16(float x, float y, float z, float *o) {
     o[15] = 0.59004358992664352f * x * (-xx + 3.0f * yy);
 }
 
-// The 64 input features of a vertex (rounded to bfloat16).
-__device__ __forceinline__ void nrc_encode(const NrcGrid &g, const wl_disney *mats,
-                                           const NrcVertex &v, float *x) {
-    float3 pn = grid_normalise(g, v.pos_mat);
+// Hash-grid features of levels [l0, l0 + 8): x[0..15] (rounded to bfloat16).
+__device__ __forceinline__ void nrc_grid_features(const NrcGrid &g, float3 pn, uint32_t l0, float *x) {
     const uint32_t F = 2;
-    for (uint32_t l = 0; l < NRC_MAX_LEVELS; l++) {
+    for (uint32_t j = 0; j < 8; j++) {
+        const uint32_t l = l0 + j;
         float f0 = 0.0f, f1 = 0.0f;
         if (l < g.levels) {
             uint32_t res = grid_res(g, l);
@@ -121,28 +120,48 @@ __device__ __forceinline__ void nrc_encode(const NrcGrid &g, const wl_disney *ma
                 f1 += w * e.y;
             }
         }
-        x[2 * l] = bf16r(f0);
-        x[2 * l + 1] = bf16r(f1);
+        x[2 * j] = bf16r(f0);
+        x[2 * j + 1] = bf16r(f1);
     }
+}
+
+// Spherical harmonics of the outgoing direction: x[0..15] (bfloat16).
+__device__ __forceinline__ void nrc_dir_features(const NrcVertex &v, float *x) {
     float sh[16];
     sh16(v.wo.x, v.wo.y, v.wo.z, sh);
-    for (int k = 0; k < 16; k++) x[32 + k] = bf16r(sh[k]);
+    for (int k = 0; k < 16; k++) x[k] = bf16r(sh[k]);
+}
+
+// Normal, roughness, albedos, transmission, constant: x[0..15] (bfloat16).
+__device__ __forceinline__ void nrc_aux_features(const wl_disney *mats, const NrcVertex &v, float *x) {
     const wl_disney &m = mats[__float_as_uint(v.pos_mat.w)];
     float dif = (1.0f - m.metallic) * (1.0f - m.trans);
     float aux[16] = {v.n.x * 0.5f + 0.5f, v.n.y * 0.5f + 0.5f, v.n.z * 0.5f + 0.5f, m.roughness,
                      m.color[0] * dif, m.color[1] * dif, m.color[2] * dif,
                      lerpf(0.04f, m.color[0], m.metallic), lerpf(0.04f, m.color[1], m.metallic),
                      lerpf(0.04f, m.color[2], m.metallic), m.trans, 1.0f, 0.f, 0.f, 0.f, 0.f};
-    for (int k = 0; k < 16; k++) x[48 + k] = bf16r(aux[k]);
+    for (int k = 0; k < 16; k++) x[k] = bf16r(aux[k]);
 }
 
-// Scatter the gradient of the first 2L inputs into the grid's gradient.
+// The 64 input features of a vertex (rounded to bfloat16).
+__device__ __forceinline__ void nrc_encode(const NrcGrid &g, const wl_disney *mats,
+                                           const NrcVertex &v, float *x) {
+    float3 pn = grid_normalise(g, v.pos_mat);
+    nrc_grid_features(g, pn, 0, x);
+    nrc_grid_features(g, pn, 8, x + 16);
+    nrc_dir_features(v, x + 32);
+    nrc_aux_features(mats, v, x + 48);
+}
+
+// Scatter the gradient of the grid features of levels [l0, l1) (gin[2 (l - l0) + f]) into the
+// grid's gradient.
 __device__ __forceinline__ void nrc_grid_backward(const NrcGrid &g, const NrcVertex &v,
-                                                  const float *gin) {
+                                                  const float *gin, uint32_t l0 = 0,
+                                                  uint32_t l1 = NRC_MAX_LEVELS) {
     float3 pn = grid_normalise(g, v.pos_mat);
     const uint32_t F = 2;
-    for (uint32_t l = 0; l < g.levels; l++) {
-        float g0 = gin[2 * l], g1 = gin[2 * l + 1];
+    for (uint32_t l = l0; l < l1 && l < g.levels; l++) {
+        float g0 = gin[2 * (l - l0)], g1 = gin[2 * (l - l0) + 1];
         if (g0 == 0.0f && g1 == 0.0f) continue;
         uint32_t res = grid_res(g, l);
         GridCell c = grid_cell(g, pn, res);
