@@ -271,11 +271,12 @@ def raycast_microbench(wl, torch, ctx, sc, scene, stream):
 
 
 def nrc_convergence(wl, torch, ctx, res=(480, 270), oracle_spp=16384, target=1e-2,
-                    budget_s=60.0, chunk=4):
+                    budget_s=60.0, chunk=4, warmup_frames=16):
     """Time to relMSE <= target against an FP64-accumulated high-spp render, for the plain path
     tracer and for the radiance-cache path tracer, on the door-slit room (about 500K triangles,
     mostly indirect light). relMSE = mean over pixels and channels of (I - R)^2 / (R^2 + 1e-2).
-    Times are device time of the render calls (CUDA events on the library's stream)."""
+    Times are device time of the render calls (CUDA events on the library's stream); the cache's
+    time includes its warm-up frames (training only, no image) from a fresh cache."""
     from wayland_b200 import scenes
     W_, H_ = res
     sc = scenes.door_slit_room(W_, H_)
@@ -306,6 +307,13 @@ def nrc_convergence(wl, torch, ctx, res=(480, 270), oracle_spp=16384, target=1e-
         curve = []
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
+        if cache is not None and warmup_frames:
+            e0.record(stream)
+            wl.render_nrc(ctx, scene, cam, wl.render_params(W_, H_, warmup_frames, first_frame=5000000,
+                                                            max_depth=16), cache, None)
+            e1.record(stream)
+            e1.synchronize()
+            t_dev += e0.elapsed_time(e1) * 1e-3
         while True:
             n = chunk
             p = wl.render_params(W_, H_, n, first_frame=spp, max_depth=16)
@@ -355,8 +363,8 @@ def main():
     ap.add_argument("--nrc-only", action="store_true",
                     help="only the radiance-cache convergence comparison (prints its JSON)")
     ap.add_argument("--no-nrc", action="store_true")
-    ap.add_argument("--nrc-res", default="480x270", help="resolution of the radiance-cache comparison")
-    ap.add_argument("--nrc-oracle-spp", type=int, default=16384)
+    ap.add_argument("--nrc-res", default="960x540", help="resolution of the radiance-cache comparison")
+    ap.add_argument("--nrc-oracle-spp", type=int, default=8192)
     ap.add_argument("--nrc-budget-s", type=float, default=60.0)
     ap.add_argument("--case", default="full", choices=["full", "small"],
                     help="small: the same 2M-triangle scene at 960x540 x 4 spp (for ncu captures)")
@@ -501,6 +509,13 @@ def main():
         }
         if not args.no_raycast:
             line["raycast"] = raycast_microbench(wl, torch, ctx, sc, scene, stream)
+        if world == 1 and not args.no_nrc:
+            # the second half of the metric: time to relMSE 1e-2 vs an FP64 high-spp render,
+            # radiance cache vs plain path tracing (door-slit room)
+            w_, h_ = (int(v) for v in args.nrc_res.split("x"))
+            line["time_to_relmse"] = nrc_convergence(wl, torch, ctx, res=(w_, h_),
+                                                     oracle_spp=args.nrc_oracle_spp,
+                                                     budget_s=args.nrc_budget_s)
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             cpu = CpuPT(scene, threads)

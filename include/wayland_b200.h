@@ -316,8 +316,10 @@ WL_API int wl_render_ao(wl_context *ctx, wl_scene *scene, const wl_camera *camer
  * (after Mueller et al. 2022) feeding an MLP that predicts the radiance reflected at a surface
  * point, trained online on the path tracer's own estimates (after Mueller et al. 2021,
  * "Real-time Neural Radiance Caching"). Paths that are not training paths stop at
- * query_depth and add throughput x cache prediction; training paths are traced unbiased to
- * max_depth and give one training sample per surface vertex. */
+ * query_depth and add throughput x cache prediction; training paths give one training sample
+ * per surface vertex and either continue train_extra vertices past query_depth and end with
+ * the cache's prediction there (self-training, after Mueller et al. 2021), or, with
+ * train_extra = 0, are traced unbiased to max_depth. */
 typedef struct wl_nrc_params {
     uint32_t levels;            /* hash-grid levels (16) */
     uint32_t log2_table;        /* entries per level = 2^log2_table (19) */
@@ -327,6 +329,7 @@ typedef struct wl_nrc_params {
     uint32_t query_depth;       /* surface vertex where other paths query the cache (2) */
     float learning_rate;        /* Adam step size (1e-2) */
     uint32_t seed;              /* initialisation */
+    uint32_t train_extra;       /* training-path vertices past query_depth (3; 0 = full paths) */
 } wl_nrc_params;
 typedef struct wl_nrc wl_nrc;
 #define WL_NRC_WEIGHTS 17408u   /* 4 x 64 x 64 + 16 x 64 */
@@ -334,7 +337,8 @@ WL_API void wl_nrc_params_default(wl_nrc_params *params);
 WL_API int wl_nrc_create(wl_context *ctx, wl_scene *scene, const wl_nrc_params *params,
                          wl_nrc **out);
 WL_API int wl_nrc_destroy(wl_nrc *nrc);
-/* Render params->spp frames with the cache (query, then train on the frame's samples). */
+/* Render params->spp frames with the cache (query, then train on the frame's samples). With
+ * film == NULL the frames train the cache and leave no image (warm-up). */
 WL_API int wl_render_nrc(wl_context *ctx, wl_scene *scene, const wl_camera *camera,
                          const wl_render_params *params, wl_nrc *nrc, wl_film *film);
 /* Network access for tests: inputs are n x 64 feature rows (FP32, device), outputs n x 4. */

@@ -292,9 +292,11 @@ class RadianceCache:
 
 
 def render_nrc(ctx, scene, camera, params, cache, film):
-    """params.spp frames with the radiance cache: query, then one training step per frame."""
+    """params.spp frames with the radiance cache: query, then one training step per frame.
+    film=None trains the cache without producing an image (warm-up frames)."""
     _abi.check("wl_render_nrc", ctx.lib.wl_render_nrc(ctx.handle, scene.handle, C.byref(camera),
-                                                      C.byref(params), cache.handle, film.handle))
+                                                      C.byref(params), cache.handle,
+                                                      film.handle if film is not None else None))
 
 
 def render(ctx, scene, camera, params, film):

@@ -64,7 +64,8 @@ class AoParams(C.Structure):
 class NrcParams(C.Structure):
     _fields_ = [("levels", C.c_uint32), ("log2_table", C.c_uint32), ("base_resolution", C.c_uint32),
                 ("per_level_scale", C.c_float), ("train_paths", C.c_uint32),
-                ("query_depth", C.c_uint32), ("learning_rate", C.c_float), ("seed", C.c_uint32)]
+                ("query_depth", C.c_uint32), ("learning_rate", C.c_float), ("seed", C.c_uint32),
+                ("train_extra", C.c_uint32)]
 
 
 NRC_WEIGHTS = 17408

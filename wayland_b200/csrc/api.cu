@@ -908,6 +908,7 @@ void wl_nrc_params_default(wl_nrc_params *p) {
     p->query_depth = 2;
     p->learning_rate = 1e-2f;
     p->seed = 1337;
+    p->train_extra = 3;
 }
 
 static void nrc_free_buffers(wl_nrc *n) {
@@ -1031,10 +1032,10 @@ int wl_nrc_stats(wl_nrc *n, uint32_t *samples, uint32_t *queries, float *loss) {
 
 int wl_render_nrc(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_params *p,
                   wl_nrc *n, wl_film *f) {
-    ARG(c && s && cam && p && n && f, "null argument");
-    ARG(s->ctx == c && f->ctx == c && n->ctx == c && n->scene == s, "objects must belong together");
+    ARG(c && s && cam && p && n, "null argument");
+    ARG(s->ctx == c && (!f || f->ctx == c) && n->ctx == c && n->scene == s, "objects must belong together");
     if (!s->built) return fail(WL_ERR_NOT_BUILT, "bvh not built");
-    ARG(p->width == f->f.W && p->height == f->f.H, "film size differs from the render size");
+    ARG(!f || (p->width == f->f.W && p->height == f->f.H), "film size differs from the render size");
     ARG(p->spp > 0 && p->max_depth > 0 && p->max_depth <= 1024, "bad spp or max_depth");
     ARG(p->strategy <= WL_STRATEGY_MIS && p->rng <= WL_RNG_PCG32 && p->math <= WL_MATH_STRICT, "bad params");
     ARG(p->lights == WL_LIGHTS_UNIFORM, "only uniform light selection is available");
@@ -1098,6 +1099,7 @@ int wl_render_nrc(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_ren
             nb.train_stride = stride;
             nb.first_g = first_g;
             nb.max_depth = p->max_depth;
+            nb.train_end = n->p.train_extra ? n->p.query_depth + n->p.train_extra : 0u;
             nb.queries = n->queries;
             nb.n_queries = n->n_queries;
             nb.rec_v = n->rec_v; nb.rec_tr = n->rec_tr; nb.rec_rb = n->rec_rb;
@@ -1107,7 +1109,9 @@ int wl_render_nrc(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_ren
             if (strict_math) strict::launch_generate(wp, c->q, st);
             else fast::launch_generate(wp, c->q, st);
             int in = 0;
-            for (uint32_t b = 0; b < p->max_depth; b++) {
+            // every path has ended by vertex train_end when training paths end at the cache
+            const uint32_t bounces = nb.train_end && nb.train_end < p->max_depth ? nb.train_end : p->max_depth;
+            for (uint32_t b = 0; b < bounces; b++) {
                 launch_extend(sc, c->q, in, false, st);
                 CK(cudaMemsetAsync(c->q.counters + (in ^ 1), 0, sizeof(uint32_t), st));
                 CK(cudaMemsetAsync(c->q.counters + 2, 0, sizeof(uint32_t), st));
@@ -1118,14 +1122,14 @@ int wl_render_nrc(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_ren
             }
             nrc_query(n->net, s->d_mats, n->queries, n->n_queries, c->q.st_rad, wp.count, st);
             nrc_collect(n->net, nb, c->q, tcount, st);
-            strict::launch_film(wp, c->q, f->f, st);
+            if (f) strict::launch_film(wp, c->q, f->f, st);
             CK(cudaGetLastError());
         }
         // clamp the sample count to the buffer and train one step on the frame's samples
         nrc_train_collected(n->net, s->d_mats, st);
         CK(cudaGetLastError());
     }
-    f->f.frames64 += p->spp;
+    if (f) f->f.frames64 += p->spp;
     return WL_OK;
 }
 

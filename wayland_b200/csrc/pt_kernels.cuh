@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(PT) k_shade(WaveParams wp, DevScene sc, Queues
                         rv.pos_mat = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, __uint_as_float(ti.w & 0x7fffffffu));
                         rv.wo = make_float4(V.x, V.y, V.z, 0.f);
                         rv.n = make_float4(Ns.x, Ns.y, Ns.z, 0.f);
-                        if (train) {
+                        if (train && depth != nb.train_end) {
                             uint32_t tl = (uint32_t)((g - nb.first_g) / nb.train_stride);
                             size_t r = (size_t)tl * nb.max_depth + (depth - 1);
                             rv.extra = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -170,7 +170,9 @@ __global__ void __launch_bounds__(PT) k_shade(WaveParams wp, DevScene sc, Queues
                             nb.rec_rb[r] = make_float4(rad.x, rad.y, rad.z, 0.f);
                             nb.rec_count[tl] = depth;
                             nb.rec_slot[tl] = slot;
-                        } else if (depth == nb.query_depth) {
+                        } else if (depth == (train ? nb.train_end : nb.query_depth)) {
+                            // a training path's last vertex takes the cache's prediction as the
+                            // rest of its radiance (self-training) and is not a sample itself
                             rv.extra = make_float4(T.x, T.y, T.z, __uint_as_float(slot));
                             uint32_t qi = atomicAdd(nb.n_queries, 1u);
                             nb.queries[qi] = rv;

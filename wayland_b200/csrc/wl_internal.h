@@ -133,6 +133,7 @@ struct NrcVertex {
 // satisfies g % train_stride == train_offset; local index (g - first_g) / train_stride.
 struct NrcWaveBuffers {
     uint32_t query_depth, train_stride;
+    uint32_t train_end;     // training paths end at the cache at this vertex (0: they do not)
     uint64_t first_g;
     uint32_t max_depth;
     NrcVertex *queries;
