@@ -337,6 +337,9 @@ WL_API void wl_nrc_params_default(wl_nrc_params *params);
 WL_API int wl_nrc_create(wl_context *ctx, wl_scene *scene, const wl_nrc_params *params,
                          wl_nrc **out);
 WL_API int wl_nrc_destroy(wl_nrc *nrc);
+/* Allocate what wl_render_nrc with these params needs (path queues, per-frame cache buffers)
+ * without rendering or training. */
+WL_API int wl_nrc_reserve(wl_context *ctx, wl_nrc *nrc, const wl_render_params *params);
 /* Render params->spp frames with the cache (query, then train on the frame's samples). With
  * film == NULL the frames train the cache and leave no image (warm-up). */
 WL_API int wl_render_nrc(wl_context *ctx, wl_scene *scene, const wl_camera *camera,

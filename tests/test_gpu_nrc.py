@@ -92,3 +92,45 @@ def test_render_with_cache(ctx):
     assert np.isfinite(st["loss"])
     c.close()
     s.close()
+
+
+def test_reserve_and_warmup_without_film(ctx):
+    """wl_nrc_reserve allocates up front; frames without a film train the cache only."""
+    sc = scenes.cornell_box(48, 32)
+    s = wl.Scene(ctx, sc)
+    c = wl.RadianceCache(ctx, s, log2_table=14, train_paths=256)
+    p = wl.render_params(48, 32, 3, max_depth=8)
+    c.reserve(p)
+    wl.render_nrc(ctx, s, sc.camera_struct(), p, c, None)
+    st = c.stats()
+    assert st["train_samples"] > 50 and np.isfinite(st["loss"])
+    film = wl.Film(ctx, 48, 32)
+    wl.render_nrc(ctx, s, sc.camera_struct(), wl.render_params(48, 32, 2, max_depth=8), c, film)
+    img = film.download()
+    assert np.isfinite(img).all() and img.mean() > 0.01
+    film.close()
+    c.close()
+    s.close()
+
+
+def test_self_training_matches_full_paths(ctx):
+    """Training paths that end at the cache after train_extra vertices and full-length training
+    paths converge to images of the same brightness (the cache learns the multi-bounce tail)."""
+    sc = scenes.cornell_box(48, 48)
+    s = wl.Scene(ctx, sc)
+    means = []
+    for extra in (0, 3):
+        c = wl.RadianceCache(ctx, s, log2_table=16, train_paths=1024, train_extra=extra)
+        wl.render_nrc(ctx, s, sc.camera_struct(), wl.render_params(48, 48, 32, max_depth=12), c, None)
+        film = wl.Film(ctx, 48, 48)
+        wl.render_nrc(ctx, s, sc.camera_struct(), wl.render_params(48, 48, 32, max_depth=12), c, film)
+        means.append(float(film.download().mean()))
+        film.close()
+        c.close()
+    ref_film = wl.Film(ctx, 48, 48)
+    wl.render(ctx, s, sc.camera_struct(), wl.render_params(48, 48, 256, max_depth=12), ref_film)
+    ref = float(ref_film.download().mean())
+    ref_film.close()
+    s.close()
+    for m in means:
+        assert abs(m - ref) < 0.1 * ref, (means, ref)

@@ -249,6 +249,11 @@ class RadianceCache:
         self.handle = h
         ctx._children.add(self)
 
+    def reserve(self, params):
+        """Allocate the buffers that render_nrc with these params needs (no rendering)."""
+        _abi.check("wl_nrc_reserve", self.lib.wl_nrc_reserve(self.ctx.handle, self.handle,
+                                                             C.byref(params)))
+
     def forward(self, d_in, d_out, n):
         _abi.check("wl_nrc_mlp_forward", self.lib.wl_nrc_mlp_forward(self.handle, C.c_void_p(d_in),
                                                                      C.c_void_p(d_out), n))

@@ -141,6 +141,7 @@ SIGNATURES = {
     "wl_nrc_params_default": (None, [C.POINTER(NrcParams)]),
     "wl_nrc_create": (C.c_int, [_P, _P, C.POINTER(NrcParams), C.POINTER(_P)]),
     "wl_nrc_destroy": (C.c_int, [_P]),
+    "wl_nrc_reserve": (C.c_int, [_P, _P, C.POINTER(RenderParams)]),
     "wl_render_nrc": (C.c_int, [_P, _P, C.POINTER(Camera), C.POINTER(RenderParams), _P, _P]),
     "wl_nrc_mlp_forward": (C.c_int, [_P, _P, _P, _U32]),
     "wl_nrc_train_step": (C.c_int, [_P, _P, _P, _U32, C.POINTER(C.c_float)]),

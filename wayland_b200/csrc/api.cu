@@ -1030,24 +1030,15 @@ int wl_nrc_stats(wl_nrc *n, uint32_t *samples, uint32_t *queries, float *loss) {
     return WL_OK;
 }
 
-int wl_render_nrc(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_params *p,
-                  wl_nrc *n, wl_film *f) {
-    ARG(c && s && cam && p && n, "null argument");
-    ARG(s->ctx == c && (!f || f->ctx == c) && n->ctx == c && n->scene == s, "objects must belong together");
-    if (!s->built) return fail(WL_ERR_NOT_BUILT, "bvh not built");
-    ARG(!f || (p->width == f->f.W && p->height == f->f.H), "film size differs from the render size");
-    ARG(p->spp > 0 && p->max_depth > 0 && p->max_depth <= 1024, "bad spp or max_depth");
-    ARG(p->strategy <= WL_STRATEGY_MIS && p->rng <= WL_RNG_PCG32 && p->math <= WL_MATH_STRICT, "bad params");
-    ARG(p->lights == WL_LIGHTS_UNIFORM, "only uniform light selection is available");
-    ARG(finite3(cam->pos) && finite3(cam->look_at) && finite3(cam->up) && finite3(cam->right), "non-finite camera");
-    CK(cudaSetDevice(c->device));
-    c->stats_pending = false;
+// Queues and per-frame cache buffers for renders with params p (one wave = at most one frame).
+static int nrc_prepare(wl_context *c, wl_nrc *n, const wl_render_params *p, uint64_t &wave,
+                       uint32_t &stride) {
     const uint32_t npix = p->width * p->height;
     uint64_t want = p->wave_paths ? p->wave_paths : (1ull << 23);
-    uint64_t wave = want < npix ? want : npix;  // one frame at a time
+    wave = want < npix ? want : npix;  // one frame at a time
     int rc = ensure_queues(c, (uint32_t)wave);
     if (rc != WL_OK) return rc;
-    uint32_t stride = npix / (n->p.train_paths ? n->p.train_paths : 1);
+    stride = npix / (n->p.train_paths ? n->p.train_paths : 1);
     if (stride < 1) stride = 1;
     uint32_t t_cap = (uint32_t)(wave / stride + 2);
     if (n->q_cap < wave || n->t_cap < t_cap || n->depth_cap < p->max_depth) {
@@ -1068,6 +1059,36 @@ int wl_render_nrc(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_ren
         n->t_cap = t_cap;
         n->depth_cap = p->max_depth;
     }
+    return WL_OK;
+}
+
+int wl_nrc_reserve(wl_context *c, wl_nrc *n, const wl_render_params *p) {
+    ARG(c && n && p, "null argument");
+    ARG(n->ctx == c, "objects must belong together");
+    ARG(p->width > 0 && p->height > 0 && p->max_depth > 0 && p->max_depth <= 1024, "bad size or max_depth");
+    CK(cudaSetDevice(c->device));
+    uint64_t wave = 0;
+    uint32_t stride = 0;
+    return nrc_prepare(c, n, p, wave, stride);
+}
+
+int wl_render_nrc(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_params *p,
+                  wl_nrc *n, wl_film *f) {
+    ARG(c && s && cam && p && n, "null argument");
+    ARG(s->ctx == c && (!f || f->ctx == c) && n->ctx == c && n->scene == s, "objects must belong together");
+    if (!s->built) return fail(WL_ERR_NOT_BUILT, "bvh not built");
+    ARG(!f || (p->width == f->f.W && p->height == f->f.H), "film size differs from the render size");
+    ARG(p->spp > 0 && p->max_depth > 0 && p->max_depth <= 1024, "bad spp or max_depth");
+    ARG(p->strategy <= WL_STRATEGY_MIS && p->rng <= WL_RNG_PCG32 && p->math <= WL_MATH_STRICT, "bad params");
+    ARG(p->lights == WL_LIGHTS_UNIFORM, "only uniform light selection is available");
+    ARG(finite3(cam->pos) && finite3(cam->look_at) && finite3(cam->up) && finite3(cam->right), "non-finite camera");
+    CK(cudaSetDevice(c->device));
+    c->stats_pending = false;
+    const uint32_t npix = p->width * p->height;
+    uint64_t wave = 0;
+    uint32_t stride = 0;
+    int rc = nrc_prepare(c, n, p, wave, stride);
+    if (rc != WL_OK) return rc;
     WaveParams wp{};
     wp.W = p->width; wp.H = p->height; wp.npix = npix;
     wp.max_depth = p->max_depth; wp.rr_depth = p->rr_depth;
