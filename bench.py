@@ -270,6 +270,72 @@ def raycast_microbench(wl, torch, ctx, sc, scene, stream):
     return out
 
 
+def bdpt_ao_leg(wl, torch, ctx, res=512, spp=256, oracle_spp=4096, ao_res=(512, 256)):
+    """Configuration 5: the glass-sphere caustic scene (158,420 sphere triangles + plane + a
+    0.05-wide quad light). BDPT with subpaths of at most 10 vertices: samples/s at res x res x
+    spp, and relMSE of that image against an FP64 film of oracle_spp BDPT samples (seeds
+    disjoint). AO: 4 camera samples x 32 occlusion rays of radius 0.1 per pixel at ao_res (about
+    2^24 rays). Device time with CUDA events on the library's stream."""
+    from wayland_b200 import scenes
+    sc = scenes.glass_sphere(res, res)
+    scene = wl.Scene(ctx, sc)
+    cam = sc.camera_struct()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    film = wl.Film(ctx, res, res, fp64=True)
+    p = wl.render_params(res, res, 8, strategy=wl.STRATEGY_BDPT, max_depth=10, first_frame=10000000)
+    wl.render(ctx, scene, cam, p, film)  # first launches
+    ctx.sync()
+    film.close()
+    film = wl.Film(ctx, res, res, fp64=True)
+    p = wl.render_params(res, res, spp, strategy=wl.STRATEGY_BDPT, max_depth=10)
+    e0.record(stream)
+    wl.render(ctx, scene, cam, p, film)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    st = ctx.stats()
+    img = film.download64()
+    film.close()
+    ref = wl.Film(ctx, res, res, fp64=True)
+    done = 0
+    t0 = time.perf_counter()
+    while done < oracle_spp:
+        k = min(512, oracle_spp - done)
+        wl.render(ctx, scene, cam, wl.render_params(res, res, k, strategy=wl.STRATEGY_BDPT, max_depth=10,
+                                                    first_frame=20000000 + done), ref)
+        done += k
+    r64 = ref.download64()
+    oracle_s = time.perf_counter() - t0
+    ref.close()
+    rel = float(((img - r64) ** 2 / (r64 * r64 + 1e-2)).mean())
+    samples = res * res * spp
+    out = {"scene": f"glass sphere {sc.num_tris} tris, roughness 0.05, {res}x{res}, subpaths <= 10 vertices",
+           "spp": spp, "ms": round(ms, 1), "msamples_s": round(samples / ms / 1e3, 2),
+           "closest_hit_rays_per_sample": round(st["segments"] / samples, 3),
+           "connection_rays_per_sample": round(st["shadow_rays"] / samples, 3),
+           "relmse_vs_fp64": rel, "oracle": f"{oracle_spp} spp BDPT, FP64 film ({oracle_s:.1f} s)"}
+    # ambient occlusion, radius 0.1
+    aw, ah = ao_res
+    afilm = wl.Film(ctx, aw, ah)
+    ap = wl.ao_params(aw, ah, 1, radius=0.1)
+    wl.render_ao(ctx, scene, cam, ap, afilm)
+    ctx.sync()
+    e0.record(stream)
+    wl.render_ao(ctx, scene, cam, wl.ao_params(aw, ah, 1, radius=0.1, first_frame=1), afilm)
+    e1.record(stream)
+    e1.synchronize()
+    ams = e0.elapsed_time(e1)
+    rays = aw * ah * 4 * (1 + 32)
+    afilm.close()
+    out["ao"] = {"res": f"{aw}x{ah}", "rays": rays, "ms": round(ams, 2),
+                 "mrays_s": round(rays / ams / 1e3, 1),
+                 "note": "rays counted as 4 camera + 128 occlusion rays per pixel"}
+    scene.close()
+    return out
+
+
 def nrc_convergence(wl, torch, ctx, res=(480, 270), oracle_spp=16384, target=1e-2,
                     budget_s=60.0, chunk=4, warmup_frames=16):
     """Time to relMSE <= target against an FP64-accumulated high-spp render, for the plain path
@@ -371,6 +437,8 @@ def main():
     ap.add_argument("--nrc-only", action="store_true",
                     help="only the radiance-cache convergence comparison (prints its JSON)")
     ap.add_argument("--no-nrc", action="store_true")
+    ap.add_argument("--no-bdpt", action="store_true")
+    ap.add_argument("--bdpt-only", action="store_true", help="only the BDPT + AO leg (prints its JSON)")
     ap.add_argument("--nrc-res", default="960x540", help="resolution of the radiance-cache comparison")
     ap.add_argument("--nrc-oracle-spp", type=int, default=8192)
     ap.add_argument("--nrc-budget-s", type=float, default=60.0)
@@ -393,6 +461,11 @@ def main():
     rank = env_int("RANK", 0)
     local = env_int("LOCAL_RANK", 0)
     torch.cuda.set_device(local)
+    if args.bdpt_only:
+        ctx = wl.Context(local)
+        print(json.dumps(bdpt_ao_leg(wl, torch, ctx)), flush=True)
+        ctx.close()
+        return 0
     if args.nrc_only:
         ctx = wl.Context(local)
         w_, h_ = (int(v) for v in args.nrc_res.split("x"))
@@ -517,6 +590,8 @@ def main():
         }
         if not args.no_raycast:
             line["raycast"] = raycast_microbench(wl, torch, ctx, sc, scene, stream)
+        if world == 1 and not args.no_bdpt:
+            line["bdpt"] = bdpt_ao_leg(wl, torch, ctx)
         if world == 1 and not args.no_nrc:
             # the second half of the metric: time to relMSE 1e-2 vs an FP64 high-spp render,
             # radiance cache vs plain path tracing (door-slit room)
