@@ -270,6 +270,33 @@ def raycast_microbench(wl, torch, ctx, sc, scene, stream):
     return out
 
 
+def graph_leg(wl, torch, ctx, sc, scene, stream, frames=16):
+    """Progressive rendering, 1 spp per call at 1920x1080 on the benchmark scene: device time per
+    call with direct launches and with every wave replayed as one CUDA graph."""
+    cam = scene.camera_struct()
+    out = {}
+    for name, flags in (("launches", 0), ("graph", wl._abi.RENDER_GRAPH)):
+        film = wl.Film(ctx, W, H)
+        p = wl.render_params(W, H, 1, max_depth=DEPTH, env=scene.env, flags=flags)
+        for f in range(3):
+            p.first_frame = f
+            wl.render(ctx, sc, cam, p, film)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        ctx.sync()
+        t0 = time.perf_counter()
+        e0.record(stream)
+        for f in range(frames):
+            p.first_frame = 3 + f
+            wl.render(ctx, sc, cam, p, film)
+        e1.record(stream)
+        e1.synchronize()
+        out[name] = {"ms_per_frame": round(e0.elapsed_time(e1) / frames, 3),
+                     "host_ms_per_call": round((time.perf_counter() - t0) * 1e3 / frames, 3)}
+        film.close()
+    return out
+
+
 def bdpt_ao_leg(wl, torch, ctx, res=512, spp=256, oracle_spp=4096, ao_res=(512, 256)):
     """Configuration 5: the glass-sphere caustic scene (158,420 sphere triangles + plane + a
     0.05-wide quad light). BDPT with subpaths of at most 10 vertices: samples/s at res x res x
@@ -590,6 +617,8 @@ def main():
         }
         if not args.no_raycast:
             line["raycast"] = raycast_microbench(wl, torch, ctx, sc, scene, stream)
+        if world == 1:
+            line["progressive_1spp"] = graph_leg(wl, torch, ctx, sc, scene, stream)
         if world == 1 and not args.no_bdpt:
             line["bdpt"] = bdpt_ao_leg(wl, torch, ctx)
         if world == 1 and not args.no_nrc:

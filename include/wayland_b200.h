@@ -151,9 +151,12 @@ typedef struct wl_render_params {
     uint32_t flags;         /* WL_RENDER_* bits */
 } wl_render_params;
 
-/* wl_render_params.flags: count BVH node visits and triangle tests of every traced ray into
- * wl_render_stats (a slower instrumented traversal; for reporting, not for timing). */
-enum { WL_RENDER_TRAVERSAL_STATS = 1u };
+/* wl_render_params.flags: TRAVERSAL_STATS counts BVH node visits and triangle tests of every
+ * traced ray into wl_render_stats (a slower instrumented traversal; for reporting, not for
+ * timing). GRAPH runs each wave as one CUDA graph, captured once and replayed for every wave and
+ * every later call with the same arguments (the wave's first sample and frame are read from
+ * device memory); wl_render_stats then reports the total time only, not the per-kernel split. */
+enum { WL_RENDER_TRAVERSAL_STATS = 1u, WL_RENDER_GRAPH = 2u };
 
 /* A ray as stored in the HBM ray queue: 32 bytes, two 16-byte vectors. */
 typedef struct wl_ray {

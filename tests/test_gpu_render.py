@@ -184,3 +184,24 @@ def test_program_pt_golden_strict(ctx):
     p = wl.render_params(48, 32, 4, math=wl.MATH_STRICT, env=(0.0, 0.0, 0.0))
     img, _, _, _ = gpu_render(ctx, sc, p)
     assert np.array_equal(bits(img), bits(g["image"]))
+
+
+@pytest.mark.parametrize("strategy", [wl.STRATEGY_MIS, wl.STRATEGY_BDPT])
+def test_graph_replay_matches_launches(ctx, strategy):
+    """WL_RENDER_GRAPH: every wave replays one captured graph (several waves per call, two calls
+    reusing the graph with new frames); the image equals direct launches bit for bit."""
+    sc = small_sphere(40, 30)
+    kw = dict(math=wl.MATH_STRICT, strategy=strategy, wave_paths=1500,
+              max_depth=10 if strategy == wl.STRATEGY_BDPT else 12)
+    imgs = []
+    for flags in (0, wl._abi.RENDER_GRAPH):
+        s = wl.Scene(ctx, sc)
+        film = wl.Film(ctx, 40, 30)
+        for first in (0, 3):
+            p = wl.render_params(40, 30, 3, first_frame=first, flags=flags, **kw)
+            wl.render(ctx, s, sc.camera_struct(), p, film)
+        imgs.append(film.download())
+        film.close()
+        s.close()
+    assert imgs[0].max() > 0
+    assert np.array_equal(bits(imgs[0]), bits(imgs[1]))

@@ -24,6 +24,7 @@ FILM_RUNNING_MEAN, FILM_FP64_SUM = 1, 2
 BVH_LBVH, BVH_SAH = 0, 1
 CAST_CLOSEST, CAST_ANY = 0, 1
 RENDER_TRAVERSAL_STATS = 1
+RENDER_GRAPH = 2
 INVALID = 0xFFFFFFFF
 
 

@@ -59,6 +59,21 @@ struct wl_context {
     int live_children = 0;  // scenes and films created on this context and not yet destroyed
     BdptWave bd{};          // bidirectional wave buffers (allocated by the first BDPT render)
     void *bd_block = nullptr;
+    bool events_on = true;  // per-launch timing events (off while a wave is captured)
+    // CUDA graphs of one wave (WL_RENDER_GRAPH): per-wave (base, first_frame) pairs, the replay
+    // counter and the current pair read by the kernels; a few instantiated graphs keyed by every
+    // argument they captured
+    uint64_t *d_dyn_all = nullptr;
+    size_t dyn_cap = 0;
+    uint32_t *d_dyn_ctr = nullptr;
+    uint64_t *d_dyn_cur = nullptr;
+    struct GraphEntry {
+        std::vector<uint8_t> key;
+        cudaGraphExec_t exec = nullptr;
+        uint64_t used = 0;
+    };
+    GraphEntry graphs[4];
+    uint64_t graph_clock = 0;
 };
 
 struct wl_scene {
@@ -194,6 +209,7 @@ int ensure_bdpt(wl_context *c, uint32_t cap, uint32_t maxv) {
 }
 
 void rec(wl_context *c, int cat, bool begin) {
+    if (!c->events_on) return;
     auto &v = c->ev[cat];
     size_t &u = c->ev_used[cat];
     if (begin) {
@@ -279,6 +295,10 @@ int wl_context_destroy(wl_context *c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->q_block) cudaFree(c->q_block);
     if (c->bd_block) cudaFree(c->bd_block);
+    if (c->d_dyn_all) cudaFree(c->d_dyn_all);
+    if (c->d_dyn_ctr) cudaFree(c->d_dyn_ctr);
+    for (auto &g : c->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
     if (c->d_misc) cudaFree(c->d_misc);
     if (c->d_cast_counts) cudaFree(c->d_cast_counts);
     for (auto &v : c->ev)
@@ -667,6 +687,107 @@ void wl_render_params_default(wl_render_params *p, uint32_t w, uint32_t h, uint3
     p->wave_paths = 0;
 }
 
+// One wave of the path tracer (PathTracing.cu:40-160 for wp.count samples): generate, then per
+// bounce extend, shade, shadow; film. Returns the launches issued.
+static uint32_t pt_wave(wl_context *c, const WaveParams &wp, const DevScene &sc, const Film &film,
+                        uint32_t max_depth, bool strict_math, bool tstats) {
+    cudaStream_t st = c->stream;
+    uint32_t launches = 0;
+    rec(c, 3, true);
+    if (strict_math) strict::launch_generate(wp, c->q, st);
+    else fast::launch_generate(wp, c->q, st);
+    rec(c, 3, false);
+    launches++;
+    int in = 0;
+    for (uint32_t b = 0; b < max_depth; b++) {
+        rec(c, 0, true);
+        launch_extend(sc, c->q, in, tstats, st);
+        rec(c, 0, false);
+        cudaMemsetAsync(c->q.counters + (in ^ 1), 0, sizeof(uint32_t), st);
+        cudaMemsetAsync(c->q.counters + 2, 0, sizeof(uint32_t), st);
+        rec(c, 1, true);
+        if (strict_math) strict::launch_shade(wp, sc, c->q, in, st);
+        else fast::launch_shade(wp, sc, c->q, in, st);
+        rec(c, 1, false);
+        rec(c, 2, true);
+        launch_shadow(sc, c->q, tstats, st);
+        rec(c, 2, false);
+        launches += 3;
+        in ^= 1;
+    }
+    rec(c, 3, true);
+    strict::launch_film(wp, c->q, film, st);
+    rec(c, 3, false);
+    launches++;
+    return launches;
+}
+
+}  // extern "C"
+
+template <class T> static void key_add(std::vector<uint8_t> &k, const T &v) {
+    const uint8_t *p = reinterpret_cast<const uint8_t *>(&v);
+    k.insert(k.end(), p, p + sizeof(T));
+}
+
+// The instantiated graph of one wave whose captured arguments are `key`: reused when an equal
+// key was captured before, else captured from `issue` (which must only enqueue work on the
+// context's stream) into the least recently used entry.
+template <class F>
+static int wave_graph(wl_context *c, const std::vector<uint8_t> &key, F issue, cudaGraphExec_t *out) {
+    c->graph_clock++;
+    for (auto &g : c->graphs)
+        if (g.exec && g.key == key) {
+            g.used = c->graph_clock;
+            *out = g.exec;
+            return WL_OK;
+        }
+    auto *slot = &c->graphs[0];
+    for (auto &g : c->graphs)
+        if (!g.exec || g.used < slot->used) slot = &g;
+    if (slot->exec) {
+        cudaGraphExecDestroy(slot->exec);
+        slot->exec = nullptr;
+    }
+    cudaGraph_t graph = nullptr;
+    const bool ev = c->events_on;
+    c->events_on = false;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    issue();
+    cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    c->events_on = ev;
+    if (e != cudaSuccess) return fail(WL_ERR_CUDA, std::string("wave capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&slot->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        slot->exec = nullptr;
+        return fail(WL_ERR_CUDA, std::string("wave graph: ") + cudaGetErrorString(e));
+    }
+    slot->key = key;
+    slot->used = c->graph_clock;
+    *out = slot->exec;
+    return WL_OK;
+}
+
+extern "C" {
+
+// Device copies of every wave's (first sample, first frame) for graph replays.
+static int upload_dyn(wl_context *c, const std::vector<uint64_t> &dyn) {
+    if (!c->d_dyn_ctr) {
+        CK(cudaMalloc(&c->d_dyn_ctr, 64));
+        c->d_dyn_cur = reinterpret_cast<uint64_t *>(reinterpret_cast<char *>(c->d_dyn_ctr) + 16);
+    }
+    if (c->dyn_cap < dyn.size()) {
+        if (c->d_dyn_all) cudaFree(c->d_dyn_all);
+        c->d_dyn_all = nullptr;
+        CK(cudaMalloc(&c->d_dyn_all, dyn.size() * sizeof(uint64_t)));
+        c->dyn_cap = dyn.size();
+    }
+    CK(cudaMemcpyAsync(c->d_dyn_all, dyn.data(), dyn.size() * sizeof(uint64_t), cudaMemcpyHostToDevice,
+                       c->stream));
+    CK(cudaMemsetAsync(c->d_dyn_ctr, 0, sizeof(uint32_t), c->stream));
+    return WL_OK;
+}
+
 // One wave of the bidirectional path tracer (BDPT.cu:522-560 for wp.count samples): eye
 // subpaths, light subpaths, connections, connection rays, film. Returns the launches issued.
 // Event categories: 0 closest-hit passes, 1 vertex and connection kernels, 2 connection rays,
@@ -786,42 +907,46 @@ int wl_render(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_
     CK(cudaEventRecord(c->ev_total[0], st));
     uint32_t launches = 0, waves = 0;
     const bool strict_math = p->math == WL_MATH_STRICT;
-    for (uint64_t base = 0; base < total && bdpt; base += wave) {
-        wp.base = base;
-        wp.count = (uint32_t)((total - base) < wave ? (total - base) : wave);
-        launches += bdpt_wave(c, wp, sc, f->f, strict_math, tstats);
-        waves++;
-        CK(cudaGetLastError());
-    }
-    for (uint64_t base = 0; base < total && !bdpt; base += wave) {
-        wp.base = base;
-        wp.count = (uint32_t)((total - base) < wave ? (total - base) : wave);
-        rec(c, 3, true);
-        if (strict_math) strict::launch_generate(wp, c->q, st);
-        else fast::launch_generate(wp, c->q, st);
-        rec(c, 3, false);
-        launches++;
-        int in = 0;
-        for (uint32_t b = 0; b < p->max_depth; b++) {
-            rec(c, 0, true);
-            launch_extend(sc, c->q, in, tstats, st);
-            rec(c, 0, false);
-            CK(cudaMemsetAsync(c->q.counters + (in ^ 1), 0, sizeof(uint32_t), st));
-            CK(cudaMemsetAsync(c->q.counters + 2, 0, sizeof(uint32_t), st));
-            rec(c, 1, true);
-            if (strict_math) strict::launch_shade(wp, sc, c->q, in, st);
-            else fast::launch_shade(wp, sc, c->q, in, st);
-            rec(c, 1, false);
-            rec(c, 2, true);
-            launch_shadow(sc, c->q, tstats, st);
-            rec(c, 2, false);
-            launches += 3;
-            in ^= 1;
+    const bool graph = (p->flags & WL_RENDER_GRAPH) != 0 && !tstats;
+    if (graph) {
+        std::vector<uint64_t> dyn;
+        for (uint64_t base = 0; base < total; base += wave) {
+            dyn.push_back(base);
+            dyn.push_back(p->first_frame);
         }
-        rec(c, 3, true);
-        strict::launch_film(wp, c->q, f->f, st);
-        rec(c, 3, false);
-        launches++;
+        int rc2 = upload_dyn(c, dyn);
+        if (rc2 != WL_OK) return rc2;
+    }
+    for (uint64_t base = 0; base < total; base += wave) {
+        wp.base = base;
+        wp.count = (uint32_t)((total - base) < wave ? (total - base) : wave);
+        if (!graph) {
+            launches += bdpt ? bdpt_wave(c, wp, sc, f->f, strict_math, tstats)
+                             : pt_wave(c, wp, sc, f->f, p->max_depth, strict_math, tstats);
+        } else {
+            WaveParams gp = wp;
+            gp.base = 0;
+            gp.first_frame = 0;
+            gp.dyn = c->d_dyn_cur;
+            std::vector<uint8_t> key;
+            key_add(key, gp);
+            key_add(key, sc);
+            key_add(key, f->f);
+            key_add(key, c->q);
+            key_add(key, c->bd);
+            key_add(key, p->max_depth);
+            key_add(key, (uint32_t)(bdpt * 2 + strict_math));
+            uint32_t nl = 0;
+            cudaGraphExec_t exec = nullptr;
+            int rc2 = wave_graph(c, key, [&] {
+                strict::launch_wave_begin(c->d_dyn_all, c->d_dyn_ctr, c->d_dyn_cur, st);
+                nl = bdpt ? bdpt_wave(c, gp, sc, f->f, strict_math, false)
+                          : pt_wave(c, gp, sc, f->f, p->max_depth, strict_math, false);
+            }, &exec);
+            if (rc2 != WL_OK) return rc2;
+            CK(cudaGraphLaunch(exec, st));
+            launches += nl ? nl + 1 : 0;
+        }
         waves++;
         CK(cudaGetLastError());
     }

@@ -183,6 +183,7 @@ __device__ __forceinline__ void bd_surface(const DevScene &sc, float4 h, v3 org,
 }
 
 __global__ void __launch_bounds__(PT) k_bd_eye_gen(WaveParams wp, Queues q, BdptWave bw) {
+    wave_dyn(wp);
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
         q.counters[0] = wp.count;
@@ -218,6 +219,7 @@ __device__ __forceinline__ Rng bd_rng(const WaveParams &wp, const Queues &q, uin
 // One eye vertex per ray of queue `in` (all at depth `depth`); TraceEyeSubpath's loop body.
 __global__ void __launch_bounds__(PT) k_bd_eye(WaveParams wp, DevScene sc, Queues q, BdptWave bw,
                                                int in, uint32_t depth) {
+    wave_dyn(wp);
     const uint32_t n = q.counters[in];
     const int out = in ^ 1;
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -306,6 +308,7 @@ __global__ void __launch_bounds__(PT) k_bd_eye(WaveParams wp, DevScene sc, Queue
 // for every slot whose eye subpath has vertices. Rays go to queue 0.
 __global__ void __launch_bounds__(PT) k_bd_light_gen(WaveParams wp, DevScene sc, Queues q,
                                                      BdptWave bw) {
+    wave_dyn(wp);
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t cap = bw.cap;
     for (uint32_t base = blockIdx.x * blockDim.x; base < wp.count; base += stride) {
@@ -367,6 +370,7 @@ __global__ void __launch_bounds__(PT) k_bd_light_gen(WaveParams wp, DevScene sc,
 // One light-subpath vertex per ray of queue `in` (all reaching vertex depth - 1).
 __global__ void __launch_bounds__(PT) k_bd_light(WaveParams wp, DevScene sc, Queues q, BdptWave bw,
                                                  int in, uint32_t depth) {
+    wave_dyn(wp);
     const uint32_t n = q.counters[in];
     const int out = in ^ 1;
     const uint32_t stride = gridDim.x * blockDim.x;

@@ -39,6 +39,7 @@ __device__ __forceinline__ uint32_t warp_append(bool want, uint32_t *ctr) {
 }
 
 __global__ void __launch_bounds__(PT) k_generate(WaveParams wp, Queues q) {
+    wave_dyn(wp);
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i == 0) {
         q.counters[0] = wp.count;
@@ -78,6 +79,7 @@ __device__ __forceinline__ float tri_area(const DevScene &sc, uint32_t t) {
 template <bool NRC>
 __global__ void __launch_bounds__(PT) k_shade(WaveParams wp, DevScene sc, Queues q, int in,
                                               NrcWaveBuffers nb) {
+    wave_dyn(wp);
     const uint32_t n = q.counters[in];
     const int out = in ^ 1;
     const uint32_t stride = gridDim.x * blockDim.x;

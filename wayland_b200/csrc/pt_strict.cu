@@ -16,6 +16,7 @@ namespace strict {
 // increasing frame; FP32 storage, double arithmetic. A path whose radiance is not finite adds 0
 // (the reference would keep the NaN in its running mean). The FP64 film sums the same values.
 __global__ void k_film(WaveParams wp, Queues q, Film f) {
+    wave_dyn(wp);
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t lim = wp.count < wp.npix ? wp.count : wp.npix;
     if (j >= lim) return;
@@ -85,6 +86,7 @@ void launch_bdpt_connections(const WaveParams &wp, const BdptWave &bw, cudaStrea
 // reference's order), the running mean is FP32 arithmetic with FP32 weights. A sample that is
 // not finite adds 0 (the reference would keep the NaN). The FP64 film sums the same values.
 __global__ void k_bd_film(WaveParams wp, uint32_t nlight, Queues q, BdptWave bw, Film f) {
+    wave_dyn(wp);
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t lim = wp.count < wp.npix ? wp.count : wp.npix;
     if (j >= lim) return;
@@ -154,6 +156,16 @@ __global__ void k_debug_rng(uint32_t mode, uint64_t seed, const uint32_t *pixels
     if (i >= npix) return;
     Rng r = make_rng(mode, seed, pixels[i], frame);
     for (uint32_t k = 0; k < count; k++) out[(size_t)i * count + k] = r.next();
+}
+
+__global__ void k_wave_begin(const uint64_t *all, uint32_t *ctr, uint64_t *cur) {
+    uint32_t w = *ctr;
+    cur[0] = all[2 * (size_t)w];
+    cur[1] = all[2 * (size_t)w + 1];
+    *ctr = w + 1;
+}
+void launch_wave_begin(const uint64_t *all, uint32_t *ctr, uint64_t *cur, cudaStream_t s) {
+    k_wave_begin<<<1, 1, 0, s>>>(all, ctr, cur);
 }
 
 void launch_film(const WaveParams &wp, const Queues &q, const Film &f, cudaStream_t s) {

@@ -118,7 +118,19 @@ struct WaveParams {
     float env[3];
     uint32_t has_env;
     float cam_pos[3], cam_look[3], cam_up[3], cam_right[3];
+    // graph replays: the wave's first sample index and first frame come from device memory
+    // (dyn[0], dyn[1]) instead of base / first_frame, so one captured wave serves every wave
+    const uint64_t *dyn;
 };
+
+#ifdef __CUDACC__
+__device__ __forceinline__ void wave_dyn(WaveParams &wp) {
+    if (wp.dyn) {
+        wp.base = wp.dyn[0];
+        wp.first_frame = (uint32_t)wp.dyn[1];
+    }
+}
+#endif
 
 // Neural radiance cache records (nrc.cu, wl_nrc.cuh): position + material, outgoing direction,
 // shading normal, and either throughput + slot (query) or target radiance (training sample).
@@ -191,6 +203,8 @@ void launch_shade(const WaveParams &wp, const DevScene &sc, const Queues &q, int
 void launch_shade_nrc(const WaveParams &wp, const DevScene &sc, const Queues &q, int in,
                       const NrcWaveBuffers &nb, cudaStream_t s);
 void launch_film(const WaveParams &wp, const Queues &q, const Film &f, cudaStream_t s);
+// graph replays: cur = all[2 w], all[2 w + 1] for the w-th replay (counter ctr)
+void launch_wave_begin(const uint64_t *all, uint32_t *ctr, uint64_t *cur, cudaStream_t s);
 void launch_bdpt_connections(const WaveParams &wp, const BdptWave &bw, cudaStream_t s);
 void launch_bdpt_film(const WaveParams &wp, const DevScene &sc, const Queues &q, const BdptWave &bw,
                       const Film &f, cudaStream_t s);
