@@ -465,6 +465,7 @@ def main():
                     help="only the radiance-cache convergence comparison (prints its JSON)")
     ap.add_argument("--no-nrc", action="store_true")
     ap.add_argument("--no-bdpt", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--bdpt-only", action="store_true", help="only the BDPT + AO leg (prints its JSON)")
     ap.add_argument("--nrc-res", default="960x540", help="resolution of the radiance-cache comparison")
     ap.add_argument("--nrc-oracle-spp", type=int, default=8192)
@@ -524,6 +525,9 @@ def main():
         if world > 1:
             dist.barrier()
 
+    # launch shapes (paths per wave, traversal CTAs per SM and refill threshold) chosen by the
+    # project's autotuner on this scene, outside the timed region
+    tune = None if args.no_autotune else ctx.autotune(sc, cam, params)
     for _ in range(args.warmup):
         wl.render(ctx, sc, cam, params, film)
     ctx.sync()
@@ -613,6 +617,7 @@ def main():
             "bvh": {"wide_nodes": info["wide_nodes"], "depth": info["wide_depth"],
                     "build_ms": round(info["ms_build"], 1)},
             "gpu_launches": launches,
+            "autotune": tune,
             "clocks": clk,
         }
         if not args.no_raycast:

@@ -314,6 +314,28 @@ WL_API void wl_ao_params_default(wl_ao_params *params, uint32_t width, uint32_t 
 WL_API int wl_render_ao(wl_context *ctx, wl_scene *scene, const wl_camera *camera,
                         const wl_ao_params *params, wl_film *film);
 
+/* ---- autotuner ---------------------------------------------------------------------- */
+/* No counterpart in the reference (OptiX chooses its own launch shapes). The launch shape of
+ * the renders: paths in flight per wave (0 = automatic), and per traversal pass the persistent
+ * CTAs per SM (0 = as many as fit) and the warp refill threshold (4, 6, 8, 12, 16 or 24 idle
+ * lanes). */
+typedef struct wl_tune_result {
+    uint32_t wave_paths;
+    uint32_t extend_ctas_per_sm, extend_refill;
+    uint32_t shadow_ctas_per_sm, shadow_refill;
+    uint32_t candidates;        /* configurations timed */
+    uint32_t spp;               /* samples per pixel of the tuning renders */
+    float ms_default;           /* tuning render with the default shape */
+    float ms_tuned;             /* tuning render with the chosen shape */
+} wl_tune_result;
+/* Times renders of (scene, camera, params with spp reduced to about 2^24 paths) for candidate
+ * shapes by coordinate descent and keeps the fastest in the context for later renders of every
+ * program. Path-tracer strategies only. */
+WL_API int wl_autotune(wl_context *ctx, wl_scene *scene, const wl_camera *camera,
+                       const wl_render_params *params, wl_tune_result *out);
+/* Sets the context's shape (as returned by wl_autotune); NULL restores the defaults. */
+WL_API int wl_set_tune(wl_context *ctx, const wl_tune_result *tune);
+
 /* ---- neural radiance cache ---------------------------------------------------------- */
 /* No counterpart in the reference: a multiresolution hash-grid encoding
  * (after Mueller et al. 2022) feeding an MLP that predicts the radiance reflected at a surface

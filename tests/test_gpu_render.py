@@ -205,3 +205,29 @@ def test_graph_replay_matches_launches(ctx, strategy):
         s.close()
     assert imgs[0].max() > 0
     assert np.array_equal(bits(imgs[0]), bits(imgs[1]))
+
+
+def test_tuned_shapes_keep_the_image(ctx):
+    """The autotuner's knobs change scheduling only: any shape renders the same strict image,
+    and wl_autotune returns a valid shape that it keeps for later renders."""
+    sc = small_sphere(48, 32)
+    s = wl.Scene(ctx, sc)
+    p = wl.render_params(48, 32, 4, math=wl.MATH_STRICT)
+    imgs = []
+    for tune in (None, dict(wave_paths=1 << 12, extend_ctas_per_sm=4, extend_refill=8,
+                            shadow_ctas_per_sm=6, shadow_refill=24)):
+        ctx.set_tune(tune)
+        film = wl.Film(ctx, 48, 32)
+        wl.render(ctx, s, sc.camera_struct(), p, film)
+        imgs.append(film.download())
+        film.close()
+    assert np.array_equal(bits(imgs[0]), bits(imgs[1]))
+    r = ctx.autotune(s, sc.camera_struct(), wl.render_params(48, 32, 64))
+    assert r["candidates"] >= 40 and r["extend_refill"] in (4, 6, 8, 12, 16, 24)
+    assert 0 < r["ms_tuned"] <= r["ms_default"] * 1.5
+    film = wl.Film(ctx, 48, 32)
+    wl.render(ctx, s, sc.camera_struct(), p, film)
+    assert np.array_equal(bits(film.download()), bits(imgs[0]))
+    film.close()
+    ctx.set_tune(None)
+    s.close()

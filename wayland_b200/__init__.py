@@ -74,6 +74,21 @@ class Context:
         _abi.check("wl_render_get_stats", self.lib.wl_render_get_stats(self.handle, C.byref(s)))
         return {k: getattr(s, k) for k, _ in s._fields_}
 
+    def autotune(self, scene, camera, params):
+        """wl_autotune: choose and keep the fastest launch shape for renders like this one."""
+        r = _abi.TuneResult()
+        _abi.check("wl_autotune", self.lib.wl_autotune(self.handle, scene.handle, C.byref(camera),
+                                                       C.byref(params), C.byref(r)))
+        return {k: getattr(r, k) for k, _ in r._fields_}
+
+    def set_tune(self, tune=None):
+        """wl_set_tune: a shape returned by autotune (dict), or None for the defaults."""
+        if tune is None:
+            _abi.check("wl_set_tune", self.lib.wl_set_tune(self.handle, None))
+            return
+        r = _abi.TuneResult(**{k: tune[k] for k, _ in _abi.TuneResult._fields_ if k in tune})
+        _abi.check("wl_set_tune", self.lib.wl_set_tune(self.handle, C.byref(r)))
+
     def debug_rng(self, rng, seed, d_pixels_ptr, npix, frame, count, d_out_ptr):
         _abi.check("wl_debug_rng", self.lib.wl_debug_rng(self.handle, rng, seed, C.c_void_p(d_pixels_ptr),
                                                          npix, frame, count, C.c_void_p(d_out_ptr)))

@@ -72,6 +72,13 @@ class NrcParams(C.Structure):
 NRC_WEIGHTS = 17408
 
 
+class TuneResult(C.Structure):
+    _fields_ = [("wave_paths", C.c_uint32), ("extend_ctas_per_sm", C.c_uint32),
+                ("extend_refill", C.c_uint32), ("shadow_ctas_per_sm", C.c_uint32),
+                ("shadow_refill", C.c_uint32), ("candidates", C.c_uint32), ("spp", C.c_uint32),
+                ("ms_default", C.c_float), ("ms_tuned", C.c_float)]
+
+
 class RenderStats(C.Structure):
     _fields_ = [("paths", C.c_uint64), ("segments", C.c_uint64), ("shadow_rays", C.c_uint64),
                 ("waves", C.c_uint32), ("kernel_launches", C.c_uint32), ("ms_total", C.c_float),
@@ -139,6 +146,8 @@ SIGNATURES = {
     "wl_debug_rng": (C.c_int, [_P, _U32, C.c_uint64, _P, _U32, _U32, _U32, _P]),
     "wl_render_noalloc": (C.c_int, [_P, _P, C.POINTER(Camera), C.POINTER(RenderParams), _P]),
     "wl_ao_params_default": (None, [C.POINTER(AoParams), _U32, _U32, _U32]),
+    "wl_autotune": (C.c_int, [_P, _P, C.POINTER(Camera), C.POINTER(RenderParams), C.POINTER(TuneResult)]),
+    "wl_set_tune": (C.c_int, [_P, _P]),
     "wl_nrc_params_default": (None, [C.POINTER(NrcParams)]),
     "wl_nrc_create": (C.c_int, [_P, _P, C.POINTER(NrcParams), C.POINTER(_P)]),
     "wl_nrc_destroy": (C.c_int, [_P]),

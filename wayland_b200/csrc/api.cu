@@ -74,6 +74,9 @@ struct wl_context {
     };
     GraphEntry graphs[4];
     uint64_t graph_clock = 0;
+    // launch shapes chosen by wl_autotune (defaults until then)
+    uint32_t tune_wave = 0;
+    TraceTune tune_extend{}, tune_shadow{};
 };
 
 struct wl_scene {
@@ -701,7 +704,7 @@ static uint32_t pt_wave(wl_context *c, const WaveParams &wp, const DevScene &sc,
     int in = 0;
     for (uint32_t b = 0; b < max_depth; b++) {
         rec(c, 0, true);
-        launch_extend(sc, c->q, in, tstats, st);
+        launch_extend(sc, c->q, in, tstats, st, c->tune_extend);
         rec(c, 0, false);
         cudaMemsetAsync(c->q.counters + (in ^ 1), 0, sizeof(uint32_t), st);
         cudaMemsetAsync(c->q.counters + 2, 0, sizeof(uint32_t), st);
@@ -710,7 +713,7 @@ static uint32_t pt_wave(wl_context *c, const WaveParams &wp, const DevScene &sc,
         else fast::launch_shade(wp, sc, c->q, in, st);
         rec(c, 1, false);
         rec(c, 2, true);
-        launch_shadow(sc, c->q, tstats, st);
+        launch_shadow(sc, c->q, tstats, st, c->tune_shadow);
         rec(c, 2, false);
         launches += 3;
         in ^= 1;
@@ -805,7 +808,7 @@ static uint32_t bdpt_wave(wl_context *c, const WaveParams &wp, const DevScene &s
     int in = 0;
     for (uint32_t d = 1; d <= bw.maxv; d++) {
         rec(c, 0, true);
-        launch_extend(sc, c->q, in, tstats, st);
+        launch_extend(sc, c->q, in, tstats, st, c->tune_extend);
         rec(c, 0, false);
         cudaMemsetAsync(c->q.counters + (in ^ 1), 0, sizeof(uint32_t), st);
         rec(c, 1, true);
@@ -824,7 +827,7 @@ static uint32_t bdpt_wave(wl_context *c, const WaveParams &wp, const DevScene &s
     in = 0;
     for (uint32_t d = 2; d <= bw.maxv; d++) {
         rec(c, 0, true);
-        launch_extend(sc, c->q, in, tstats, st);
+        launch_extend(sc, c->q, in, tstats, st, c->tune_extend);
         rec(c, 0, false);
         cudaMemsetAsync(c->q.counters + (in ^ 1), 0, sizeof(uint32_t), st);
         rec(c, 1, true);
@@ -843,7 +846,7 @@ static uint32_t bdpt_wave(wl_context *c, const WaveParams &wp, const DevScene &s
     else fast::launch_bdpt_connect(wp, sc, c->q, bw, st);
     rec(c, 1, false);
     rec(c, 2, true);
-    launch_connection_rays(sc, c->q, bw, tstats, st);
+    launch_connection_rays(sc, c->q, bw, tstats, st, c->tune_shadow);
     rec(c, 2, false);
     rec(c, 3, true);
     strict::launch_bdpt_film(wp, sc, c->q, bw, film, st);
@@ -873,7 +876,8 @@ int wl_render(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_
     const uint64_t total = (uint64_t)npix * p->spp;
     const bool bdpt = p->strategy == WL_STRATEGY_BDPT;
     const uint64_t maxv2 = (uint64_t)p->max_depth * p->max_depth;
-    uint64_t want = p->wave_paths ? p->wave_paths : (bdpt ? (1ull << 25) / maxv2 : (1ull << 23));
+    uint64_t want = p->wave_paths ? p->wave_paths
+                                  : (bdpt ? (1ull << 25) / maxv2 : (c->tune_wave ? c->tune_wave : (1ull << 23)));
     if (want < 1024) want = 1024;
     if (want > (1ull << 26)) want = 1ull << 26;
     if (bdpt && want > (1ull << 26) / maxv2) want = (1ull << 26) / maxv2;
@@ -936,6 +940,8 @@ int wl_render(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_
             key_add(key, c->bd);
             key_add(key, p->max_depth);
             key_add(key, (uint32_t)(bdpt * 2 + strict_math));
+            key_add(key, c->tune_extend);
+            key_add(key, c->tune_shadow);
             uint32_t nl = 0;
             cudaGraphExec_t exec = nullptr;
             int rc2 = wave_graph(c, key, [&] {
@@ -1258,12 +1264,12 @@ int wl_render_nrc(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_ren
             // every path has ended by vertex train_end when training paths end at the cache
             const uint32_t bounces = nb.train_end && nb.train_end < p->max_depth ? nb.train_end : p->max_depth;
             for (uint32_t b = 0; b < bounces; b++) {
-                launch_extend(sc, c->q, in, false, st);
+                launch_extend(sc, c->q, in, false, st, c->tune_extend);
                 CK(cudaMemsetAsync(c->q.counters + (in ^ 1), 0, sizeof(uint32_t), st));
                 CK(cudaMemsetAsync(c->q.counters + 2, 0, sizeof(uint32_t), st));
                 if (strict_math) strict::launch_shade_nrc(wp, sc, c->q, in, nb, st);
                 else fast::launch_shade_nrc(wp, sc, c->q, in, nb, st);
-                launch_shadow(sc, c->q, false, st);
+                launch_shadow(sc, c->q, false, st, c->tune_shadow);
                 in ^= 1;
             }
             nrc_query(n->net, s->d_mats, n->queries, n->n_queries, c->q.st_rad, wp.count, st);
@@ -1276,6 +1282,117 @@ int wl_render_nrc(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_ren
         CK(cudaGetLastError());
     }
     if (f) f->f.frames64 += p->spp;
+    return WL_OK;
+}
+
+// Autotuner: coordinate descent over the launch shapes that the renders use, each candidate timed
+// (CUDA events, after one untimed run) on a render of the caller's scene, camera and params with
+// spp reduced to about 2^24 paths: first the paths in flight per wave, then the extend pass's
+// persistent CTAs per SM and warp refill threshold, then the shadow pass's. The fastest shape
+// stays in the context for later renders.
+int wl_autotune(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_params *p,
+                wl_tune_result *out) {
+    ARG(c && s && cam && p && out, "null argument");
+    ARG(s->ctx == c, "scene must belong to the context");
+    ARG(p->strategy <= WL_STRATEGY_MIS, "the autotuner times the path tracer (UPT, NEE or MIS)");
+    CK(cudaSetDevice(c->device));
+    wl_film *film = nullptr;
+    int rc = wl_film_create(c, p->width, p->height, 0, &film);
+    if (rc != WL_OK) return rc;
+    wl_render_params q = *p;
+    const uint64_t npix = (uint64_t)p->width * p->height;
+    uint64_t spp = (1ull << 24) / (npix ? npix : 1);
+    q.spp = (uint32_t)(spp < 1 ? 1 : (spp > p->spp ? p->spp : spp));
+    q.flags = 0;
+    q.wave_paths = 0;
+    uint32_t candidates = 0;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto timed = [&](float &ms) -> int {
+        for (int rep = 0; rep < 2; rep++) {
+            cudaEventRecord(e0, c->stream);
+            int r = wl_render(c, s, cam, &q, film);
+            if (r != WL_OK) return r;
+            cudaEventRecord(e1, c->stream);
+            if (cudaEventSynchronize(e1) != cudaSuccess) return fail(WL_ERR_CUDA, "autotune timing");
+            cudaEventElapsedTime(&ms, e0, e1);
+        }
+        c->stats_pending = false;
+        candidates++;
+        return WL_OK;
+    };
+    const uint32_t saved_wave = c->tune_wave;
+    const TraceTune saved_e = c->tune_extend, saved_s = c->tune_shadow;
+    c->tune_wave = 0;
+    c->tune_extend = TraceTune{};
+    c->tune_shadow = TraceTune{};
+    float ms_default = 0.f, best = 0.f;
+    rc = timed(ms_default);
+    best = ms_default;
+    uint32_t best_wave = 0;
+    const uint32_t waves[] = {1u << 21, 1u << 22, 1u << 23, 1u << 24, 1u << 25};
+    for (uint32_t w : waves) {
+        if (rc != WL_OK) break;
+        c->tune_wave = w;
+        float ms = 0.f;
+        rc = timed(ms);
+        if (rc == WL_OK && ms < best) { best = ms; best_wave = w; }
+    }
+    c->tune_wave = best_wave;
+    const uint32_t ctas[] = {0u, 6u, 4u};
+    const uint32_t refills[] = {4u, 6u, 8u, 12u, 16u, 24u};
+    for (int pass = 0; pass < 2 && rc == WL_OK; pass++) {
+        TraceTune &t = pass == 0 ? c->tune_extend : c->tune_shadow;
+        TraceTune bt = t;
+        for (uint32_t ct : ctas)
+            for (uint32_t rf : refills) {
+                if (rc != WL_OK) break;
+                t.ctas_per_sm = ct;
+                t.refill = rf;
+                float ms = 0.f;
+                rc = timed(ms);
+                if (rc == WL_OK && ms < best) { best = ms; bt = t; }
+            }
+        t = bt;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    wl_film_destroy(film);
+    if (rc != WL_OK) {
+        c->tune_wave = saved_wave;
+        c->tune_extend = saved_e;
+        c->tune_shadow = saved_s;
+        return rc;
+    }
+    out->wave_paths = c->tune_wave;
+    out->extend_ctas_per_sm = c->tune_extend.ctas_per_sm;
+    out->extend_refill = c->tune_extend.refill;
+    out->shadow_ctas_per_sm = c->tune_shadow.ctas_per_sm;
+    out->shadow_refill = c->tune_shadow.refill;
+    out->candidates = candidates;
+    out->ms_default = ms_default;
+    out->ms_tuned = best;
+    out->spp = q.spp;
+    return WL_OK;
+}
+
+int wl_set_tune(wl_context *c, const wl_tune_result *t) {
+    ARG(c, "null context");
+    if (!t) {
+        c->tune_wave = 0;
+        c->tune_extend = TraceTune{};
+        c->tune_shadow = TraceTune{};
+        return WL_OK;
+    }
+    auto ok_refill = [](uint32_t r) { return r == 4 || r == 6 || r == 8 || r == 12 || r == 16 || r == 24; };
+    ARG(ok_refill(t->extend_refill) && ok_refill(t->shadow_refill), "refill must be 4, 6, 8, 12, 16 or 24");
+    ARG(t->wave_paths == 0 || (t->wave_paths >= 1024 && t->wave_paths <= (1u << 26)), "wave_paths out of range");
+    c->tune_wave = t->wave_paths;
+    c->tune_extend.ctas_per_sm = t->extend_ctas_per_sm;
+    c->tune_extend.refill = t->extend_refill;
+    c->tune_shadow.ctas_per_sm = t->shadow_ctas_per_sm;
+    c->tune_shadow.refill = t->shadow_refill;
     return WL_OK;
 }
 

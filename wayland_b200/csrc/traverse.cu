@@ -39,17 +39,17 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
-// Refill threshold: a warp fetches new rays for its idle lanes once this many are idle (or
-// when none is busy), so that long rays no longer hold the whole warp (Aila & Laine 2009,
-// persistent threads with dynamic fetch).
-constexpr int REFILL = 12;
+// Refill threshold R: a warp fetches new rays for its idle lanes once R are idle (or when none
+// is busy), so that long rays no longer hold the whole warp (Aila & Laine 2009, persistent
+// threads with dynamic fetch). Instantiated for R in {4, 6, 8, 12, 16, 24}; the autotuner picks
+// one.
 
 // Persistent traversal over a queue of n rays. MODE 0: closest hit of ray queue `in`, hit
 // written to q.hit. MODE 1: any hit of the shadow queue; an unoccluded ray adds its light
 // sample to the path radiance. MODE 2: any hit of the bidirectional connection rays (passed as
 // the shadow queue); an unoccluded ray stores its value as the result of its connection
 // (EvalContri's visibility ray, BDPT.cu:460-467).
-template <int MODE, bool STATS>
+template <int MODE, bool STATS, int REFILL>
 __global__ void __launch_bounds__(TT) k_trace(DevScene sc, Queues q, int in, uint32_t *fetch) {
     constexpr bool ANY = MODE != 0;
     const uint32_t n = MODE == 0 ? q.counters[in] : q.counters[2];
@@ -102,7 +102,9 @@ __global__ void __launch_bounds__(TT) k_trace(DevScene sc, Queues q, int in, uin
     if (STATS) add_stats(q.totals + (MODE == 0 ? 2 : 4), cn, ct);
 }
 
-// wl_cast_rays: the same persistent traversal over an array of 32-byte wl_ray records.
+// wl_cast_rays: the same persistent traversal over an array of 32-byte wl_ray records
+// (refill threshold 12).
+constexpr int CAST_REFILL = 12;
 template <bool ANY>
 __global__ void __launch_bounds__(TT) k_cast(DevScene sc, const float4 *rays, float4 *hits,
                                               uint32_t n, uint32_t *fetch) {
@@ -114,7 +116,7 @@ __global__ void __launch_bounds__(TT) k_cast(DevScene sc, const float4 *rays, fl
     while (true) {
         uint32_t idle = __ballot_sync(0xffffffffu, !active && !exhausted);
         uint32_t busy = __ballot_sync(0xffffffffu, active);
-        if (idle && (__popc(idle) >= REFILL || busy == 0)) {
+        if (idle && (__popc(idle) >= CAST_REFILL || busy == 0)) {
             uint32_t base = 0;
             if (lane == 0) base = atomicAdd(fetch, (uint32_t)__popc(idle));
             base = __shfl_sync(0xffffffffu, base, 0);
@@ -180,38 +182,66 @@ __global__ void __launch_bounds__(TT) k_cast_stats(DevScene sc, const wl_ray *ra
     }
 }
 
-int grid_for(const void *kernel) {
-    // persistent grid: every SM filled to the occupancy the kernel reaches
+int grid_for(const void *kernel, uint32_t ctas_per_sm = 0) {
+    // persistent grid: every SM filled to the occupancy the kernel reaches (or to ctas_per_sm
+    // CTAs when that is lower)
     int dev = 0, sms = 0, per = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, TT, 0);
     if (per < 1) per = 1;
+    if (ctas_per_sm && (int)ctas_per_sm < per) per = (int)ctas_per_sm;
     return sms * per;
+}
+
+template <int MODE, bool STATS, int R>
+void trace_launch(const DevScene &sc, const Queues &q, int in, uint32_t *fetch, uint32_t ctas,
+                  cudaStream_t s) {
+    static int full = grid_for((const void *)k_trace<MODE, STATS, R>);
+    int grid = full;
+    if (ctas) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if ((int)ctas * sms < full) grid = (int)ctas * sms;
+    }
+    k_trace<MODE, STATS, R><<<grid, TT, 0, s>>>(sc, q, in, fetch);
+}
+
+template <int MODE, bool STATS>
+void trace_dispatch(const DevScene &sc, const Queues &q, int in, uint32_t *fetch, const TraceTune &t,
+                    cudaStream_t s) {
+    switch (t.refill) {
+    case 4: trace_launch<MODE, STATS, 4>(sc, q, in, fetch, t.ctas_per_sm, s); break;
+    case 6: trace_launch<MODE, STATS, 6>(sc, q, in, fetch, t.ctas_per_sm, s); break;
+    case 8: trace_launch<MODE, STATS, 8>(sc, q, in, fetch, t.ctas_per_sm, s); break;
+    case 16: trace_launch<MODE, STATS, 16>(sc, q, in, fetch, t.ctas_per_sm, s); break;
+    case 24: trace_launch<MODE, STATS, 24>(sc, q, in, fetch, t.ctas_per_sm, s); break;
+    default: trace_launch<MODE, STATS, 12>(sc, q, in, fetch, t.ctas_per_sm, s); break;
+    }
 }
 
 }  // namespace
 
 // Work counters live in the queues' counter block: [6] extend, [7] shadow, [8] cast.
-void launch_extend(const DevScene &sc, const Queues &q, int in, bool stats, cudaStream_t s) {
-    static int grid = grid_for((const void *)k_trace<0, false>);
+void launch_extend(const DevScene &sc, const Queues &q, int in, bool stats, cudaStream_t s,
+                   const TraceTune &t) {
     cudaMemsetAsync(q.counters + 6, 0, sizeof(uint32_t), s);
-    if (stats) k_trace<0, true><<<grid, TT, 0, s>>>(sc, q, in, q.counters + 6);
-    else k_trace<0, false><<<grid, TT, 0, s>>>(sc, q, in, q.counters + 6);
+    if (stats) trace_dispatch<0, true>(sc, q, in, q.counters + 6, t, s);
+    else trace_dispatch<0, false>(sc, q, in, q.counters + 6, t, s);
 }
 
-void launch_shadow(const DevScene &sc, const Queues &q, bool stats, cudaStream_t s) {
-    static int grid = grid_for((const void *)k_trace<1, false>);
+void launch_shadow(const DevScene &sc, const Queues &q, bool stats, cudaStream_t s,
+                   const TraceTune &t) {
     cudaMemsetAsync(q.counters + 7, 0, sizeof(uint32_t), s);
-    if (stats) k_trace<1, true><<<grid, TT, 0, s>>>(sc, q, 0, q.counters + 7);
-    else k_trace<1, false><<<grid, TT, 0, s>>>(sc, q, 0, q.counters + 7);
+    if (stats) trace_dispatch<1, true>(sc, q, 0, q.counters + 7, t, s);
+    else trace_dispatch<1, false>(sc, q, 0, q.counters + 7, t, s);
 }
 
 // Connection rays of a bidirectional wave: the shadow-queue fields of q are pointed at the
 // wave's connection-ray queue and counters ([2] queue size, [7] work counter).
 void launch_connection_rays(const DevScene &sc, const Queues &q, const BdptWave &bw, bool stats,
-                            cudaStream_t s) {
-    static int grid = grid_for((const void *)k_trace<2, false>);
+                            cudaStream_t s, const TraceTune &t) {
     Queues cq = q;
     cq.sh_o = bw.cs_o;
     cq.sh_d = bw.cs_d;
@@ -219,8 +249,8 @@ void launch_connection_rays(const DevScene &sc, const Queues &q, const BdptWave 
     cq.counters = bw.counters;
     cq.conn_val = bw.conn_val;
     cudaMemsetAsync(bw.counters + 7, 0, sizeof(uint32_t), s);
-    if (stats) k_trace<2, true><<<grid, TT, 0, s>>>(sc, cq, 0, bw.counters + 7);
-    else k_trace<2, false><<<grid, TT, 0, s>>>(sc, cq, 0, bw.counters + 7);
+    if (stats) trace_dispatch<2, true>(sc, cq, 0, bw.counters + 7, t, s);
+    else trace_dispatch<2, false>(sc, cq, 0, bw.counters + 7, t, s);
 }
 
 void launch_cast(const DevScene &sc, const wl_ray *rays, wl_hit *hits, uint32_t n, uint32_t mode,

@@ -213,11 +213,19 @@ void launch_tonemap(const Film &f, cudaStream_t s);
 void launch_debug_rng(uint32_t rng, uint64_t seed, const uint32_t *pixels, uint32_t npix,
                       uint32_t frame, uint32_t count, float *out, cudaStream_t s);
 }
-// traverse.cu
-void launch_extend(const DevScene &sc, const Queues &q, int in, bool stats, cudaStream_t s);
-void launch_shadow(const DevScene &sc, const Queues &q, bool stats, cudaStream_t s);
+// traverse.cu. TraceTune: the launch shape of a traversal pass (the autotuner's knobs):
+// persistent CTAs per SM (0 = as many as fit) and the warp refill threshold (4, 6, 8, 12, 16
+// or 24).
+struct TraceTune {
+    uint32_t ctas_per_sm = 0;
+    uint32_t refill = 12;
+};
+void launch_extend(const DevScene &sc, const Queues &q, int in, bool stats, cudaStream_t s,
+                   const TraceTune &t = TraceTune{});
+void launch_shadow(const DevScene &sc, const Queues &q, bool stats, cudaStream_t s,
+                   const TraceTune &t = TraceTune{});
 void launch_connection_rays(const DevScene &sc, const Queues &q, const BdptWave &bw, bool stats,
-                            cudaStream_t s);
+                            cudaStream_t s, const TraceTune &t = TraceTune{});
 void launch_cast(const DevScene &sc, const wl_ray *rays, wl_hit *hits, uint32_t n, uint32_t mode,
                  uint32_t *fetch, cudaStream_t s);
 void launch_cast_stats(const DevScene &sc, const wl_ray *rays, uint32_t n, uint32_t mode,
