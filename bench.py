@@ -297,6 +297,40 @@ def graph_leg(wl, torch, ctx, sc, scene, stream, frames=16):
     return out
 
 
+def batch_leg(wl, torch, ctx, stream, jobs=64):
+    """Configuration 3: 64 procedural scenes (scenes.batch_scene: triangles lognormal in [10K, 5M],
+    resolution, spp, depth and 1-8 lights drawn per scene), rendered one wl_render call per scene
+    and as one wl_render_batch. Device time; Mpaths/s = all jobs' W x H x spp / time."""
+    from wayland_b200 import scenes
+    datas = [scenes.batch_scene(i) for i in range(jobs)]
+    objs = [wl.Scene(ctx, d) for d in datas]
+    params = [wl.render_params(d.width, d.height, d.spp, max_depth=d.max_depth) for d in datas]
+    cams = [d.camera_struct() for d in datas]
+    paths = sum(d.width * d.height * d.spp for d in datas)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    out = {"jobs": jobs, "triangles": int(sum(d.num_tris for d in datas)), "paths": int(paths)}
+    for mode in ("separate", "batch", "separate", "batch"):  # second round timed
+        films = [wl.Film(ctx, d.width, d.height) for d in datas]
+        ctx.sync()
+        e0.record(stream)
+        if mode == "batch":
+            wl.render_batch(ctx, objs, cams, params, films)
+        else:
+            for o, c, p, f in zip(objs, cams, params, films):
+                wl.render(ctx, o, c, p, f)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[mode] = {"ms": round(ms, 1), "mpaths_s": round(paths / ms / 1e3, 1)}
+        for f in films:
+            f.close()
+    for o in objs:
+        o.close()
+    out["batch_gain"] = round(out["separate"]["ms"] / out["batch"]["ms"], 3)
+    return out
+
+
 def bdpt_ao_leg(wl, torch, ctx, res=512, spp=256, oracle_spp=4096, ao_res=(512, 256)):
     """Configuration 5: the glass-sphere caustic scene (158,420 sphere triangles + plane + a
     0.05-wide quad light). BDPT with subpaths of at most 10 vertices: samples/s at res x res x
@@ -466,6 +500,7 @@ def main():
     ap.add_argument("--no-nrc", action="store_true")
     ap.add_argument("--no-bdpt", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--bdpt-only", action="store_true", help="only the BDPT + AO leg (prints its JSON)")
     ap.add_argument("--nrc-res", default="960x540", help="resolution of the radiance-cache comparison")
     ap.add_argument("--nrc-oracle-spp", type=int, default=8192)
@@ -624,6 +659,8 @@ def main():
             line["raycast"] = raycast_microbench(wl, torch, ctx, sc, scene, stream)
         if world == 1:
             line["progressive_1spp"] = graph_leg(wl, torch, ctx, sc, scene, stream)
+        if world == 1 and not args.no_batch:
+            line["batch"] = batch_leg(wl, torch, ctx, stream)
         if world == 1 and not args.no_bdpt:
             line["bdpt"] = bdpt_ao_leg(wl, torch, ctx)
         if world == 1 and not args.no_nrc:

@@ -314,6 +314,15 @@ WL_API void wl_ao_params_default(wl_ao_params *params, uint32_t width, uint32_t 
 WL_API int wl_render_ao(wl_context *ctx, wl_scene *scene, const wl_camera *camera,
                         const wl_ao_params *params, wl_film *film);
 
+/* Batched rendering (no counterpart in the reference): n jobs, each a scene, camera, params and
+ * film as for wl_render (UPT, NEE or MIS; one math mode for all jobs; a film per job), rendered
+ * together. Every wave is a range of the concatenated sample space of the jobs, so the passes
+ * mix scenes, resolutions and path depths and stay full while some jobs' paths are still deep.
+ * Each film receives exactly the image wl_render would give it. n <= 65535. */
+WL_API int wl_render_batch(wl_context *ctx, uint32_t n, wl_scene *const *scenes,
+                           const wl_camera *cameras, const wl_render_params *params,
+                           wl_film *const *films);
+
 /* ---- autotuner ---------------------------------------------------------------------- */
 /* No counterpart in the reference (OptiX chooses its own launch shapes). The launch shape of
  * the renders: paths in flight per wave (0 = automatic), and per traversal pass the persistent

@@ -231,3 +231,41 @@ def test_tuned_shapes_keep_the_image(ctx):
     film.close()
     ctx.set_tune(None)
     s.close()
+
+
+def test_batch_matches_separate_renders(ctx):
+    """wl_render_batch: jobs of different scenes, sizes, spp, depths and random streams share
+    waves (small waves make jobs span several, and waves span several jobs); every film equals
+    the film of a separate wl_render call bit for bit."""
+    jobs = [
+        (scenes.cornell_box(40, 30), dict(spp=3, max_depth=8)),
+        (small_sphere(48, 32), dict(spp=5, max_depth=12, rng=wl.RNG_PCG32, seed=9)),
+        (scenes.glass_sphere(32, 32, subdiv=10), dict(spp=2, max_depth=6, first_frame=4)),
+        (scenes.cornell_box(17, 13), dict(spp=7, max_depth=3, strategy=wl.STRATEGY_NEE)),
+    ]
+    ctx.set_tune(dict(wave_paths=1500, extend_ctas_per_sm=0, extend_refill=12,
+                      shadow_ctas_per_sm=0, shadow_refill=12))
+    try:
+        objs, params, films, refs = [], [], [], []
+        for sc, kw in jobs:
+            kw = dict(kw)
+            spp = kw.pop("spp")
+            p = wl.render_params(sc.width, sc.height, spp, math=wl.MATH_STRICT, env=sc.env, **kw)
+            s = wl.Scene(ctx, sc)
+            objs.append(s)
+            params.append(p)
+            films.append(wl.Film(ctx, sc.width, sc.height))
+            rf = wl.Film(ctx, sc.width, sc.height)
+            wl.render(ctx, s, sc.camera_struct(), p, rf)
+            refs.append(rf.download())
+            rf.close()
+        wl.render_batch(ctx, objs, [sc.camera_struct() for sc, _ in jobs], params, films)
+        for f, r in zip(films, refs):
+            assert r.max() > 0
+            assert np.array_equal(bits(f.download()), bits(r))
+        for f in films:
+            f.close()
+        for s in objs:
+            s.close()
+    finally:
+        ctx.set_tune(None)

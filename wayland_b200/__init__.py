@@ -319,6 +319,16 @@ def render_nrc(ctx, scene, camera, params, cache, film):
                                                       film.handle if film is not None else None))
 
 
+def render_batch(ctx, scenes, cameras, params, films):
+    """wl_render_batch: several (scene, camera, params, film) jobs rendered together."""
+    n = len(scenes)
+    sh = (C.c_void_p * n)(*[s.handle for s in scenes])
+    fh = (C.c_void_p * n)(*[f.handle for f in films])
+    cams = (_abi.Camera * n)(*cameras)
+    ps = (_abi.RenderParams * n)(*params)
+    _abi.check("wl_render_batch", ctx.lib.wl_render_batch(ctx.handle, n, sh, cams, ps, fh))
+
+
 def render(ctx, scene, camera, params, film):
     _abi.check("wl_render", ctx.lib.wl_render(ctx.handle, scene.handle, C.byref(camera),
                                               C.byref(params), film.handle))

@@ -146,6 +146,7 @@ SIGNATURES = {
     "wl_debug_rng": (C.c_int, [_P, _U32, C.c_uint64, _P, _U32, _U32, _U32, _P]),
     "wl_render_noalloc": (C.c_int, [_P, _P, C.POINTER(Camera), C.POINTER(RenderParams), _P]),
     "wl_ao_params_default": (None, [C.POINTER(AoParams), _U32, _U32, _U32]),
+    "wl_render_batch": (C.c_int, [_P, _U32, _P, _P, _P, _P]),
     "wl_autotune": (C.c_int, [_P, _P, C.POINTER(Camera), C.POINTER(RenderParams), C.POINTER(TuneResult)]),
     "wl_set_tune": (C.c_int, [_P, _P]),
     "wl_nrc_params_default": (None, [C.POINTER(NrcParams)]),

@@ -77,6 +77,11 @@ struct wl_context {
     // launch shapes chosen by wl_autotune (defaults until then)
     uint32_t tune_wave = 0;
     TraceTune tune_extend{}, tune_shadow{};
+    // batched renders: the job table and the job of every wave slot
+    BatchJob *d_jobs = nullptr;
+    size_t jobs_cap = 0;
+    uint16_t *d_slot_job = nullptr;
+    size_t slot_job_cap = 0;
 };
 
 struct wl_scene {
@@ -298,6 +303,8 @@ int wl_context_destroy(wl_context *c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->q_block) cudaFree(c->q_block);
     if (c->bd_block) cudaFree(c->bd_block);
+    if (c->d_jobs) cudaFree(c->d_jobs);
+    if (c->d_slot_job) cudaFree(c->d_slot_job);
     if (c->d_dyn_all) cudaFree(c->d_dyn_all);
     if (c->d_dyn_ctr) cudaFree(c->d_dyn_ctr);
     for (auto &g : c->graphs)
@@ -958,6 +965,123 @@ int wl_render(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_
     }
     CK(cudaEventRecord(c->ev_total[1], st));
     f->f.frames64 += p->spp;
+    c->stats = wl_render_stats{};
+    c->stats.paths = total;
+    c->stats.waves = waves;
+    c->stats.kernel_launches = launches;
+    c->stats_pending = true;
+    return WL_OK;
+}
+
+// Batched rendering: every wave is a range of the batch's sample space (jobs in order, each job's
+// samples in the order wl_render would trace them), so the passes mix scenes and stay full while
+// a few jobs' paths are still deep. Each film receives exactly what wl_render would give it.
+int wl_render_batch(wl_context *c, uint32_t n, wl_scene *const *scenes, const wl_camera *cams,
+                    const wl_render_params *params, wl_film *const *films) {
+    ARG(c && scenes && cams && params && films, "null argument");
+    ARG(n > 0 && n <= 65535, "1 to 65535 jobs");
+    CK(cudaSetDevice(c->device));
+    c->stats_pending = false;
+    std::vector<BatchJob> jobs(n);
+    uint64_t total = 0;
+    uint32_t maxd = 0;
+    const uint32_t math = params[0].math;
+    for (uint32_t j = 0; j < n; j++) {
+        wl_scene *s = scenes[j];
+        wl_film *f = films[j];
+        const wl_render_params *p = &params[j];
+        const wl_camera *cam = &cams[j];
+        ARG(s && f, "null scene or film");
+        ARG(s->ctx == c && f->ctx == c, "scenes and films must belong to the context");
+        if (!s->built) return fail(WL_ERR_NOT_BUILT, "bvh not built");
+        ARG(p->width == f->f.W && p->height == f->f.H, "film size differs from the render size");
+        ARG(p->spp > 0, "spp must be > 0");
+        ARG(p->max_depth > 0 && p->max_depth <= 1024, "max_depth out of range");
+        ARG(p->strategy <= WL_STRATEGY_MIS, "batched renders run the path tracer (UPT, NEE or MIS)");
+        ARG(p->rng <= WL_RNG_PCG32, "bad rng");
+        ARG(p->math == math && math <= WL_MATH_STRICT, "one math mode for all jobs");
+        ARG(p->lights == WL_LIGHTS_UNIFORM, "only uniform light selection is available");
+        ARG(p->rr_prob > 0.0f && p->rr_prob <= 1.0f, "rr_prob must be in (0, 1]");
+        ARG(finite3(cam->pos) && finite3(cam->look_at) && finite3(cam->up) && finite3(cam->right), "non-finite camera");
+        for (uint32_t k = 0; k < j; k++) ARG(films[k] != f, "each job needs its own film");
+        BatchJob &J = jobs[j];
+        std::memset(&J, 0, sizeof(J));
+        WaveParams &wp = J.wp;
+        wp.W = p->width; wp.H = p->height; wp.npix = p->width * p->height;
+        wp.first_frame = p->first_frame;
+        wp.max_depth = p->max_depth; wp.rr_depth = p->rr_depth;
+        wp.rr_prob = p->rr_prob; wp.eps = p->eps;
+        wp.strategy = p->strategy; wp.rng = p->rng; wp.lights = p->lights; wp.seed = p->seed;
+        for (int k = 0; k < 3; k++) {
+            wp.env[k] = p->env[k];
+            wp.cam_pos[k] = cam->pos[k]; wp.cam_look[k] = cam->look_at[k];
+            wp.cam_up[k] = cam->up[k]; wp.cam_right[k] = cam->right[k];
+        }
+        wp.has_env = (p->env[0] != 0.f || p->env[1] != 0.f || p->env[2] != 0.f) ? 1u : 0u;
+        J.sc = dev_scene(s);
+        J.film = f->f;
+        J.off = total;
+        J.n = (uint64_t)wp.npix * p->spp;
+        total += J.n;
+        if (p->max_depth > maxd) maxd = p->max_depth;
+    }
+    uint64_t wave = c->tune_wave ? c->tune_wave : (1ull << 23);
+    if (wave > total) wave = total;
+    int rc = ensure_queues(c, (uint32_t)wave);
+    if (rc != WL_OK) return rc;
+    if (c->jobs_cap < n) {
+        if (c->d_jobs) cudaFree(c->d_jobs);
+        c->d_jobs = nullptr;
+        CK(cudaMalloc(&c->d_jobs, sizeof(BatchJob) * n));
+        c->jobs_cap = n;
+    }
+    if (c->slot_job_cap < wave) {
+        if (c->d_slot_job) cudaFree(c->d_slot_job);
+        c->d_slot_job = nullptr;
+        CK(cudaMalloc(&c->d_slot_job, sizeof(uint16_t) * wave));
+        c->slot_job_cap = wave;
+    }
+    cudaStream_t st = c->stream;
+    CK(cudaMemcpyAsync(c->d_jobs, jobs.data(), sizeof(BatchJob) * n, cudaMemcpyHostToDevice, st));
+    for (auto &u : c->ev_used) u = 0;
+    CK(cudaMemsetAsync(c->q.totals, 0, 6 * sizeof(unsigned long long), st));
+    CK(cudaEventRecord(c->ev_total[0], st));
+    const bool strict_math = math == WL_MATH_STRICT;
+    const DevScene sc0 = jobs[0].sc;
+    uint32_t launches = 0, waves = 0;
+    for (uint64_t base = 0; base < total; base += wave) {
+        const uint32_t count = (uint32_t)((total - base) < wave ? (total - base) : wave);
+        BatchView bv{c->d_jobs, n, base, c->d_slot_job};
+        rec(c, 3, true);
+        if (strict_math) strict::launch_generate_batch(bv, c->q, count, st);
+        else fast::launch_generate_batch(bv, c->q, count, st);
+        rec(c, 3, false);
+        int in = 0;
+        for (uint32_t b = 0; b < maxd; b++) {
+            rec(c, 0, true);
+            launch_extend(sc0, c->q, in, false, st, c->tune_extend, bv);
+            rec(c, 0, false);
+            cudaMemsetAsync(c->q.counters + (in ^ 1), 0, sizeof(uint32_t), st);
+            cudaMemsetAsync(c->q.counters + 2, 0, sizeof(uint32_t), st);
+            rec(c, 1, true);
+            if (strict_math) strict::launch_shade_batch(bv, c->q, in, st);
+            else fast::launch_shade_batch(bv, c->q, in, st);
+            rec(c, 1, false);
+            rec(c, 2, true);
+            launch_shadow(sc0, c->q, false, st, c->tune_shadow, bv);
+            rec(c, 2, false);
+            in ^= 1;
+            launches += 3;
+        }
+        rec(c, 3, true);
+        strict::launch_film_batch(bv, c->q, count, st);
+        rec(c, 3, false);
+        launches += 2;
+        waves++;
+        CK(cudaGetLastError());
+    }
+    CK(cudaEventRecord(c->ev_total[1], st));
+    for (uint32_t j = 0; j < n; j++) films[j]->f.frames64 += params[j].spp;
     c->stats = wl_render_stats{};
     c->stats.paths = total;
     c->stats.waves = waves;

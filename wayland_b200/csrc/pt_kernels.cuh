@@ -76,21 +76,25 @@ __device__ __forceinline__ float tri_area(const DevScene &sc, uint32_t t) {
     return 0.5f * length(cross(b - a, c - a));
 }
 
+// What one lane of the shade pass emits: the next ray and the shadow ray with its light sample.
+struct ShadeOut {
+    bool push_ray = false, push_shadow = false;
+    uint32_t slot = 0;
+    float eps = 0.f, sh_tmax = 0.f;
+    v3 new_o, new_d, sh_d, ld;
+};
+
+// __closesthit__radiance + the NEE block of __raygen__RenderFrame for ray i of queue `in`,
+// with the path's own scene and parameters (wp.base + slot = the path's sample index).
 template <bool NRC>
-__global__ void __launch_bounds__(PT) k_shade(WaveParams wp, DevScene sc, Queues q, int in,
-                                              NrcWaveBuffers nb) {
-    wave_dyn(wp);
-    const uint32_t n = q.counters[in];
-    const int out = in ^ 1;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
-        uint32_t i = base + threadIdx.x;
-        bool valid = i < n;
-        bool push_ray = false, push_shadow = false;
-        uint32_t slot = 0;
-        v3 new_o, new_d, sh_d, ld;
-        float sh_tmax = 0.f;
-        if (valid) {
+__device__ __forceinline__ void shade_lane(const WaveParams &wp, const DevScene &sc, const Queues &q,
+                                           int in, uint32_t i, const NrcWaveBuffers &nb, ShadeOut &o) {
+    bool push_ray = false, push_shadow = false;
+    uint32_t slot = 0;
+    v3 new_o, new_d, sh_d, ld;
+    float sh_tmax = 0.f;
+    {
+        {
             slot = q.ray_slot[in][i];
             float4 h = q.hit[i];
             float4 ro = q.ray_o[in][i], rd = q.ray_d[in][i];
@@ -259,26 +263,119 @@ __global__ void __launch_bounds__(PT) k_shade(WaveParams wp, DevScene sc, Queues
             q.st_rad[slot] = make_float4(rad.x, rad.y, rad.z, 0.f);
             q.st_rng[slot] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
         }
-        uint32_t rpos = warp_append(push_ray, &q.counters[out]);
-        if (push_ray) {
-            q.ray_o[out][rpos] = make_float4(new_o.x, new_o.y, new_o.z, wp.eps);
-            q.ray_d[out][rpos] = make_float4(new_d.x, new_d.y, new_d.z, 1e30f);
-            q.ray_slot[out][rpos] = slot;
-        }
-        uint32_t spos = warp_append(push_shadow, &q.counters[2]);
-        if (push_shadow) {
-            q.sh_o[spos] = make_float4(new_o.x, new_o.y, new_o.z, wp.eps);
-            q.sh_d[spos] = make_float4(sh_d.x, sh_d.y, sh_d.z, sh_tmax);
-            q.sh_l[spos] = make_float4(ld.x, ld.y, ld.z, __uint_as_float(slot));
-        }
-        // segment and shadow-ray totals (one atomic per warp)
-        uint32_t nv = __popc(__ballot_sync(0xffffffffu, valid));
-        uint32_t ns = __popc(__ballot_sync(0xffffffffu, push_shadow));
-        if ((threadIdx.x & 31) == 0) {
-            if (nv) atomicAdd(&q.totals[0], (unsigned long long)nv);
-            if (ns) atomicAdd(&q.totals[1], (unsigned long long)ns);
-        }
     }
+    o.push_ray = push_ray;
+    o.push_shadow = push_shadow;
+    o.slot = slot;
+    o.eps = wp.eps;
+    o.sh_tmax = sh_tmax;
+    o.new_o = new_o;
+    o.new_d = new_d;
+    o.sh_d = sh_d;
+    o.ld = ld;
+}
+
+// Appends of the shade pass (warp-collective): next rays to queue `out`, shadow rays.
+__device__ __forceinline__ void shade_emit(const Queues &q, int out, bool valid, const ShadeOut &o) {
+    uint32_t rpos = warp_append(o.push_ray, &q.counters[out]);
+    if (o.push_ray) {
+        q.ray_o[out][rpos] = make_float4(o.new_o.x, o.new_o.y, o.new_o.z, o.eps);
+        q.ray_d[out][rpos] = make_float4(o.new_d.x, o.new_d.y, o.new_d.z, 1e30f);
+        q.ray_slot[out][rpos] = o.slot;
+    }
+    uint32_t spos = warp_append(o.push_shadow, &q.counters[2]);
+    if (o.push_shadow) {
+        q.sh_o[spos] = make_float4(o.new_o.x, o.new_o.y, o.new_o.z, o.eps);
+        q.sh_d[spos] = make_float4(o.sh_d.x, o.sh_d.y, o.sh_d.z, o.sh_tmax);
+        q.sh_l[spos] = make_float4(o.ld.x, o.ld.y, o.ld.z, __uint_as_float(o.slot));
+    }
+    // segment and shadow-ray totals (one atomic per warp)
+    uint32_t nv = __popc(__ballot_sync(0xffffffffu, valid));
+    uint32_t ns = __popc(__ballot_sync(0xffffffffu, o.push_shadow));
+    if ((threadIdx.x & 31) == 0) {
+        if (nv) atomicAdd(&q.totals[0], (unsigned long long)nv);
+        if (ns) atomicAdd(&q.totals[1], (unsigned long long)ns);
+    }
+}
+
+template <bool NRC>
+__global__ void __launch_bounds__(PT) k_shade(WaveParams wp, DevScene sc, Queues q, int in,
+                                              NrcWaveBuffers nb) {
+    wave_dyn(wp);
+    const uint32_t n = q.counters[in];
+    const int out = in ^ 1;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        uint32_t i = base + threadIdx.x;
+        bool valid = i < n;
+        ShadeOut o;
+        if (valid) shade_lane<NRC>(wp, sc, q, in, i, nb, o);
+        shade_emit(q, out, valid, o);
+    }
+}
+
+// The job of batch sample G: the last job whose first sample is <= G (jobs in sample order).
+__device__ __forceinline__ uint32_t batch_job_of(const BatchView &bv, uint64_t G) {
+    uint32_t lo = 0, hi = bv.njobs;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (bv.jobs[mid].off <= G) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Camera rays of a batch wave: slot i is batch sample wave_base + i of its job.
+__global__ void __launch_bounds__(PT) k_generate_batch(BatchView bv, Queues q, uint32_t count) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        q.counters[0] = count;
+        q.counters[1] = 0;
+        q.counters[2] = 0;
+    }
+    if (i >= count) return;
+    uint32_t j = batch_job_of(bv, bv.wave_base + i);
+    bv.slot_job[i] = (uint16_t)j;
+    const WaveParams &wp = bv.jobs[j].wp;
+    uint64_t g = bv.wave_base + i - bv.jobs[j].off;
+    uint32_t pixel = (uint32_t)(g % wp.npix);
+    uint32_t frame = wp.first_frame + (uint32_t)(g / wp.npix);
+    uint32_t px = pixel % wp.W, py = pixel / wp.W;
+    Rng rng = make_rng(wp.rng, wp.seed, pixel, frame);
+    float u = 2.f * ((float)px + rng.next()) / (float)wp.W - 1.f;
+    float v = 2.f * ((float)py + rng.next()) / (float)wp.H - 1.f;
+    v3 dir = normalize(ld3(wp.cam_look) + ld3(wp.cam_right) * u + ld3(wp.cam_up) * v);
+    q.ray_o[0][i] = make_float4(wp.cam_pos[0], wp.cam_pos[1], wp.cam_pos[2], wp.eps);
+    q.ray_d[0][i] = make_float4(dir.x, dir.y, dir.z, 1e30f);
+    q.ray_slot[0][i] = i;
+    q.st_thr[i] = make_float4(1.f, 1.f, 1.f, 1.f);
+    q.st_term[i] = make_float4(1.f, 1.f, 1.f, __uint_as_float(0u));
+    q.st_rad[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    q.st_rng[i] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
+}
+
+// The shade pass of a batch wave: each ray with its job's scene and parameters.
+__global__ void __launch_bounds__(PT) k_shade_batch(BatchView bv, Queues q, int in) {
+    const uint32_t n = q.counters[in];
+    const int out = in ^ 1;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        uint32_t i = base + threadIdx.x;
+        bool valid = i < n;
+        ShadeOut o;
+        if (valid) {
+            const BatchJob &J = bv.jobs[bv.slot_job[q.ray_slot[in][i]]];
+            WaveParams wp = J.wp;
+            wp.base = bv.wave_base - J.off;  // so that wp.base + slot is the job's sample index
+            shade_lane<false>(wp, J.sc, q, in, i, NrcWaveBuffers{}, o);
+        }
+        shade_emit(q, out, valid, o);
+    }
+}
+
+void launch_generate_batch(const BatchView &bv, const Queues &q, uint32_t count, cudaStream_t s) {
+    uint32_t blocks = (count + PT - 1) / PT;
+    k_generate_batch<<<blocks ? blocks : 1, PT, 0, s>>>(bv, q, count);
 }
 
 void launch_generate(const WaveParams &wp, const Queues &q, cudaStream_t s) {
@@ -298,6 +395,11 @@ static int shade_grid(const void *k) {
 void launch_shade(const WaveParams &wp, const DevScene &sc, const Queues &q, int in, cudaStream_t s) {
     static int grid = shade_grid((const void *)k_shade<false>);
     k_shade<false><<<grid, PT, 0, s>>>(wp, sc, q, in, NrcWaveBuffers{});
+}
+
+void launch_shade_batch(const BatchView &bv, const Queues &q, int in, cudaStream_t s) {
+    static int grid = shade_grid((const void *)k_shade_batch);
+    k_shade_batch<<<grid, PT, 0, s>>>(bv, q, in);
 }
 
 void launch_shade_nrc(const WaveParams &wp, const DevScene &sc, const Queues &q, int in,

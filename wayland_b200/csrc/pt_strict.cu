@@ -132,6 +132,53 @@ void launch_bdpt_film(const WaveParams &wp, const DevScene &sc, const Queues &q,
     k_bd_film<<<(lim + 255) / 256, 256, 0, s>>>(wp, sc.nLight, q, bw, f);
 }
 
+// Film update of a batch wave: per job, per pixel, the job's samples of this wave in increasing
+// frame (the same arithmetic as k_film). Thread i leads pixel g % npix of its job when g is
+// among the first npix samples of the job in this wave.
+__global__ void k_film_batch(BatchView bv, Queues q, uint32_t count) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const BatchJob &J = bv.jobs[bv.slot_job[i]];
+    const WaveParams &wp = J.wp;
+    const uint64_t G = bv.wave_base + i;
+    const uint64_t seg_lo = (bv.wave_base > J.off ? bv.wave_base : J.off) - J.off;
+    const uint64_t wave_end = bv.wave_base + count, job_end = J.off + J.n;
+    const uint64_t seg_hi = (wave_end < job_end ? wave_end : job_end) - J.off;
+    const uint64_t g0 = G - J.off;
+    if (g0 >= seg_lo + wp.npix) return;
+    const Film &f = J.film;
+    uint32_t pixel = (uint32_t)(g0 % wp.npix);
+    float acc[3];
+    double sum[3] = {0.0, 0.0, 0.0};
+    if (f.rgb)
+        for (int c = 0; c < 3; c++) acc[c] = f.rgb[3 * (size_t)pixel + c];
+    for (uint64_t g = g0; g < seg_hi; g += wp.npix) {
+        uint32_t slot = (uint32_t)(g + J.off - bv.wave_base);
+        uint32_t frame = wp.first_frame + (uint32_t)(g / wp.npix);
+        float4 r = q.st_rad[slot];
+        float rc[3] = {r.x, r.y, r.z};
+        if (!(isfinite(rc[0]) && isfinite(rc[1]) && isfinite(rc[2]))) rc[0] = rc[1] = rc[2] = 0.f;
+        for (int c = 0; c < 3; c++) {
+            if (frame == 0) {
+                acc[c] = rc[c];
+            } else {
+                double w0 = (double)((float)frame / ((float)frame + 1.0f));
+                double w1 = (double)(1.0f / ((float)frame + 1.0f));
+                acc[c] = (float)((double)acc[c] * w0 + (double)rc[c] * w1);
+            }
+            sum[c] += (double)rc[c];
+        }
+    }
+    if (f.rgb)
+        for (int c = 0; c < 3; c++) f.rgb[3 * (size_t)pixel + c] = acc[c];
+    if (f.sum64)
+        for (int c = 0; c < 3; c++) f.sum64[3 * (size_t)pixel + c] += sum[c];
+}
+
+void launch_film_batch(const BatchView &bv, const Queues &q, uint32_t count, cudaStream_t s) {
+    k_film_batch<<<(count + 255) / 256, 256, 0, s>>>(bv, q, count);
+}
+
 // colorBuffer = u8vec4(vec4(AceApprox(clamp(radiance, 0, 1e30)), 1) * 255) (PathTracing.cu:157-158)
 __global__ void k_tonemap(Film f) {
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;

@@ -50,7 +50,8 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 // the shadow queue); an unoccluded ray stores its value as the result of its connection
 // (EvalContri's visibility ray, BDPT.cu:460-467).
 template <int MODE, bool STATS, int REFILL>
-__global__ void __launch_bounds__(TT) k_trace(DevScene sc, Queues q, int in, uint32_t *fetch) {
+__global__ void __launch_bounds__(TT) k_trace(DevScene sc, Queues q, int in, uint32_t *fetch,
+                                              BatchView bv) {
     constexpr bool ANY = MODE != 0;
     const uint32_t n = MODE == 0 ? q.counters[in] : q.counters[2];
     const float4 *ro = MODE == 0 ? q.ray_o[in] : q.sh_o;
@@ -60,6 +61,7 @@ __global__ void __launch_bounds__(TT) k_trace(DevScene sc, Queues q, int in, uin
     uint2 stack[TRAV_STACK];
     uint32_t my = 0, cn = 0, ct = 0;
     bool active = false, exhausted = false;
+    const float4 *nodes = sc.nodes, *tris = sc.tris;  // per ray in a batch
     while (true) {
         uint32_t idle = __ballot_sync(0xffffffffu, !active && !exhausted);
         uint32_t busy = __ballot_sync(0xffffffffu, active);
@@ -72,6 +74,12 @@ __global__ void __launch_bounds__(TT) k_trace(DevScene sc, Queues q, int in, uin
                 if (r < n) {
                     float4 o = ro[r], d = rd[r];
                     trav_init(st, o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w);
+                    if (bv.jobs) {
+                        uint32_t slot = MODE == 0 ? q.ray_slot[in][r] : __float_as_uint(q.sh_l[r].w);
+                        const DevScene &js = bv.jobs[bv.slot_job[slot]].sc;
+                        nodes = js.nodes;
+                        tris = js.tris;
+                    }
                     my = r;
                     active = true;
                 } else {
@@ -81,7 +89,7 @@ __global__ void __launch_bounds__(TT) k_trace(DevScene sc, Queues q, int in, uin
             busy = __ballot_sync(0xffffffffu, active);
         }
         if (busy == 0) break;
-        if (active && trav_step<ANY, STATS>(st, stack, sc.nodes, sc.tris, &cn, &ct)) {
+        if (active && trav_step<ANY, STATS>(st, stack, nodes, tris, &cn, &ct)) {
             active = false;
             if (MODE == 0) {
                 q.hit[my] = make_float4(st.res.t, __uint_as_float(st.res.prim), st.res.u, st.res.v);
@@ -196,7 +204,7 @@ int grid_for(const void *kernel, uint32_t ctas_per_sm = 0) {
 
 template <int MODE, bool STATS, int R>
 void trace_launch(const DevScene &sc, const Queues &q, int in, uint32_t *fetch, uint32_t ctas,
-                  cudaStream_t s) {
+                  const BatchView &bv, cudaStream_t s) {
     static int full = grid_for((const void *)k_trace<MODE, STATS, R>);
     int grid = full;
     if (ctas) {
@@ -205,19 +213,19 @@ void trace_launch(const DevScene &sc, const Queues &q, int in, uint32_t *fetch, 
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if ((int)ctas * sms < full) grid = (int)ctas * sms;
     }
-    k_trace<MODE, STATS, R><<<grid, TT, 0, s>>>(sc, q, in, fetch);
+    k_trace<MODE, STATS, R><<<grid, TT, 0, s>>>(sc, q, in, fetch, bv);
 }
 
 template <int MODE, bool STATS>
 void trace_dispatch(const DevScene &sc, const Queues &q, int in, uint32_t *fetch, const TraceTune &t,
-                    cudaStream_t s) {
+                    const BatchView &bv, cudaStream_t s) {
     switch (t.refill) {
-    case 4: trace_launch<MODE, STATS, 4>(sc, q, in, fetch, t.ctas_per_sm, s); break;
-    case 6: trace_launch<MODE, STATS, 6>(sc, q, in, fetch, t.ctas_per_sm, s); break;
-    case 8: trace_launch<MODE, STATS, 8>(sc, q, in, fetch, t.ctas_per_sm, s); break;
-    case 16: trace_launch<MODE, STATS, 16>(sc, q, in, fetch, t.ctas_per_sm, s); break;
-    case 24: trace_launch<MODE, STATS, 24>(sc, q, in, fetch, t.ctas_per_sm, s); break;
-    default: trace_launch<MODE, STATS, 12>(sc, q, in, fetch, t.ctas_per_sm, s); break;
+    case 4: trace_launch<MODE, STATS, 4>(sc, q, in, fetch, t.ctas_per_sm, bv, s); break;
+    case 6: trace_launch<MODE, STATS, 6>(sc, q, in, fetch, t.ctas_per_sm, bv, s); break;
+    case 8: trace_launch<MODE, STATS, 8>(sc, q, in, fetch, t.ctas_per_sm, bv, s); break;
+    case 16: trace_launch<MODE, STATS, 16>(sc, q, in, fetch, t.ctas_per_sm, bv, s); break;
+    case 24: trace_launch<MODE, STATS, 24>(sc, q, in, fetch, t.ctas_per_sm, bv, s); break;
+    default: trace_launch<MODE, STATS, 12>(sc, q, in, fetch, t.ctas_per_sm, bv, s); break;
     }
 }
 
@@ -225,17 +233,17 @@ void trace_dispatch(const DevScene &sc, const Queues &q, int in, uint32_t *fetch
 
 // Work counters live in the queues' counter block: [6] extend, [7] shadow, [8] cast.
 void launch_extend(const DevScene &sc, const Queues &q, int in, bool stats, cudaStream_t s,
-                   const TraceTune &t) {
+                   const TraceTune &t, const BatchView &bv) {
     cudaMemsetAsync(q.counters + 6, 0, sizeof(uint32_t), s);
-    if (stats) trace_dispatch<0, true>(sc, q, in, q.counters + 6, t, s);
-    else trace_dispatch<0, false>(sc, q, in, q.counters + 6, t, s);
+    if (stats) trace_dispatch<0, true>(sc, q, in, q.counters + 6, t, bv, s);
+    else trace_dispatch<0, false>(sc, q, in, q.counters + 6, t, bv, s);
 }
 
 void launch_shadow(const DevScene &sc, const Queues &q, bool stats, cudaStream_t s,
-                   const TraceTune &t) {
+                   const TraceTune &t, const BatchView &bv) {
     cudaMemsetAsync(q.counters + 7, 0, sizeof(uint32_t), s);
-    if (stats) trace_dispatch<1, true>(sc, q, 0, q.counters + 7, t, s);
-    else trace_dispatch<1, false>(sc, q, 0, q.counters + 7, t, s);
+    if (stats) trace_dispatch<1, true>(sc, q, 0, q.counters + 7, t, bv, s);
+    else trace_dispatch<1, false>(sc, q, 0, q.counters + 7, t, bv, s);
 }
 
 // Connection rays of a bidirectional wave: the shadow-queue fields of q are pointed at the
@@ -249,8 +257,8 @@ void launch_connection_rays(const DevScene &sc, const Queues &q, const BdptWave 
     cq.counters = bw.counters;
     cq.conn_val = bw.conn_val;
     cudaMemsetAsync(bw.counters + 7, 0, sizeof(uint32_t), s);
-    if (stats) trace_dispatch<2, true>(sc, cq, 0, bw.counters + 7, t, s);
-    else trace_dispatch<2, false>(sc, cq, 0, bw.counters + 7, t, s);
+    if (stats) trace_dispatch<2, true>(sc, cq, 0, bw.counters + 7, t, BatchView{}, s);
+    else trace_dispatch<2, false>(sc, cq, 0, bw.counters + 7, t, BatchView{}, s);
 }
 
 void launch_cast(const DevScene &sc, const wl_ray *rays, wl_hit *hits, uint32_t n, uint32_t mode,

@@ -132,6 +132,22 @@ __device__ __forceinline__ void wave_dyn(WaveParams &wp) {
 }
 #endif
 
+// A batched render (wl_render_batch): job j is one (scene, camera, params, film); its samples
+// are [off, off + n) of the batch's sample space, and a wave covers any range of that space, so
+// paths of several scenes share every pass. slot_job gives each wave slot's job.
+struct BatchJob {
+    WaveParams wp;  // the job's parameters; kernels set base = wave_base - off
+    DevScene sc;
+    Film film;
+    uint64_t off, n;
+};
+struct BatchView {
+    const BatchJob *jobs;  // null: a single-scene render
+    uint32_t njobs;
+    uint64_t wave_base;    // batch sample index of slot 0
+    uint16_t *slot_job;
+};
+
 // Neural radiance cache records (nrc.cu, wl_nrc.cuh): position + material, outgoing direction,
 // shading normal, and either throughput + slot (query) or target radiance (training sample).
 struct NrcVertex {
@@ -174,6 +190,8 @@ void launch_ao(const AoWave &w, const DevScene &sc, const Queues &q, const Film 
 
 // launch functions (pt_kernels.cuh instantiated in pt_fast.cu / pt_strict.cu)
 namespace fast {
+void launch_generate_batch(const BatchView &bv, const Queues &q, uint32_t count, cudaStream_t s);
+void launch_shade_batch(const BatchView &bv, const Queues &q, int in, cudaStream_t s);
 void launch_bdpt_eye_gen(const WaveParams &wp, const Queues &q, const BdptWave &bw, cudaStream_t s);
 void launch_bdpt_eye(const WaveParams &wp, const DevScene &sc, const Queues &q, const BdptWave &bw,
                      int in, uint32_t depth, cudaStream_t s);
@@ -189,6 +207,8 @@ void launch_shade_nrc(const WaveParams &wp, const DevScene &sc, const Queues &q,
                       const NrcWaveBuffers &nb, cudaStream_t s);
 }
 namespace strict {
+void launch_generate_batch(const BatchView &bv, const Queues &q, uint32_t count, cudaStream_t s);
+void launch_shade_batch(const BatchView &bv, const Queues &q, int in, cudaStream_t s);
 void launch_bdpt_eye_gen(const WaveParams &wp, const Queues &q, const BdptWave &bw, cudaStream_t s);
 void launch_bdpt_eye(const WaveParams &wp, const DevScene &sc, const Queues &q, const BdptWave &bw,
                      int in, uint32_t depth, cudaStream_t s);
@@ -203,6 +223,7 @@ void launch_shade(const WaveParams &wp, const DevScene &sc, const Queues &q, int
 void launch_shade_nrc(const WaveParams &wp, const DevScene &sc, const Queues &q, int in,
                       const NrcWaveBuffers &nb, cudaStream_t s);
 void launch_film(const WaveParams &wp, const Queues &q, const Film &f, cudaStream_t s);
+void launch_film_batch(const BatchView &bv, const Queues &q, uint32_t count, cudaStream_t s);
 // graph replays: cur = all[2 w], all[2 w + 1] for the w-th replay (counter ctr)
 void launch_wave_begin(const uint64_t *all, uint32_t *ctr, uint64_t *cur, cudaStream_t s);
 void launch_bdpt_connections(const WaveParams &wp, const BdptWave &bw, cudaStream_t s);
@@ -221,9 +242,9 @@ struct TraceTune {
     uint32_t refill = 12;
 };
 void launch_extend(const DevScene &sc, const Queues &q, int in, bool stats, cudaStream_t s,
-                   const TraceTune &t = TraceTune{});
+                   const TraceTune &t = TraceTune{}, const BatchView &bv = BatchView{});
 void launch_shadow(const DevScene &sc, const Queues &q, bool stats, cudaStream_t s,
-                   const TraceTune &t = TraceTune{});
+                   const TraceTune &t = TraceTune{}, const BatchView &bv = BatchView{});
 void launch_connection_rays(const DevScene &sc, const Queues &q, const BdptWave &bw, bool stats,
                             cudaStream_t s, const TraceTune &t = TraceTune{});
 void launch_cast(const DevScene &sc, const wl_ray *rays, wl_hit *hits, uint32_t n, uint32_t mode,

@@ -336,6 +336,70 @@ def glass_sphere(width=1024, height=1024, spp=256, max_depth=10, subdiv=89, ligh
                  width=width, height=height, spp=spp, max_depth=max_depth)
 
 
+def icosphere_soup(n):
+    """Each icosahedron face split into n^2 triangles (20 n^2 in total), 3 vertices per triangle
+    (not welded: fast to build for millions of triangles; flat shading)."""
+    V0, F = _icosahedron()
+    a_i, a_j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    up = (a_i + a_j) <= n - 1
+    ui, uj = a_i[up].astype(np.float64), a_j[up].astype(np.float64)
+    dn = (a_i + a_j) <= n - 2
+    di, dj = a_i[dn].astype(np.float64), a_j[dn].astype(np.float64)
+    # lattice coordinates of the three corners of every triangle of one face
+    ci = np.concatenate([np.stack([ui, ui + 1, ui], 1), np.stack([di + 1, di + 1, di], 1)])
+    cj = np.concatenate([np.stack([uj, uj, uj + 1], 1), np.stack([dj, dj + 1, dj + 1], 1)])
+    out = []
+    for a, b, c in F:
+        A, B, Cc = V0[a], V0[b], V0[c]
+        pts = A[None, None] + (B - A)[None, None] * (ci[..., None] / n) + (Cc - A)[None, None] * (cj[..., None] / n)
+        out.append(pts)
+    P = np.concatenate(out).reshape(-1, 3)
+    P /= np.linalg.norm(P, axis=1, keepdims=True)
+    return P.astype(np.float32), np.arange(len(P), dtype=np.uint32).reshape(-1, 3)
+
+
+def batch_scene(seed):
+    """One job of the batched configuration: a procedural scene from its seed. Triangles
+    lognormal (median 200K) clipped to [10K, 5M] on an ellipsoid soup over a ground quad;
+    random Disney material; 1-8 quad lights; resolution uniform in [256, 1024] per axis; spp
+    uniform in [4, 64]; depth uniform in [4, 16]."""
+    rng = np.random.default_rng(1000 + seed)
+    ntris = int(np.clip(rng.lognormal(np.log(2e5), 1.2), 1e4, 5e6))
+    n = max(int(round(np.sqrt(ntris / 20.0))), 1)
+    P, I = icosphere_soup(n)
+    P = P * rng.uniform(0.7, 1.3, 3)[None].astype(np.float32)
+    y = float(P[:, 1].min()) - 0.01
+    Vg, Ig = _quad((-10, y, -10), (-10, y, 10), (10, y, 10), (10, y, -10))
+    k = int(rng.integers(1, 9))
+    Vl, Il = [], []
+    lights = np.zeros(k, LIGHT)
+    for j in range(k):
+        cx, cz = rng.uniform(-3, 3, 2)
+        cy = rng.uniform(2.0, 4.0)
+        h = rng.uniform(0.1, 0.6)
+        v, i = _quad((cx - h, cy, cz - h), (cx + h, cy, cz - h), (cx + h, cy, cz + h), (cx - h, cy, cz + h))
+        Vl.append(v)
+        Il.append(i + 4 * j)
+        lights[j]["L"] = tuple(rng.uniform(2.0, 10.0, 3))
+        lights[j]["two_sided"] = int(rng.integers(0, 2))
+    nS = len(P)
+    V = np.concatenate([P, Vg, *Vl]).astype(np.float32)
+    I = np.concatenate([I, Ig + nS, *(i + nS + 4 for i in Il)]).astype(np.uint32)
+    mats = np.array([random_disney(rng), matte(tuple(rng.uniform(0.3, 0.9, 3))), matte((0.8, 0.8, 0.8))])
+    nT = len(I)
+    M = np.concatenate([np.zeros(nT - 2 - 2 * k, np.uint32), np.ones(2, np.uint32), np.full(2 * k, 2, np.uint32)])
+    first = nT - 2 * k
+    for j in range(k):
+        lights[j]["first_tri"] = first + 2 * j
+        lights[j]["tri_count"] = 2
+    W = int(rng.integers(256, 1025))
+    H = int(rng.integers(256, 1025))
+    ang = rng.uniform(0, 2 * np.pi)
+    cam = pinhole((3.5 * np.sin(ang), 1.2, 3.5 * np.cos(ang)), (0.0, 0.0, 0.0), (0, 1, 0), 45.0, W, H)
+    return Scene(f"batch_{seed}", V, I.reshape(-1, 3), M, mats, lights, camera=cam, width=W, height=H,
+                 spp=int(rng.integers(4, 65)), max_depth=int(rng.integers(4, 17)))
+
+
 def _grid(p0, du, dv, nu, nv):
     """Quad p0 + [0,1] du + [0,1] dv tessellated into nu x nv cells (2 nu nv triangles);
     normal = cross(du, dv)."""
