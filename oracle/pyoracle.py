@@ -80,7 +80,8 @@ class OrScene(C.Structure):
     _fields_ = [("V", C.c_void_p), ("nV", C.c_uint32), ("N", C.c_void_p), ("I", C.c_void_p),
                 ("nT", C.c_uint32), ("tri_material", C.c_void_p), ("tri_flags", C.c_void_p),
                 ("mats", C.c_void_p), ("nMat", C.c_uint32), ("lights", C.c_void_p),
-                ("nLight", C.c_uint32)]
+                ("nLight", C.c_uint32), ("UV", C.c_void_p), ("nTex", C.c_uint32),
+                ("tex_rgba", C.c_void_p), ("tex_w", C.c_void_p), ("tex_h", C.c_void_p)]
 
 
 RAY_DTYPE = np.dtype([("org", np.float32, 3), ("tmin", np.float32), ("dir", np.float32, 3),
@@ -110,12 +111,20 @@ def make_or_scene(scene):
     tf = None if scene.tri_flags is None else np.ascontiguousarray(scene.tri_flags, np.uint32)
     mats = np.ascontiguousarray(scene.mats).view(DISNEY_DTYPE)
     lights = np.ascontiguousarray(scene.lights).view(LIGHT_DTYPE)
+    UV = getattr(scene, "UV", None)
+    UV = None if UV is None else _f32(UV, (-1, 2))
+    texs = [np.ascontiguousarray(t, np.uint8).reshape(t.shape[0], t.shape[1], 4)
+            for t in (getattr(scene, "textures", None) or [])]
+    tex_ptrs = (C.c_void_p * max(len(texs), 1))(*[t.ctypes.data for t in texs])
+    tw = np.array([t.shape[1] for t in texs] or [0], np.uint32)
+    th = np.array([t.shape[0] for t in texs] or [0], np.uint32)
     s = OrScene(V=V.ctypes.data, nV=len(V), N=None if N is None else N.ctypes.data,
                 I=I.ctypes.data, nT=len(I), tri_material=tm.ctypes.data,
                 tri_flags=None if tf is None else tf.ctypes.data, mats=mats.ctypes.data,
                 nMat=len(mats), lights=lights.ctypes.data if len(lights) else None,
-                nLight=len(lights))
-    return (V, N, I, tm, tf, mats, lights), s
+                nLight=len(lights), UV=None if UV is None else UV.ctypes.data, nTex=len(texs),
+                tex_rgba=C.cast(tex_ptrs, C.c_void_p), tex_w=tw.ctypes.data, tex_h=th.ctypes.data)
+    return (V, N, I, tm, tf, mats, lights, UV, texs, tex_ptrs, tw, th), s
 
 
 def ptr(a):

@@ -953,6 +953,41 @@ void sample_light(const SceneView &sv, Rng &rng, V3<T> &pos, V3<T> &N, T &pdf, u
     lid = idx;
 }
 
+// Texture colour of a hit (PathTracing.cu:262-268): interpolated texture coordinates
+// (BarycentricByIndices, Common.h:40-51) and a bilinear, wrapping, normalised RGBA8 read with the
+// texture unit's documented arithmetic (coordinates u W - 0.5, weights with 8 fractional bits),
+// in FP32 as the GPU's strict mode computes it.
+V3<float> tex_color(const or_scene *s, uint32_t prim, float bu, float bv) {
+    int32_t t = s->mats[s->tri_material[prim]].texture;
+    if (t < 0 || (uint32_t)t >= s->nTex || !s->UV) return V3<float>(1.0f);
+    const float *a = s->UV + 2 * (size_t)s->I[3 * prim], *b = s->UV + 2 * (size_t)s->I[3 * prim + 1],
+                *c = s->UV + 2 * (size_t)s->I[3 * prim + 2];
+    float w0 = 1.0f - bu - bv;
+    float tu = a[0] * w0 + b[0] * bu + c[0] * bv;
+    float tv = a[1] * w0 + b[1] * bu + c[1] * bv;
+    const int W = (int)s->tex_w[t], H = (int)s->tex_h[t];
+    const uint32_t *px = s->tex_rgba[t];
+    float x = (tu - std::floor(tu)) * (float)W - 0.5f;
+    float y = (tv - std::floor(tv)) * (float)H - 0.5f;
+    float fx = std::floor(x), fy = std::floor(y);
+    float al = (float)(int)((x - fx) * 256.0f + 0.5f) * (1.0f / 256.0f);
+    float be = (float)(int)((y - fy) * 256.0f + 0.5f) * (1.0f / 256.0f);
+    int i0 = (int)fx, j0 = (int)fy;
+    i0 = ((i0 % W) + W) % W;
+    j0 = ((j0 % H) + H) % H;
+    int i1 = i0 + 1 == W ? 0 : i0 + 1, j1 = j0 + 1 == H ? 0 : j0 + 1;
+    uint32_t p00 = px[(size_t)j0 * W + i0], p10 = px[(size_t)j0 * W + i1];
+    uint32_t p01 = px[(size_t)j1 * W + i0], p11 = px[(size_t)j1 * W + i1];
+    float w00 = (1.0f - al) * (1.0f - be), w10 = al * (1.0f - be), w01 = (1.0f - al) * be, w11 = al * be;
+    float o[3];
+    for (int k = 0; k < 3; k++) {
+        float c00 = (float)((p00 >> (8 * k)) & 0xffu) / 255.0f, c10 = (float)((p10 >> (8 * k)) & 0xffu) / 255.0f;
+        float c01 = (float)((p01 >> (8 * k)) & 0xffu) / 255.0f, c11 = (float)((p11 >> (8 * k)) & 0xffu) / 255.0f;
+        o[k] = w00 * c00 + w10 * c10 + w01 * c01 + w11 * c11;
+    }
+    return V3<float>(o[0], o[1], o[2]);
+}
+
 template <class T> struct PathOut { V3<T> radiance; uint32_t segments; };
 
 template <class T>
@@ -1037,7 +1072,8 @@ PathOut<T> trace_path(const SceneView &sv, const wl_camera &cam, const wl_render
         ndir = normalize(ndir);
         T pdf = pdf_disney(m, Ns, Ng, -dir, ndir);
         if (pdf < T(0) || std::isnan(pdf)) break;
-        V3<T> tex(T(1));
+        V3<float> tf = tex_color(s, prim, hit.u, hit.v);
+        V3<T> tex(T(tf.x), T(tf.y), T(tf.z));
         throughput = throughput * last_term;
         T cosw = dot(ndir, Ns);
         V3<T> bsdf = clampv(eval_disney(m, Ns, Ng, -dir, ndir, tex), T(0), K(1e30));

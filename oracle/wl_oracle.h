@@ -69,6 +69,10 @@ typedef struct or_scene {
     const uint32_t *tri_flags;
     const wl_disney *mats; uint32_t nMat;
     const wl_area_light *lights; uint32_t nLight;
+    const float *UV;                 /* 2 nV texture coordinates or null */
+    uint32_t nTex;                   /* RGBA8 textures: texel arrays and sizes */
+    const uint32_t *const *tex_rgba;
+    const uint32_t *tex_w, *tex_h;
 } or_scene;
 void *or_bvh_create(const float *V, const uint32_t *I, uint32_t nT);
 void or_bvh_destroy(void *bvh);

@@ -269,3 +269,26 @@ def test_batch_matches_separate_renders(ctx):
             s.close()
     finally:
         ctx.set_tune(None)
+
+
+def test_textured_strict_vs_oracle(ctx, oracle, tmp_path):
+    """A texture (bilinear, wrapping, normalised RGBA8) on two walls: strict mode (software filter
+    with the texture unit's documented arithmetic) equals the oracle bit for bit; fast mode (the
+    texture unit itself) is within the relMSE tolerance of the FP64 oracle; the film's PNG has
+    the film's size."""
+    sc = scenes.textured_cornell_box(48, 40)
+    p = wl.render_params(48, 40, 4, math=wl.MATH_STRICT, max_depth=8)
+    img, _, film, _ = gpu_render(ctx, sc, p)
+    ref, _, _ = oracle.render(sc, ocam(sc), oparams(p))
+    assert np.array_equal(bits(img), bits(ref))
+    plain = scenes.cornell_box(48, 40)
+    ref_plain, _, _ = oracle.render(plain, ocam(plain), oparams(p))
+    assert np.abs(ref - ref_plain).max() > 0.05  # the texture shows
+    film.save_png(tmp_path / "t.png")
+    from wayland_b200.png import read_png
+    assert read_png(tmp_path / "t.png").shape == (40, 48, 4)
+    pf = wl.render_params(48, 40, 64, max_depth=8)
+    _, img64, _, _ = gpu_render(ctx, sc, pf, fp64=True)
+    _, ref64, _ = oracle.render(sc, ocam(sc), oparams(pf), prec=1, want64=True)
+    rel = float(((img64 - ref64) ** 2 / (ref64 ** 2 + 1e-2)).mean())
+    assert rel < FAST_RELMSE_TOL

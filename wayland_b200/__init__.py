@@ -108,13 +108,20 @@ class Scene:
         tf = None if data.tri_flags is None else np.ascontiguousarray(data.tri_flags, np.uint32)
         mats = np.ascontiguousarray(data.mats).view(_abi.DISNEY_DTYPE)
         lights = np.ascontiguousarray(data.lights).view(_abi.LIGHT_DTYPE)
+        UV = getattr(data, "UV", None)
+        UV = None if UV is None else np.ascontiguousarray(UV, np.float32).reshape(-1, 2)
         h = C.c_void_p()
         _abi.check("wl_scene_create", self.lib.wl_scene_create(
-            ctx.handle, _p(V), len(V), _p(N), None, _p(I), len(I), _p(tm), _p(tf), _p(mats),
+            ctx.handle, _p(V), len(V), _p(N), _p(UV), _p(I), len(I), _p(tm), _p(tf), _p(mats),
             len(mats), _p(lights) if len(lights) else None, len(lights), C.byref(h)))
         self.handle = h
         ctx._children.add(self)
         self.num_tris = len(I)
+        for tex in (getattr(data, "textures", None) or []):
+            t = np.ascontiguousarray(tex, np.uint8)
+            idx = C.c_int32()
+            _abi.check("wl_scene_add_texture", self.lib.wl_scene_add_texture(
+                self.handle, _p(t), t.shape[1], t.shape[0], C.byref(idx)))
         if build:
             self.build_bvh(bvh_kind)
 
@@ -202,6 +209,12 @@ class Film:
         out = np.empty((self.height, self.width, 4), np.uint8)
         _abi.check("wl_film_download_ldr", self.lib.wl_film_download_ldr(self.handle, _p(out)))
         return out
+
+    def save_png(self, path):
+        """The tone-mapped film (AceApprox, 8-bit) as a PNG file, flipped vertically like the
+        reference's output (Renderer.cpp:94-105)."""
+        from .png import write_png
+        write_png(path, self.download_ldr())
 
     def device_ptrs(self):
         a, b, c = C.c_void_p(), C.c_void_p(), C.c_void_p()

@@ -95,6 +95,10 @@ struct wl_scene {
     DevLight *d_lights = nullptr;
     std::vector<cudaArray_t> tex_arrays;
     std::vector<cudaTextureObject_t> tex_objs;
+    std::vector<uint32_t *> tex_lin;
+    std::vector<uint2> tex_dims;
+    uint32_t **d_tex_lin = nullptr;
+    uint2 *d_tex_size = nullptr;
     cudaTextureObject_t *d_tex = nullptr;
     BvhBuild bvh{};
     bool built = false;
@@ -134,6 +138,8 @@ DevScene dev_scene(const wl_scene *s) {
     d.has_bvh = (s->built && s->nT > 0) ? 1u : 0u;
     d.tex = s->d_tex;
     d.nTex = (uint32_t)s->tex_objs.size();
+    d.tex_rgba = s->d_tex_lin;
+    d.tex_size = s->d_tex_size;
     return d;
 }
 
@@ -434,6 +440,9 @@ int wl_scene_destroy(wl_scene *s) {
         if (p) cudaFree(p);
     for (auto t : s->tex_objs) cudaDestroyTextureObject(t);
     for (auto a : s->tex_arrays) cudaFreeArray(a);
+    for (auto p : s->tex_lin) cudaFree(p);
+    if (s->d_tex_lin) cudaFree(s->d_tex_lin);
+    if (s->d_tex_size) cudaFree(s->d_tex_size);
     bvh_free(s->bvh);
     delete s;
     return WL_OK;
@@ -470,6 +479,20 @@ int wl_scene_add_texture(wl_scene *s, const uint8_t *rgba8, uint32_t w, uint32_t
     CK(cudaMalloc(&s->d_tex, sizeof(cudaTextureObject_t) * s->tex_objs.size()));
     CK(cudaMemcpy(s->d_tex, s->tex_objs.data(), sizeof(cudaTextureObject_t) * s->tex_objs.size(),
                   cudaMemcpyHostToDevice));
+    // linear copy for the strict-mode filter
+    uint32_t *lin = nullptr;
+    CK(cudaMalloc(&lin, (size_t)w * h * 4));
+    s->tex_lin.push_back(lin);
+    s->tex_dims.push_back(make_uint2(w, h));
+    CK(cudaMemcpy(lin, rgba8, (size_t)w * h * 4, cudaMemcpyHostToDevice));
+    if (s->d_tex_lin) cudaFree(s->d_tex_lin);
+    if (s->d_tex_size) cudaFree(s->d_tex_size);
+    s->d_tex_lin = nullptr;
+    s->d_tex_size = nullptr;
+    CK(cudaMalloc(&s->d_tex_lin, sizeof(uint32_t *) * s->tex_lin.size()));
+    CK(cudaMalloc(&s->d_tex_size, sizeof(uint2) * s->tex_dims.size()));
+    CK(cudaMemcpy(s->d_tex_lin, s->tex_lin.data(), sizeof(uint32_t *) * s->tex_lin.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s->d_tex_size, s->tex_dims.data(), sizeof(uint2) * s->tex_dims.size(), cudaMemcpyHostToDevice));
     *index = (int32_t)s->tex_objs.size() - 1;
     return WL_OK;
 }

@@ -76,6 +76,48 @@ __device__ __forceinline__ float tri_area(const DevScene &sc, uint32_t t) {
     return 0.5f * length(cross(b - a, c - a));
 }
 
+// Texture colour of a hit (PathTracing.cu:262-268): the material's texture at the interpolated
+// texture coordinates (BarycentricByIndices, Common.h:40-51), RGB of a bilinear, wrapping,
+// normalised read. WL_MATH_FAST reads through the texture unit, as the reference does. Strict
+// mode filters in software with the texture unit's documented arithmetic (coordinates
+// u W - 0.5, weights with 8 fractional bits), so that it matches the CPU oracle bit for bit.
+__device__ __forceinline__ v3 tex_color(const DevScene &sc, uint32_t mid, uint4 ti, float bu,
+                                        float bv) {
+    int32_t t = sc.mats[mid].texture;
+    if (t < 0 || (uint32_t)t >= sc.nTex || !sc.UV) return v3(1.0f);
+    const float2 *UV = reinterpret_cast<const float2 *>(sc.UV);
+    float2 a = UV[ti.x], b = UV[ti.y], c = UV[ti.z];
+    float w0 = 1.0f - bu - bv;
+    float tu = a.x * w0 + b.x * bu + c.x * bv;
+    float tv = a.y * w0 + b.y * bu + c.y * bv;
+#ifdef WL_STRICT_MATH
+    const uint2 dim = sc.tex_size[t];
+    const uint32_t *px = sc.tex_rgba[t];
+    float x = (tu - floorf(tu)) * (float)dim.x - 0.5f;
+    float y = (tv - floorf(tv)) * (float)dim.y - 0.5f;
+    float fx = floorf(x), fy = floorf(y);
+    float al = (float)(int)((x - fx) * 256.0f + 0.5f) * (1.0f / 256.0f);
+    float be = (float)(int)((y - fy) * 256.0f + 0.5f) * (1.0f / 256.0f);
+    int i0 = (int)fx, j0 = (int)fy;
+    i0 = ((i0 % (int)dim.x) + (int)dim.x) % (int)dim.x;
+    j0 = ((j0 % (int)dim.y) + (int)dim.y) % (int)dim.y;
+    int i1 = i0 + 1 == (int)dim.x ? 0 : i0 + 1, j1 = j0 + 1 == (int)dim.y ? 0 : j0 + 1;
+    uint32_t p00 = px[(size_t)j0 * dim.x + i0], p10 = px[(size_t)j0 * dim.x + i1];
+    uint32_t p01 = px[(size_t)j1 * dim.x + i0], p11 = px[(size_t)j1 * dim.x + i1];
+    float w00 = (1.0f - al) * (1.0f - be), w10 = al * (1.0f - be), w01 = (1.0f - al) * be, w11 = al * be;
+    float o[3];
+    for (int k = 0; k < 3; k++) {
+        float c00 = (float)((p00 >> (8 * k)) & 0xffu) / 255.0f, c10 = (float)((p10 >> (8 * k)) & 0xffu) / 255.0f;
+        float c01 = (float)((p01 >> (8 * k)) & 0xffu) / 255.0f, c11 = (float)((p11 >> (8 * k)) & 0xffu) / 255.0f;
+        o[k] = w00 * c00 + w10 * c10 + w01 * c01 + w11 * c11;
+    }
+    return v3(o[0], o[1], o[2]);
+#else
+    float4 r = tex2D<float4>(sc.tex[t], tu, tv);
+    return v3(r.x, r.y, r.z);
+#endif
+}
+
 // What one lane of the shade pass emits: the next ray and the shadow ray with its light sample.
 struct ShadeOut {
     bool push_ray = false, push_shadow = false;
@@ -192,7 +234,7 @@ __device__ __forceinline__ void shade_lane(const WaveParams &wp, const DevScene 
                     } else if (pdf < 0.0f || isnan(pdf)) {
                         alive = false;
                     } else {
-                        v3 tex(1.0f);
+                        v3 tex = tex_color(sc, ti.w & 0x7fffffffu, ti, h.z, h.w);
                         thr = thr * term;
                         float cosw = dot(ndir, Ns);
                         v3 bsdf = clampv(eval_disney(m, Ns, Ng, V, ndir, tex), 0.f, 1e30f);

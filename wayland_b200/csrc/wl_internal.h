@@ -41,6 +41,9 @@ struct DevScene {
     uint32_t nEmit;
     const cudaTextureObject_t *tex;
     uint32_t nTex;
+    // the same textures as RGBA8 texels in linear memory (the strict-mode software filter)
+    const uint32_t *const *tex_rgba;
+    const uint2 *tex_size;
 };
 
 // Path-state arrays of one wave (structure of arrays in HBM, indexed by path slot).

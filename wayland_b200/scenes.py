@@ -47,6 +47,8 @@ class Scene:
     spp: int = 16
     max_depth: int = 8
     env: tuple = (0.0, 0.0, 0.0)
+    UV: np.ndarray = None              # (nV, 2) float32 texture coordinates or None
+    textures: list = field(default_factory=list)  # RGBA8 images (h, w, 4) uint8; mats' texture indexes them
 
     @property
     def num_tris(self):
@@ -160,6 +162,43 @@ def cornell_box(width=256, height=256, spp=16, max_depth=8):
     cam = pinhole((0.5, 0.5, 2.4), (0.5, 0.5, 0.0), (0, 1, 0), 39.3, width, height)
     return Scene("cornell_box", V, I, M, mats, lights, camera=cam, width=width, height=height,
                  spp=spp, max_depth=max_depth)
+
+
+def checker_texture(n=32, seed=0):
+    """An n x n RGBA8 test image: a two-colour checkerboard of 4 x 4 texel squares with seeded
+    per-texel noise (so that bilinear filtering has something to interpolate)."""
+    rng = np.random.default_rng(seed)
+    y, x = np.mgrid[0:n, 0:n]
+    board = ((x // 4 + y // 4) % 2).astype(np.float64)
+    a = np.array([0.85, 0.8, 0.7]) * 255
+    b = np.array([0.2, 0.35, 0.6]) * 255
+    img = board[..., None] * a + (1 - board[..., None]) * b + rng.uniform(-20, 20, (n, n, 3))
+    out = np.empty((n, n, 4), np.uint8)
+    out[..., :3] = np.clip(img, 0, 255).astype(np.uint8)
+    out[..., 3] = 255
+    return out
+
+
+def textured_cornell_box(width=256, height=256, spp=16, max_depth=8):
+    """The Cornell box with a checker texture (material 3, texture 0) tiled 4 x 4 on the floor and
+    3 x 3 on the back wall, through per-vertex texture coordinates (the reference's ImageMap Kd
+    path, PathTracing.cu:262-268)."""
+    sc = cornell_box(width, height, spp, max_depth)
+    nV = len(sc.V)
+    UV = np.zeros((nV, 2), np.float32)
+    # floor = vertices 0..3 (triangles 0, 1); back wall = vertices 8..11 (triangles 4, 5)
+    UV[0:4] = np.array([[0, 0], [4, 0], [4, 4], [0, 4]], np.float32)
+    UV[8:12] = np.array([[0, 0], [0, 3], [3, 3], [3, 0]], np.float32) + 0.37
+    tex_mat = matte((0.9, 0.9, 0.9))
+    tex_mat["texture"] = 0
+    sc.mats = np.concatenate([sc.mats, np.array([tex_mat])])
+    tm = sc.tri_material.copy()
+    tm[[0, 1, 4, 5]] = len(sc.mats) - 1
+    sc.tri_material = tm
+    sc.UV = UV
+    sc.textures = [checker_texture(32)]
+    sc.name = "cornell_box_textured"
+    return sc
 
 
 # ---- config 2 ------------------------------------------------------------------------------
