@@ -292,3 +292,16 @@ def test_textured_strict_vs_oracle(ctx, oracle, tmp_path):
     _, ref64, _ = oracle.render(sc, ocam(sc), oparams(pf), prec=1, want64=True)
     rel = float(((img64 - ref64) ** 2 / (ref64 ** 2 + 1e-2)).mean())
     assert rel < FAST_RELMSE_TOL
+
+
+def test_pbrt_scene_strict_vs_oracle(ctx, oracle, tmp_path):
+    """A scene read from a pbrt-v3 file (trianglemesh, binary PLY, matte/plastic/disney/glass,
+    texture, area light) renders bit-exactly like the oracle in strict mode."""
+    from wayland_b200 import pbrt
+    from pbrt_fixture import write_scene
+    sc = pbrt.load(str(write_scene(tmp_path)))
+    p = wl.render_params(sc.width, sc.height, sc.spp, math=wl.MATH_STRICT, max_depth=sc.max_depth)
+    img, _, _, _ = gpu_render(ctx, sc, p)
+    ref, _, _ = oracle.render(sc, ocam(sc), oparams(p))
+    assert img.max() > 0
+    assert np.array_equal(bits(img), bits(ref))

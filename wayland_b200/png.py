@@ -29,48 +29,78 @@ def write_png(path, rgba, flip=True):
         f.write(data)
 
 
-def read_png(path):
-    """Reads an 8-bit RGBA non-interlaced PNG as written by write_png (filter types 0-4)."""
+def _unfilter(raw, h, w, bpp):
+    stride = bpp * w
+    out = np.zeros((h, stride), np.uint8)
+    prev = np.zeros(stride, np.int32)
+    for y in range(h):
+        base = y * (stride + 1)
+        ft = raw[base]
+        line = np.frombuffer(raw, np.uint8, stride, base + 1).astype(np.int32)
+        if ft == 0:
+            cur = line
+        elif ft == 1:  # Sub: running sum per channel
+            cur = np.cumsum(line.reshape(w, bpp), axis=0).reshape(-1) & 0xFF
+        elif ft == 2:  # Up
+            cur = (line + prev) & 0xFF
+        else:
+            cur = np.zeros(stride, np.int32)
+            left = np.zeros(bpp, np.int32)
+            upleft = np.zeros(bpp, np.int32)
+            for x in range(w):
+                sl = slice(x * bpp, (x + 1) * bpp)
+                up = prev[sl]
+                if ft == 3:  # Average
+                    pred = (left + up) // 2
+                else:  # Paeth
+                    pa, pb, pc = np.abs(up - upleft), np.abs(left - upleft), np.abs(left + up - 2 * upleft)
+                    pred = np.where((pa <= pb) & (pa <= pc), left, np.where(pb <= pc, up, upleft))
+                v = (line[sl] + pred) & 0xFF
+                cur[sl] = v
+                left = v
+                upleft = up
+        out[y] = cur
+        prev = cur.astype(np.int32)
+    return out
+
+
+def read_png_any(path):
+    """An 8-bit RGB, RGBA or palette non-interlaced PNG as (h, w, 4) uint8 (alpha 255 where the
+    file has none), first row = the top of the image (as stbi_load returns it)."""
     with open(path, "rb") as f:
         data = f.read()
     if data[:8] != b"\x89PNG\r\n\x1a\n":
-        raise ValueError("not a PNG file")
-    pos, idat, w = 8, b"", 0
+        raise ValueError(f"not a PNG file: {path}")
+    pos, idat, w, h, ctype = 8, b"", 0, 0, 6
+    palette, trns = None, None
     while pos < len(data):
         n, = struct.unpack(">I", data[pos:pos + 4])
         kind = data[pos + 4:pos + 8]
         body = data[pos + 8:pos + 8 + n]
         if kind == b"IHDR":
             w, h, depth, ctype, _, _, interlace = struct.unpack(">IIBBBBB", body)
-            if depth != 8 or ctype != 6 or interlace != 0:
-                raise ValueError("only 8-bit RGBA non-interlaced PNG")
+            if depth != 8 or ctype not in (2, 3, 6) or interlace != 0:
+                raise ValueError("only 8-bit RGB, RGBA or palette non-interlaced PNG files")
+        elif kind == b"PLTE":
+            palette = np.frombuffer(body, np.uint8).reshape(-1, 3)
+        elif kind == b"tRNS":
+            trns = np.frombuffer(body, np.uint8)
         elif kind == b"IDAT":
             idat += body
         pos += 12 + n
-    raw = zlib.decompress(idat)
-    stride = 4 * w
-    out = np.zeros((h, stride), np.uint8)
-    prev = np.zeros(stride, np.int32)
-    for y in range(h):
-        ft = raw[y * (stride + 1)]
-        line = np.frombuffer(raw, np.uint8, stride, y * (stride + 1) + 1).astype(np.int32)
-        cur = np.zeros(stride, np.int32)
-        for x in range(stride):
-            a = cur[x - 4] if x >= 4 else 0
-            b = prev[x]
-            c = prev[x - 4] if x >= 4 else 0
-            if ft == 0:
-                p = 0
-            elif ft == 1:
-                p = a
-            elif ft == 2:
-                p = b
-            elif ft == 3:
-                p = (a + b) // 2
-            else:
-                pa, pb, pc = abs(b - c), abs(a - c), abs(a + b - 2 * c)
-                p = a if (pa <= pb and pa <= pc) else (b if pb <= pc else c)
-            cur[x] = (line[x] + p) & 0xFF
-        out[y] = cur
-        prev = cur
-    return out.reshape(h, w, 4)
+    bpp = {6: 4, 2: 3, 3: 1}[ctype]
+    img = _unfilter(zlib.decompress(idat), h, w, bpp).reshape(h, w, bpp)
+    if ctype == 3:
+        rgba = np.full((len(palette), 4), 255, np.uint8)
+        rgba[:, :3] = palette
+        if trns is not None:
+            rgba[:len(trns), 3] = trns
+        return rgba[img[..., 0]]
+    if bpp == 3:
+        img = np.concatenate([img, np.full((h, w, 1), 255, np.uint8)], 2)
+    return img
+
+
+def read_png(path):
+    """Reads an 8-bit RGBA (or RGB) non-interlaced PNG as written by write_png."""
+    return read_png_any(path)
