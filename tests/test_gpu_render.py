@@ -305,3 +305,31 @@ def test_pbrt_scene_strict_vs_oracle(ctx, oracle, tmp_path):
     ref, _, _ = oracle.render(sc, ocam(sc), oparams(p))
     assert img.max() > 0
     assert np.array_equal(bits(img), bits(ref))
+
+
+def test_distributed_film_reduction_one_rank(ctx):
+    """render_distributed over an NCCL group of one rank: the film's FP64 sums are all-reduced on
+    the device (through the CUDA array interface) and equal the single render's FP64 mean."""
+    import socket
+    import torch
+    import torch.distributed as dist
+    from wayland_b200 import multi
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1)
+    try:
+        sc = scenes.cornell_box(40, 30)
+        s = wl.Scene(ctx, sc)
+        p = wl.render_params(40, 30, 6, max_depth=8)
+        film = wl.Film(ctx, 40, 30, fp64=True)
+        img, n = multi.render_distributed(wl, ctx, s, sc.camera_struct(), p, film, 0, 1)
+        assert n == 6
+        ref = wl.Film(ctx, 40, 30, fp64=True)
+        wl.render(ctx, s, sc.camera_struct(), p, ref)
+        assert np.allclose(img.cpu().numpy(), ref.download64(), rtol=1e-12, atol=1e-14)
+        film.close()
+        ref.close()
+        s.close()
+    finally:
+        dist.destroy_process_group()
