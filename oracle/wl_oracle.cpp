@@ -903,7 +903,65 @@ struct SceneView {
     const or_scene *s;
     std::vector<uint32_t> tri_light;
     const OBvh *bvh;
+    // WL_LIGHTS_POWER: emissive triangles in light order, their FP64 CDF and each light's area
+    // pdf lum(L) / total (float and double)
+    std::vector<uint32_t> emit_tri;
+    std::vector<double> emit_cdf;
+    std::vector<float> pdf_power;
+    std::vector<double> pdf_power64;
 };
+
+// The emitter CDF in the device's order (pt_strict.cu, k_emit_*): weights area * luminance(L),
+// chunks of 256 summed sequentially, chunk sums sequentially, cdf = (local + offset) / total.
+void build_emit_cdf(SceneView &sv) {
+    const or_scene *s = sv.s;
+    std::vector<uint32_t> emit_light;
+    for (uint32_t l = 0; l < s->nLight; l++)
+        for (uint32_t t = 0; t < s->lights[l].tri_count; t++) {
+            sv.emit_tri.push_back(s->lights[l].first_tri + t);
+            emit_light.push_back(l);
+        }
+    const size_t n = sv.emit_tri.size();
+    auto lum = [&](uint32_t l) {
+        const float *L = s->lights[l].L;
+        return 0.2126 * (double)L[0] + 0.7152 * (double)L[1] + 0.0722 * (double)L[2];
+    };
+    sv.emit_cdf.assign(n, 0.0);
+    const size_t CH = 256, chunks = (n + CH - 1) / CH;
+    std::vector<double> chunk(chunks + 1, 0.0);
+    for (size_t c = 0; c < chunks; c++) {
+        double acc = 0.0;
+        for (size_t i = c * CH; i < std::min(n, (c + 1) * CH); i++) {
+            const uint32_t *t = s->I + 3 * (size_t)sv.emit_tri[i];
+            const float *a = s->V + 3 * (size_t)t[0], *b = s->V + 3 * (size_t)t[1], *cc = s->V + 3 * (size_t)t[2];
+            double ax = a[0], ay = a[1], az = a[2];
+            double e1x = b[0] - ax, e1y = b[1] - ay, e1z = b[2] - az;
+            double e2x = cc[0] - ax, e2y = cc[1] - ay, e2z = cc[2] - az;
+            double cx = e1y * e2z - e1z * e2y, cy = e1z * e2x - e1x * e2z, cz = e1x * e2y - e1y * e2x;
+            double area = 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
+            acc = acc + area * lum(emit_light[i]);
+            sv.emit_cdf[i] = acc;
+        }
+        chunk[c] = acc;
+    }
+    double off = 0.0;
+    for (size_t c = 0; c < chunks; c++) {
+        double v = chunk[c];
+        chunk[c] = off;
+        off = off + v;
+    }
+    for (size_t i = 0; i < n; i++) sv.emit_cdf[i] = off > 0.0 ? (sv.emit_cdf[i] + chunk[i / CH]) / off : 0.0;
+    sv.pdf_power.assign(s->nLight, 0.0f);
+    sv.pdf_power64.assign(s->nLight, 0.0);
+    for (uint32_t l = 0; l < s->nLight; l++) {
+        sv.pdf_power64[l] = off > 0.0 ? lum(l) / off : 0.0;
+        sv.pdf_power[l] = (float)sv.pdf_power64[l];
+    }
+}
+
+template <class T> T power_pdf(const SceneView &sv, uint32_t l);
+template <> float power_pdf<float>(const SceneView &sv, uint32_t l) { return sv.pdf_power[l]; }
+template <> double power_pdf<double>(const SceneView &sv, uint32_t l) { return sv.pdf_power64[l]; }
 
 template <class T> V3<T> vload(const float *p, uint32_t i) {
     return V3<T>(p[3 * (size_t)i], p[3 * (size_t)i + 1], p[3 * (size_t)i + 2]);
@@ -924,23 +982,41 @@ T tri_area(const or_scene *s, uint32_t t) {  // GetTriangleArea, Common.h:59-62
 // The light-normal interpolation keeps the reference's weights: Barycentric(n0, n1, n2, coord)
 // with coord = (1-u-v, u, v) reads coord.x and coord.y (Common.h:40-51).
 template <class T>
-void sample_light(const SceneView &sv, Rng &rng, V3<T> &pos, V3<T> &N, T &pdf, uint32_t &lid) {
+void sample_light(const SceneView &sv, Rng &rng, V3<T> &pos, V3<T> &N, T &pdf, uint32_t &lid,
+                  bool power = false) {
     const or_scene *s = sv.s;
-    uint32_t idx = (uint32_t)((float)s->nLight * rng.next());
-    if (idx >= s->nLight) idx = s->nLight - 1;
+    uint32_t idx, t;
+    T p;
+    if (power) {
+        // an emissive triangle from the FP64 CDF (first entry above the random number)
+        const double target = (double)rng.next();
+        size_t lo = 0, hi = sv.emit_cdf.size() - 1;
+        while (lo < hi) {
+            size_t mid = (lo + hi) >> 1;
+            if (sv.emit_cdf[mid] > target) hi = mid;
+            else lo = mid + 1;
+        }
+        t = sv.emit_tri[lo];
+        idx = sv.tri_light[t];
+        p = power_pdf<T>(sv, idx);
+    } else {
+        idx = (uint32_t)((float)s->nLight * rng.next());
+        if (idx >= s->nLight) idx = s->nLight - 1;
+        const wl_area_light &lt0 = s->lights[idx];
+        p = T(1) / T(s->nLight);
+        uint32_t tri = (uint32_t)(rng.next() * (float)lt0.tri_count);
+        if (tri >= lt0.tri_count) tri = lt0.tri_count - 1;
+        p = p / T(lt0.tri_count);
+        t = lt0.first_tri + tri;
+    }
     const wl_area_light &lt = s->lights[idx];
-    T p = T(1) / T(s->nLight);
-    uint32_t tri = (uint32_t)(rng.next() * (float)lt.tri_count);
-    if (tri >= lt.tri_count) tri = lt.tri_count - 1;
-    p = p / T(lt.tri_count);
-    uint32_t t = lt.first_tri + tri;
     V3<T> v0 = vload<T>(s->V, s->I[3 * t]), v1 = vload<T>(s->V, s->I[3 * t + 1]),
           v2 = vload<T>(s->V, s->I[3 * t + 2]);
     T u = rng.next(), v = rng.next();
     if (u + v > T(1)) { u = T(1) - u; v = T(1) - v; }
     V3<T> coord(T(1) - u - v, u, v);
     pos = v0 + u * (v1 - v0) + v * (v2 - v0);
-    p = p / tri_area<T>(s, t);
+    if (!power) p = p / tri_area<T>(s, t);
     if (tri_has_normal(s, lt.first_tri)) {
         V3<T> n0 = vload<T>(s->N, s->I[3 * t]), n1 = vload<T>(s->N, s->I[3 * t + 1]),
               n2 = vload<T>(s->N, s->I[3 * t + 2]);
@@ -1049,10 +1125,15 @@ PathOut<T> trace_path(const SceneView &sv, const wl_camera &cam, const wl_render
             if (depth == 1 || (P.strategy != WL_STRATEGY_NEE && (lt.two_sided || dot(Ns, dir) < T(0)))) {
                 T nee_pdf = T(0);
                 if (P.strategy != WL_STRATEGY_UPT && depth > 1) {
-                    // PdfAreaLightPos, Pdf.h:28-39
-                    T lp = T(1) / T(s->nLight);
-                    lp /= T(lt.tri_count);
-                    lp /= tri_area<T>(s, prim);
+                    // PdfAreaLightPos, Pdf.h:28-39 (or the power CDF's area pdf)
+                    T lp;
+                    if (P.lights == WL_LIGHTS_POWER) {
+                        lp = power_pdf<T>(sv, lid);
+                    } else {
+                        lp = T(1) / T(s->nLight);
+                        lp /= T(lt.tri_count);
+                        lp /= tri_area<T>(s, prim);
+                    }
                     nee_pdf = lp * tt * tt / std::fabs(dot(Ns, dir));
                 }
                 T upt_pdf = last_pdf;
@@ -1089,7 +1170,7 @@ PathOut<T> trace_path(const SceneView &sv, const wl_camera &cam, const wl_render
         // next-event estimation (PathTracing.cu:81-129)
         if (P.strategy != WL_STRATEGY_UPT && s->nLight > 0) {
             V3<T> lpos, lN; T lpdf; uint32_t li;
-            sample_light(sv, rng, lpos, lN, lpdf, li);
+            sample_light(sv, rng, lpos, lN, lpdf, li, P.lights == WL_LIGHTS_POWER);
             V3<T> vis = lpos - pos;
             T dist = length(vis);
             vis = vis / dist;
@@ -1642,6 +1723,7 @@ uint64_t or_render(const or_scene *scene, void *bvh, const wl_camera *cam,
     for (uint32_t l = 0; l < scene->nLight; l++)
         for (uint32_t t = 0; t < scene->lights[l].tri_count; t++)
             sv.tri_light[scene->lights[l].first_tri + t] = l;
+    build_emit_cdf(sv);
     uint32_t npix = p->width * p->height;
     if (pixel_end > npix) pixel_end = npix;
     uint64_t segs = 0;

@@ -95,6 +95,9 @@ struct wl_scene {
     DevLight *d_lights = nullptr;
     std::vector<cudaArray_t> tex_arrays;
     std::vector<cudaTextureObject_t> tex_objs;
+    uint32_t nEmit = 0;
+    uint32_t *d_emit_tri = nullptr, *d_emit_light = nullptr;
+    double *d_emit_cdf = nullptr, *d_emit_chunk = nullptr;
     std::vector<uint32_t *> tex_lin;
     std::vector<uint2> tex_dims;
     uint32_t **d_tex_lin = nullptr;
@@ -140,6 +143,9 @@ DevScene dev_scene(const wl_scene *s) {
     d.nTex = (uint32_t)s->tex_objs.size();
     d.tex_rgba = s->d_tex_lin;
     d.tex_size = s->d_tex_size;
+    d.emit_cdf = s->d_emit_cdf;
+    d.emit_tri = s->d_emit_tri;
+    d.nEmit = s->nEmit;
     return d;
 }
 
@@ -402,8 +408,16 @@ int wl_scene_create(wl_context *c, const float *V, uint32_t nV, const float *N, 
         dl[l].first_tri = lights[l].first_tri;
         dl[l].tri_count = lights[l].tri_count;
         dl[l].has_normal = (N && (!tri_flags || (tri_flags[lights[l].first_tri] & 1u))) ? 1u : 0u;
-        dl[l].pad = 0;
+        dl[l].pdf_power = 0.0f;
     }
+    // emissive triangles in light order, for the WL_LIGHTS_POWER CDF
+    std::vector<uint32_t> emit_tri, emit_light;
+    for (uint32_t l = 0; l < nLight; l++)
+        for (uint32_t t = 0; t < lights[l].tri_count; t++) {
+            emit_tri.push_back(lights[l].first_tri + t);
+            emit_light.push_back(l);
+        }
+    s->nEmit = (uint32_t)emit_tri.size();
     auto up = [&](void **dst, const void *src, size_t bytes) -> cudaError_t {
         if (!bytes) return cudaSuccess;
         cudaError_t e = cudaMalloc(dst, bytes);
@@ -419,6 +433,15 @@ int wl_scene_create(wl_context *c, const float *V, uint32_t nV, const float *N, 
     if (e == cudaSuccess) e = up((void **)&s->d_tri_light, tri_light.data(), sizeof(uint32_t) * (size_t)nT);
     if (e == cudaSuccess) e = up((void **)&s->d_mats, mats, sizeof(wl_disney) * (size_t)nMat);
     if (e == cudaSuccess) e = up((void **)&s->d_lights, dl.data(), sizeof(DevLight) * (size_t)nLight);
+    if (e == cudaSuccess) e = up((void **)&s->d_emit_tri, emit_tri.data(), sizeof(uint32_t) * emit_tri.size());
+    if (e == cudaSuccess) e = up((void **)&s->d_emit_light, emit_light.data(), sizeof(uint32_t) * emit_light.size());
+    if (e == cudaSuccess && s->nEmit) e = cudaMalloc(&s->d_emit_cdf, sizeof(double) * s->nEmit);
+    if (e == cudaSuccess && s->nEmit) e = cudaMalloc(&s->d_emit_chunk, sizeof(double) * (s->nEmit / 256 + 2));
+    if (e == cudaSuccess && s->nEmit) {
+        strict::launch_emit_cdf(s->d_V, s->d_tri, s->d_emit_tri, s->d_emit_light, s->nEmit, s->d_lights,
+                                nLight, s->d_emit_cdf, s->d_emit_chunk, c->stream);
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) {
         c->live_children++;
@@ -435,7 +458,8 @@ int wl_scene_destroy(wl_scene *s) {
     s->ctx->live_children--;
     cudaSetDevice(s->ctx->device);
     cudaStreamSynchronize(s->ctx->stream);
-    void *ps[] = {s->d_V, s->d_N, s->d_UV, s->d_I, s->d_tri, s->d_tri_light, s->d_mats, s->d_lights, s->d_tex};
+    void *ps[] = {s->d_V, s->d_N, s->d_UV, s->d_I, s->d_tri, s->d_tri_light, s->d_mats, s->d_lights, s->d_tex,
+                  s->d_emit_tri, s->d_emit_light, s->d_emit_cdf, s->d_emit_chunk};
     for (void *p : ps)
         if (p) cudaFree(p);
     for (auto t : s->tex_objs) cudaDestroyTextureObject(t);
@@ -897,7 +921,9 @@ int wl_render(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_
         "bidirectional subpaths hold at most WL_BDPT_MAX_VERTICES vertices (max_depth)");
     ARG(p->rng <= WL_RNG_PCG32, "bad rng");
     ARG(p->math <= WL_MATH_STRICT, "bad math mode");
-    ARG(p->lights == WL_LIGHTS_UNIFORM, "only uniform light selection is available");
+    ARG(p->lights <= WL_LIGHTS_POWER, "bad light selection");
+    ARG(p->strategy != WL_STRATEGY_BDPT || p->lights == WL_LIGHTS_UNIFORM,
+        "the bidirectional program samples lights uniformly (BDPT.cu:341-366)");
     ARG(p->rr_prob > 0.0f && p->rr_prob <= 1.0f, "rr_prob must be in (0, 1]");
     ARG(finite3(cam->pos) && finite3(cam->look_at) && finite3(cam->up) && finite3(cam->right), "non-finite camera");
     CK(cudaSetDevice(c->device));
@@ -1023,7 +1049,7 @@ int wl_render_batch(wl_context *c, uint32_t n, wl_scene *const *scenes, const wl
         ARG(p->strategy <= WL_STRATEGY_MIS, "batched renders run the path tracer (UPT, NEE or MIS)");
         ARG(p->rng <= WL_RNG_PCG32, "bad rng");
         ARG(p->math == math && math <= WL_MATH_STRICT, "one math mode for all jobs");
-        ARG(p->lights == WL_LIGHTS_UNIFORM, "only uniform light selection is available");
+        ARG(p->lights <= WL_LIGHTS_POWER, "bad light selection");
         ARG(p->rr_prob > 0.0f && p->rr_prob <= 1.0f, "rr_prob must be in (0, 1]");
         ARG(finite3(cam->pos) && finite3(cam->look_at) && finite3(cam->up) && finite3(cam->right), "non-finite camera");
         for (uint32_t k = 0; k < j; k++) ARG(films[k] != f, "each job needs its own film");
@@ -1358,7 +1384,7 @@ int wl_render_nrc(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_ren
     ARG(!f || (p->width == f->f.W && p->height == f->f.H), "film size differs from the render size");
     ARG(p->spp > 0 && p->max_depth > 0 && p->max_depth <= 1024, "bad spp or max_depth");
     ARG(p->strategy <= WL_STRATEGY_MIS && p->rng <= WL_RNG_PCG32 && p->math <= WL_MATH_STRICT, "bad params");
-    ARG(p->lights == WL_LIGHTS_UNIFORM, "only uniform light selection is available");
+    ARG(p->lights <= WL_LIGHTS_POWER, "bad light selection");
     ARG(finite3(cam->pos) && finite3(cam->look_at) && finite3(cam->up) && finite3(cam->right), "non-finite camera");
     CK(cudaSetDevice(c->device));
     c->stats_pending = false;
@@ -1570,7 +1596,7 @@ int noalloc_render_inputs(wl_context *c, wl_scene *s, const wl_camera *cam,
     ARG(p->strategy <= WL_STRATEGY_MIS, "bad strategy");
     ARG(p->rng <= WL_RNG_PCG32, "bad rng");
     ARG(p->math <= WL_MATH_STRICT, "bad math mode");
-    ARG(p->lights == WL_LIGHTS_UNIFORM, "only uniform light selection is available");
+    ARG(p->lights <= WL_LIGHTS_POWER, "bad light selection");
     ARG(p->rr_prob > 0.0f && p->rr_prob <= 1.0f, "rr_prob must be in (0, 1]");
     ARG(finite3(cam->pos) && finite3(cam->look_at) && finite3(cam->up) && finite3(cam->right),
         "non-finite camera");

@@ -181,10 +181,15 @@ __device__ __forceinline__ void shade_lane(const WaveParams &wp, const DevScene 
                                        (lt.two_sided || dot(Ns, dir) < 0.0f))) {
                         float nee_pdf = 0.0f;
                         if (wp.strategy != WL_STRATEGY_UPT && depth > 1) {
-                            // PdfAreaLightPos, Pdf.h:28-39
-                            float lp = 1.0f / (float)sc.nLight;
-                            lp /= (float)lt.tri_count;
-                            lp /= tri_area(sc, prim);
+                            // PdfAreaLightPos, Pdf.h:28-39 (or the power CDF's area pdf)
+                            float lp;
+                            if (wp.lights == WL_LIGHTS_POWER) {
+                                lp = lt.pdf_power;
+                            } else {
+                                lp = 1.0f / (float)sc.nLight;
+                                lp /= (float)lt.tri_count;
+                                lp /= tri_area(sc, prim);
+                            }
                             nee_pdf = lp * t * t / fabsf(dot(Ns, dir));
                         }
                         rad = rad + thr * ld3(lt.L) * term * (last_pdf / (last_pdf + nee_pdf));
@@ -242,22 +247,38 @@ __device__ __forceinline__ void shade_lane(const WaveParams &wp, const DevScene 
                         last_pdf = pdf;
                         // next-event estimation (PathTracing.cu:81-129) at this vertex
                         if (wp.strategy != WL_STRATEGY_UPT && sc.nLight > 0) {
-                            // SampleAreaLightPos, Sample.h:105-132
-                            uint32_t li = (uint32_t)((float)sc.nLight * rng.next());
-                            if (li >= sc.nLight) li = sc.nLight - 1;
+                            // SampleAreaLightPos, Sample.h:105-132; or, with WL_LIGHTS_POWER, an
+                            // emissive triangle from the FP64 CDF (one random number)
+                            uint32_t li, lt_tri;
+                            float lp;
+                            if (wp.lights == WL_LIGHTS_POWER) {
+                                const double target = (double)rng.next();
+                                uint32_t lo = 0, hi = sc.nEmit - 1;
+                                while (lo < hi) {
+                                    uint32_t mid = (lo + hi) >> 1;
+                                    if (sc.emit_cdf[mid] > target) hi = mid;
+                                    else lo = mid + 1;
+                                }
+                                lt_tri = sc.emit_tri[lo];
+                                li = sc.tri_light[lt_tri];
+                                lp = sc.lights[li].pdf_power;
+                            } else {
+                                li = (uint32_t)((float)sc.nLight * rng.next());
+                                if (li >= sc.nLight) li = sc.nLight - 1;
+                                lp = 1.0f / (float)sc.nLight;
+                                uint32_t tk = (uint32_t)(rng.next() * (float)sc.lights[li].tri_count);
+                                if (tk >= sc.lights[li].tri_count) tk = sc.lights[li].tri_count - 1;
+                                lp = lp / (float)sc.lights[li].tri_count;
+                                lt_tri = sc.lights[li].first_tri + tk;
+                            }
                             const DevLight &lt = sc.lights[li];
-                            float lp = 1.0f / (float)sc.nLight;
-                            uint32_t tk = (uint32_t)(rng.next() * (float)lt.tri_count);
-                            if (tk >= lt.tri_count) tk = lt.tri_count - 1;
-                            lp = lp / (float)lt.tri_count;
-                            uint32_t lt_tri = lt.first_tri + tk;
                             uint4 li4 = sc.tri[lt_tri];
                             v3 v0 = vtx(sc.V, li4.x), v1 = vtx(sc.V, li4.y), v2 = vtx(sc.V, li4.z);
                             float su = rng.next(), sv = rng.next();
                             if (su + sv > 1.0f) { su = 1.0f - su; sv = 1.0f - sv; }
                             float cx = 1.0f - su - sv, cy = su;
                             v3 lpos = v0 + su * (v1 - v0) + sv * (v2 - v0);
-                            lp = lp / tri_area(sc, lt_tri);
+                            if (wp.lights != WL_LIGHTS_POWER) lp = lp / tri_area(sc, lt_tri);
                             v3 lN;
                             if (lt.has_normal) {
                                 lN = normalize(vtx(sc.N, li4.x) * (1.0f - cx - cy) + vtx(sc.N, li4.y) * cx +

@@ -179,6 +179,61 @@ void launch_film_batch(const BatchView &bv, const Queues &q, uint32_t count, cud
     k_film_batch<<<(count + 255) / 256, 256, 0, s>>>(bv, q, count);
 }
 
+// Emitter CDF of WL_LIGHTS_POWER, in FP64 and in a fixed summation order (the oracle sums in the
+// same order, so both select the same triangle for every random number): emissive triangle i
+// (light order, each light's triangles in order) has weight area_i * luminance(L) (Rec. 709
+// weights); chunks of 256 are summed sequentially, then the chunk sums sequentially, then
+// cdf_i = (chunk-local sum + chunk offset) / total, so the last entry is exactly 1.
+constexpr uint32_t EMIT_CHUNK = 256;
+__device__ __forceinline__ double emit_lum(const DevLight &l) {
+    return 0.2126 * (double)l.L[0] + 0.7152 * (double)l.L[1] + 0.0722 * (double)l.L[2];
+}
+__global__ void k_emit_chunks(const float *V, const uint4 *tri, const uint32_t *emit_tri,
+                              const uint32_t *emit_light, uint32_t n, const DevLight *lights,
+                              double *cdf, double *chunk) {
+    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if ((uint64_t)c * EMIT_CHUNK >= n) return;
+    double acc = 0.0;
+    uint32_t end = (c + 1) * EMIT_CHUNK < n ? (c + 1) * EMIT_CHUNK : n;
+    for (uint32_t i = c * EMIT_CHUNK; i < end; i++) {
+        uint4 t = tri[emit_tri[i]];
+        double ax = V[3 * (size_t)t.x], ay = V[3 * (size_t)t.x + 1], az = V[3 * (size_t)t.x + 2];
+        double e1x = V[3 * (size_t)t.y] - ax, e1y = V[3 * (size_t)t.y + 1] - ay, e1z = V[3 * (size_t)t.y + 2] - az;
+        double e2x = V[3 * (size_t)t.z] - ax, e2y = V[3 * (size_t)t.z + 1] - ay, e2z = V[3 * (size_t)t.z + 2] - az;
+        double cx = e1y * e2z - e1z * e2y, cy = e1z * e2x - e1x * e2z, cz = e1x * e2y - e1y * e2x;
+        double area = 0.5 * sqrt(cx * cx + cy * cy + cz * cz);
+        acc = acc + area * emit_lum(lights[emit_light[i]]);
+        cdf[i] = acc;
+    }
+    chunk[c] = acc;
+}
+__global__ void k_emit_offsets(uint32_t chunks, double *chunk, DevLight *lights, uint32_t nLight) {
+    double off = 0.0;
+    for (uint32_t c = 0; c < chunks; c++) {
+        double v = chunk[c];
+        chunk[c] = off;
+        off = off + v;
+    }
+    chunk[chunks] = off;  // total
+    for (uint32_t l = 0; l < nLight; l++)
+        lights[l].pdf_power = off > 0.0 ? (float)(emit_lum(lights[l]) / off) : 0.0f;
+}
+__global__ void k_emit_normalise(uint32_t n, uint32_t chunks, double *cdf, const double *chunk) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double total = chunk[chunks];
+    cdf[i] = total > 0.0 ? (cdf[i] + chunk[i / EMIT_CHUNK]) / total : 0.0;
+}
+void launch_emit_cdf(const float *V, const uint4 *tri, const uint32_t *emit_tri,
+                     const uint32_t *emit_light, uint32_t n, DevLight *lights, uint32_t nLight,
+                     double *cdf, double *chunk, cudaStream_t s) {
+    if (n == 0) return;
+    uint32_t chunks = (n + EMIT_CHUNK - 1) / EMIT_CHUNK;
+    k_emit_chunks<<<(chunks + 127) / 128, 128, 0, s>>>(V, tri, emit_tri, emit_light, n, lights, cdf, chunk);
+    k_emit_offsets<<<1, 1, 0, s>>>(chunks, chunk, lights, nLight);
+    k_emit_normalise<<<(n + 255) / 256, 256, 0, s>>>(n, chunks, cdf, chunk);
+}
+
 // colorBuffer = u8vec4(vec4(AceApprox(clamp(radiance, 0, 1e30)), 1) * 255) (PathTracing.cu:157-158)
 __global__ void k_tonemap(Film f) {
     uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;

@@ -18,7 +18,7 @@ struct DevLight {
     uint32_t first_tri;
     uint32_t tri_count;
     uint32_t has_normal;
-    uint32_t pad;
+    float pdf_power;  // area pdf of a point of this light under WL_LIGHTS_POWER: lum(L) / total
 };
 
 // Everything a kernel needs to shade a hit (HitData of PathTracingLaunchParams.h:64-78, one
@@ -227,6 +227,10 @@ void launch_shade_nrc(const WaveParams &wp, const DevScene &sc, const Queues &q,
                       const NrcWaveBuffers &nb, cudaStream_t s);
 void launch_film(const WaveParams &wp, const Queues &q, const Film &f, cudaStream_t s);
 void launch_film_batch(const BatchView &bv, const Queues &q, uint32_t count, cudaStream_t s);
+// emitter CDF of WL_LIGHTS_POWER (FP64): cdf (n), chunk (n / 256 + 1 scratch); sets pdf_power
+void launch_emit_cdf(const float *V, const uint4 *tri, const uint32_t *emit_tri,
+                     const uint32_t *emit_light, uint32_t n, DevLight *lights, uint32_t nLight,
+                     double *cdf, double *chunk, cudaStream_t s);
 // graph replays: cur = all[2 w], all[2 w + 1] for the w-th replay (counter ctr)
 void launch_wave_begin(const uint64_t *all, uint32_t *ctr, uint64_t *cur, cudaStream_t s);
 void launch_bdpt_connections(const WaveParams &wp, const BdptWave &bw, cudaStream_t s);
