@@ -1363,6 +1363,7 @@ static int nrc_prepare(wl_context *c, wl_nrc *n, const wl_render_params *p, uint
         n->t_cap = t_cap;
         n->depth_cap = p->max_depth;
     }
+    if (nrc_reserve_queries(n->net, (uint32_t)wave) != WL_OK) return fail(WL_ERR_OOM, "cache query tiles");
     return WL_OK;
 }
 

@@ -2,8 +2,9 @@
 // render loop. Encoding: wl_nrc.cuh; tensor-core forward/backward: nrc_tc.cu.
 //
 // Training step on n samples (relative L2 loss, Mueller et al. 2021):
-//   k_train_tc (nrc_tc.cu)  encode, forward, loss, backward, weight gradients and the hash-grid
-//                           gradient in one persistent tensor-core kernel
+//   k_encode_tiles, k_train_tc, k_grid_scatter (nrc_tc.cu): encode into tensor-core tiles; then
+//                           forward, loss, backward and weight gradients in one persistent
+//                           tensor-core kernel; then the hash-grid gradient
 //   k_adam                  Adam on the MLP weights and on the hash grid
 #include <cmath>
 #include <cstring>
@@ -75,6 +76,12 @@ struct NrcNet {
     float *w = nullptr, *w_grad = nullptr, *w_m = nullptr, *w_v = nullptr;
     uint32_t max_samples = 0;
     float *loss = nullptr;
+    // training scratch: encoded input tiles (32 KB per 128 rows) and grid-feature gradients
+    uint8_t *tiles = nullptr;
+    float *gin = nullptr;
+    uint32_t raw_cap = 0;  // rows the scratch holds
+    uint8_t *q_tiles = nullptr;  // encoded queries, 16 KB per 128 rows
+    uint32_t q_cap = 0;
     uint32_t *counters = nullptr;  // [0] samples of the current frame, [1] queries
     NrcVertex *samples = nullptr;
     float lr = 1e-2f;
@@ -91,7 +98,7 @@ static void *nrc_alloc(size_t bytes, cudaError_t &e) {
 void nrc_free(NrcNet *n) {
     if (!n) return;
     void *ps[] = {n->grid.params, n->grid.grad, n->grid_m, n->grid_v, n->w, n->w_grad, n->w_m, n->w_v,
-                  n->loss, n->counters, n->samples};
+                  n->loss, n->counters, n->samples, n->tiles, n->gin, n->q_tiles};
     for (void *p : ps)
         if (p) cudaFree(p);
     delete n;
@@ -121,6 +128,9 @@ int nrc_create(const wl_nrc_params &p, const float *bbox_lo, const float *bbox_h
     n->w_m = (float *)nrc_alloc(NRC_WEIGHTS * 4, e);
     n->w_v = (float *)nrc_alloc(NRC_WEIGHTS * 4, e);
     n->max_samples = max_samples;
+    n->tiles = (uint8_t *)nrc_alloc(((size_t)max_samples + 127) / 128 * 32768, e);
+    n->gin = (float *)nrc_alloc((size_t)max_samples * 32 * 4, e);
+    n->raw_cap = max_samples;
     n->loss = (float *)nrc_alloc(16, e);
     n->counters = (uint32_t *)nrc_alloc(64, e);
     n->samples = (NrcVertex *)nrc_alloc((size_t)max_samples * sizeof(NrcVertex), e);
@@ -171,12 +181,24 @@ void nrc_forward_raw(NrcNet *n, const float *in, float *out, uint32_t count, cud
 // and the grid gradient in grid.grad; the loss in n->loss[0].
 static void nrc_gradients(NrcNet *n, bool enc, const wl_disney *mats, const float *in,
                           const float *target, uint32_t count, cudaStream_t s) {
+    if (!enc && count > n->raw_cap) {
+        // raw batches larger than the sample buffer: grow the tile scratch
+        cudaStreamSynchronize(s);
+        if (n->tiles) cudaFree(n->tiles);
+        n->tiles = nullptr;
+        if (cudaMalloc(&n->tiles, ((size_t)count + 127) / 128 * 32768) != cudaSuccess) {
+            n->tiles = nullptr;
+            n->raw_cap = 0;
+            return;
+        }
+        n->raw_cap = count;
+    }
     if (enc)
         nrc_tc_train(n->w, n->grid, mats, n->samples, n->counters, n->max_samples, nullptr, nullptr,
-                     n->w_grad, n->loss, n->counters + 2, s);
+                     n->w_grad, n->loss, n->counters + 2, n->tiles, n->gin, s);
     else
         nrc_tc_train(n->w, n->grid, mats, nullptr, nullptr, count, in, target, n->w_grad, n->loss,
-                     n->counters + 2, s);
+                     n->counters + 2, n->tiles, nullptr, s);
 }
 
 static void nrc_adam(NrcNet *n, bool grid, cudaStream_t s) {
@@ -205,9 +227,23 @@ void nrc_train_collected(NrcNet *n, const wl_disney *mats, cudaStream_t s) {
     nrc_adam(n, true, s);
 }
 
+int nrc_reserve_queries(NrcNet *n, uint32_t rows) {
+    if (n->q_cap >= rows && n->q_tiles) return WL_OK;
+    if (n->q_tiles) cudaFree(n->q_tiles);
+    n->q_tiles = nullptr;
+    n->q_cap = 0;
+    if (cudaMalloc(&n->q_tiles, ((size_t)rows + 127) / 128 * 16384) != cudaSuccess) {
+        n->q_tiles = nullptr;
+        return WL_ERR_OOM;
+    }
+    n->q_cap = rows;
+    return WL_OK;
+}
+
 void nrc_query(NrcNet *n, const wl_disney *mats, const NrcVertex *q, const uint32_t *nq,
                float4 *rad, uint32_t max_q, cudaStream_t s) {
-    nrc_tc_query(n->w, n->grid, mats, q, nq, rad, max_q, n->counters + 2, s);
+    if (max_q > n->q_cap) max_q = n->q_cap;  // the render reserved the query rows beforehand
+    nrc_tc_query(n->w, n->grid, mats, q, nq, rad, max_q, n->counters + 2, n->q_tiles, s);
 }
 
 void nrc_collect(NrcNet *n, NrcWaveBuffers b, const Queues &q, uint32_t tcount, cudaStream_t s) {

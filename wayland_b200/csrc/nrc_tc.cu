@@ -118,12 +118,14 @@ __device__ __forceinline__ void store_row(uint8_t *tile, uint32_t r, const float
     }
 }
 
-// MODE 0: raw rows in[n][64] -> out[n][4]. MODE 1: cache queries of the render loop.
+// MODE 0: raw rows in[n][64] -> out[n][4]. MODE 1: cache queries of the render loop, encoded
+// here. MODE 2: the same queries, encoded beforehand into 16 KB tiles (k_encode_tiles).
 template <int MODE>
 __global__ void __launch_bounds__(TC_THREADS) k_mlp_tc(const float *w, NrcGrid g, const wl_disney *mats,
                                                         const NrcVertex *q, const uint32_t *nq,
                                                         float4 *rad, const float *in, float *out,
-                                                        uint32_t n_raw, uint32_t *err) {
+                                                        uint32_t n_raw, uint32_t *err,
+                                                        const uint8_t *tiles = nullptr) {
     extern __shared__ __align__(1024) uint8_t smem[];
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const uint32_t bar = smem_u32(smem + SM_BAR);
@@ -156,19 +158,26 @@ __global__ void __launch_bounds__(TC_THREADS) k_mlp_tc(const float *w, NrcGrid g
     for (uint32_t tile = blockIdx.x * TC_THREADS; tile < n && ok; tile += gridDim.x * TC_THREADS) {
         const uint32_t i = tile + tid;
         const bool valid = i < n;
-        float x[NRC_IN];
         NrcVertex v;
-        if (valid) {
-            if (MODE == 0) {
-                for (int k = 0; k < NRC_IN; k++) x[k] = in[(size_t)i * NRC_IN + k];
-            } else {
-                v = q[i];
-                nrc_encode(g, mats, v, x);
-            }
+        if (MODE == 2) {
+            const uint4 *src = reinterpret_cast<const uint4 *>(tiles + (size_t)(tile / 128u) * 16384u);
+            uint4 *dst = reinterpret_cast<uint4 *>(smem + SM_A);
+            for (uint32_t k = tid; k < 1024u; k += TC_THREADS) dst[k] = src[k];
+            if (valid) v.extra = q[i].extra;
         } else {
-            for (int k = 0; k < NRC_IN; k++) x[k] = 0.0f;
+            float x[NRC_IN];
+            if (valid) {
+                if (MODE == 0) {
+                    for (int k = 0; k < NRC_IN; k++) x[k] = in[(size_t)i * NRC_IN + k];
+                } else {
+                    v = q[i];
+                    nrc_encode(g, mats, v, x);
+                }
+            } else {
+                for (int k = 0; k < NRC_IN; k++) x[k] = 0.0f;
+            }
+            store_row(smem + SM_A, tid, x);
         }
-        store_row(smem + SM_A, tid, x);
         fence_async_smem();
         tc_before_sync();
         __syncthreads();
@@ -305,13 +314,71 @@ __device__ __forceinline__ void smem_to_tc() {
     tc_after_sync();
 }
 
+// Encoded inputs of a training step in the tensor-core operand layout, one 32 KB record per
+// 128 rows: the K-major tile (row = sample) and its transpose (row = feature). Thread (r, h)
+// encodes row r's columns [16h, 16h + 16) and [32 + 16h, 32 + 16h + 16): grid levels 8h..8h+7
+// and the direction (h = 0) or auxiliary (h = 1) features. Many CTAs per SM hide the grid
+// gathers' latency, which the tensor-core kernel (one CTA per SM) could not.
+template <int MODE, bool TRANSPOSE = true>
+__global__ void __launch_bounds__(256) k_encode_tiles(NrcGrid g, const wl_disney *mats,
+                                                      const NrcVertex *samples, const uint32_t *n_ptr,
+                                                      uint32_t n_fixed, const float *in, uint8_t *tiles) {
+    const uint32_t n = MODE == 1 ? min(*n_ptr, n_fixed) : n_fixed;
+    const uint32_t tile = blockIdx.x;
+    if (tile * 128u >= n) return;
+    const uint32_t r = threadIdx.x & 127u, h = threadIdx.x >> 7;
+    const uint32_t i = tile * 128u + r;
+    float x[32];
+    if (i < n) {
+        if (MODE == 1) {
+            NrcVertex v = samples[i];
+            float3 pn = grid_normalise(g, v.pos_mat);
+            nrc_grid_features(g, pn, 8u * h, x);
+            if (h == 0) nrc_dir_features(v, x + 16);
+            else nrc_aux_features(mats, v, x + 16);
+        } else {
+            for (int k = 0; k < 16; k++) {
+                x[k] = in[(size_t)i * NRC_IN + 16 * h + k];
+                x[16 + k] = in[(size_t)i * NRC_IN + 32 + 16 * h + k];
+            }
+        }
+    } else {
+        for (int k = 0; k < 32; k++) x[k] = 0.0f;
+    }
+    uint8_t *A = tiles + (size_t)tile * (TRANSPOSE ? 32768u : 16384u);
+    store8(A, r, 16 * h, x);
+    store8(A, r, 16 * h + 8, x + 8);
+    store8(A, r, 32 + 16 * h, x + 16);
+    store8(A, r, 32 + 16 * h + 8, x + 24);
+    if (TRANSPOSE) {
+        uint8_t *AT = A + 16384u;
+        for (int k = 0; k < 16; k++) {
+            store_t(AT, 16 * h + k, r, x[k]);
+            store_t(AT, 32 + 16 * h + k, r, x[16 + k]);
+        }
+    }
+}
+
+// The hash-grid gradient: thread (sample, level) adds its two feature gradients, weighted
+// trilinearly, to the 8 corner entries (nrc_grid_backward).
+__global__ void __launch_bounds__(256) k_grid_scatter(NrcGrid g, const NrcVertex *samples,
+                                                      const uint32_t *n_ptr, uint32_t n_fixed,
+                                                      const float *gin) {
+    const uint32_t n = min(*n_ptr, n_fixed);
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t s = k >> 4, l = k & 15u;
+    if (s >= n || l >= g.levels) return;
+    float g2[2] = {gin[(size_t)s * 32u + 2u * l], gin[(size_t)s * 32u + 2u * l + 1u]};
+    nrc_grid_backward(g, samples[s], g2, l, l + 1u);
+}
+
 // MODE 0: raw rows in[n][64], targets target[n][4]. MODE 1: the collected training samples
 // (count on the device), encoded here; the input gradient goes to the hash grid.
 template <int MODE>
 __global__ void __launch_bounds__(TR_THREADS, 1)
-    k_train_tc(const float *w, NrcGrid g, const wl_disney *mats, const NrcVertex *samples,
-               const uint32_t *n_ptr, uint32_t n_fixed, const float *in, const float *target,
-               float *w_grad, float *loss, uint32_t *err) {
+    k_train_tc(const float *w, const NrcVertex *samples, const uint32_t *n_ptr, uint32_t n_fixed,
+               const float *target, const uint8_t *tiles, float *gin_out, float *w_grad,
+               float *loss, uint32_t *err) {
     extern __shared__ __align__(1024) uint8_t smem[];
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const uint32_t r = tid & 127u, h = tid >> 7;
@@ -352,34 +419,24 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
     for (uint32_t tile = blockIdx.x * 128u; tile < n && ok; tile += gridDim.x * 128u) {
         const uint32_t i = tile + r;
         const bool valid = i < n;
-        // ---- inputs: columns [16h, 16h + 16) and [32 + 16h, 32 + 16h + 16)
-        float x[32], t3[3] = {0.f, 0.f, 0.f};
-        NrcVertex v{};
-        if (valid) {
+        // ---- inputs: the encoded tile and its transpose (k_encode_tiles), 32 KB
+        float t3[3] = {0.f, 0.f, 0.f};
+        {
+            const uint4 *src = reinterpret_cast<const uint4 *>(tiles + (size_t)(tile / 128u) * 32768u);
+            uint4 *dA = reinterpret_cast<uint4 *>(smem + TS_T0);
+            uint4 *dT = reinterpret_cast<uint4 *>(smem + TS_AT);
+            for (uint32_t k = tid; k < 1024u; k += TR_THREADS) {
+                dA[k] = src[k];
+                dT[k] = src[1024u + k];
+            }
+        }
+        if (valid && h == 0) {
             if (MODE == 1) {
-                v = samples[i];
-                float3 pn = grid_normalise(g, v.pos_mat);
-                nrc_grid_features(g, pn, 8u * h, x);
-                if (h == 0) nrc_dir_features(v, x + 16);
-                else nrc_aux_features(mats, v, x + 16);
-                t3[0] = v.extra.x; t3[1] = v.extra.y; t3[2] = v.extra.z;
+                float4 e = samples[i].extra;
+                t3[0] = e.x; t3[1] = e.y; t3[2] = e.z;
             } else {
-                for (int k = 0; k < 16; k++) {
-                    x[k] = in[(size_t)i * NRC_IN + 16 * h + k];
-                    x[16 + k] = in[(size_t)i * NRC_IN + 32 + 16 * h + k];
-                }
                 for (int c = 0; c < 3; c++) t3[c] = target[(size_t)i * 4 + c];
             }
-        } else {
-            for (int k = 0; k < 32; k++) x[k] = 0.0f;
-        }
-        store8(smem + TS_T0, r, 16 * h, x);
-        store8(smem + TS_T0, r, 16 * h + 8, x + 8);
-        store8(smem + TS_T0, r, 32 + 16 * h, x + 16);
-        store8(smem + TS_T0, r, 32 + 16 * h + 8, x + 24);
-        for (int k = 0; k < 16; k++) {
-            store_t(smem + TS_AT, 16 * h + k, r, x[k]);
-            store_t(smem + TS_AT, 32 + 16 * h + k, r, x[16 + k]);
         }
         smem_to_tc();
         // ---- forward
@@ -474,12 +531,16 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
             ok = tc_step(bar, phase);
         }
         if (!ok) break;
-        // ---- input gradient of the grid features: levels [8h, 8h + 8)
+        // ---- input gradient of the grid features (levels [8h, 8h + 8)), scattered into the grid
+        // by k_grid_scatter
         {
             float gin[16];
             tmem_ld16(tmem + lane + 64u + 16u * h, gin);
             tmem_wait_ld();
-            if (MODE == 1 && valid) nrc_grid_backward(g, v, gin, 8u * h, 8u * h + 8u);
+            if (MODE == 1 && valid) {
+                float4 *o = reinterpret_cast<float4 *>(gin_out + (size_t)i * 32u + 16u * h);
+                for (int c = 0; c < 4; c++) o[c] = make_float4(gin[4 * c], gin[4 * c + 1], gin[4 * c + 2], gin[4 * c + 3]);
+            }
         }
         any = true;
         tc_before_sync();
@@ -516,9 +577,13 @@ int tc_grid(const void *k) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BYTES);
+    cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, TC_THREADS, SM_BYTES);
-    if (per < 1) per = 1;
-    if (per > 4) per = 4;  // 4 x 64 tensor-memory columns per SM
+    // 4 CTAs per SM fit by shared memory (4 x 51 KB), registers and tensor memory (4 x 64
+    // columns); launch that many even where the occupancy query reports fewer (CTAs that do not
+    // fit wait for a free slot; they never wait on one another)
+    if (per < 4) per = 4;
+    if (per > 4) per = 4;
     return sms * per;
 }
 
@@ -534,39 +599,53 @@ void nrc_tc_forward_raw(const float *w, const float *in, float *out, uint32_t n,
                                                       in, out, n, err);
 }
 
+// Cache queries: encoded into tiles by a many-CTA kernel (the grid gathers are latency-bound),
+// then the tensor-core MLP over the tiles. tiles: 16 KB per 128 queries (max_q rows).
 void nrc_tc_query(const float *w, const NrcGrid &g, const wl_disney *mats, const NrcVertex *q,
-                  const uint32_t *nq, float4 *rad, uint32_t max_q, uint32_t *err, cudaStream_t s) {
-    static int grid = tc_grid((const void *)k_mlp_tc<1>);
-    uint32_t tiles = (max_q + TC_THREADS - 1) / TC_THREADS;
-    uint32_t blocks = tiles < (uint32_t)grid ? tiles : (uint32_t)grid;
-    if (blocks == 0) blocks = 1;
-    k_mlp_tc<1><<<blocks, TC_THREADS, SM_BYTES, s>>>(w, g, mats, q, nq, rad, nullptr, nullptr, 0, err);
+                  const uint32_t *nq, float4 *rad, uint32_t max_q, uint32_t *err, uint8_t *tiles,
+                  cudaStream_t s) {
+    static int grid = tc_grid((const void *)k_mlp_tc<2>);
+    uint32_t ntiles = (max_q + TC_THREADS - 1) / TC_THREADS;
+    if (ntiles == 0) return;
+    k_encode_tiles<1, false><<<ntiles, 256, 0, s>>>(g, mats, q, nq, max_q, nullptr, tiles);
+    uint32_t blocks = ntiles < (uint32_t)grid ? ntiles : (uint32_t)grid;
+    k_mlp_tc<2><<<blocks, TC_THREADS, SM_BYTES, s>>>(w, g, mats, q, nq, rad, nullptr, nullptr, 0, err,
+                                                     tiles);
 }
 
 // Gradients of one training step into w_grad (zeroed here) and the grid gradient; loss (zeroed
-// here) receives the mean relative L2 loss. Raw rows when samples is null.
+// here) receives the mean relative L2 loss. Raw rows when samples is null. tiles: 32 KB per 128
+// rows; gin: 32 floats per row.
 void nrc_tc_train(const float *w, const NrcGrid &g, const wl_disney *mats, const NrcVertex *samples,
                   const uint32_t *n_ptr, uint32_t n_max, const float *in, const float *target,
-                  float *w_grad, float *loss, uint32_t *err, cudaStream_t s) {
+                  float *w_grad, float *loss, uint32_t *err, uint8_t *tiles, float *gin,
+                  cudaStream_t s) {
     static int sms = [] {
         int dev = 0, v = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
         cudaFuncSetAttribute(k_train_tc<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS_BYTES);
         cudaFuncSetAttribute(k_train_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TS_BYTES);
+        cudaFuncSetAttribute(k_train_tc<0>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        cudaFuncSetAttribute(k_train_tc<1>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         return v;
     }();
     cudaMemsetAsync(w_grad, 0, NRC_WEIGHTS * sizeof(float), s);
     cudaMemsetAsync(loss, 0, sizeof(float), s);
-    uint32_t tiles = (n_max + 127u) / 128u;
-    uint32_t blocks = tiles < (uint32_t)sms ? tiles : (uint32_t)sms;
+    uint32_t tiles_n = (n_max + 127u) / 128u;
+    uint32_t blocks = tiles_n < (uint32_t)sms ? tiles_n : (uint32_t)sms;
     if (blocks == 0) return;
-    if (samples)
-        k_train_tc<1><<<blocks, TR_THREADS, TS_BYTES, s>>>(w, g, mats, samples, n_ptr, n_max, nullptr,
+    if (samples) {
+        k_encode_tiles<1><<<tiles_n, 256, 0, s>>>(g, mats, samples, n_ptr, n_max, nullptr, tiles);
+        k_train_tc<1><<<blocks, TR_THREADS, TS_BYTES, s>>>(w, samples, n_ptr, n_max, nullptr, tiles, gin,
+                                                           w_grad, loss, err);
+        uint64_t threads = (uint64_t)n_max * 16u;
+        k_grid_scatter<<<(uint32_t)((threads + 255) / 256), 256, 0, s>>>(g, samples, n_ptr, n_max, gin);
+    } else {
+        k_encode_tiles<0><<<tiles_n, 256, 0, s>>>(g, mats, nullptr, nullptr, n_max, in, tiles);
+        k_train_tc<0><<<blocks, TR_THREADS, TS_BYTES, s>>>(w, nullptr, nullptr, n_max, target, tiles,
                                                            nullptr, w_grad, loss, err);
-    else
-        k_train_tc<0><<<blocks, TR_THREADS, TS_BYTES, s>>>(w, g, mats, nullptr, nullptr, n_max, in,
-                                                           target, w_grad, loss, err);
+    }
 }
 
 }  // namespace wl

@@ -301,9 +301,12 @@ struct NrcGrid;
 void nrc_tc_forward_raw(const float *w, const float *in, float *out, uint32_t n, uint32_t *err,
                         cudaStream_t s);
 void nrc_tc_query(const float *w, const NrcGrid &g, const wl_disney *mats, const NrcVertex *q,
-                  const uint32_t *nq, float4 *rad, uint32_t max_q, uint32_t *err, cudaStream_t s);
+                  const uint32_t *nq, float4 *rad, uint32_t max_q, uint32_t *err, uint8_t *tiles,
+                  cudaStream_t s);
+int nrc_reserve_queries(NrcNet *n, uint32_t rows);
 void nrc_tc_train(const float *w, const NrcGrid &g, const wl_disney *mats, const NrcVertex *samples,
                   const uint32_t *n_ptr, uint32_t n_max, const float *in, const float *target,
-                  float *w_grad, float *loss, uint32_t *err, cudaStream_t s);
+                  float *w_grad, float *loss, uint32_t *err, uint8_t *tiles, float *gin,
+                  cudaStream_t s);
 
 }  // namespace wl

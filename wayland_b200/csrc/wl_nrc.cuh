@@ -171,8 +171,8 @@ __device__ __forceinline__ void nrc_grid_backward(const NrcGrid &g, const NrcVer
             uint32_t dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
             float w = (dx ? c.fx : 1.0f - c.fx) * (dy ? c.fy : 1.0f - c.fy) * (dz ? c.fz : 1.0f - c.fz);
             uint32_t idx = grid_index(g, res, c.cx + dx, c.cy + dy, c.cz + dz);
-            atomicAdd(tab + (size_t)idx * F, w * g0);
-            atomicAdd(tab + (size_t)idx * F + 1, w * g1);
+            // one vector atomic for both features (8-byte aligned entry)
+            atomicAdd(reinterpret_cast<float2 *>(tab + (size_t)idx * F), make_float2(w * g0, w * g1));
         }
     }
 }
