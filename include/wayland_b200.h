@@ -333,13 +333,15 @@ typedef struct wl_tune_result {
     uint32_t extend_ctas_per_sm, extend_refill;
     uint32_t shadow_ctas_per_sm, shadow_refill;
     uint32_t candidates;        /* configurations timed */
-    uint32_t spp;               /* samples per pixel of the tuning renders */
-    float ms_default;           /* tuning render with the default shape */
-    float ms_tuned;             /* tuning render with the chosen shape */
+    uint32_t spp;               /* samples per pixel of the wave-size renders */
+    float ms_default;           /* wave-size render with the default shape */
+    float ms_tuned;             /* wave-size render with the chosen shape */
 } wl_tune_result;
-/* Times renders of (scene, camera, params with spp reduced to about 2^24 paths) for candidate
- * shapes by coordinate descent and keeps the fastest in the context for later renders of every
- * program. Path-tracer strategies only. */
+/* Times renders of (scene, camera, params with spp reduced) for candidate shapes by coordinate
+ * descent and keeps the fastest in the context for later renders of every program: wave sizes
+ * on renders of about 2^26 paths (two waves of the largest candidate, so that per-wave tails
+ * weigh as in a long render), then the traversal launch shapes on renders of about 2^24 paths.
+ * Path-tracer strategies only. */
 WL_API int wl_autotune(wl_context *ctx, wl_scene *scene, const wl_camera *camera,
                        const wl_render_params *params, wl_tune_result *out);
 /* Sets the context's shape (as returned by wl_autotune); NULL restores the defaults. */

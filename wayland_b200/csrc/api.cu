@@ -1473,20 +1473,27 @@ int wl_autotune(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_rende
     wl_film *film = nullptr;
     int rc = wl_film_create(c, p->width, p->height, 0, &film);
     if (rc != WL_OK) return rc;
-    wl_render_params q = *p;
+    // Wave sizes are compared on renders of about 2^26 paths (two waves of the largest
+    // candidate), so that each candidate pays its per-wave tail as often per path as in a long
+    // render; launch shapes on renders of about 2^24 paths.
     const uint64_t npix = (uint64_t)p->width * p->height;
-    uint64_t spp = (1ull << 24) / (npix ? npix : 1);
-    q.spp = (uint32_t)(spp < 1 ? 1 : (spp > p->spp ? p->spp : spp));
-    q.flags = 0;
-    q.wave_paths = 0;
+    auto sample = [&](uint64_t paths) {
+        wl_render_params r = *p;
+        uint64_t spp = paths / (npix ? npix : 1);
+        r.spp = (uint32_t)(spp < 1 ? 1 : (spp > p->spp ? p->spp : spp));
+        r.flags = 0;
+        r.wave_paths = 0;
+        return r;
+    };
+    const wl_render_params qw = sample(1ull << 26), q = sample(1ull << 24);
     uint32_t candidates = 0;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    auto timed = [&](float &ms) -> int {
+    auto timed = [&](const wl_render_params &rp, float &ms) -> int {
         for (int rep = 0; rep < 2; rep++) {
             cudaEventRecord(e0, c->stream);
-            int r = wl_render(c, s, cam, &q, film);
+            int r = wl_render(c, s, cam, &rp, film);
             if (r != WL_OK) return r;
             cudaEventRecord(e1, c->stream);
             if (cudaEventSynchronize(e1) != cudaSuccess) return fail(WL_ERR_CUDA, "autotune timing");
@@ -1501,8 +1508,8 @@ int wl_autotune(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_rende
     c->tune_wave = 0;
     c->tune_extend = TraceTune{};
     c->tune_shadow = TraceTune{};
-    float ms_default = 0.f, best = 0.f;
-    rc = timed(ms_default);
+    float ms_default = 0.f, best = 0.f, ms_tuned = 0.f;
+    rc = timed(qw, ms_default);
     best = ms_default;
     uint32_t best_wave = 0;
     const uint32_t waves[] = {1u << 21, 1u << 22, 1u << 23, 1u << 24, 1u << 25};
@@ -1510,10 +1517,11 @@ int wl_autotune(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_rende
         if (rc != WL_OK) break;
         c->tune_wave = w;
         float ms = 0.f;
-        rc = timed(ms);
+        rc = timed(qw, ms);
         if (rc == WL_OK && ms < best) { best = ms; best_wave = w; }
     }
     c->tune_wave = best_wave;
+    if (rc == WL_OK) rc = timed(q, best);
     const uint32_t ctas[] = {0u, 6u, 4u};
     const uint32_t refills[] = {4u, 6u, 8u, 12u, 16u, 24u};
     for (int pass = 0; pass < 2 && rc == WL_OK; pass++) {
@@ -1525,11 +1533,12 @@ int wl_autotune(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_rende
                 t.ctas_per_sm = ct;
                 t.refill = rf;
                 float ms = 0.f;
-                rc = timed(ms);
+                rc = timed(q, ms);
                 if (rc == WL_OK && ms < best) { best = ms; bt = t; }
             }
         t = bt;
     }
+    if (rc == WL_OK) rc = timed(qw, ms_tuned);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     wl_film_destroy(film);
@@ -1546,8 +1555,8 @@ int wl_autotune(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_rende
     out->shadow_refill = c->tune_shadow.refill;
     out->candidates = candidates;
     out->ms_default = ms_default;
-    out->ms_tuned = best;
-    out->spp = q.spp;
+    out->ms_tuned = ms_tuned;
+    out->spp = qw.spp;
     return WL_OK;
 }
 

@@ -426,21 +426,32 @@ WL_HD bool trav_step(TravState &s, uint2 *stack, const float4 *__restrict__ node
         uint32_t qhy0 = as_uint(n4.x), qhy1 = as_uint(n4.y), qhz0 = as_uint(n4.z), qhz1 = as_uint(n4.w);
         const float tcur = s.res.t;
         uint32_t ihits = 0, thits = 0;
+        // Slab distances in one FMA per plane: t = q A + B with A = scale / d (exact: power-of-two
+        // scale) and B = (origin - o) / d. The absolute error of such a t is below
+        // 3 u (255 |A| + |B|) (u = 2^-24: one rounding in origin - o, one in the product, one in
+        // the FMA). Each axis widens its own slab by e = 8 u (255 |A| + |B|): the entry plane
+        // (the low plane when d >= 0, the high plane when d < 0) uses B - e, the exit plane B + e,
+        // so the test never rejects a child whose triangle the triangle test accepts.
+        const float ax = XMUL(scx, s.idx), ay = XMUL(scy, s.idy), az = XMUL(scz, s.idz);
+        const float bx = XMUL(XSUB(n0.x, s.ox), s.idx), by = XMUL(XSUB(n0.y, s.oy), s.idy),
+                    bz = XMUL(XSUB(n0.z, s.oz), s.idz);
+        const float ex = fmaf(fabsf(ax), 255.0f, fabsf(bx)) * 0x1p-21f;
+        const float ey = fmaf(fabsf(ay), 255.0f, fabsf(by)) * 0x1p-21f;
+        const float ez = fmaf(fabsf(az), 255.0f, fabsf(bz)) * 0x1p-21f;
+        const float bnx = bx - ex, bfx = bx + ex, bny = by - ey, bfy = by + ey, bnz = bz - ez, bfz = bz + ez;
+        const bool sx = s.oct & 1u, sy = s.oct & 2u, sz = s.oct & 4u;
+        const uint32_t qnx0 = sx ? qhx0 : qlx0, qnx1 = sx ? qhx1 : qlx1, qfx0 = sx ? qlx0 : qhx0, qfx1 = sx ? qlx1 : qhx1;
+        const uint32_t qny0 = sy ? qhy0 : qly0, qny1 = sy ? qhy1 : qly1, qfy0 = sy ? qly0 : qhy0, qfy1 = sy ? qly1 : qhy1;
+        const uint32_t qnz0 = sz ? qhz0 : qlz0, qnz1 = sz ? qhz1 : qlz1, qfz0 = sz ? qlz0 : qhz0, qfz1 = sz ? qlz1 : qhz1;
 #pragma unroll
         for (int c = 0; c < 8; c++) {
             uint32_t meta = byte_of(m0, m1, c);
             if (meta == 0) continue;
-            float lx = fmaf((float)byte_of(qlx0, qlx1, c), scx, n0.x);
-            float ly = fmaf((float)byte_of(qly0, qly1, c), scy, n0.y);
-            float lz = fmaf((float)byte_of(qlz0, qlz1, c), scz, n0.z);
-            float hx = fmaf((float)byte_of(qhx0, qhx1, c), scx, n0.x);
-            float hy = fmaf((float)byte_of(qhy0, qhy1, c), scy, n0.y);
-            float hz = fmaf((float)byte_of(qhz0, qhz1, c), scz, n0.z);
-            float t0x = XMUL(XSUB(lx, s.ox), s.idx), t1x = XMUL(XSUB(hx, s.ox), s.idx);
-            float t0y = XMUL(XSUB(ly, s.oy), s.idy), t1y = XMUL(XSUB(hy, s.oy), s.idy);
-            float t0z = XMUL(XSUB(lz, s.oz), s.idz), t1z = XMUL(XSUB(hz, s.oz), s.idz);
-            float tn = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), s.tmin));
-            float tf = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), tcur));
+            float tnx = fmaf((float)byte_of(qnx0, qnx1, c), ax, bnx), tfx = fmaf((float)byte_of(qfx0, qfx1, c), ax, bfx);
+            float tny = fmaf((float)byte_of(qny0, qny1, c), ay, bny), tfy = fmaf((float)byte_of(qfy0, qfy1, c), ay, bfy);
+            float tnz = fmaf((float)byte_of(qnz0, qnz1, c), az, bnz), tfz = fmaf((float)byte_of(qfz0, qfz1, c), az, bfz);
+            float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, s.tmin));
+            float tf = fminf(fminf(tfx, tfy), fminf(tfz, tcur));
             if (tn <= XMUL(tf, grow)) {
                 if (imask & (1u << c)) ihits |= 1u << ((uint32_t)c ^ s.oct);
                 else thits |= (meta >> 5) << (meta & 31u);
