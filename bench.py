@@ -190,8 +190,9 @@ def reference_arm(args):
 
 
 def raycast_microbench(wl, torch, ctx, sc, scene, stream):
-    """2^24 coherent primary rays (4096 x 4096 view) and 2^24 cosine-distributed bounce rays from
-    the primary hit points; Mrays/s and traversal counts."""
+    """2^24 coherent primary rays (4096 x 4096 view), 2^24 cosine-distributed bounce rays from
+    the primary hit points and 2^24 any-hit shadow rays from the same points to uniform points of
+    random lights; Mrays/s and traversal counts."""
     n_side = 4096
     dev = torch.device("cuda")
     cam = {k: torch.tensor(np.asarray(scene.camera[k], np.float32), device=dev) for k in scene.camera}
@@ -210,15 +211,15 @@ def raycast_microbench(wl, torch, ctx, sc, scene, stream):
     rays[:, 7] = 1e30
     hits = torch.empty((n, 4), dtype=torch.float32, device=dev)
 
-    def timed(rbuf, reps=5):
+    def timed(rbuf, reps=5, mode=wl.CAST_CLOSEST):
         with torch.cuda.stream(stream):
-            sc.cast(rbuf.data_ptr(), hits.data_ptr(), n, wl.CAST_CLOSEST)
+            sc.cast(rbuf.data_ptr(), hits.data_ptr(), n, mode)
             torch.cuda.synchronize()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             for _ in range(reps):
-                sc.cast(rbuf.data_ptr(), hits.data_ptr(), n, wl.CAST_CLOSEST)
+                sc.cast(rbuf.data_ptr(), hits.data_ptr(), n, mode)
             e1.record(stream)
             torch.cuda.synchronize()
         return e0.elapsed_time(e1) / reps
@@ -257,10 +258,30 @@ def raycast_microbench(wl, torch, ctx, sc, scene, stream):
     brays[:, 7] = 1e30
     # rays whose primary missed become copies of primary rays (still 2^24 traced)
     brays = torch.where(ok[:, None], brays, rays)
+    # shadow rays (any hit) from the same surface points to a uniform point of a random light
+    nl = len(scene.lights)
+    li = torch.randint(0, nl, (n,), device=dev, generator=g)
+    first = torch.from_numpy(scene.lights["first_tri"].astype(np.int64)).to(dev)
+    count = torch.from_numpy(scene.lights["tri_count"].astype(np.int64)).to(dev)
+    lt = first[li] + (torch.rand(n, device=dev, generator=g) * count[li]).long().clamp_max(count[li] - 1)
+    s1 = torch.sqrt(torch.rand(n, device=dev, generator=g))[:, None]
+    s2 = torch.rand(n, device=dev, generator=g)[:, None]
+    la, lb, lc = V[I[lt, 0]], V[I[lt, 1]], V[I[lt, 2]]
+    lp = la * (1 - s1) + lb * (s1 * (1 - s2)) + lc * (s1 * s2)
+    sd = lp - brays[:, 0:3]
+    dist = torch.linalg.norm(sd, dim=1, keepdim=True).clamp_min(1e-6)
+    srays = torch.zeros_like(rays)
+    srays[:, 0:3] = brays[:, 0:3]
+    srays[:, 3] = 1e-3
+    srays[:, 4:7] = sd / dist
+    srays[:, 7] = (dist * (1 - 1e-3))[:, 0]
+    t_shadow = timed(srays, mode=wl.CAST_ANY)
+    nodes_s, tris_s = sc.cast_stats(srays.data_ptr(), n, wl.CAST_ANY)
     t_bounce = timed(brays)
     nodes_b, tris_b = sc.cast_stats(brays.data_ptr(), n)
     out = {}
-    for name, t, nn, tt in (("primary", t_primary, nodes_p, tris_p), ("bounce", t_bounce, nodes_b, tris_b)):
+    for name, t, nn, tt in (("primary", t_primary, nodes_p, tris_p), ("bounce", t_bounce, nodes_b, tris_b),
+                            ("shadow", t_shadow, nodes_s, tris_s)):
         nodes_per, tris_per = nn / n, tt / n
         bytes_per = 48 + 80 * nodes_per + 48 * tris_per
         out[name] = {"rays": n, "ms": round(t, 3), "mrays_s": round(n / t / 1e3, 1),
@@ -649,6 +670,8 @@ def main():
             "segments_per_path": round(seg_per_path, 3),
             "shadow_rays_per_path": round(tstats["shadow_rays"] / paths, 3),
             "extend_nodes_per_ray": round(nodes_per, 2), "extend_tris_per_ray": round(tris_per, 2),
+            "shadow_nodes_per_ray": round(tstats["shadow_node_visits"] / max(tstats["shadow_rays"], 1), 2),
+            "shadow_tris_per_ray": round(tstats["shadow_tri_tests"] / max(tstats["shadow_rays"], 1), 2),
             "bvh": {"wide_nodes": info["wide_nodes"], "depth": info["wide_depth"],
                     "build_ms": round(info["ms_build"], 1)},
             "gpu_launches": launches,

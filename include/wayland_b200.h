@@ -326,8 +326,9 @@ WL_API int wl_render_batch(wl_context *ctx, uint32_t n, wl_scene *const *scenes,
 /* ---- autotuner ---------------------------------------------------------------------- */
 /* No counterpart in the reference (OptiX chooses its own launch shapes). The launch shape of
  * the renders: paths in flight per wave (0 = automatic), and per traversal pass the persistent
- * CTAs per SM (0 = as many as fit) and the warp refill threshold (4, 6, 8, 12, 16 or 24 idle
- * lanes). */
+ * CTAs per SM (0 = as many as fit), the warp refill threshold (4, 6, 8, 12, 16 or 24 idle
+ * lanes) and the triangle-phase threshold (0..32; wl_cast_rays uses the extend pass's for
+ * closest hits and the shadow pass's for any hits). */
 typedef struct wl_tune_result {
     uint32_t wave_paths;
     uint32_t extend_ctas_per_sm, extend_refill;
@@ -336,12 +337,14 @@ typedef struct wl_tune_result {
     uint32_t spp;               /* samples per pixel of the wave-size renders */
     float ms_default;           /* wave-size render with the default shape */
     float ms_tuned;             /* wave-size render with the chosen shape */
+    uint32_t extend_postpone, shadow_postpone;  /* triangle phase when at least this many
+                                                   32nds of a warp's busy lanes hold triangles */
 } wl_tune_result;
 /* Times renders of (scene, camera, params with spp reduced) for candidate shapes by coordinate
  * descent and keeps the fastest in the context for later renders of every program: wave sizes
  * on renders of about 2^26 paths (two waves of the largest candidate, so that per-wave tails
- * weigh as in a long render), then the traversal launch shapes on renders of about 2^24 paths.
- * Path-tracer strategies only. */
+ * weigh as in a long render), then the traversal launch shapes and triangle-phase thresholds
+ * on renders of about 2^24 paths. Path-tracer strategies only. */
 WL_API int wl_autotune(wl_context *ctx, wl_scene *scene, const wl_camera *camera,
                        const wl_render_params *params, wl_tune_result *out);
 /* Sets the context's shape (as returned by wl_autotune); NULL restores the defaults. */

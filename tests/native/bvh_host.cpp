@@ -173,4 +173,86 @@ void hb_cast(void *p, const float *rays, uint32_t n, uint32_t mode, float *hits,
     stats[1] = ct;
 }
 
+// The batched traversal of the GPU kernels (trav_node / trav_tri with the warp's phase choice
+// and refill of idle lanes), played for one simulated 32-lane warp in lock step. post: the
+// triangle-phase threshold in 32nds of the busy lanes; refill: idle lanes that trigger a fetch.
+void hb_cast_batched(void *p, const float *rays, uint32_t n, uint32_t mode, uint32_t post,
+                     uint32_t refill, float *hits, uint64_t *stats) {
+    HostBvh *b = (HostBvh *)p;
+    const float4 *nodes = (const float4 *)b->nodes.data();
+    const float4 *tris = b->tris.data();
+    const bool any = mode == 1;
+    std::vector<TravState> st(32);
+    std::vector<uint2> stack(32 * (size_t)TRAV_STACK);
+    bool active[32] = {}, exhausted[32] = {}, has_t[32], can_n[32], fin[32];
+    uint32_t my[32] = {}, next = 0, cn = 0, ct = 0;
+    auto write = [&](uint32_t i, const TraceResult &r) {
+        uint32_t prim = r.prim;
+        if (any && prim != INVALID) prim = 0;
+        hits[4 * (size_t)i] = r.t;
+        hits[4 * (size_t)i + 1] = as_float(prim);
+        hits[4 * (size_t)i + 2] = r.u;
+        hits[4 * (size_t)i + 3] = r.v;
+    };
+    if (b->nodes.empty()) {
+        for (uint32_t i = 0; i < n; i++) write(i, TraceResult{rays[8 * (size_t)i + 7], 0.f, 0.f, INVALID});
+        stats[0] = stats[1] = 0;
+        return;
+    }
+    while (true) {
+        uint32_t idle = 0, busy = 0;
+        for (int l = 0; l < 32; l++) {
+            if (!active[l] && !exhausted[l]) idle |= 1u << l;
+            if (active[l]) busy |= 1u << l;
+        }
+        if (idle && ((uint32_t)__builtin_popcount(idle) >= refill || busy == 0)) {
+            for (int l = 0; l < 32; l++) {
+                if (!(idle & (1u << l))) continue;
+                if (next < n) {
+                    const float *r = rays + 8 * (size_t)next;
+                    trav_init(st[l], r[0], r[1], r[2], r[4], r[5], r[6], r[3], r[7]);
+                    my[l] = next++;
+                    active[l] = true;
+                    busy |= 1u << l;
+                } else {
+                    exhausted[l] = true;
+                }
+            }
+        }
+        if (busy == 0) break;
+        uint32_t nm = 0, tm = 0;
+        for (int l = 0; l < 32; l++) {
+            can_n[l] = active[l] && trav_can_node(st[l]);
+            has_t[l] = active[l] && st[l].tg.y != 0;
+            fin[l] = false;
+            nm |= (uint32_t)can_n[l] << l;
+            tm |= (uint32_t)has_t[l] << l;
+        }
+        const uint32_t need = (uint32_t)__builtin_popcount(busy) * post;
+        if (tm && (!nm || (uint32_t)__builtin_popcount(tm) * 32u >= need)) {
+            do {
+                tm = 0;
+                for (int l = 0; l < 32; l++) {
+                    if (has_t[l])
+                        fin[l] = any ? trav_tri<true, true>(st[l], tris, &ct)
+                                     : trav_tri<false, true>(st[l], tris, &ct);
+                    has_t[l] = has_t[l] && !fin[l] && st[l].tg.y != 0;
+                    tm |= (uint32_t)has_t[l] << l;
+                }
+            } while (tm && (!nm || (uint32_t)__builtin_popcount(tm) * 32u >= need));
+        } else {
+            for (int l = 0; l < 32; l++)
+                if (can_n[l]) trav_node<true>(st[l], stack.data() + (size_t)l * TRAV_STACK, nodes, &cn);
+        }
+        for (int l = 0; l < 32; l++) {
+            if (active[l] && (fin[l] || trav_done(st[l]))) {
+                write(my[l], st[l].res);
+                active[l] = false;
+            }
+        }
+    }
+    stats[0] = cn;
+    stats[1] = ct;
+}
+
 }  // extern "C"

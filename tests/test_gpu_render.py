@@ -215,13 +215,18 @@ def test_tuned_shapes_keep_the_image(ctx):
     p = wl.render_params(48, 32, 4, math=wl.MATH_STRICT)
     imgs = []
     for tune in (None, dict(wave_paths=1 << 12, extend_ctas_per_sm=4, extend_refill=8,
-                            shadow_ctas_per_sm=6, shadow_refill=24)):
+                            shadow_ctas_per_sm=6, shadow_refill=24, extend_postpone=0,
+                            shadow_postpone=32),
+                 dict(wave_paths=1 << 13, extend_ctas_per_sm=0, extend_refill=4,
+                      shadow_ctas_per_sm=0, shadow_refill=4, extend_postpone=32,
+                      shadow_postpone=0)):
         ctx.set_tune(tune)
         film = wl.Film(ctx, 48, 32)
         wl.render(ctx, s, sc.camera_struct(), p, film)
         imgs.append(film.download())
         film.close()
     assert np.array_equal(bits(imgs[0]), bits(imgs[1]))
+    assert np.array_equal(bits(imgs[0]), bits(imgs[2]))
     r = ctx.autotune(s, sc.camera_struct(), wl.render_params(48, 32, 64))
     assert r["candidates"] >= 40 and r["extend_refill"] in (4, 6, 8, 12, 16, 24)
     assert 0 < r["ms_tuned"] <= r["ms_default"] * 1.5

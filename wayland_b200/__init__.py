@@ -82,11 +82,14 @@ class Context:
         return {k: getattr(r, k) for k, _ in r._fields_}
 
     def set_tune(self, tune=None):
-        """wl_set_tune: a shape returned by autotune (dict), or None for the defaults."""
+        """wl_set_tune: a shape returned by autotune (dict), or None for the defaults (missing
+        triangle-phase thresholds default to 12)."""
         if tune is None:
             _abi.check("wl_set_tune", self.lib.wl_set_tune(self.handle, None))
             return
-        r = _abi.TuneResult(**{k: tune[k] for k, _ in _abi.TuneResult._fields_ if k in tune})
+        full = dict(extend_postpone=12, shadow_postpone=12)
+        full.update(tune)
+        r = _abi.TuneResult(**{k: full[k] for k, _ in _abi.TuneResult._fields_ if k in full})
         _abi.check("wl_set_tune", self.lib.wl_set_tune(self.handle, C.byref(r)))
 
     def debug_rng(self, rng, seed, d_pixels_ptr, npix, frame, count, d_out_ptr):

@@ -601,7 +601,8 @@ int wl_cast_rays(wl_scene *s, const wl_ray *d_rays, wl_hit *d_hits, uint32_t n, 
     ARG(d_rays && d_hits, "null ray or hit buffer");
     ARG(((uintptr_t)d_rays & 15) == 0 && ((uintptr_t)d_hits & 15) == 0, "buffers must be 16-byte aligned");
     CK(cudaSetDevice(s->ctx->device));
-    launch_cast(dev_scene(s), d_rays, d_hits, n, mode, s->ctx->d_misc, s->ctx->stream);
+    const TraceTune &tt = mode == WL_CAST_ANY ? s->ctx->tune_shadow : s->ctx->tune_extend;
+    launch_cast(dev_scene(s), d_rays, d_hits, n, mode, s->ctx->d_misc, tt.postpone, s->ctx->stream);
     CK(cudaGetLastError());
     return WL_OK;
 }
@@ -1538,6 +1539,19 @@ int wl_autotune(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_rende
             }
         t = bt;
     }
+    const uint32_t posts[] = {4u, 8u, 12u, 16u, 20u};
+    for (int pass = 0; pass < 2 && rc == WL_OK; pass++) {
+        TraceTune &t = pass == 0 ? c->tune_extend : c->tune_shadow;
+        TraceTune bt = t;
+        for (uint32_t pp : posts) {
+            if (rc != WL_OK || pp == bt.postpone) continue;
+            t.postpone = pp;
+            float ms = 0.f;
+            rc = timed(q, ms);
+            if (rc == WL_OK && ms < best) { best = ms; bt = t; }
+        }
+        t = bt;
+    }
     if (rc == WL_OK) rc = timed(qw, ms_tuned);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -1553,6 +1567,8 @@ int wl_autotune(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_rende
     out->extend_refill = c->tune_extend.refill;
     out->shadow_ctas_per_sm = c->tune_shadow.ctas_per_sm;
     out->shadow_refill = c->tune_shadow.refill;
+    out->extend_postpone = c->tune_extend.postpone;
+    out->shadow_postpone = c->tune_shadow.postpone;
     out->candidates = candidates;
     out->ms_default = ms_default;
     out->ms_tuned = ms_tuned;
@@ -1570,12 +1586,15 @@ int wl_set_tune(wl_context *c, const wl_tune_result *t) {
     }
     auto ok_refill = [](uint32_t r) { return r == 4 || r == 6 || r == 8 || r == 12 || r == 16 || r == 24; };
     ARG(ok_refill(t->extend_refill) && ok_refill(t->shadow_refill), "refill must be 4, 6, 8, 12, 16 or 24");
+    ARG(t->extend_postpone <= 32 && t->shadow_postpone <= 32, "postpone must be in [0, 32]");
     ARG(t->wave_paths == 0 || (t->wave_paths >= 1024 && t->wave_paths <= (1u << 26)), "wave_paths out of range");
     c->tune_wave = t->wave_paths;
     c->tune_extend.ctas_per_sm = t->extend_ctas_per_sm;
     c->tune_extend.refill = t->extend_refill;
     c->tune_shadow.ctas_per_sm = t->shadow_ctas_per_sm;
     c->tune_shadow.refill = t->shadow_refill;
+    c->tune_extend.postpone = t->extend_postpone;
+    c->tune_shadow.postpone = t->shadow_postpone;
     return WL_OK;
 }
 

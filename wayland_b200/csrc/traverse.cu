@@ -44,6 +44,31 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 // threads with dynamic fetch). Instantiated for R in {4, 6, 8, 12, 16, 24}; the autotuner picks
 // one.
 
+// One warp iteration of the batched traversal (trav_node / trav_tri): a triangle phase when the
+// lanes holding triangles are at least post/32 of the busy lanes (or no lane can visit a node),
+// kept up while that holds; otherwise a node phase. Returns true for a lane whose ray finished.
+template <bool ANY, bool STATS>
+__device__ __forceinline__ bool warp_trav(bool active, uint32_t busy, uint32_t post, TravState &st,
+                                          uint2 *stack, const float4 *__restrict__ nodes,
+                                          const float4 *__restrict__ tris, uint32_t &cn, uint32_t &ct) {
+    const bool can_n = active && trav_can_node(st);
+    bool has_t = active && st.tg.y != 0;
+    const uint32_t nm = __ballot_sync(0xffffffffu, can_n);
+    uint32_t tm = __ballot_sync(0xffffffffu, has_t);
+    const uint32_t need = (uint32_t)__popc(busy) * post;
+    bool fin = false;
+    if (tm && (!nm || (uint32_t)__popc(tm) * 32u >= need)) {
+        do {
+            if (has_t) fin = trav_tri<ANY, STATS>(st, tris, &ct);
+            has_t = has_t && !fin && st.tg.y != 0;
+            tm = __ballot_sync(0xffffffffu, has_t);
+        } while (tm && (!nm || (uint32_t)__popc(tm) * 32u >= need));
+    } else if (can_n) {
+        trav_node<STATS>(st, stack, nodes, &cn);
+    }
+    return active && (fin || trav_done(st));
+}
+
 // Persistent traversal over a queue of n rays. MODE 0: closest hit of ray queue `in`, hit
 // written to q.hit. MODE 1: any hit of the shadow queue; an unoccluded ray adds its light
 // sample to the path radiance. MODE 2: any hit of the bidirectional connection rays (passed as
@@ -51,7 +76,7 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 // (EvalContri's visibility ray, BDPT.cu:460-467).
 template <int MODE, bool STATS, int REFILL>
 __global__ void __launch_bounds__(TT) k_trace(DevScene sc, Queues q, int in, uint32_t *fetch,
-                                              BatchView bv) {
+                                              BatchView bv, uint32_t post) {
     constexpr bool ANY = MODE != 0;
     const uint32_t n = MODE == 0 ? q.counters[in] : q.counters[2];
     const float4 *ro = MODE == 0 ? q.ray_o[in] : q.sh_o;
@@ -89,7 +114,7 @@ __global__ void __launch_bounds__(TT) k_trace(DevScene sc, Queues q, int in, uin
             busy = __ballot_sync(0xffffffffu, active);
         }
         if (busy == 0) break;
-        if (active && trav_step<ANY, STATS>(st, stack, nodes, tris, &cn, &ct)) {
+        if (warp_trav<ANY, STATS>(active, busy, post, st, stack, nodes, tris, cn, ct)) {
             active = false;
             if (MODE == 0) {
                 q.hit[my] = make_float4(st.res.t, __uint_as_float(st.res.prim), st.res.u, st.res.v);
@@ -110,16 +135,16 @@ __global__ void __launch_bounds__(TT) k_trace(DevScene sc, Queues q, int in, uin
     if (STATS) add_stats(q.totals + (MODE == 0 ? 2 : 4), cn, ct);
 }
 
-// wl_cast_rays: the same persistent traversal over an array of 32-byte wl_ray records
+// wl_cast_rays: the same persistent batched traversal over an array of 32-byte wl_ray records
 // (refill threshold 12).
 constexpr int CAST_REFILL = 12;
 template <bool ANY>
 __global__ void __launch_bounds__(TT) k_cast(DevScene sc, const float4 *rays, float4 *hits,
-                                              uint32_t n, uint32_t *fetch) {
+                                              uint32_t n, uint32_t *fetch, uint32_t post) {
     const uint32_t lane = threadIdx.x & 31;
     TravState st;
     uint2 stack[TRAV_STACK];
-    uint32_t my = 0;
+    uint32_t my = 0, cn = 0, ct = 0;
     bool active = false, exhausted = false;
     while (true) {
         uint32_t idle = __ballot_sync(0xffffffffu, !active && !exhausted);
@@ -142,7 +167,7 @@ __global__ void __launch_bounds__(TT) k_cast(DevScene sc, const float4 *rays, fl
             busy = __ballot_sync(0xffffffffu, active);
         }
         if (busy == 0) break;
-        if (active && trav_step<ANY, false>(st, stack, sc.nodes, sc.tris, nullptr, nullptr)) {
+        if (warp_trav<ANY, false>(active, busy, post, st, stack, sc.nodes, sc.tris, cn, ct)) {
             active = false;
             uint32_t prim = st.res.prim;
             if (ANY && prim != INVALID) prim = 0;
@@ -204,7 +229,7 @@ int grid_for(const void *kernel, uint32_t ctas_per_sm = 0) {
 
 template <int MODE, bool STATS, int R>
 void trace_launch(const DevScene &sc, const Queues &q, int in, uint32_t *fetch, uint32_t ctas,
-                  const BatchView &bv, cudaStream_t s) {
+                  uint32_t post, const BatchView &bv, cudaStream_t s) {
     static int full = grid_for((const void *)k_trace<MODE, STATS, R>);
     int grid = full;
     if (ctas) {
@@ -213,19 +238,19 @@ void trace_launch(const DevScene &sc, const Queues &q, int in, uint32_t *fetch, 
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if ((int)ctas * sms < full) grid = (int)ctas * sms;
     }
-    k_trace<MODE, STATS, R><<<grid, TT, 0, s>>>(sc, q, in, fetch, bv);
+    k_trace<MODE, STATS, R><<<grid, TT, 0, s>>>(sc, q, in, fetch, bv, post);
 }
 
 template <int MODE, bool STATS>
 void trace_dispatch(const DevScene &sc, const Queues &q, int in, uint32_t *fetch, const TraceTune &t,
                     const BatchView &bv, cudaStream_t s) {
     switch (t.refill) {
-    case 4: trace_launch<MODE, STATS, 4>(sc, q, in, fetch, t.ctas_per_sm, bv, s); break;
-    case 6: trace_launch<MODE, STATS, 6>(sc, q, in, fetch, t.ctas_per_sm, bv, s); break;
-    case 8: trace_launch<MODE, STATS, 8>(sc, q, in, fetch, t.ctas_per_sm, bv, s); break;
-    case 16: trace_launch<MODE, STATS, 16>(sc, q, in, fetch, t.ctas_per_sm, bv, s); break;
-    case 24: trace_launch<MODE, STATS, 24>(sc, q, in, fetch, t.ctas_per_sm, bv, s); break;
-    default: trace_launch<MODE, STATS, 12>(sc, q, in, fetch, t.ctas_per_sm, bv, s); break;
+    case 4: trace_launch<MODE, STATS, 4>(sc, q, in, fetch, t.ctas_per_sm, t.postpone, bv, s); break;
+    case 6: trace_launch<MODE, STATS, 6>(sc, q, in, fetch, t.ctas_per_sm, t.postpone, bv, s); break;
+    case 8: trace_launch<MODE, STATS, 8>(sc, q, in, fetch, t.ctas_per_sm, t.postpone, bv, s); break;
+    case 16: trace_launch<MODE, STATS, 16>(sc, q, in, fetch, t.ctas_per_sm, t.postpone, bv, s); break;
+    case 24: trace_launch<MODE, STATS, 24>(sc, q, in, fetch, t.ctas_per_sm, t.postpone, bv, s); break;
+    default: trace_launch<MODE, STATS, 12>(sc, q, in, fetch, t.ctas_per_sm, t.postpone, bv, s); break;
     }
 }
 
@@ -262,7 +287,7 @@ void launch_connection_rays(const DevScene &sc, const Queues &q, const BdptWave 
 }
 
 void launch_cast(const DevScene &sc, const wl_ray *rays, wl_hit *hits, uint32_t n, uint32_t mode,
-                 uint32_t *fetch, cudaStream_t s) {
+                 uint32_t *fetch, uint32_t post, cudaStream_t s) {
     static int grid = grid_for((const void *)k_cast<false>);
     const float4 *r = reinterpret_cast<const float4 *>(rays);
     float4 *h = reinterpret_cast<float4 *>(hits);
@@ -271,8 +296,8 @@ void launch_cast(const DevScene &sc, const wl_ray *rays, wl_hit *hits, uint32_t 
         return;
     }
     cudaMemsetAsync(fetch, 0, sizeof(uint32_t), s);
-    if (mode == WL_CAST_ANY) k_cast<true><<<grid, TT, 0, s>>>(sc, r, h, n, fetch);
-    else k_cast<false><<<grid, TT, 0, s>>>(sc, r, h, n, fetch);
+    if (mode == WL_CAST_ANY) k_cast<true><<<grid, TT, 0, s>>>(sc, r, h, n, fetch, post);
+    else k_cast<false><<<grid, TT, 0, s>>>(sc, r, h, n, fetch, post);
 }
 
 void launch_cast_stats(const DevScene &sc, const wl_ray *rays, uint32_t n, uint32_t mode,

@@ -13,9 +13,9 @@
 //      nodes with 8-bit quantised child boxes, leaves of up to 3 triangles, children placed in
 //      slots by ray octant so that visiting slots in order (slot XOR octant) is near-to-far;
 //   5. traversal with a stack of node groups and the watertight triangle test of wl_math.cuh.
-// Child boxes decode exactly (the grid origin is a multiple of the power-of-two scale) and the
-// slab test keeps a relative margin of 2^-20, so a box never rejects a triangle the triangle
-// test accepts: closest hits equal the brute-force definition bit for bit.
+// The slab test widens every child box by a bound on its own rounding error (and the far
+// distance by a relative 2^-20), so a box never rejects a triangle the triangle test accepts:
+// closest hits equal the brute-force definition bit for bit.
 #pragma once
 #include "wl_math.cuh"
 
@@ -362,13 +362,14 @@ WL_HD uint32_t popcount(uint32_t x) {
 
 // Traversal state of one ray: the ray and its precomputed terms, the best hit so far, the
 // current node group (child base, internal hit bits in [24, 32) ordered by slot XOR octant,
-// imask in [0, 8)), the current triangle group (base, hit bits) and the stack depth.
+// imask in [0, 8)), the current triangle group (base, hit bits), a postponed triangle group
+// (batched traversal only; y = 0 when empty) and the stack depth.
 struct TravState {
     float ox, oy, oz, dx, dy, dz, idx, idy, idz, tmin, tmax;
     RayPre pre;
     uint32_t oct;
     TraceResult res;
-    uint2 ng, tg;
+    uint2 ng, tg, tq;
     int sp;
     bool ok;
 };
@@ -390,19 +391,90 @@ WL_HD void trav_init(TravState &s, float ox, float oy, float oz, float dx, float
     s.res.u = s.res.v = 0.f;
     s.ng = make_uint2(0u, (1u << (24 + s.oct)) | 1u);  // the root as the only child of a group
     s.tg = make_uint2(0u, 0u);
+    s.tq = make_uint2(0u, 0u);
     s.sp = 0;
     s.ok = true;
 }
 
+// Loads the node at np and tests the ray against its children's boxes. Returns the node's
+// group of hit internal children (child base; hit bits in [24, 32) ordered by slot XOR
+// octant; imask in [0, 8)) in ng and its group of hit triangles (triangle base, hit bits) in tg.
+WL_HD void node_test(const TravState &s, const float4 *__restrict__ np, uint2 &ng, uint2 &tg) {
+    float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3), n4 = ldg4(np + 4);
+    uint32_t ew = as_uint(n0.w);
+    float scx = as_float((ew & 0xffu) << 23), scy = as_float(((ew >> 8) & 0xffu) << 23),
+          scz = as_float(((ew >> 16) & 0xffu) << 23);
+    uint32_t imask = ew >> 24;
+    uint32_t m0 = as_uint(n1.z), m1 = as_uint(n1.w);
+    uint32_t qlx0 = as_uint(n2.x), qlx1 = as_uint(n2.y), qly0 = as_uint(n2.z), qly1 = as_uint(n2.w);
+    uint32_t qlz0 = as_uint(n3.x), qlz1 = as_uint(n3.y), qhx0 = as_uint(n3.z), qhx1 = as_uint(n3.w);
+    uint32_t qhy0 = as_uint(n4.x), qhy1 = as_uint(n4.y), qhz0 = as_uint(n4.z), qhz1 = as_uint(n4.w);
+    const float tcur = s.res.t;
+    const float grow = 1.0f + 0x1p-20f;
+    uint32_t ihits = 0, thits = 0;
+    // Slab distances in one FMA per plane: t = q A + B with A = scale / d (exact: power-of-two
+    // scale) and B = (origin - o) / d. The absolute error of such a t is below
+    // 3 u (255 |A| + |B|) (u = 2^-24: one rounding in origin - o, one in the product, one in
+    // the FMA). Each axis widens its own slab by e = 8 u (255 |A| + |B|): the entry plane
+    // (the low plane when d >= 0, the high plane when d < 0) uses B - e, the exit plane B + e,
+    // so the test never rejects a child whose triangle the triangle test accepts.
+    const float ax = XMUL(scx, s.idx), ay = XMUL(scy, s.idy), az = XMUL(scz, s.idz);
+    const float bx = XMUL(XSUB(n0.x, s.ox), s.idx), by = XMUL(XSUB(n0.y, s.oy), s.idy),
+                bz = XMUL(XSUB(n0.z, s.oz), s.idz);
+    const float ex = fmaf(fabsf(ax), 255.0f, fabsf(bx)) * 0x1p-21f;
+    const float ey = fmaf(fabsf(ay), 255.0f, fabsf(by)) * 0x1p-21f;
+    const float ez = fmaf(fabsf(az), 255.0f, fabsf(bz)) * 0x1p-21f;
+    const float bnx = bx - ex, bfx = bx + ex, bny = by - ey, bfy = by + ey, bnz = bz - ez, bfz = bz + ez;
+    const bool sx = s.oct & 1u, sy = s.oct & 2u, sz = s.oct & 4u;
+    const uint32_t qnx0 = sx ? qhx0 : qlx0, qnx1 = sx ? qhx1 : qlx1, qfx0 = sx ? qlx0 : qhx0, qfx1 = sx ? qlx1 : qhx1;
+    const uint32_t qny0 = sy ? qhy0 : qly0, qny1 = sy ? qhy1 : qly1, qfy0 = sy ? qly0 : qhy0, qfy1 = sy ? qly1 : qhy1;
+    const uint32_t qnz0 = sz ? qhz0 : qlz0, qnz1 = sz ? qhz1 : qlz1, qfz0 = sz ? qlz0 : qhz0, qfz1 = sz ? qlz1 : qhz1;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        uint32_t meta = byte_of(m0, m1, c);
+        if (meta == 0) continue;
+        float tnx = fmaf((float)byte_of(qnx0, qnx1, c), ax, bnx), tfx = fmaf((float)byte_of(qfx0, qfx1, c), ax, bfx);
+        float tny = fmaf((float)byte_of(qny0, qny1, c), ay, bny), tfy = fmaf((float)byte_of(qfy0, qfy1, c), ay, bfy);
+        float tnz = fmaf((float)byte_of(qnz0, qnz1, c), az, bnz), tfz = fmaf((float)byte_of(qfz0, qfz1, c), az, bfz);
+        float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, s.tmin));
+        float tf = fminf(fminf(tfx, tfy), fminf(tfz, tcur));
+        if (tn <= XMUL(tf, grow)) {
+            if (imask & (1u << c)) ihits |= 1u << ((uint32_t)c ^ s.oct);
+            else thits |= (meta >> 5) << (meta & 31u);
+        }
+    }
+    ng = make_uint2(as_uint(n1.x), (ihits << 24) | imask);
+    tg = make_uint2(as_uint(n1.y), thits);
+}
+
+// Tests the lowest pending triangle of s.tg (and removes it from the group). Returns true for
+// an any-hit (ANY) or when the triangle becomes the closest hit so far.
+template <bool ANY>
+WL_HD bool tri_test_next(TravState &s, const float4 *__restrict__ tris) {
+    int k = lowest_bit(s.tg.y);
+    s.tg.y &= s.tg.y - 1u;
+    const float4 *tp = tris + 3 * (size_t)(s.tg.x + (uint32_t)k);
+    float4 v0 = ldg4(tp), v1 = ldg4(tp + 1), v2 = ldg4(tp + 2);
+    float t, u, v;
+    if (tri_hit(s.pre, s.ox, s.oy, s.oz, v0, v1, v2, s.tmin, s.tmax, t, u, v)) {
+        uint32_t prim = as_uint(v0.w);
+        if (ANY || t < s.res.t || (t == s.res.t && prim < s.res.prim)) {
+            s.res.t = t;
+            s.res.prim = prim;
+            s.res.u = u;
+            s.res.v = v;
+            return true;
+        }
+    }
+    return false;
+}
+
 // One step: visit the nearest pending child node (if the current group has one), test the
 // triangles of its hit leaves, and pop the stack when the group is exhausted. Returns true when
-// the ray is finished (stack empty, or an any-hit found). The box test decodes child bounds
-// exactly (grid origin = multiple of the power-of-two scale) and keeps a relative margin of
-// 2^-20, so it never rejects a triangle the triangle test accepts.
+// the ray is finished (stack empty, or an any-hit found).
 template <bool ANY, bool STATS>
 WL_HD bool trav_step(TravState &s, uint2 *stack, const float4 *__restrict__ nodes,
                      const float4 *__restrict__ tris, uint32_t *n_nodes, uint32_t *n_tris) {
-    const float grow = 1.0f + 0x1p-20f;
     if (s.ng.y & 0xff000000u) {
         int k = lowest_bit(s.ng.y >> 24);
         s.ng.y &= ~(1u << (24 + k));
@@ -412,83 +484,72 @@ WL_HD bool trav_step(TravState &s, uint2 *stack, const float4 *__restrict__ node
             if (s.sp < TRAV_STACK) stack[s.sp++] = s.ng;
             else s.ok = false;
         }
-        const float4 *np = nodes + 5 * (size_t)node;
-        float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3),
-               n4 = ldg4(np + 4);
         if (STATS) (*n_nodes)++;
-        uint32_t ew = as_uint(n0.w);
-        float scx = as_float((ew & 0xffu) << 23), scy = as_float(((ew >> 8) & 0xffu) << 23),
-              scz = as_float(((ew >> 16) & 0xffu) << 23);
-        uint32_t imask = ew >> 24;
-        uint32_t m0 = as_uint(n1.z), m1 = as_uint(n1.w);
-        uint32_t qlx0 = as_uint(n2.x), qlx1 = as_uint(n2.y), qly0 = as_uint(n2.z), qly1 = as_uint(n2.w);
-        uint32_t qlz0 = as_uint(n3.x), qlz1 = as_uint(n3.y), qhx0 = as_uint(n3.z), qhx1 = as_uint(n3.w);
-        uint32_t qhy0 = as_uint(n4.x), qhy1 = as_uint(n4.y), qhz0 = as_uint(n4.z), qhz1 = as_uint(n4.w);
-        const float tcur = s.res.t;
-        uint32_t ihits = 0, thits = 0;
-        // Slab distances in one FMA per plane: t = q A + B with A = scale / d (exact: power-of-two
-        // scale) and B = (origin - o) / d. The absolute error of such a t is below
-        // 3 u (255 |A| + |B|) (u = 2^-24: one rounding in origin - o, one in the product, one in
-        // the FMA). Each axis widens its own slab by e = 8 u (255 |A| + |B|): the entry plane
-        // (the low plane when d >= 0, the high plane when d < 0) uses B - e, the exit plane B + e,
-        // so the test never rejects a child whose triangle the triangle test accepts.
-        const float ax = XMUL(scx, s.idx), ay = XMUL(scy, s.idy), az = XMUL(scz, s.idz);
-        const float bx = XMUL(XSUB(n0.x, s.ox), s.idx), by = XMUL(XSUB(n0.y, s.oy), s.idy),
-                    bz = XMUL(XSUB(n0.z, s.oz), s.idz);
-        const float ex = fmaf(fabsf(ax), 255.0f, fabsf(bx)) * 0x1p-21f;
-        const float ey = fmaf(fabsf(ay), 255.0f, fabsf(by)) * 0x1p-21f;
-        const float ez = fmaf(fabsf(az), 255.0f, fabsf(bz)) * 0x1p-21f;
-        const float bnx = bx - ex, bfx = bx + ex, bny = by - ey, bfy = by + ey, bnz = bz - ez, bfz = bz + ez;
-        const bool sx = s.oct & 1u, sy = s.oct & 2u, sz = s.oct & 4u;
-        const uint32_t qnx0 = sx ? qhx0 : qlx0, qnx1 = sx ? qhx1 : qlx1, qfx0 = sx ? qlx0 : qhx0, qfx1 = sx ? qlx1 : qhx1;
-        const uint32_t qny0 = sy ? qhy0 : qly0, qny1 = sy ? qhy1 : qly1, qfy0 = sy ? qly0 : qhy0, qfy1 = sy ? qly1 : qhy1;
-        const uint32_t qnz0 = sz ? qhz0 : qlz0, qnz1 = sz ? qhz1 : qlz1, qfz0 = sz ? qlz0 : qhz0, qfz1 = sz ? qlz1 : qhz1;
-#pragma unroll
-        for (int c = 0; c < 8; c++) {
-            uint32_t meta = byte_of(m0, m1, c);
-            if (meta == 0) continue;
-            float tnx = fmaf((float)byte_of(qnx0, qnx1, c), ax, bnx), tfx = fmaf((float)byte_of(qfx0, qfx1, c), ax, bfx);
-            float tny = fmaf((float)byte_of(qny0, qny1, c), ay, bny), tfy = fmaf((float)byte_of(qfy0, qfy1, c), ay, bfy);
-            float tnz = fmaf((float)byte_of(qnz0, qnz1, c), az, bnz), tfz = fmaf((float)byte_of(qfz0, qfz1, c), az, bfz);
-            float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, s.tmin));
-            float tf = fminf(fminf(tfx, tfy), fminf(tfz, tcur));
-            if (tn <= XMUL(tf, grow)) {
-                if (imask & (1u << c)) ihits |= 1u << ((uint32_t)c ^ s.oct);
-                else thits |= (meta >> 5) << (meta & 31u);
-            }
-        }
-        s.ng = make_uint2(as_uint(n1.x), (ihits << 24) | imask);
-        s.tg = make_uint2(as_uint(n1.y), thits);
+        node_test(s, nodes + 5 * (size_t)node, s.ng, s.tg);
     }
     while (s.tg.y) {
-        int k = lowest_bit(s.tg.y);
-        s.tg.y &= s.tg.y - 1u;
-        const float4 *tp = tris + 3 * (size_t)(s.tg.x + (uint32_t)k);
-        float4 v0 = ldg4(tp), v1 = ldg4(tp + 1), v2 = ldg4(tp + 2);
         if (STATS) (*n_tris)++;
-        float t, u, v;
-        if (tri_hit(s.pre, s.ox, s.oy, s.oz, v0, v1, v2, s.tmin, s.tmax, t, u, v)) {
-            uint32_t prim = as_uint(v0.w);
-            if (ANY) {
-                s.res.t = t;
-                s.res.prim = prim;
-                s.res.u = u;
-                s.res.v = v;
-                return true;
-            }
-            if (t < s.res.t || (t == s.res.t && prim < s.res.prim)) {
-                s.res.t = t;
-                s.res.prim = prim;
-                s.res.u = u;
-                s.res.v = v;
-            }
-        }
+        if (tri_test_next<ANY>(s, tris) && ANY) return true;
     }
     if (!(s.ng.y & 0xff000000u)) {
         if (s.sp == 0) return true;
         s.ng = stack[--s.sp];
     }
     return false;
+}
+
+// Batched traversal (the postponed-triangle scheme of Ylitie, Karras and Laine 2017): a warp
+// alternates node phases, in which every lane that can visits one node, and triangle phases,
+// in which every lane holding triangles tests one. A lane that reaches a leaf while it still
+// holds untested triangles parks the new triangle group in s.tq and stops visiting nodes until
+// a triangle phase has emptied s.tg; the warp chooses the phase from how many lanes hold
+// triangles. The stack holds node groups only, bounded by the tree depth as in trav_step.
+// Closest hits are the same, since culling by the current hit distance only drops triangles
+// that cannot become the closest hit.
+
+// Whether the lane can take a node step: it has a pending child or a stack entry, and no
+// postponed triangle group.
+WL_HD bool trav_can_node(const TravState &s) {
+    return ((s.ng.y & 0xff000000u) || s.sp > 0) && s.tq.y == 0;
+}
+// Whether the ray is finished (no pending child, stack entry or triangle).
+WL_HD bool trav_done(const TravState &s) {
+    return !(s.ng.y & 0xff000000u) && s.sp == 0 && s.tg.y == 0;
+}
+
+// Node step (requires trav_can_node): pop the stack when the current group is exhausted, then
+// visit the group's nearest pending child.
+template <bool STATS>
+WL_HD void trav_node(TravState &s, uint2 *stack, const float4 *__restrict__ nodes, uint32_t *n_nodes) {
+    if (!(s.ng.y & 0xff000000u)) s.ng = stack[--s.sp];
+    int k = lowest_bit(s.ng.y >> 24);
+    s.ng.y &= ~(1u << (24 + k));
+    uint32_t slot = (uint32_t)k ^ s.oct;
+    uint32_t node = s.ng.x + popcount(s.ng.y & 0xffu & ((1u << slot) - 1u));
+    if (s.ng.y & 0xff000000u) {
+        if (s.sp < TRAV_STACK) stack[s.sp++] = s.ng;
+        else s.ok = false;
+    }
+    if (STATS) (*n_nodes)++;
+    uint2 tg;
+    node_test(s, nodes + 5 * (size_t)node, s.ng, tg);
+    if (tg.y) {
+        if (s.tg.y == 0) s.tg = tg;
+        else s.tq = tg;
+    }
+}
+
+// Triangle step (requires s.tg.y != 0): test one triangle; an emptied group takes the postponed
+// one. Returns true for an any-hit (ANY).
+template <bool ANY, bool STATS>
+WL_HD bool trav_tri(TravState &s, const float4 *__restrict__ tris, uint32_t *n_tris) {
+    if (STATS) (*n_tris)++;
+    const bool hit = tri_test_next<ANY>(s, tris);
+    if (s.tg.y == 0) {
+        s.tg = s.tq;
+        s.tq.y = 0;
+    }
+    return ANY && hit;
 }
 
 // ANY: stop at the first hit (shadow rays). STATS: count node visits and triangle tests.

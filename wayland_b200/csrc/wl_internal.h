@@ -247,6 +247,7 @@ void launch_debug_rng(uint32_t rng, uint64_t seed, const uint32_t *pixels, uint3
 struct TraceTune {
     uint32_t ctas_per_sm = 0;
     uint32_t refill = 12;
+    uint32_t postpone = 12;  // triangle phase when >= postpone/32 of the busy lanes hold triangles
 };
 void launch_extend(const DevScene &sc, const Queues &q, int in, bool stats, cudaStream_t s,
                    const TraceTune &t = TraceTune{}, const BatchView &bv = BatchView{});
@@ -255,7 +256,7 @@ void launch_shadow(const DevScene &sc, const Queues &q, bool stats, cudaStream_t
 void launch_connection_rays(const DevScene &sc, const Queues &q, const BdptWave &bw, bool stats,
                             cudaStream_t s, const TraceTune &t = TraceTune{});
 void launch_cast(const DevScene &sc, const wl_ray *rays, wl_hit *hits, uint32_t n, uint32_t mode,
-                 uint32_t *fetch, cudaStream_t s);
+                 uint32_t *fetch, uint32_t postpone, cudaStream_t s);
 void launch_cast_stats(const DevScene &sc, const wl_ray *rays, uint32_t n, uint32_t mode,
                        unsigned long long *counts, uint32_t *fetch, cudaStream_t s);
 
