@@ -11,6 +11,9 @@ namespace wl {
 namespace {
 
 constexpr int TT = 128;
+// 8 resident CTAs of 128 threads per SM: caps the traversal kernels at 64 registers, which
+// measured faster than the 72 they take uncapped (more warps to hide node-fetch latency).
+constexpr int TRACE_MIN_CTAS = 8;
 
 // Work is fetched per warp from an atomic counter, 32 rays at a time, so that warps that finish
 // early take more rays (persistent threads, Aila & Laine 2009).
@@ -75,7 +78,7 @@ __device__ __forceinline__ bool warp_trav(bool active, uint32_t busy, uint32_t p
 // the shadow queue); an unoccluded ray stores its value as the result of its connection
 // (EvalContri's visibility ray, BDPT.cu:460-467).
 template <int MODE, bool STATS, int REFILL>
-__global__ void __launch_bounds__(TT) k_trace(DevScene sc, Queues q, int in, uint32_t *fetch,
+__global__ void __launch_bounds__(TT, TRACE_MIN_CTAS) k_trace(DevScene sc, Queues q, int in, uint32_t *fetch,
                                               BatchView bv, uint32_t post) {
     constexpr bool ANY = MODE != 0;
     const uint32_t n = MODE == 0 ? q.counters[in] : q.counters[2];
@@ -139,7 +142,7 @@ __global__ void __launch_bounds__(TT) k_trace(DevScene sc, Queues q, int in, uin
 // (refill threshold 12).
 constexpr int CAST_REFILL = 12;
 template <bool ANY>
-__global__ void __launch_bounds__(TT) k_cast(DevScene sc, const float4 *rays, float4 *hits,
+__global__ void __launch_bounds__(TT, TRACE_MIN_CTAS) k_cast(DevScene sc, const float4 *rays, float4 *hits,
                                               uint32_t n, uint32_t *fetch, uint32_t post) {
     const uint32_t lane = threadIdx.x & 31;
     TravState st;
