@@ -32,6 +32,9 @@ EXTEND_DRAM_BYTES_PER_LAUNCH = 221.2e6
 WORKLOAD = "plain PT at scale: displaced icosphere 1,997,120 tris + ground, 4 quad lights + env 0.1, 1920x1080, 64 spp, depth 16, FP32"
 
 
+# BVH build used for every scene (set from --bvh)
+BVH_KIND = [1]
+
 def env_int(k, d):
     try:
         return int(os.environ.get(k, d))
@@ -324,7 +327,7 @@ def batch_leg(wl, torch, ctx, stream, jobs=64):
     and as one wl_render_batch. Device time; Mpaths/s = all jobs' W x H x spp / time."""
     from wayland_b200 import scenes
     datas = [scenes.batch_scene(i) for i in range(jobs)]
-    objs = [wl.Scene(ctx, d) for d in datas]
+    objs = [wl.Scene(ctx, d, bvh_kind=BVH_KIND[0]) for d in datas]
     params = [wl.render_params(d.width, d.height, d.spp, max_depth=d.max_depth) for d in datas]
     cams = [d.camera_struct() for d in datas]
     paths = sum(d.width * d.height * d.spp for d in datas)
@@ -360,7 +363,7 @@ def bdpt_ao_leg(wl, torch, ctx, res=512, spp=256, oracle_spp=4096, ao_res=(512, 
     2^24 rays). Device time with CUDA events on the library's stream."""
     from wayland_b200 import scenes
     sc = scenes.glass_sphere(res, res)
-    scene = wl.Scene(ctx, sc)
+    scene = wl.Scene(ctx, sc, bvh_kind=BVH_KIND[0])
     cam = sc.camera_struct()
     stream = torch.cuda.ExternalStream(ctx.stream)
     e0 = torch.cuda.Event(enable_timing=True)
@@ -428,7 +431,7 @@ def nrc_convergence(wl, torch, ctx, res=(480, 270), oracle_spp=16384, target=1e-
     from wayland_b200 import scenes
     W_, H_ = res
     sc = scenes.door_slit_room(W_, H_)
-    scene = wl.Scene(ctx, sc)
+    scene = wl.Scene(ctx, sc, bvh_kind=BVH_KIND[0])
     cam = sc.camera_struct()
     stream = torch.cuda.ExternalStream(ctx.stream)
     # oracle: FP64 film, plain path tracer, fast math
@@ -526,10 +529,13 @@ def main():
     ap.add_argument("--nrc-res", default="960x540", help="resolution of the radiance-cache comparison")
     ap.add_argument("--nrc-oracle-spp", type=int, default=8192)
     ap.add_argument("--nrc-budget-s", type=float, default=60.0)
+    ap.add_argument("--bvh", default="sah", choices=["sah", "lbvh"],
+                    help="BVH build of every scene: binned SAH (default) or Morton LBVH")
     ap.add_argument("--case", default="full", choices=["full", "small"],
                     help="small: the same 2M-triangle scene at 960x540 x 4 spp (for ncu captures)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    BVH_KIND[0] = 1 if args.bvh == "sah" else 0  # wl.BVH_SAH / wl.BVH_LBVH
     if args.impl == "reference":
         return reference_arm(args)
     global W, H, SPP
@@ -565,7 +571,7 @@ def main():
     if args.case == "small":
         scene.camera = scenes.pinhole((0.0, 0.6, 4.2), (0.0, -0.2, 0.0), (0, 1, 0), 40.0, W, H)
     ctx = wl.Context(local)
-    sc = wl.Scene(ctx, scene)
+    sc = wl.Scene(ctx, scene, bvh_kind=BVH_KIND[0])
     info = sc.info()
     film = wl.Film(ctx, W, H)
     stream = torch.cuda.ExternalStream(ctx.stream)
@@ -672,7 +678,8 @@ def main():
             "extend_nodes_per_ray": round(nodes_per, 2), "extend_tris_per_ray": round(tris_per, 2),
             "shadow_nodes_per_ray": round(tstats["shadow_node_visits"] / max(tstats["shadow_rays"], 1), 2),
             "shadow_tris_per_ray": round(tstats["shadow_tri_tests"] / max(tstats["shadow_rays"], 1), 2),
-            "bvh": {"wide_nodes": info["wide_nodes"], "depth": info["wide_depth"],
+            "bvh": {"kind": "binned SAH" if BVH_KIND[0] == 1 else "LBVH",
+                    "wide_nodes": info["wide_nodes"], "depth": info["wide_depth"],
                     "build_ms": round(info["ms_build"], 1)},
             "gpu_launches": launches,
             "autotune": tune,

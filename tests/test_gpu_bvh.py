@@ -134,3 +134,79 @@ def test_full_size_properties(ctx, oracle):
     ob = oracle.bvh(s.V, s.I)
     assert hits_equal(cast_device(ctx, sc, rays, wl.CAST_CLOSEST), ob.cast(rays, 0))
     sc.close()
+
+
+def check_binary_tree(sp, left, right, parent, bounds, n):
+    """A valid binary BVH in the Karras layout: leaves n-1+p over a permutation of the triangles,
+    every node but the root 0 the child of exactly one parent, and every internal node's box
+    (and triangle count) the union (sum) of its children's."""
+    assert np.array_equal(np.sort(sp), np.arange(n, dtype=np.uint32))
+    if n == 1:
+        return
+    kids = np.concatenate([left, right])
+    assert np.array_equal(np.sort(kids), np.arange(1, 2 * n - 1))
+    assert parent[0] == -1
+    idx = np.arange(n - 1)
+    assert np.array_equal(parent[left], idx) and np.array_equal(parent[right], idx)
+    b = bounds.reshape(-1, 6)
+    lo = np.minimum(b[left, :3], b[right, :3])
+    hi = np.maximum(b[left, 3:], b[right, 3:])
+    assert np.array_equal(b[:n - 1, :3], lo) and np.array_equal(b[:n - 1, 3:], hi)
+
+
+@pytest.mark.parametrize("name,V,I", GEOMS, ids=[g[0] for g in GEOMS])
+def test_sah_build_and_cast(ctx, oracle, name, V, I):
+    """Binned-SAH build: a valid binary tree over a permutation of the triangles (including
+    coincident centroids, flat and degenerate triangles), the same Morton codes as the LBVH, and
+    closest hits bit-exact against brute force with any-hit occlusion identical."""
+    g = Geo(V, I)
+    sc = wl.Scene(ctx, g, bvh_kind=wl.BVH_SAH)
+    assert sc.info()["kind"] == wl.BVH_SAH
+    assert np.array_equal(sc.export_morton(), oracle.morton63(g.V, g.I))
+    check_binary_tree(*sc.export_binary(), len(g.I))
+    rays = np.concatenate([random_rays(6000, 21), axis_rays(2000, 22)])
+    if name == "cornell":
+        rays["org"] = np.random.default_rng(4).uniform(0.01, 0.99, (len(rays), 3))
+    assert hits_equal(cast_device(ctx, sc, rays, wl.CAST_CLOSEST), oracle.cast_bruteforce(g.V, g.I, rays, 0))
+    anyr = oracle.cast_bruteforce(g.V, g.I, rays, 1)
+    anyg = cast_device(ctx, sc, rays, wl.CAST_ANY)
+    assert np.array_equal(anyg["prim"] == wl.INVALID, anyr["prim"] == wl.INVALID)
+    sc.close()
+
+
+@pytest.mark.parametrize("n", [2, 3, 32, 33, 34, 65, 2049, 5000])
+def test_sah_sizes(ctx, oracle, n):
+    """Triangle counts around the small-node limit (32) and the binning chunk (2048)."""
+    V, I = scenes.random_triangles(n, 100 + n)
+    g = Geo(V, I)
+    sc = wl.Scene(ctx, g, bvh_kind=wl.BVH_SAH)
+    check_binary_tree(*sc.export_binary(), n)
+    rays = random_rays(3000, 7 + n)
+    assert hits_equal(cast_device(ctx, sc, rays, wl.CAST_CLOSEST), oracle.cast_bruteforce(g.V, g.I, rays, 0))
+    sc.close()
+
+
+def test_sah_full_size(ctx, oracle):
+    """The benchmark's 2M-triangle scene with the SAH build: a valid tree, the same tree on a
+    second build (deterministic), fewer node visits than the LBVH for the same rays, and a ray
+    batch bit-exact against the oracle's CPU BVH."""
+    s = scenes.displaced_sphere()
+    n = s.num_tris
+    sc = wl.Scene(ctx, s, bvh_kind=wl.BVH_SAH)
+    t1 = sc.export_binary()
+    check_binary_tree(*t1, n)
+    sc.build_bvh(wl.BVH_SAH)
+    t2 = sc.export_binary()
+    for a, b in zip(t1, t2):
+        assert np.array_equal(np.asarray(a).view(np.uint8), np.asarray(b).view(np.uint8))
+    assert sc.info()["wide_depth"] <= 64
+    rays = random_rays(20000, 41, -3.0, 3.0)
+    ob = oracle.bvh(s.V, s.I)
+    assert hits_equal(cast_device(ctx, sc, rays, wl.CAST_CLOSEST), ob.cast(rays, 0))
+    d_r = dev(rays)
+    nodes_sah, _ = sc.cast_stats(d_r.data_ptr(), len(rays))
+    lb = wl.Scene(ctx, s)
+    nodes_lbvh, _ = lb.cast_stats(d_r.data_ptr(), len(rays))
+    assert nodes_sah < nodes_lbvh
+    lb.close()
+    sc.close()

@@ -524,7 +524,7 @@ int wl_scene_add_texture(wl_scene *s, const uint8_t *rgba8, uint32_t w, uint32_t
 // ---------------------------------------------------------------------------------------
 int wl_bvh_build(wl_scene *s, uint32_t kind) {
     ARG(s, "null scene");
-    ARG(kind == WL_BVH_LBVH, "only WL_BVH_LBVH is available");
+    ARG(kind == WL_BVH_LBVH || kind == WL_BVH_SAH, "kind must be WL_BVH_LBVH or WL_BVH_SAH");
     CK(cudaSetDevice(s->ctx->device));
     bvh_free(s->bvh);
     s->built = false;
@@ -532,7 +532,7 @@ int wl_bvh_build(wl_scene *s, uint32_t kind) {
     s->bvh.I = s->d_I;
     s->bvh.nT = s->nT;
     std::string err;
-    int rc = bvh_build_lbvh(s->bvh, s->ctx->stream, err);
+    int rc = bvh_build(s->bvh, kind, s->ctx->stream, err);
     if (rc != WL_OK) {
         bvh_free(s->bvh);
         return fail(rc, "bvh build: " + err);

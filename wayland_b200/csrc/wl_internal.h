@@ -276,7 +276,9 @@ struct BvhBuild {
     uint32_t wide_nodes, wide_depth;
     float ms;
 };
-int bvh_build_lbvh(BvhBuild &b, cudaStream_t s, std::string &err);
+// kind: WL_BVH_LBVH (Karras radix tree) or WL_BVH_SAH (binned SAH); both end in the same
+// bottom-up bounds and 8-wide collapse.
+int bvh_build(BvhBuild &b, uint32_t kind, cudaStream_t s, std::string &err);
 void bvh_free(BvhBuild &b);
 
 // nrc.cu
