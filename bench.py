@@ -28,7 +28,10 @@ sys.path.insert(0, ROOT)
 
 W, H, SPP, DEPTH = 1920, 1080, 64, 16
 METRIC = "Mpaths/s"
-EXTEND_DRAM_BYTES_PER_LAUNCH = 221.2e6
+# DRAM bytes (read + write) per extend ray of this workload: 759.9 MB per launch on average over
+# the 64 extend launches of one step (4 waves of 2^25 paths) in the ncu launch list of
+# profiles/launches_plain_pt_displaced_sphere_1920x1080x64spp.md, / 298.3 M rays per step / 64
+EXTEND_DRAM_BYTES_PER_RAY = 163.0
 WORKLOAD = "plain PT at scale: displaced icosphere 1,997,120 tris + ground, 4 quad lights + env 0.1, 1920x1080, 64 spp, depth 16, FP32"
 
 
@@ -529,6 +532,8 @@ def main():
     ap.add_argument("--nrc-res", default="960x540", help="resolution of the radiance-cache comparison")
     ap.add_argument("--nrc-oracle-spp", type=int, default=8192)
     ap.add_argument("--nrc-budget-s", type=float, default=60.0)
+    ap.add_argument("--tune", default=None,
+                    help="fixed launch shape as JSON (wl_set_tune fields) instead of the autotuner")
     ap.add_argument("--bvh", default="sah", choices=["sah", "lbvh"],
                     help="BVH build of every scene: binned SAH (default) or Morton LBVH")
     ap.add_argument("--case", default="full", choices=["full", "small"],
@@ -589,7 +594,11 @@ def main():
 
     # launch shapes (paths per wave, traversal CTAs per SM and refill threshold) chosen by the
     # project's autotuner on this scene, outside the timed region
-    tune = None if args.no_autotune else ctx.autotune(sc, cam, params)
+    if args.tune:
+        ctx.set_tune(json.loads(args.tune))
+        tune = dict(json.loads(args.tune), fixed=True)
+    else:
+        tune = None if args.no_autotune else ctx.autotune(sc, cam, params)
     for _ in range(args.warmup):
         wl.render(ctx, sc, cam, params, film)
     ctx.sync()
@@ -605,11 +614,13 @@ def main():
     clocks.start()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed")  # the window a profiler can select (--nvtx-include timed/)
     e0.record(stream)
     for _ in range(args.steps):
         wl.render(ctx, sc, cam, params, film)
     e1.record(stream)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     barrier()
     clk = clocks.stop()
     # per-kernel device times of the last timed render (CUDA events the library records around
@@ -648,9 +659,10 @@ def main():
         b_ray = 48 + 80 * nodes_per + 48 * tris_per
         achieved = segs * b_ray / (ext_ms * 1e-3) / 1e9
         b_path = 96 + 364 * seg_per_path
-        # DRAM bytes (read + write) per extend launch of this workload, from the ncu launch list
-        # in profiles/launches_plain_pt_displaced_sphere_1920x1080x64spp.md
-        traffic = EXTEND_DRAM_BYTES_PER_LAUNCH if args.case == "full" else None
+        # DRAM bytes per extend launch: the profiled bytes per ray x this run's rays per extend
+        # launch (a wave launches generate and film once and extend, shade, shadow per bounce)
+        ext_launches = max((st["kernel_launches"] - 2 * st["waves"]) // 3, 1)
+        traffic = round(EXTEND_DRAM_BYTES_PER_RAY * segs / ext_launches) if args.case == "full" else None
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 2),
@@ -667,6 +679,7 @@ def main():
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "peak_kind": peak_kind,
                          "bytes_per_ray": round(b_ray, 1),
+                         "algorithmic_bytes_per_launch": round(segs * b_ray / ext_launches),
                          "note": "algorithmic bytes = rays x (48 + 80 N_node + 48 N_tri); BVH nodes are mostly L2 hits, so DRAM traffic is far below this"},
             "roofline_path": {"bytes_per_path": round(b_path, 1),
                               "achieved_gbs": round(b_path * value * 1e6 / world / 1e9, 1),

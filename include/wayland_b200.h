@@ -241,7 +241,11 @@ WL_API int wl_scene_add_texture(wl_scene *scene, const uint8_t *rgba8, uint32_t 
 /* ---- acceleration structure -------------------------------------------------------- */
 /* StaticAccelStructure (AccelStructure.cpp:133-162): build the BVH of the scene on the GPU.
  * WL_BVH_LBVH: 63-bit Morton codes -> radix tree (Karras 2012) -> bottom-up refit ->
- *              8-wide compressed BVH. WL_BVH_SAH: binned-SAH top levels over the same. */
+ *              8-wide compressed BVH.
+ * WL_BVH_SAH:  the same Morton order split top down by binned SAH (Wald 2007, 16 bins per
+ *              axis; subtrees of <= 32 triangles one thread each) -> the same refit and
+ *              collapse. Slower to build (about 4x), faster to trace. Both builds are
+ *              deterministic. */
 WL_API int wl_bvh_build(wl_scene *scene, uint32_t kind);
 WL_API int wl_bvh_get_info(wl_scene *scene, wl_bvh_info *info);
 /* Parity exports (host arrays). Morton codes in the scene's triangle order; the binary radix
