@@ -147,7 +147,10 @@ typedef struct wl_render_params {
     uint32_t lights;        /* WL_LIGHTS_* */
     uint64_t seed;          /* PCG32 seed (ignored for TEA_LCG) */
     float env[3];           /* constant radiance returned by a miss (reference: 0) */
-    uint32_t wave_paths;    /* paths in flight per wave; 0 = automatic */
+    uint32_t wave_paths;    /* paths in flight per wave (<= 2^27); 0 = automatic: the context's
+                               tuned size, else as many as the render has, up to 2^27 paths
+                               (192 B of queues each) and a quarter of the device memory free
+                               at the context's first render */
     uint32_t flags;         /* WL_RENDER_* bits */
 } wl_render_params;
 
@@ -329,7 +332,8 @@ WL_API int wl_render_batch(wl_context *ctx, uint32_t n, wl_scene *const *scenes,
 
 /* ---- autotuner ---------------------------------------------------------------------- */
 /* No counterpart in the reference (OptiX chooses its own launch shapes). The launch shape of
- * the renders: paths in flight per wave (0 = automatic), and per traversal pass the persistent
+ * the renders: paths in flight per wave (0 = automatic, see wl_render_params), and per
+ * traversal pass the persistent
  * CTAs per SM (0 = as many as fit), the warp refill threshold (4, 6, 8, 12, 16 or 24 idle
  * lanes) and the triangle-phase threshold (0..32; wl_cast_rays uses the extend pass's for
  * closest hits and the shadow pass's for any hits). */
