@@ -159,7 +159,11 @@ typedef struct wl_render_params {
  * timing). GRAPH runs each wave as one CUDA graph, captured once and replayed for every wave and
  * every later call with the same arguments (the wave's first sample and frame are read from
  * device memory); wl_render_stats then reports the total time only, not the per-kernel split. */
-enum { WL_RENDER_TRAVERSAL_STATS = 1u, WL_RENDER_GRAPH = 2u };
+enum { WL_RENDER_TRAVERSAL_STATS = 1u, WL_RENDER_GRAPH = 2u, WL_RENDER_SORT_MATERIALS = 4u };
+/* WL_RENDER_SORT_MATERIALS: the shade pass counting-sorts each block of 256 rays by shading
+ * class (miss, emitter hit, material bucket) before shading it. Same image; off by default, as
+ * it measured slower on the benchmark scenes (the reorder costs more than the divergence it
+ * removes there). */
 
 /* A ray as stored in the HBM ray queue: 32 bytes, two 16-byte vectors. */
 typedef struct wl_ray {

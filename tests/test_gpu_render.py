@@ -207,6 +207,35 @@ def test_graph_replay_matches_launches(ctx, strategy):
     assert np.array_equal(bits(imgs[0]), bits(imgs[1]))
 
 
+def test_sorted_shading_keeps_the_image(ctx):
+    """WL_RENDER_SORT_MATERIALS (each shading block counting-sorted by miss / emitter / material
+    before shading): the same strict image as unsorted shading, bit for bit, for a single render
+    and for a batch mixing two scenes."""
+    sc = small_sphere(40, 30)
+    cb = scenes.cornell_box(24, 20)
+    imgs = []
+    for flags in (0, wl._abi.RENDER_SORT_MATERIALS):
+        s = wl.Scene(ctx, sc)
+        film = wl.Film(ctx, 40, 30)
+        p = wl.render_params(40, 30, 3, math=wl.MATH_STRICT, env=sc.env, flags=flags, wave_paths=1500)
+        wl.render(ctx, s, sc.camera_struct(), p, film)
+        imgs.append(film.download())
+        film.close()
+        jobs = [(sc, s), (cb, wl.Scene(ctx, cb))]
+        films = [wl.Film(ctx, d.width, d.height) for d, _ in jobs]
+        ps = [wl.render_params(d.width, d.height, 2, math=wl.MATH_STRICT, env=d.env, flags=flags)
+              for d, _ in jobs]
+        wl.render_batch(ctx, [o for _, o in jobs], [d.camera_struct() for d, _ in jobs], ps, films)
+        imgs += [f.download() for f in films]
+        for f in films:
+            f.close()
+        for _, o in jobs:
+            o.close()
+    assert imgs[0].max() > 0
+    for a, b in zip(imgs[:3], imgs[3:]):
+        assert np.array_equal(bits(a), bits(b))
+
+
 def test_tuned_shapes_keep_the_image(ctx):
     """The autotuner's knobs change scheduling only: any shape renders the same strict image,
     and wl_autotune returns a valid shape that it keeps for later renders."""

@@ -25,6 +25,7 @@ BVH_LBVH, BVH_SAH = 0, 1
 CAST_CLOSEST, CAST_ANY = 0, 1
 RENDER_TRAVERSAL_STATS = 1
 RENDER_GRAPH = 2
+RENDER_SORT_MATERIALS = 4
 INVALID = 0xFFFFFFFF
 
 

@@ -982,6 +982,7 @@ int wl_render(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_
         wp.cam_up[k] = cam->up[k]; wp.cam_right[k] = cam->right[k];
     }
     wp.has_env = (p->env[0] != 0.f || p->env[1] != 0.f || p->env[2] != 0.f) ? 1u : 0u;
+    wp.sort_materials = (p->flags & WL_RENDER_SORT_MATERIALS) ? 1u : 0u;
     DevScene sc = dev_scene(s);
     cudaStream_t st = c->stream;
     for (auto &u : c->ev_used) u = 0;
@@ -1057,6 +1058,7 @@ int wl_render_batch(wl_context *c, uint32_t n, wl_scene *const *scenes, const wl
     std::vector<BatchJob> jobs(n);
     uint64_t total = 0;
     uint32_t maxd = 0;
+    bool sort_batch = false;  // any job with WL_RENDER_SORT_MATERIALS sorts every shade pass
     const uint32_t math = params[0].math;
     for (uint32_t j = 0; j < n; j++) {
         wl_scene *s = scenes[j];
@@ -1090,6 +1092,8 @@ int wl_render_batch(wl_context *c, uint32_t n, wl_scene *const *scenes, const wl
             wp.cam_up[k] = cam->up[k]; wp.cam_right[k] = cam->right[k];
         }
         wp.has_env = (p->env[0] != 0.f || p->env[1] != 0.f || p->env[2] != 0.f) ? 1u : 0u;
+        wp.sort_materials = (p->flags & WL_RENDER_SORT_MATERIALS) ? 1u : 0u;
+        if (wp.sort_materials) sort_batch = true;
         J.sc = dev_scene(s);
         J.film = f->f;
         J.off = total;
@@ -1136,8 +1140,8 @@ int wl_render_batch(wl_context *c, uint32_t n, wl_scene *const *scenes, const wl
             cudaMemsetAsync(c->q.counters + (in ^ 1), 0, sizeof(uint32_t), st);
             cudaMemsetAsync(c->q.counters + 2, 0, sizeof(uint32_t), st);
             rec(c, 1, true);
-            if (strict_math) strict::launch_shade_batch(bv, c->q, in, st);
-            else fast::launch_shade_batch(bv, c->q, in, st);
+            if (strict_math) strict::launch_shade_batch(bv, c->q, in, sort_batch, st);
+            else fast::launch_shade_batch(bv, c->q, in, sort_batch, st);
             rec(c, 1, false);
             rec(c, 2, true);
             launch_shadow(sc0, c->q, false, st, c->tune_shadow, bv);
@@ -1428,6 +1432,7 @@ int wl_render_nrc(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_ren
         wp.cam_up[k] = cam->up[k]; wp.cam_right[k] = cam->right[k];
     }
     wp.has_env = (p->env[0] != 0.f || p->env[1] != 0.f || p->env[2] != 0.f) ? 1u : 0u;
+    wp.sort_materials = (p->flags & WL_RENDER_SORT_MATERIALS) ? 1u : 0u;
     DevScene sc = dev_scene(s);
     cudaStream_t st = c->stream;
     const bool strict_math = p->math == WL_MATH_STRICT;

@@ -128,6 +128,7 @@ extern "C" int wl_render_noalloc(wl_context *ctx, wl_scene *scene, const wl_came
         wp.cam_up[k] = cam->up[k]; wp.cam_right[k] = cam->right[k];
     }
     wp.has_env = (p->env[0] != 0.f || p->env[1] != 0.f || p->env[2] != 0.f) ? 1u : 0u;
+    wp.sort_materials = (p->flags & WL_RENDER_SORT_MATERIALS) ? 1u : 0u;
     const bool strict_math = p->math == WL_MATH_STRICT;
     for (uint64_t b0 = 0; b0 < total; b0 += wave) {
         wp.base = b0;

@@ -361,7 +361,65 @@ __device__ __forceinline__ void shade_emit(const Queues &q, int out, bool valid,
     }
 }
 
-template <bool NRC>
+// Material-sorted shading (WL_RENDER_SORT_MATERIALS): each block of PT rays is counting-sorted
+// by a shading class (miss, light hit, surface material bucket; slots past the queue end last)
+// before it is shaded, so that a warp runs one class where the block's mix allows instead of
+// idling the lanes of short classes (misses, emitters) through the BSDF work of the others.
+// Keys are counted per warp with ballots and placed by an exclusive prefix sum over (key,
+// warp); the order within a key is the queue order. Per-path results do not depend on which
+// thread shades a ray. Off by default: on the benchmark scenes the barriers and the permuted
+// queue reads cost more than the divergence saves (shade pass 30.2 -> 37.9 ms per 1080p x 64
+// spp step).
+constexpr uint32_t SHADE_KEYS = 16;
+static_assert(SHADE_KEYS * (PT / 32) == 128, "the key scan covers 4 (key, warp) counts per lane");
+
+__device__ __forceinline__ uint32_t shade_key(const DevScene &sc, uint32_t prim) {
+    if (prim == INVALID) return 0u;
+    if (sc.tri_light[prim] != INVALID) return 1u;
+    return 2u + (sc.tri[prim].w & 0x7fffffffu) % (SHADE_KEYS - 3);
+}
+
+// Returns the queue index this thread shades (block-collective: every thread of the block
+// calls it with its own key and index).
+__device__ __forceinline__ uint32_t block_sort_by_key(uint32_t key, uint32_t i) {
+    __shared__ uint32_t s_off[SHADE_KEYS][PT / 32];
+    __shared__ uint32_t s_ray[PT];
+    const uint32_t lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint32_t rank = 0;
+    for (uint32_t b = 0; b < SHADE_KEYS; b++) {
+        const uint32_t m = __ballot_sync(0xffffffffu, key == b);
+        if (key == b) rank = __popc(m & lanemask_lt());
+        if (lane == 0) s_off[b][w] = __popc(m);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        uint32_t v[4], sum = 0;
+        for (int k = 0; k < 4; k++) {
+            const uint32_t e = lane * 4 + k;
+            v[k] = s_off[e / (PT / 32)][e % (PT / 32)];
+            sum += v[k];
+        }
+        uint32_t incl = sum;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (uint32_t)o) incl += t;
+        }
+        uint32_t run = incl - sum;
+        for (int k = 0; k < 4; k++) {
+            const uint32_t e = lane * 4 + k;
+            s_off[e / (PT / 32)][e % (PT / 32)] = run;
+            run += v[k];
+        }
+    }
+    __syncthreads();
+    s_ray[s_off[key][w] + rank] = i;
+    __syncthreads();
+    const uint32_t r = s_ray[threadIdx.x];
+    __syncthreads();  // the shared arrays are reused by the block's next call
+    return r;
+}
+
+template <bool NRC, bool SORT>
 __global__ void __launch_bounds__(PT) k_shade(WaveParams wp, DevScene sc, Queues q, int in,
                                               NrcWaveBuffers nb) {
     wave_dyn(wp);
@@ -370,7 +428,11 @@ __global__ void __launch_bounds__(PT) k_shade(WaveParams wp, DevScene sc, Queues
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
         uint32_t i = base + threadIdx.x;
-        bool valid = i < n;
+        if (SORT) {
+            const uint32_t key = i < n ? shade_key(sc, __float_as_uint(q.hit[i].y)) : SHADE_KEYS - 1;
+            i = block_sort_by_key(key, i);
+        }
+        const bool valid = i < n;
         ShadeOut o;
         if (valid) shade_lane<NRC>(wp, sc, q, in, i, nb, o);
         shade_emit(q, out, valid, o);
@@ -418,13 +480,19 @@ __global__ void __launch_bounds__(PT) k_generate_batch(BatchView bv, Queues q, u
 }
 
 // The shade pass of a batch wave: each ray with its job's scene and parameters.
+template <bool SORT>
 __global__ void __launch_bounds__(PT) k_shade_batch(BatchView bv, Queues q, int in) {
     const uint32_t n = q.counters[in];
     const int out = in ^ 1;
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
         uint32_t i = base + threadIdx.x;
-        bool valid = i < n;
+        if (SORT) {
+            uint32_t key = SHADE_KEYS - 1;
+            if (i < n) key = shade_key(bv.jobs[bv.slot_job[q.ray_slot[in][i]]].sc, __float_as_uint(q.hit[i].y));
+            i = block_sort_by_key(key, i);
+        }
+        const bool valid = i < n;
         ShadeOut o;
         if (valid) {
             const BatchJob &J = bv.jobs[bv.slot_job[q.ray_slot[in][i]]];
@@ -456,19 +524,25 @@ static int shade_grid(const void *k) {
 }
 
 void launch_shade(const WaveParams &wp, const DevScene &sc, const Queues &q, int in, cudaStream_t s) {
-    static int grid = shade_grid((const void *)k_shade<false>);
-    k_shade<false><<<grid, PT, 0, s>>>(wp, sc, q, in, NrcWaveBuffers{});
+    static int grid = shade_grid((const void *)k_shade<false, false>);
+    static int grid_sorted = shade_grid((const void *)k_shade<false, true>);
+    if (wp.sort_materials) k_shade<false, true><<<grid_sorted, PT, 0, s>>>(wp, sc, q, in, NrcWaveBuffers{});
+    else k_shade<false, false><<<grid, PT, 0, s>>>(wp, sc, q, in, NrcWaveBuffers{});
 }
 
-void launch_shade_batch(const BatchView &bv, const Queues &q, int in, cudaStream_t s) {
-    static int grid = shade_grid((const void *)k_shade_batch);
-    k_shade_batch<<<grid, PT, 0, s>>>(bv, q, in);
+void launch_shade_batch(const BatchView &bv, const Queues &q, int in, bool sort, cudaStream_t s) {
+    static int grid = shade_grid((const void *)k_shade_batch<false>);
+    static int grid_sorted = shade_grid((const void *)k_shade_batch<true>);
+    if (sort) k_shade_batch<true><<<grid_sorted, PT, 0, s>>>(bv, q, in);
+    else k_shade_batch<false><<<grid, PT, 0, s>>>(bv, q, in);
 }
 
 void launch_shade_nrc(const WaveParams &wp, const DevScene &sc, const Queues &q, int in,
                       const NrcWaveBuffers &nb, cudaStream_t s) {
-    static int grid = shade_grid((const void *)k_shade<true>);
-    k_shade<true><<<grid, PT, 0, s>>>(wp, sc, q, in, nb);
+    static int grid = shade_grid((const void *)k_shade<true, false>);
+    static int grid_sorted = shade_grid((const void *)k_shade<true, true>);
+    if (wp.sort_materials) k_shade<true, true><<<grid_sorted, PT, 0, s>>>(wp, sc, q, in, nb);
+    else k_shade<true, false><<<grid, PT, 0, s>>>(wp, sc, q, in, nb);
 }
 
 }  // namespace WL_NS

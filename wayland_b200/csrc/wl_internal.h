@@ -120,6 +120,7 @@ struct WaveParams {
     uint64_t seed;
     float env[3];
     uint32_t has_env;
+    uint32_t sort_materials;  // WL_RENDER_SORT_MATERIALS
     float cam_pos[3], cam_look[3], cam_up[3], cam_right[3];
     // graph replays: the wave's first sample index and first frame come from device memory
     // (dyn[0], dyn[1]) instead of base / first_frame, so one captured wave serves every wave
@@ -194,7 +195,7 @@ void launch_ao(const AoWave &w, const DevScene &sc, const Queues &q, const Film 
 // launch functions (pt_kernels.cuh instantiated in pt_fast.cu / pt_strict.cu)
 namespace fast {
 void launch_generate_batch(const BatchView &bv, const Queues &q, uint32_t count, cudaStream_t s);
-void launch_shade_batch(const BatchView &bv, const Queues &q, int in, cudaStream_t s);
+void launch_shade_batch(const BatchView &bv, const Queues &q, int in, bool sort, cudaStream_t s);
 void launch_bdpt_eye_gen(const WaveParams &wp, const Queues &q, const BdptWave &bw, cudaStream_t s);
 void launch_bdpt_eye(const WaveParams &wp, const DevScene &sc, const Queues &q, const BdptWave &bw,
                      int in, uint32_t depth, cudaStream_t s);
@@ -211,7 +212,7 @@ void launch_shade_nrc(const WaveParams &wp, const DevScene &sc, const Queues &q,
 }
 namespace strict {
 void launch_generate_batch(const BatchView &bv, const Queues &q, uint32_t count, cudaStream_t s);
-void launch_shade_batch(const BatchView &bv, const Queues &q, int in, cudaStream_t s);
+void launch_shade_batch(const BatchView &bv, const Queues &q, int in, bool sort, cudaStream_t s);
 void launch_bdpt_eye_gen(const WaveParams &wp, const Queues &q, const BdptWave &bw, cudaStream_t s);
 void launch_bdpt_eye(const WaveParams &wp, const DevScene &sc, const Queues &q, const BdptWave &bw,
                      int in, uint32_t depth, cudaStream_t s);
