@@ -136,9 +136,10 @@ struct Entries {
     int ne;
 };
 
-// Children of the wide node made from binary node b: open the largest-area internal entry
-// holding more than LEAF_MAX triangles until 8 entries exist; if slots remain, open further
-// internal entries by area. Ties keep the earlier entry (deterministic).
+// Children of the wide node made from binary node b: open the internal entry holding more than
+// LEAF_MAX triangles with the largest area x triangle count (its share of the SAH cost) until 8
+// entries exist; if slots remain, open further internal entries by area. Ties keep the earlier
+// entry (deterministic).
 WL_HD void select_entries(const BinTree &T, int b, Entries &E) {
     E.ne = 0;
     if (T.leaf(b)) {
@@ -154,9 +155,10 @@ WL_HD void select_entries(const BinTree &T, int b, Entries &E) {
         float best_a = -1.0f;
         for (int k = 0; k < E.ne; k++) {
             int x = E.ent[k];
-            if (!T.leaf(x) && T.count(x) > (uint32_t)LEAF_MAX && T.area(x) > best_a) {
+            const float pr = T.area(x) * (float)T.count(x);
+            if (!T.leaf(x) && T.count(x) > (uint32_t)LEAF_MAX && pr > best_a) {
                 best = k;
-                best_a = T.area(x);
+                best_a = pr;
             }
         }
         if (best < 0) {
