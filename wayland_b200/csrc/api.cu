@@ -45,6 +45,10 @@ struct TimedPair {
 struct wl_context {
     int device = 0;
     cudaStream_t stream = nullptr;
+    // a second stream of the library's own: a bounce's shadow pass runs on it while the main
+    // stream traces the next bounce's extension rays (joined before the next shade pass)
+    cudaStream_t side = nullptr;
+    std::vector<cudaEvent_t> fork_ev, join_ev;
     bool own_stream = false;
     Queues q{};
     void *q_block = nullptr;
@@ -250,7 +254,7 @@ int ensure_bdpt(wl_context *c, uint32_t cap, uint32_t maxv) {
     return WL_OK;
 }
 
-void rec(wl_context *c, int cat, bool begin) {
+void rec(wl_context *c, int cat, bool begin, cudaStream_t on = nullptr) {
     if (!c->events_on) return;
     auto &v = c->ev[cat];
     size_t &u = c->ev_used[cat];
@@ -261,11 +265,24 @@ void rec(wl_context *c, int cat, bool begin) {
             cudaEventCreate(&tp.b);
             v.push_back(tp);
         }
-        cudaEventRecord(v[u].a, c->stream);
+        cudaEventRecord(v[u].a, on ? on : c->stream);
     } else {
-        cudaEventRecord(v[u].b, c->stream);
+        cudaEventRecord(v[u].b, on ? on : c->stream);
         u++;
     }
+}
+
+// Fork / join events of bounce b (created once, reused by every wave).
+void fork_join(wl_context *c, uint32_t b, cudaEvent_t &fork, cudaEvent_t &join) {
+    while (c->fork_ev.size() <= b) {
+        cudaEvent_t f = nullptr, j = nullptr;
+        cudaEventCreateWithFlags(&f, cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&j, cudaEventDisableTiming);
+        c->fork_ev.push_back(f);
+        c->join_ev.push_back(j);
+    }
+    fork = c->fork_ev[b];
+    join = c->join_ev[b];
 }
 
 int finish_stats(wl_context *c) {
@@ -317,7 +334,8 @@ int wl_context_create(int device, wl_context **out) {
         return fail(WL_ERR_CUDA, cudaGetErrorString(e));
     }
     c->own_stream = true;
-    if (cudaMalloc(&c->d_misc, 256) != cudaSuccess ||
+    if (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&c->d_misc, 256) != cudaSuccess ||
         cudaMalloc(&c->d_cast_counts, 2 * sizeof(unsigned long long)) != cudaSuccess ||
         cudaEventCreate(&c->ev_total[0]) != cudaSuccess ||
         cudaEventCreate(&c->ev_total[1]) != cudaSuccess) {
@@ -352,6 +370,12 @@ int wl_context_destroy(wl_context *c) {
         }
     for (auto e : c->ev_total)
         if (e) cudaEventDestroy(e);
+    if (c->side) {
+        cudaStreamSynchronize(c->side);
+        cudaStreamDestroy(c->side);
+    }
+    for (auto e : c->fork_ev) cudaEventDestroy(e);
+    for (auto e : c->join_ev) cudaEventDestroy(e);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return WL_OK;
@@ -778,23 +802,38 @@ static uint32_t pt_wave(wl_context *c, const WaveParams &wp, const DevScene &sc,
     else fast::launch_generate(wp, c->q, st);
     rec(c, 3, false);
     launches++;
+    // Bounce b: extend and shade on the main stream; the shadow pass of bounce b on the side
+    // stream, concurrently with the extension rays of bounce b + 1 (which touch neither the
+    // shadow queue nor the path radiance). The shade pass of bounce b + 1, the next writer of
+    // both, waits for it, so the radiance still sums emission b, light sample b, emission b + 1
+    // in the reference's order.
+    cudaStream_t sd = c->side;
+    cudaEvent_t join_prev = nullptr;
     int in = 0;
     for (uint32_t b = 0; b < max_depth; b++) {
         rec(c, 0, true);
         launch_extend(sc, c->q, in, tstats, st, c->tune_extend);
         rec(c, 0, false);
+        if (join_prev) cudaStreamWaitEvent(st, join_prev, 0);
         cudaMemsetAsync(c->q.counters + (in ^ 1), 0, sizeof(uint32_t), st);
         cudaMemsetAsync(c->q.counters + 2, 0, sizeof(uint32_t), st);
         rec(c, 1, true);
         if (strict_math) strict::launch_shade(wp, sc, c->q, in, st);
         else fast::launch_shade(wp, sc, c->q, in, st);
         rec(c, 1, false);
-        rec(c, 2, true);
-        launch_shadow(sc, c->q, tstats, st, c->tune_shadow);
-        rec(c, 2, false);
+        cudaEvent_t fk, jn;
+        fork_join(c, b, fk, jn);
+        cudaEventRecord(fk, st);
+        cudaStreamWaitEvent(sd, fk, 0);
+        rec(c, 2, true, sd);
+        launch_shadow(sc, c->q, tstats, sd, c->tune_shadow);
+        rec(c, 2, false, sd);
+        cudaEventRecord(jn, sd);
+        join_prev = jn;
         launches += 3;
         in ^= 1;
     }
+    if (join_prev) cudaStreamWaitEvent(st, join_prev, 0);
     rec(c, 3, true);
     strict::launch_film(wp, c->q, film, st);
     rec(c, 3, false);
@@ -810,8 +849,9 @@ template <class T> static void key_add(std::vector<uint8_t> &k, const T &v) {
 }
 
 // The instantiated graph of one wave whose captured arguments are `key`: reused when an equal
-// key was captured before, else captured from `issue` (which must only enqueue work on the
-// context's stream) into the least recently used entry.
+// key was captured before, else captured from `issue` (which enqueues work on the context's
+// stream, and on its side stream only between a fork from and a join back to the main stream)
+// into the least recently used entry.
 template <class F>
 static int wave_graph(wl_context *c, const std::vector<uint8_t> &key, F issue, cudaGraphExec_t *out) {
     c->graph_clock++;
@@ -1024,6 +1064,8 @@ int wl_render(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_
             key_add(key, c->tune_shadow);
             uint32_t nl = 0;
             cudaGraphExec_t exec = nullptr;
+            cudaEvent_t fk, jn;  // the wave's fork / join events exist before the capture
+            fork_join(c, p->max_depth ? p->max_depth - 1 : 0, fk, jn);
             int rc2 = wave_graph(c, key, [&] {
                 strict::launch_wave_begin(c->d_dyn_all, c->d_dyn_ctr, c->d_dyn_cur, st);
                 nl = bdpt ? bdpt_wave(c, gp, sc, f->f, strict_math, false)
@@ -1132,23 +1174,33 @@ int wl_render_batch(wl_context *c, uint32_t n, wl_scene *const *scenes, const wl
         if (strict_math) strict::launch_generate_batch(bv, c->q, count, st);
         else fast::launch_generate_batch(bv, c->q, count, st);
         rec(c, 3, false);
+        // the shadow pass of bounce b overlaps the extension rays of bounce b + 1 (as pt_wave)
+        cudaEvent_t join_prev = nullptr;
         int in = 0;
         for (uint32_t b = 0; b < maxd; b++) {
             rec(c, 0, true);
             launch_extend(sc0, c->q, in, false, st, c->tune_extend, bv);
             rec(c, 0, false);
+            if (join_prev) cudaStreamWaitEvent(st, join_prev, 0);
             cudaMemsetAsync(c->q.counters + (in ^ 1), 0, sizeof(uint32_t), st);
             cudaMemsetAsync(c->q.counters + 2, 0, sizeof(uint32_t), st);
             rec(c, 1, true);
             if (strict_math) strict::launch_shade_batch(bv, c->q, in, sort_batch, st);
             else fast::launch_shade_batch(bv, c->q, in, sort_batch, st);
             rec(c, 1, false);
-            rec(c, 2, true);
-            launch_shadow(sc0, c->q, false, st, c->tune_shadow, bv);
-            rec(c, 2, false);
+            cudaEvent_t fk, jn;
+            fork_join(c, b, fk, jn);
+            cudaEventRecord(fk, st);
+            cudaStreamWaitEvent(c->side, fk, 0);
+            rec(c, 2, true, c->side);
+            launch_shadow(sc0, c->q, false, c->side, c->tune_shadow, bv);
+            rec(c, 2, false, c->side);
+            cudaEventRecord(jn, c->side);
+            join_prev = jn;
             in ^= 1;
             launches += 3;
         }
+        if (join_prev) cudaStreamWaitEvent(st, join_prev, 0);
         rec(c, 3, true);
         strict::launch_film_batch(bv, c->q, count, st);
         rec(c, 3, false);
