@@ -242,7 +242,7 @@ void hb_cast_batched(void *p, const float *rays, uint32_t n, uint32_t mode, uint
             } while (tm && (!nm || (uint32_t)__builtin_popcount(tm) * 32u >= need));
         } else {
             for (int l = 0; l < 32; l++)
-                if (can_n[l]) trav_node<true>(st[l], stack.data() + (size_t)l * TRAV_STACK, nodes, &cn);
+                if (can_n[l]) trav_node<true>(st[l], ArrayStack{stack.data() + (size_t)l * TRAV_STACK}, nodes, &cn);
         }
         for (int l = 0; l < 32; l++) {
             if (active[l] && (fin[l] || trav_done(st[l]))) {

@@ -47,12 +47,29 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
 // threads with dynamic fetch). Instantiated for R in {4, 6, 8, 12, 16, 24}; the autotuner picks
 // one.
 
+// The traversal stack of a k_trace / k_cast thread: the top SHARED_STACK entries in shared
+// memory ([entry][thread], so a warp's accesses fall in distinct banks), deeper ones in local
+// memory. Keeping the busy top of the stack out of L1 leaves L1 to the node and triangle
+// fetches.
+constexpr int SHARED_STACK = 8;  // 8 KB per CTA of 128 threads (4 and 16 measured slower)
+struct SplitStack {
+    uint2 *sh;   // this thread's entry 0; entry i at sh[i * TT]
+    uint2 *loc;  // entries SHARED_STACK and deeper
+    __device__ __forceinline__ void put(int i, uint2 v) const {
+        if (i < SHARED_STACK) sh[i * TT] = v;
+        else loc[i - SHARED_STACK] = v;
+    }
+    __device__ __forceinline__ uint2 get(int i) const {
+        return i < SHARED_STACK ? sh[i * TT] : loc[i - SHARED_STACK];
+    }
+};
+
 // One warp iteration of the batched traversal (trav_node / trav_tri): a triangle phase when the
 // lanes holding triangles are at least post/32 of the busy lanes (or no lane can visit a node),
 // kept up while that holds; otherwise a node phase. Returns true for a lane whose ray finished.
 template <bool ANY, bool STATS>
 __device__ __forceinline__ bool warp_trav(bool active, uint32_t busy, uint32_t post, TravState &st,
-                                          uint2 *stack, const float4 *__restrict__ nodes,
+                                          const SplitStack &stack, const float4 *__restrict__ nodes,
                                           const float4 *__restrict__ tris, uint32_t &cn, uint32_t &ct) {
     const bool can_n = active && trav_can_node(st);
     bool has_t = active && st.tg.y != 0;
@@ -86,7 +103,9 @@ __global__ void __launch_bounds__(TT, TRACE_MIN_CTAS) k_trace(DevScene sc, Queue
     const float4 *rd = MODE == 0 ? q.ray_d[in] : q.sh_d;
     const uint32_t lane = threadIdx.x & 31;
     TravState st;
-    uint2 stack[TRAV_STACK];
+    __shared__ uint2 s_stack[SHARED_STACK * TT];
+    uint2 l_stack[TRAV_STACK - SHARED_STACK];
+    const SplitStack stack{s_stack + threadIdx.x, l_stack};
     uint32_t my = 0, cn = 0, ct = 0;
     bool active = false, exhausted = false;
     const float4 *nodes = sc.nodes, *tris = sc.tris;  // per ray in a batch
@@ -146,7 +165,9 @@ __global__ void __launch_bounds__(TT, TRACE_MIN_CTAS) k_cast(DevScene sc, const 
                                               uint32_t n, uint32_t *fetch, uint32_t post) {
     const uint32_t lane = threadIdx.x & 31;
     TravState st;
-    uint2 stack[TRAV_STACK];
+    __shared__ uint2 s_stack[SHARED_STACK * TT];
+    uint2 l_stack[TRAV_STACK - SHARED_STACK];
+    const SplitStack stack{s_stack + threadIdx.x, l_stack};
     uint32_t my = 0, cn = 0, ct = 0;
     bool active = false, exhausted = false;
     while (true) {

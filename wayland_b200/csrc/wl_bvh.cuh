@@ -519,17 +519,24 @@ WL_HD bool trav_done(const TravState &s) {
     return !(s.ng.y & 0xff000000u) && s.sp == 0 && s.tg.y == 0;
 }
 
+// A traversal stack as one array (the host, and kernels that keep it in local memory).
+struct ArrayStack {
+    uint2 *a;
+    WL_HD void put(int i, uint2 v) const { a[i] = v; }
+    WL_HD uint2 get(int i) const { return a[i]; }
+};
+
 // Node step (requires trav_can_node): pop the stack when the current group is exhausted, then
-// visit the group's nearest pending child.
-template <bool STATS>
-WL_HD void trav_node(TravState &s, uint2 *stack, const float4 *__restrict__ nodes, uint32_t *n_nodes) {
-    if (!(s.ng.y & 0xff000000u)) s.ng = stack[--s.sp];
+// visit the group's nearest pending child. Stack: put(i, v) / get(i) of entry i.
+template <bool STATS, class Stack>
+WL_HD void trav_node(TravState &s, const Stack &stack, const float4 *__restrict__ nodes, uint32_t *n_nodes) {
+    if (!(s.ng.y & 0xff000000u)) s.ng = stack.get(--s.sp);
     int k = lowest_bit(s.ng.y >> 24);
     s.ng.y &= ~(1u << (24 + k));
     uint32_t slot = (uint32_t)k ^ s.oct;
     uint32_t node = s.ng.x + popcount(s.ng.y & 0xffu & ((1u << slot) - 1u));
     if (s.ng.y & 0xff000000u) {
-        if (s.sp < TRAV_STACK) stack[s.sp++] = s.ng;
+        if (s.sp < TRAV_STACK) stack.put(s.sp++, s.ng);
         else s.ok = false;
     }
     if (STATS) (*n_nodes)++;
