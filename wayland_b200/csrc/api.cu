@@ -1517,15 +1517,25 @@ int wl_render_nrc(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_ren
             int in = 0;
             // every path has ended by vertex train_end when training paths end at the cache
             const uint32_t bounces = nb.train_end && nb.train_end < p->max_depth ? nb.train_end : p->max_depth;
+            // the shadow pass of bounce b overlaps the extension rays of bounce b + 1 (as pt_wave)
+            cudaEvent_t join_prev = nullptr;
             for (uint32_t b = 0; b < bounces; b++) {
                 launch_extend(sc, c->q, in, false, st, c->tune_extend);
+                if (join_prev) CK(cudaStreamWaitEvent(st, join_prev, 0));
                 CK(cudaMemsetAsync(c->q.counters + (in ^ 1), 0, sizeof(uint32_t), st));
                 CK(cudaMemsetAsync(c->q.counters + 2, 0, sizeof(uint32_t), st));
                 if (strict_math) strict::launch_shade_nrc(wp, sc, c->q, in, nb, st);
                 else fast::launch_shade_nrc(wp, sc, c->q, in, nb, st);
-                launch_shadow(sc, c->q, false, st, c->tune_shadow);
+                cudaEvent_t fk, jn;
+                fork_join(c, b, fk, jn);
+                CK(cudaEventRecord(fk, st));
+                CK(cudaStreamWaitEvent(c->side, fk, 0));
+                launch_shadow(sc, c->q, false, c->side, c->tune_shadow);
+                CK(cudaEventRecord(jn, c->side));
+                join_prev = jn;
                 in ^= 1;
             }
+            if (join_prev) CK(cudaStreamWaitEvent(st, join_prev, 0));
             nrc_query(n->net, s->d_mats, n->queries, n->n_queries, c->q.st_rad, wp.count, st);
             nrc_collect(n->net, nb, c->q, tcount, st);
             if (f) strict::launch_film(wp, c->q, f->f, st);
