@@ -39,6 +39,15 @@ WL_HD uint8_t byte_of(uint32_t lo, uint32_t hi, int s) {
     uint32_t w = s < 4 ? lo : hi;
     return (uint8_t)((w >> (8 * (s & 3))) & 0xffu);
 }
+// 2^23 + byte s of the pair (lo, hi), as a float: one byte permute on the GPU (bytes: the
+// selected one, two zeros, 0x4B), exact; minus 2^23 it is the byte's value.
+WL_HD float byte_plus_2p23(uint32_t lo, uint32_t hi, int s) {
+#ifdef __CUDA_ARCH__
+    return __uint_as_float(__byte_perm(s < 4 ? lo : hi, 0x4B000000u, (uint32_t)(s & 3) | 0x7540u));
+#else
+    return __builtin_bit_cast(float, 0x4B000000u | byte_of(lo, hi, s));
+#endif
+}
 
 // ---------------------------------------------------------------------------------------
 // Morton codes
@@ -435,9 +444,11 @@ WL_HD void node_test(const TravState &s, const float4 *__restrict__ np, uint2 &n
     for (int c = 0; c < 8; c++) {
         uint32_t meta = byte_of(m0, m1, c);
         if (meta == 0) continue;
-        float tnx = fmaf((float)byte_of(qnx0, qnx1, c), ax, bnx), tfx = fmaf((float)byte_of(qfx0, qfx1, c), ax, bfx);
-        float tny = fmaf((float)byte_of(qny0, qny1, c), ay, bny), tfy = fmaf((float)byte_of(qfy0, qfy1, c), ay, bfy);
-        float tnz = fmaf((float)byte_of(qnz0, qnz1, c), az, bnz), tfz = fmaf((float)byte_of(qfz0, qfz1, c), az, bfz);
+        // plane q of a child: (2^23 + q) - 2^23, exact, built by a byte permute (no I2F)
+        const float K = 8388608.0f;
+        float tnx = fmaf(byte_plus_2p23(qnx0, qnx1, c) - K, ax, bnx), tfx = fmaf(byte_plus_2p23(qfx0, qfx1, c) - K, ax, bfx);
+        float tny = fmaf(byte_plus_2p23(qny0, qny1, c) - K, ay, bny), tfy = fmaf(byte_plus_2p23(qfy0, qfy1, c) - K, ay, bfy);
+        float tnz = fmaf(byte_plus_2p23(qnz0, qnz1, c) - K, az, bnz), tfz = fmaf(byte_plus_2p23(qfz0, qfz1, c) - K, az, bfz);
         float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, s.tmin));
         float tf = fminf(fminf(tfx, tfy), fminf(tfz, tcur));
         if (tn <= XMUL(tf, grow)) {
