@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(AT) k_ao_occlude(AoWave w, DevScene sc, Queues
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= w.count) return;
     float4 h = q.hit[i];
-    uint32_t prim = __float_as_uint(h.y);
+    uint32_t prim = leaf_prim(sc, __float_as_uint(h.y));  // the extend pass reports leaf indices
     float rad = 0.0f;
     if (prim != INVALID) {
         float4 ro = q.ray_o[0][i], rd = q.ray_d[0][i];

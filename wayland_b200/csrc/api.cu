@@ -143,7 +143,7 @@ DevScene dev_scene(const wl_scene *s) {
     d.V = s->d_V; d.N = s->d_N; d.UV = s->d_UV;
     d.tri = s->d_tri; d.tri_light = s->d_tri_light;
     d.mats = s->d_mats; d.lights = s->d_lights;
-    d.nodes = s->bvh.nodes; d.tris = s->bvh.tris;
+    d.nodes = s->bvh.nodes; d.tris = s->bvh.tris; d.shd = s->bvh.shd;
     d.has_bvh = (s->built && s->nT > 0) ? 1u : 0u;
     d.tex = s->d_tex;
     d.nTex = (uint32_t)s->tex_objs.size();
@@ -583,6 +583,8 @@ int wl_bvh_build(wl_scene *s, uint32_t kind) {
         bvh_free(s->bvh);
         return fail(rc, "bvh build: " + err);
     }
+    bvh_fill_shading(s->bvh, s->d_tri, s->d_N, s->d_tri_light, s->ctx->stream);
+    CK(cudaGetLastError());
     s->built = true;
     wl_bvh_info &in = s->info;
     in.kind = kind;
@@ -592,7 +594,7 @@ int wl_bvh_build(wl_scene *s, uint32_t kind) {
     in.wide_depth = s->bvh.wide_depth;
     in.leaf_tris = s->nT;
     in.ms_build = s->bvh.ms;
-    in.bytes = (uint64_t)s->bvh.wide_nodes * 80 + (uint64_t)s->nT * 48;
+    in.bytes = (uint64_t)s->bvh.wide_nodes * 80 + (uint64_t)s->nT * 96;
     return WL_OK;
 }
 

@@ -232,6 +232,7 @@ __global__ void __launch_bounds__(PT) k_bd_eye(WaveParams wp, DevScene sc, Queue
         if (i < n) {
             slot = q.ray_slot[in][i];
             float4 h = q.hit[i];
+            h.y = __uint_as_float(leaf_prim(sc, __float_as_uint(h.y)));  // leaf -> triangle id
             v3 org = f4xyz(q.ray_o[in][i]), dir = f4xyz(q.ray_d[in][i]);
             if (__float_as_uint(h.y) != INVALID) {
                 const uint32_t v = depth - 1;
@@ -383,6 +384,7 @@ __global__ void __launch_bounds__(PT) k_bd_light(WaveParams wp, DevScene sc, Que
         if (i < n) {
             slot = q.ray_slot[in][i];
             float4 h = q.hit[i];
+            h.y = __uint_as_float(leaf_prim(sc, __float_as_uint(h.y)));  // leaf -> triangle id
             v3 org = f4xyz(q.ray_o[in][i]), dir = f4xyz(q.ray_d[in][i]);
             if (__float_as_uint(h.y) != INVALID) {
                 BdV v;

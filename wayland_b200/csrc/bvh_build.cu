@@ -601,12 +601,38 @@ struct Scratch {
         }                                                                         \
     } while (0)
 
+// Shading record of every leaf triangle L (the triangle of tris[3 L]): its vertex normals (zero
+// without), material | has_normal << 31, light id and triangle id, so that the shade pass reads
+// one contiguous record in the spatial order of the tree instead of gathering by triangle id.
+__global__ void k_fill_shading(const float4 *tris, uint32_t n, const uint4 *tri, const float *N,
+                               const uint32_t *tri_light, float4 *shd) {
+    const uint32_t L = blockIdx.x * blockDim.x + threadIdx.x;
+    if (L >= n) return;
+    const uint32_t prim = __float_as_uint(tris[3 * (size_t)L].w);
+    const uint4 ti = tri[prim];
+    float nn[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (N && (ti.w >> 31)) {
+        const uint32_t vi[3] = {ti.x, ti.y, ti.z};
+        for (int k = 0; k < 3; k++)
+            for (int a = 0; a < 3; a++) nn[3 * k + a] = N[3 * (size_t)vi[k] + a];
+    }
+    shd[3 * (size_t)L] = make_float4(nn[0], nn[1], nn[2], __uint_as_float(ti.w));
+    shd[3 * (size_t)L + 1] = make_float4(nn[3], nn[4], nn[5], __uint_as_float(tri_light[prim]));
+    shd[3 * (size_t)L + 2] = make_float4(nn[6], nn[7], nn[8], __uint_as_float(prim));
+}
+
+void bvh_fill_shading(BvhBuild &b, const uint4 *tri, const float *N, const uint32_t *tri_light,
+                      cudaStream_t s) {
+    if (b.nT == 0 || !b.shd) return;
+    k_fill_shading<<<nblk(b.nT), BT, 0, s>>>(b.tris, b.nT, tri, N, tri_light, b.shd);
+}
+
 void bvh_free(BvhBuild &b) {
-    void *ps[] = {b.morton, b.sorted, b.left, b.right, b.parent, b.blo, b.bhi, b.nodes, b.tris};
+    void *ps[] = {b.morton, b.sorted, b.left, b.right, b.parent, b.blo, b.bhi, b.nodes, b.tris, b.shd};
     for (void *p : ps)
         if (p) cudaFree(p);
     b.morton = nullptr; b.sorted = nullptr; b.left = b.right = b.parent = nullptr;
-    b.blo = b.bhi = nullptr; b.nodes = b.tris = nullptr;
+    b.blo = b.bhi = nullptr; b.nodes = b.tris = b.shd = nullptr;
     b.wide_nodes = b.wide_depth = 0;
 }
 
@@ -724,6 +750,7 @@ int bvh_build(BvhBuild &b, uint32_t kind, cudaStream_t s, std::string &err) {
     BCHK(cudaMalloc(&b.blo, total * sizeof(float4)));
     BCHK(cudaMalloc(&b.bhi, total * sizeof(float4)));
     BCHK(cudaMalloc(&b.tris, 3 * (size_t)n * sizeof(float4)));
+    BCHK(cudaMalloc(&b.shd, 3 * (size_t)n * sizeof(float4)));
     const uint32_t max_nodes = n > 1 ? n - 1 : 1;
     BCHK(cudaMalloc(&b.nodes, 5 * (size_t)max_nodes * sizeof(float4)));
 

@@ -70,21 +70,23 @@ __device__ __forceinline__ v3 vtx(const float *V, uint32_t i) {
 }
 
 // GetTriangleArea, Common.h:59-62
+__device__ __forceinline__ float tri_area(v3 a, v3 b, v3 c) { return 0.5f * length(cross(b - a, c - a)); }
 __device__ __forceinline__ float tri_area(const DevScene &sc, uint32_t t) {
     uint4 ti = sc.tri[t];
-    v3 a = vtx(sc.V, ti.x), b = vtx(sc.V, ti.y), c = vtx(sc.V, ti.z);
-    return 0.5f * length(cross(b - a, c - a));
+    return tri_area(vtx(sc.V, ti.x), vtx(sc.V, ti.y), vtx(sc.V, ti.z));
 }
+
 
 // Texture colour of a hit (PathTracing.cu:262-268): the material's texture at the interpolated
 // texture coordinates (BarycentricByIndices, Common.h:40-51), RGB of a bilinear, wrapping,
 // normalised read. WL_MATH_FAST reads through the texture unit, as the reference does. Strict
 // mode filters in software with the texture unit's documented arithmetic (coordinates
 // u W - 0.5, weights with 8 fractional bits), so that it matches the CPU oracle bit for bit.
-__device__ __forceinline__ v3 tex_color(const DevScene &sc, uint32_t mid, uint4 ti, float bu,
+__device__ __forceinline__ v3 tex_color(const DevScene &sc, uint32_t mid, uint32_t prim, float bu,
                                         float bv) {
     int32_t t = sc.mats[mid].texture;
     if (t < 0 || (uint32_t)t >= sc.nTex || !sc.UV) return v3(1.0f);
+    const uint4 ti = sc.tri[prim];
     const float2 *UV = reinterpret_cast<const float2 *>(sc.UV);
     float2 a = UV[ti.x], b = UV[ti.y], c = UV[ti.z];
     float w0 = 1.0f - bu - bv;
@@ -151,9 +153,9 @@ __device__ __forceinline__ void shade_lane(const WaveParams &wp, const DevScene 
             rng.pixel = (uint32_t)(g % wp.npix);
             rng.state = (uint64_t)rs.x | ((uint64_t)rs.y << 32);
             v3 pos = f4xyz(ro), dir = f4xyz(rd);
-            uint32_t prim = __float_as_uint(h.y);
+            const uint32_t leaf = __float_as_uint(h.y);
             bool alive = true;
-            if (prim == INVALID) {
+            if (leaf == INVALID) {
                 // __miss__radiance (PathTracing.cu:163-171); a constant environment is weighted
                 // by the last BSDF term as well (the reference's background is 0)
                 if (wp.has_env) rad = rad + thr * term * ld3(wp.env);
@@ -162,19 +164,22 @@ __device__ __forceinline__ void shade_lane(const WaveParams &wp, const DevScene 
                 // __closesthit__radiance (PathTracing.cu:181-288)
                 depth += 1;
                 float t = h.x;
-                uint4 ti = sc.tri[prim];
-                v3 a = vtx(sc.V, ti.x), b = vtx(sc.V, ti.y), c = vtx(sc.V, ti.z);
+                // the triangle's vertices (the tree's leaf record) and shading record, both in
+                // leaf order; the same values as the scene's vertex and normal arrays
+                const float4 *lr = sc.tris + 3 * (size_t)leaf, *sr = sc.shd + 3 * (size_t)leaf;
+                const float4 s0 = sr[0], s1 = sr[1], s2 = sr[2];
+                const uint32_t tiw = __float_as_uint(s0.w), prim = __float_as_uint(s2.w);
+                v3 a = f4xyz(lr[0]), b = f4xyz(lr[1]), c = f4xyz(lr[2]);
                 v3 Ng = normalize(cross(b - a, c - a));
                 v3 Ns;
-                if (ti.w >> 31) {
+                if (tiw >> 31) {
                     float bu = h.z, bv = h.w;
-                    Ns = normalize(vtx(sc.N, ti.x) * (1.0f - bu - bv) + vtx(sc.N, ti.y) * bu +
-                                   vtx(sc.N, ti.z) * bv);
+                    Ns = normalize(f4xyz(s0) * (1.0f - bu - bv) + f4xyz(s1) * bu + f4xyz(s2) * bv);
                 } else {
                     Ns = Ng;
                 }
                 v3 hit_pos = pos + dir * t;
-                uint32_t lid = sc.tri_light[prim];
+                uint32_t lid = __float_as_uint(s1.w);
                 if (lid != INVALID) {
                     const DevLight &lt = sc.lights[lid];
                     if (depth == 1 || (wp.strategy != WL_STRATEGY_NEE &&
@@ -188,7 +193,7 @@ __device__ __forceinline__ void shade_lane(const WaveParams &wp, const DevScene 
                             } else {
                                 lp = 1.0f / (float)sc.nLight;
                                 lp /= (float)lt.tri_count;
-                                lp /= tri_area(sc, prim);
+                                lp /= tri_area(a, b, c);
                             }
                             nee_pdf = lp * t * t / fabsf(dot(Ns, dir));
                         }
@@ -198,7 +203,7 @@ __device__ __forceinline__ void shade_lane(const WaveParams &wp, const DevScene 
                 } else if (depth >= wp.max_depth) {
                     alive = false;
                 } else {
-                    Mat m = load_mat(sc.mats + (ti.w & 0x7fffffffu));
+                    Mat m = load_mat(sc.mats + (tiw & 0x7fffffffu));
                     if (m.trans < 0.1f) {
                         if (dot(Ng, dir) > 0.0f) Ng = -Ng;
                         if (dot(Ns, dir) > 0.0f) Ns = -Ns;
@@ -211,7 +216,7 @@ __device__ __forceinline__ void shade_lane(const WaveParams &wp, const DevScene 
                         bool train = (g % nb.train_stride) == (nb.first_g % nb.train_stride);
                         v3 T = thr * term;
                         NrcVertex rv;
-                        rv.pos_mat = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, __uint_as_float(ti.w & 0x7fffffffu));
+                        rv.pos_mat = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, __uint_as_float(tiw & 0x7fffffffu));
                         rv.wo = make_float4(V.x, V.y, V.z, 0.f);
                         rv.n = make_float4(Ns.x, Ns.y, Ns.z, 0.f);
                         if (train && depth != nb.train_end) {
@@ -239,7 +244,7 @@ __device__ __forceinline__ void shade_lane(const WaveParams &wp, const DevScene 
                     } else if (pdf < 0.0f || isnan(pdf)) {
                         alive = false;
                     } else {
-                        v3 tex = tex_color(sc, ti.w & 0x7fffffffu, ti, h.z, h.w);
+                        v3 tex = tex_color(sc, tiw & 0x7fffffffu, prim, h.z, h.w);
                         thr = thr * term;
                         float cosw = dot(ndir, Ns);
                         v3 bsdf = clampv(eval_disney(m, Ns, Ng, V, ndir, tex), 0.f, 1e30f);
@@ -373,10 +378,10 @@ __device__ __forceinline__ void shade_emit(const Queues &q, int out, bool valid,
 constexpr uint32_t SHADE_KEYS = 16;
 static_assert(SHADE_KEYS * (PT / 32) == 128, "the key scan covers 4 (key, warp) counts per lane");
 
-__device__ __forceinline__ uint32_t shade_key(const DevScene &sc, uint32_t prim) {
-    if (prim == INVALID) return 0u;
-    if (sc.tri_light[prim] != INVALID) return 1u;
-    return 2u + (sc.tri[prim].w & 0x7fffffffu) % (SHADE_KEYS - 3);
+__device__ __forceinline__ uint32_t shade_key(const DevScene &sc, uint32_t leaf) {
+    if (leaf == INVALID) return 0u;
+    if (__float_as_uint(sc.shd[3 * (size_t)leaf + 1].w) != INVALID) return 1u;
+    return 2u + (__float_as_uint(sc.shd[3 * (size_t)leaf].w) & 0x7fffffffu) % (SHADE_KEYS - 3);
 }
 
 // Returns the queue index this thread shades (block-collective: every thread of the block

@@ -139,7 +139,8 @@ __global__ void __launch_bounds__(TT, TRACE_MIN_CTAS) k_trace(DevScene sc, Queue
         if (warp_trav<ANY, STATS>(active, busy, post, st, stack, nodes, tris, cn, ct)) {
             active = false;
             if (MODE == 0) {
-                q.hit[my] = make_float4(st.res.t, __uint_as_float(st.res.prim), st.res.u, st.res.v);
+                // the hit by leaf index (INVALID on a miss): shading reads the leaf-ordered records
+                q.hit[my] = make_float4(st.res.t, __uint_as_float(st.res.leaf), st.res.u, st.res.v);
             } else if (MODE == 2 && st.res.prim == INVALID) {
                 float4 l = q.sh_l[my];
                 q.conn_val[__float_as_uint(l.w)] = make_float4(l.x, l.y, l.z, 0.f);

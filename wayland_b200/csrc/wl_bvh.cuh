@@ -353,7 +353,8 @@ inline float4 ldg4(const float4 *p) { return *p; }
 
 struct TraceResult {
     float t, u, v;
-    uint32_t prim;
+    uint32_t prim;  // triangle id (INVALID on a miss)
+    uint32_t leaf;  // its position in the leaf-ordered triangle records
 };
 
 WL_HD int lowest_bit(uint32_t x) {
@@ -399,6 +400,7 @@ WL_HD void trav_init(TravState &s, float ox, float oy, float oz, float dx, float
     s.oct = (dx < 0.0f ? 1u : 0u) | (dy < 0.0f ? 2u : 0u) | (dz < 0.0f ? 4u : 0u);
     s.res.t = tmax;
     s.res.prim = INVALID;
+    s.res.leaf = INVALID;
     s.res.u = s.res.v = 0.f;
     s.ng = make_uint2(0u, (1u << (24 + s.oct)) | 1u);  // the root as the only child of a group
     s.tg = make_uint2(0u, 0u);
@@ -466,7 +468,8 @@ template <bool ANY>
 WL_HD bool tri_test_next(TravState &s, const float4 *__restrict__ tris) {
     int k = lowest_bit(s.tg.y);
     s.tg.y &= s.tg.y - 1u;
-    const float4 *tp = tris + 3 * (size_t)(s.tg.x + (uint32_t)k);
+    const uint32_t leaf = s.tg.x + (uint32_t)k;
+    const float4 *tp = tris + 3 * (size_t)leaf;
     float4 v0 = ldg4(tp), v1 = ldg4(tp + 1), v2 = ldg4(tp + 2);
     float t, u, v;
     if (tri_hit(s.pre, s.ox, s.oy, s.oz, v0, v1, v2, s.tmin, s.tmax, t, u, v)) {
@@ -474,6 +477,7 @@ WL_HD bool tri_test_next(TravState &s, const float4 *__restrict__ tris) {
         if (ANY || t < s.res.t || (t == s.res.t && prim < s.res.prim)) {
             s.res.t = t;
             s.res.prim = prim;
+            s.res.leaf = leaf;
             s.res.u = u;
             s.res.v = v;
             return true;

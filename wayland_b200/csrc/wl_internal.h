@@ -34,6 +34,9 @@ struct DevScene {
     const DevLight *lights;
     const float4 *nodes;     // 8-wide BVH, 5 float4 per node
     const float4 *tris;      // triangle records in leaf order, 3 float4 each
+    // shading records in the same leaf order, 3 float4 each: (n0, material | has_normal << 31),
+    // (n1, light id), (n2, triangle id); the extend pass reports hits by leaf index
+    const float4 *shd;
     uint32_t has_bvh;
     // power-proportional light selection: FP64 CDF over emissive triangles
     const double *emit_cdf;  // nEmit, inclusive prefix sums / total
@@ -45,6 +48,14 @@ struct DevScene {
     const uint32_t *const *tex_rgba;
     const uint2 *tex_size;
 };
+
+#ifdef __CUDACC__
+// Triangle id of a hit that the extend pass reported by leaf index (DevScene::shd); a miss
+// (0xFFFFFFFF) stays a miss.
+__device__ __forceinline__ uint32_t leaf_prim(const DevScene &sc, uint32_t leaf) {
+    return leaf == 0xFFFFFFFFu ? leaf : __float_as_uint(sc.shd[3 * (size_t)leaf + 2].w);
+}
+#endif
 
 // Path-state arrays of one wave (structure of arrays in HBM, indexed by path slot).
 struct Queues {
@@ -274,12 +285,16 @@ struct BvhBuild {
     float4 *blo, *bhi;     // 2 nT - 1
     float4 *nodes;         // 5 per wide node
     float4 *tris;          // 3 per triangle
+    float4 *shd;           // 3 per triangle, leaf order (DevScene::shd)
     uint32_t wide_nodes, wide_depth;
     float ms;
 };
 // kind: WL_BVH_LBVH (Karras radix tree) or WL_BVH_SAH (binned SAH); both end in the same
 // bottom-up bounds and 8-wide collapse.
 int bvh_build(BvhBuild &b, uint32_t kind, cudaStream_t s, std::string &err);
+// Fills b.shd from the scene's triangle table, normals (or null) and light ids.
+void bvh_fill_shading(BvhBuild &b, const uint4 *tri, const float *N, const uint32_t *tri_light,
+                      cudaStream_t s);
 void bvh_free(BvhBuild &b);
 
 // nrc.cu
