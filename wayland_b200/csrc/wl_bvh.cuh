@@ -424,7 +424,7 @@ WL_HD void node_test(const TravState &s, const float4 *__restrict__ np, uint2 &n
     uint32_t qhy0 = as_uint(n4.x), qhy1 = as_uint(n4.y), qhz0 = as_uint(n4.z), qhz1 = as_uint(n4.w);
     const float tcur = s.res.t;
     const float grow = 1.0f + 0x1p-20f;
-    uint32_t ihits = 0, thits = 0;
+    uint32_t hits = 0;
     // Slab distances in one FMA per plane: t = q A + B with A = scale / d (exact: power-of-two
     // scale) and B = (origin - o) / d. The absolute error of such a t is below
     // 3 u (255 |A| + |B|) (u = 2^-24: one rounding in origin - o, one in the product, one in
@@ -437,7 +437,7 @@ WL_HD void node_test(const TravState &s, const float4 *__restrict__ np, uint2 &n
     const float ex = fmaf(fabsf(ax), 255.0f, fabsf(bx)) * 0x1p-21f;
     const float ey = fmaf(fabsf(ay), 255.0f, fabsf(by)) * 0x1p-21f;
     const float ez = fmaf(fabsf(az), 255.0f, fabsf(bz)) * 0x1p-21f;
-    const float bnx = bx - ex, bfx = bx + ex, bny = by - ey, bfy = by + ey, bnz = bz - ez, bfz = bz + ez;
+    const float bnx = bx - ex, bny = by - ey, bnz = bz - ez, bfx = bx + ex, bfy = by + ey, bfz = bz + ez;
     const bool sx = s.oct & 1u, sy = s.oct & 2u, sz = s.oct & 4u;
     const uint32_t qnx0 = sx ? qhx0 : qlx0, qnx1 = sx ? qhx1 : qlx1, qfx0 = sx ? qlx0 : qhx0, qfx1 = sx ? qlx1 : qhx1;
     const uint32_t qny0 = sy ? qhy0 : qly0, qny1 = sy ? qhy1 : qly1, qfy0 = sy ? qly0 : qhy0, qfy1 = sy ? qly1 : qhy1;
@@ -453,13 +453,17 @@ WL_HD void node_test(const TravState &s, const float4 *__restrict__ np, uint2 &n
         float tnz = fmaf(byte_plus_2p23(qnz0, qnz1, c) - K, az, bnz), tfz = fmaf(byte_plus_2p23(qfz0, qfz1, c) - K, az, bfz);
         float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, s.tmin));
         float tf = fminf(fminf(tfx, tfy), fminf(tfz, tcur));
-        if (tn <= XMUL(tf, grow)) {
-            if (imask & (1u << c)) ihits |= 1u << ((uint32_t)c ^ s.oct);
-            else thits |= (meta >> 5) << (meta & 31u);
-        }
+        // meta of an internal child is 0x20 | (24 + c): its hit lands on bit 24 + c, a leaf's
+        // triangles on bits [offset, offset + count)
+        if (tn <= XMUL(tf, grow)) hits |= (meta >> 5) << (meta & 31u);
     }
-    ng = make_uint2(as_uint(n1.x), (ihits << 24) | imask);
-    tg = make_uint2(as_uint(n1.y), thits);
+    // internal hits from slot order to visiting order (bit c -> bit c XOR octant)
+    uint32_t ih = hits >> 24;
+    if (s.oct & 1u) ih = ((ih & 0x55u) << 1) | ((ih >> 1) & 0x55u);
+    if (s.oct & 2u) ih = ((ih & 0x33u) << 2) | ((ih >> 2) & 0x33u);
+    if (s.oct & 4u) ih = ((ih & 0x0fu) << 4) | ((ih >> 4) & 0x0fu);
+    ng = make_uint2(as_uint(n1.x), (ih << 24) | imask);
+    tg = make_uint2(as_uint(n1.y), hits & 0x00ffffffu);
 }
 
 // Tests the lowest pending triangle of s.tg (and removes it from the group). Returns true for
