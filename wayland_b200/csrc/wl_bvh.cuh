@@ -444,8 +444,7 @@ WL_HD void node_test(const TravState &s, const float4 *__restrict__ np, uint2 &n
     const uint32_t qnz0 = sz ? qhz0 : qlz0, qnz1 = sz ? qhz1 : qlz1, qfz0 = sz ? qlz0 : qhz0, qfz1 = sz ? qlz1 : qhz1;
 #pragma unroll
     for (int c = 0; c < 8; c++) {
-        uint32_t meta = byte_of(m0, m1, c);
-        if (meta == 0) continue;
+        uint32_t meta = byte_of(m0, m1, c);  // 0 for an empty slot, which then adds no bits
         // plane q of a child: (2^23 + q) - 2^23, exact, built by a byte permute (no I2F)
         const float K = 8388608.0f;
         float tnx = fmaf(byte_plus_2p23(qnx0, qnx1, c) - K, ax, bnx), tfx = fmaf(byte_plus_2p23(qfx0, qfx1, c) - K, ax, bfx);
