@@ -445,11 +445,13 @@ WL_HD void node_test(const TravState &s, const float4 *__restrict__ np, uint2 &n
 #pragma unroll
     for (int c = 0; c < 8; c++) {
         uint32_t meta = byte_of(m0, m1, c);  // 0 for an empty slot, which then adds no bits
-        // plane q of a child: (2^23 + q) - 2^23, exact, built by a byte permute (no I2F)
+        // x and y planes of a child: (2^23 + q) - 2^23, exact, built by a byte permute
         const float K = 8388608.0f;
         float tnx = fmaf(byte_plus_2p23(qnx0, qnx1, c) - K, ax, bnx), tfx = fmaf(byte_plus_2p23(qfx0, qfx1, c) - K, ax, bfx);
         float tny = fmaf(byte_plus_2p23(qny0, qny1, c) - K, ay, bny), tfy = fmaf(byte_plus_2p23(qfy0, qfy1, c) - K, ay, bfy);
-        float tnz = fmaf(byte_plus_2p23(qnz0, qnz1, c) - K, az, bnz), tfz = fmaf(byte_plus_2p23(qfz0, qfz1, c) - K, az, bfz);
+        // z planes by I2F on the otherwise idle conversion pipe: a third of the conversions off
+        // the ALU/FMA issue slots (measured best against none or two thirds)
+        float tnz = fmaf((float)byte_of(qnz0, qnz1, c), az, bnz), tfz = fmaf((float)byte_of(qfz0, qfz1, c), az, bfz);
         float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, s.tmin));
         float tf = fminf(fminf(tfx, tfy), fminf(tfz, tcur));
         // meta of an internal child is 0x20 | (24 + c): its hit lands on bit 24 + c, a leaf's
