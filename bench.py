@@ -28,10 +28,10 @@ sys.path.insert(0, ROOT)
 
 W, H, SPP, DEPTH = 1920, 1080, 64, 16
 METRIC = "Mpaths/s"
-# DRAM bytes (read + write) per extend ray of this workload: 45.04 GB over the 16 extend launches
+# DRAM bytes (read + write) per extend ray of this workload: 45.64 GB over the 16 extend launches
 # of one step (one wave) in the ncu launch list of
 # profiles/launches_plain_pt_displaced_sphere_1920x1080x64spp.md, / 298.3 M rays per step
-EXTEND_DRAM_BYTES_PER_RAY = 151.0
+EXTEND_DRAM_BYTES_PER_RAY = 153.0
 WORKLOAD = "plain PT at scale: displaced icosphere 1,997,120 tris + ground, 4 quad lights + env 0.1, 1920x1080, 64 spp, depth 16, FP32"
 
 
