@@ -660,8 +660,9 @@ def main():
         achieved = segs * b_ray / (ext_ms * 1e-3) / 1e9
         b_path = 96 + 364 * seg_per_path
         # DRAM bytes per extend launch: the profiled bytes per ray x this run's rays per extend
-        # launch (a wave launches generate and film once and extend, shade, shadow per bounce)
-        ext_launches = max((st["kernel_launches"] - 2 * st["waves"]) // 3, 1)
+        # launch (a wave launches generate, a counter reset and film once, and extend, a counter
+        # reset, shade and shadow per bounce)
+        ext_launches = max((st["kernel_launches"] - 3 * st["waves"]) // 4, 1)
         traffic = round(EXTEND_DRAM_BYTES_PER_RAY * segs / ext_launches) if args.case == "full" else None
         line = {
             "metric": METRIC, "value": round(value, 2), "unit": METRIC, "n_gpus": world,

@@ -803,22 +803,25 @@ static uint32_t pt_wave(wl_context *c, const WaveParams &wp, const DevScene &sc,
     if (strict_math) strict::launch_generate(wp, c->q, st);
     else fast::launch_generate(wp, c->q, st);
     rec(c, 3, false);
-    launches++;
+    launches += 2;  // generate and the first counter reset
     // Bounce b: extend and shade on the main stream; the shadow pass of bounce b on the side
     // stream, concurrently with the extension rays of bounce b + 1 (which touch neither the
     // shadow queue nor the path radiance). The shade pass of bounce b + 1, the next writer of
     // both, waits for it, so the radiance still sums emission b, light sample b, emission b + 1
     // in the reference's order.
+    // counters: one reset launch per bounce zeroes the next ray queue's size [in ^ 1], the
+    // shadow queue's size [2] and the extend / shadow work counters [6] / [7] (the extend pass
+    // before it and the shadow pass it joins have finished with them)
     cudaStream_t sd = c->side;
     cudaEvent_t join_prev = nullptr;
+    launch_reset_counters(c->q.counters, (1u << 6) | (1u << 7), st);
     int in = 0;
     for (uint32_t b = 0; b < max_depth; b++) {
         rec(c, 0, true);
-        launch_extend(sc, c->q, in, tstats, st, c->tune_extend);
+        launch_extend(sc, c->q, in, tstats, st, c->tune_extend, BatchView{}, false);
         rec(c, 0, false);
         if (join_prev) cudaStreamWaitEvent(st, join_prev, 0);
-        cudaMemsetAsync(c->q.counters + (in ^ 1), 0, sizeof(uint32_t), st);
-        cudaMemsetAsync(c->q.counters + 2, 0, sizeof(uint32_t), st);
+        launch_reset_counters(c->q.counters, (1u << (in ^ 1)) | (1u << 2) | (1u << 6) | (1u << 7), st);
         rec(c, 1, true);
         if (strict_math) strict::launch_shade(wp, sc, c->q, in, st);
         else fast::launch_shade(wp, sc, c->q, in, st);
@@ -828,11 +831,11 @@ static uint32_t pt_wave(wl_context *c, const WaveParams &wp, const DevScene &sc,
         cudaEventRecord(fk, st);
         cudaStreamWaitEvent(sd, fk, 0);
         rec(c, 2, true, sd);
-        launch_shadow(sc, c->q, tstats, sd, c->tune_shadow);
+        launch_shadow(sc, c->q, tstats, sd, c->tune_shadow, BatchView{}, false);
         rec(c, 2, false, sd);
         cudaEventRecord(jn, sd);
         join_prev = jn;
-        launches += 3;
+        launches += 4;  // extend, counter reset, shade, shadow
         in ^= 1;
     }
     if (join_prev) cudaStreamWaitEvent(st, join_prev, 0);

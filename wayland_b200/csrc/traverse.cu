@@ -281,17 +281,28 @@ void trace_dispatch(const DevScene &sc, const Queues &q, int in, uint32_t *fetch
 
 }  // namespace
 
-// Work counters live in the queues' counter block: [6] extend, [7] shadow, [8] cast.
+__global__ void k_reset_counters(uint32_t *c, uint32_t mask) {
+    const uint32_t i = threadIdx.x;
+    if (i < 32 && ((mask >> i) & 1u)) c[i] = 0u;
+}
+
+// Zeroes counters[i] for every bit i of mask (i < 32) in one launch.
+void launch_reset_counters(uint32_t *counters, uint32_t mask, cudaStream_t s) {
+    k_reset_counters<<<1, 32, 0, s>>>(counters, mask);
+}
+
+// Work counters live in the queues' counter block: [6] extend, [7] shadow, [8] cast. With
+// zero_fetch false the caller has zeroed the work counter already (launch_reset_counters).
 void launch_extend(const DevScene &sc, const Queues &q, int in, bool stats, cudaStream_t s,
-                   const TraceTune &t, const BatchView &bv) {
-    cudaMemsetAsync(q.counters + 6, 0, sizeof(uint32_t), s);
+                   const TraceTune &t, const BatchView &bv, bool zero_fetch) {
+    if (zero_fetch) cudaMemsetAsync(q.counters + 6, 0, sizeof(uint32_t), s);
     if (stats) trace_dispatch<0, true>(sc, q, in, q.counters + 6, t, bv, s);
     else trace_dispatch<0, false>(sc, q, in, q.counters + 6, t, bv, s);
 }
 
 void launch_shadow(const DevScene &sc, const Queues &q, bool stats, cudaStream_t s,
-                   const TraceTune &t, const BatchView &bv) {
-    cudaMemsetAsync(q.counters + 7, 0, sizeof(uint32_t), s);
+                   const TraceTune &t, const BatchView &bv, bool zero_fetch) {
+    if (zero_fetch) cudaMemsetAsync(q.counters + 7, 0, sizeof(uint32_t), s);
     if (stats) trace_dispatch<1, true>(sc, q, 0, q.counters + 7, t, bv, s);
     else trace_dispatch<1, false>(sc, q, 0, q.counters + 7, t, bv, s);
 }

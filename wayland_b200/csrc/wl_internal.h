@@ -262,9 +262,12 @@ struct TraceTune {
     uint32_t postpone = 12;  // triangle phase when >= postpone/32 of the busy lanes hold triangles
 };
 void launch_extend(const DevScene &sc, const Queues &q, int in, bool stats, cudaStream_t s,
-                   const TraceTune &t = TraceTune{}, const BatchView &bv = BatchView{});
+                   const TraceTune &t = TraceTune{}, const BatchView &bv = BatchView{},
+                   bool zero_fetch = true);
 void launch_shadow(const DevScene &sc, const Queues &q, bool stats, cudaStream_t s,
-                   const TraceTune &t = TraceTune{}, const BatchView &bv = BatchView{});
+                   const TraceTune &t = TraceTune{}, const BatchView &bv = BatchView{},
+                   bool zero_fetch = true);
+void launch_reset_counters(uint32_t *counters, uint32_t mask, cudaStream_t s);
 void launch_connection_rays(const DevScene &sc, const Queues &q, const BdptWave &bw, bool stats,
                             cudaStream_t s, const TraceTune &t = TraceTune{});
 void launch_cast(const DevScene &sc, const wl_ray *rays, wl_hit *hits, uint32_t n, uint32_t mode,
