@@ -1522,20 +1522,21 @@ int wl_render_nrc(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_ren
             int in = 0;
             // every path has ended by vertex train_end when training paths end at the cache
             const uint32_t bounces = nb.train_end && nb.train_end < p->max_depth ? nb.train_end : p->max_depth;
-            // the shadow pass of bounce b overlaps the extension rays of bounce b + 1 (as pt_wave)
+            // the shadow pass of bounce b overlaps the extension rays of bounce b + 1, and one
+            // reset launch per bounce zeroes the counters (as pt_wave)
             cudaEvent_t join_prev = nullptr;
+            launch_reset_counters(c->q.counters, (1u << 6) | (1u << 7), st);
             for (uint32_t b = 0; b < bounces; b++) {
-                launch_extend(sc, c->q, in, false, st, c->tune_extend);
+                launch_extend(sc, c->q, in, false, st, c->tune_extend, BatchView{}, false);
                 if (join_prev) CK(cudaStreamWaitEvent(st, join_prev, 0));
-                CK(cudaMemsetAsync(c->q.counters + (in ^ 1), 0, sizeof(uint32_t), st));
-                CK(cudaMemsetAsync(c->q.counters + 2, 0, sizeof(uint32_t), st));
+                launch_reset_counters(c->q.counters, (1u << (in ^ 1)) | (1u << 2) | (1u << 6) | (1u << 7), st);
                 if (strict_math) strict::launch_shade_nrc(wp, sc, c->q, in, nb, st);
                 else fast::launch_shade_nrc(wp, sc, c->q, in, nb, st);
                 cudaEvent_t fk, jn;
                 fork_join(c, b, fk, jn);
                 CK(cudaEventRecord(fk, st));
                 CK(cudaStreamWaitEvent(c->side, fk, 0));
-                launch_shadow(sc, c->q, false, c->side, c->tune_shadow);
+                launch_shadow(sc, c->q, false, c->side, c->tune_shadow, BatchView{}, false);
                 CK(cudaEventRecord(jn, c->side));
                 join_prev = jn;
                 in ^= 1;
