@@ -150,7 +150,9 @@ typedef struct wl_render_params {
     uint32_t wave_paths;    /* paths in flight per wave (<= 2^27); 0 = automatic: the context's
                                tuned size, else as many as the render has, up to 2^27 paths
                                (192 B of queues each) and a quarter of the device memory free
-                               at the context's first render */
+                               at the context's first render. WL_STRATEGY_BDPT: samples per
+                               wave, automatic = as many as a quarter of the free device
+                               memory holds (about 8.4 KB each at 10 vertices) */
     uint32_t flags;         /* WL_RENDER_* bits */
 } wl_render_params;
 

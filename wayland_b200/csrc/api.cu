@@ -80,8 +80,10 @@ struct wl_context {
     uint64_t graph_clock = 0;
     // launch shapes chosen by wl_autotune (defaults until then)
     uint32_t tune_wave = 0;
-    // automatic paths per wave (set on first use, see auto_wave)
+    // automatic paths per wave (set on first use, see auto_wave), and the device memory that
+    // automatic bidirectional waves may use (set on first use, see auto_bdpt_wave)
     uint64_t auto_wave = 0;
+    uint64_t bdpt_budget = 0;
     TraceTune tune_extend{}, tune_shadow{};
     // batched renders: the job table and the job of every wave slot
     BatchJob *d_jobs = nullptr;
@@ -175,6 +177,24 @@ uint64_t auto_wave(wl_context *c) {
         c->auto_wave = w < (1ull << 20) ? (1ull << 20) : w;
     }
     return c->auto_wave;
+}
+
+// Automatic samples per bidirectional wave for subpaths of maxv vertices: as many as fit in a
+// quarter of the device memory free at the context's first bidirectional render, at the
+// worst case of ensure_bdpt (10 vertex arrays of maxv float4, maxv^2 connections of 68 B per
+// sample), with at most 2^30 connection slots. Few, large waves: every wave ends in a tail of
+// small launches (256 waves of 1 spp of 512^2 ran 2.9x slower than 26).
+uint64_t auto_bdpt_wave(wl_context *c, uint32_t maxv) {
+    if (!c->bdpt_budget) {
+        size_t free_b = 0, total_b = 0;
+        c->bdpt_budget = cudaMemGetInfo(&free_b, &total_b) == cudaSuccess ? (uint64_t)free_b / 4 : (1ull << 31);
+        if (c->bdpt_budget < (1ull << 28)) c->bdpt_budget = 1ull << 28;
+    }
+    const uint64_t per = 160ull * maxv + 68ull * maxv * maxv + 32;
+    uint64_t w = c->bdpt_budget / per;
+    const uint64_t cap = (1ull << 30) / ((uint64_t)maxv * maxv);
+    if (w > cap) w = cap;
+    return w < 1024 ? 1024 : w;
 }
 
 // Path-state and queue arrays for `cap` paths in one allocation.
@@ -1001,10 +1021,10 @@ int wl_render(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_
     const bool bdpt = p->strategy == WL_STRATEGY_BDPT;
     const uint64_t maxv2 = (uint64_t)p->max_depth * p->max_depth;
     uint64_t want = p->wave_paths ? p->wave_paths
-                                  : (bdpt ? (1ull << 25) / maxv2 : (c->tune_wave ? c->tune_wave : auto_wave(c)));
+                                  : (bdpt ? auto_bdpt_wave(c, p->max_depth) : (c->tune_wave ? c->tune_wave : auto_wave(c)));
     if (want < 1024) want = 1024;
     if (want > (1ull << 27)) want = 1ull << 27;
-    if (bdpt && want > (1ull << 26) / maxv2) want = (1ull << 26) / maxv2;
+    if (bdpt && want > (1ull << 30) / maxv2) want = (1ull << 30) / maxv2;
     uint32_t spp_per_wave = (uint32_t)(want / npix);
     uint64_t wave = spp_per_wave >= 1 ? (uint64_t)spp_per_wave * npix : want;
     if (wave > total) wave = total;
