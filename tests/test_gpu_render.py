@@ -385,3 +385,36 @@ def test_power_lights_strict_vs_oracle(ctx, oracle, rng):
     _, ia, _, _ = gpu_render(ctx, sc, a, fp64=True)
     _, ib, _, _ = gpu_render(ctx, sc, b, fp64=True)
     assert abs(ia.mean() - ib.mean()) < 0.02 * ib.mean()
+
+
+def test_user_stream_orders_the_whole_render(ctx):
+    """A render issued on a caller's stream (wl_context_set_stream) is ordered on that stream as a
+    whole: the library's second stream, which runs the shadow passes, joins back before the
+    render's last kernel. A copy of the film enqueued on the caller's stream right after the call,
+    with no other synchronisation, reads the finished image: the strict image of the same render
+    on the context's own stream, bit for bit."""
+    from wayland_b200.multi import _DeviceArray
+    sc = small_sphere(48, 32)
+    s = wl.Scene(ctx, sc)
+    p = wl.render_params(48, 32, 8, math=wl.MATH_STRICT, env=sc.env)
+    ref = wl.Film(ctx, 48, 32)
+    wl.render(ctx, s, sc.camera_struct(), p, ref)
+    expected = ref.download()
+    ref.close()
+    user = torch.cuda.Stream()
+    ctx.set_stream(user.cuda_stream)
+    try:
+        film = wl.Film(ctx, 48, 32)
+        wl.render(ctx, s, sc.camera_struct(), p, film)
+        rgb = film.device_ptrs()[0]
+        with torch.cuda.stream(user):
+            view = torch.as_tensor(_DeviceArray(rgb, (32, 48, 3), "<f4"), device="cuda")
+            got = view.clone()
+        user.synchronize()
+        got = got.cpu().numpy()
+        film.close()
+    finally:
+        ctx.set_stream(None)
+    assert expected.max() > 0
+    assert np.array_equal(bits(got), bits(expected))
+    s.close()
