@@ -67,7 +67,8 @@ struct SplitStack {
 
 // One warp iteration of the batched traversal (trav_node / trav_tri): a triangle phase when the
 // lanes holding triangles are at least post/32 of the busy lanes (or no lane can visit a node),
-// kept up while that holds; otherwise a node phase. Returns true for a lane whose ray finished.
+// kept up while that holds; otherwise a node phase of up to NODE_STEPS node visits per lane.
+// Returns true for a lane whose ray finished.
 template <bool ANY, bool STATS>
 __device__ __forceinline__ bool warp_trav(bool active, uint32_t busy, uint32_t post, TravState &st,
                                           const SplitStack &stack, const float4 *__restrict__ nodes,
@@ -97,7 +98,7 @@ __device__ __forceinline__ bool warp_trav(bool active, uint32_t busy, uint32_t p
 }
 
 // Persistent traversal over a queue of n rays. MODE 0: closest hit of ray queue `in`, hit
-// written to q.hit. MODE 1: any hit of the shadow queue; an unoccluded ray adds its light
+// written to q.hit with the triangle's leaf index in place of its id. MODE 1: any hit of the shadow queue; an unoccluded ray adds its light
 // sample to the path radiance. MODE 2: any hit of the bidirectional connection rays (passed as
 // the shadow queue); an unoccluded ray stores its value as the result of its connection
 // (EvalContri's visibility ray, BDPT.cu:460-467).

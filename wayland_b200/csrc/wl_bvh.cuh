@@ -521,7 +521,8 @@ WL_HD bool trav_step(TravState &s, uint2 *stack, const float4 *__restrict__ node
 }
 
 // Batched traversal (the postponed-triangle scheme of Ylitie, Karras and Laine 2017): a warp
-// alternates node phases, in which every lane that can visits one node, and triangle phases,
+// alternates node phases, in which every lane that can visits a node (or a few in a row), and
+// triangle phases,
 // in which every lane holding triangles tests one. A lane that reaches a leaf while it still
 // holds untested triangles parks the new triangle group in s.tq and stops visiting nodes until
 // a triangle phase has emptied s.tg; the warp chooses the phase from how many lanes hold
