@@ -66,7 +66,7 @@ def host_bvh():
     lib.hb_destroy.argtypes = [C.c_void_p]
     lib.hb_cast.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]
     lib.hb_cast_batched.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
-                                    C.c_uint32, C.c_void_p, C.c_void_p]
+                                    C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]
     lib.hb_info.restype = C.c_uint32
     lib.hb_info.argtypes = [C.c_void_p, C.c_void_p]
     lib.hb_export.argtypes = [C.c_void_p] * 5

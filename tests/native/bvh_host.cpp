@@ -175,9 +175,10 @@ void hb_cast(void *p, const float *rays, uint32_t n, uint32_t mode, float *hits,
 
 // The batched traversal of the GPU kernels (trav_node / trav_tri with the warp's phase choice
 // and refill of idle lanes), played for one simulated 32-lane warp in lock step. post: the
-// triangle-phase threshold in 32nds of the busy lanes; refill: idle lanes that trigger a fetch.
+// triangle-phase threshold in 32nds of the busy lanes; refill: idle lanes that trigger a fetch;
+// node_steps: node visits per lane in a node phase.
 void hb_cast_batched(void *p, const float *rays, uint32_t n, uint32_t mode, uint32_t post,
-                     uint32_t refill, float *hits, uint64_t *stats) {
+                     uint32_t refill, uint32_t node_steps, float *hits, uint64_t *stats) {
     HostBvh *b = (HostBvh *)p;
     const float4 *nodes = (const float4 *)b->nodes.data();
     const float4 *tris = b->tris.data();
@@ -241,8 +242,13 @@ void hb_cast_batched(void *p, const float *rays, uint32_t n, uint32_t mode, uint
                 }
             } while (tm && (!nm || (uint32_t)__builtin_popcount(tm) * 32u >= need));
         } else {
-            for (int l = 0; l < 32; l++)
-                if (can_n[l]) trav_node<true>(st[l], ArrayStack{stack.data() + (size_t)l * TRAV_STACK}, nodes, &cn);
+            // a node phase: up to node_steps visits per lane (the kernels' NODE_STEPS)
+            for (int l = 0; l < 32; l++) {
+                const ArrayStack stk{stack.data() + (size_t)l * TRAV_STACK};
+                if (can_n[l]) trav_node<true>(st[l], stk, nodes, &cn);
+                for (uint32_t k = 1; k < node_steps; k++)
+                    if (active[l] && trav_can_node(st[l])) trav_node<true>(st[l], stk, nodes, &cn);
+            }
         }
         for (int l = 0; l < 32; l++) {
             if (active[l] && (fin[l] || trav_done(st[l]))) {

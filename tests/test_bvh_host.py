@@ -78,20 +78,22 @@ def test_rays_from_surfaces(host_bvh, oracle):
     host_bvh.hb_destroy(h)
 
 
-def host_cast_batched(host_bvh, h, rays, mode, post, refill):
+def host_cast_batched(host_bvh, h, rays, mode, post, refill, node_steps=3):
     hits = np.zeros(len(rays), po.HIT_DTYPE)
     st = np.zeros(2, np.uint64)
-    host_bvh.hb_cast_batched(h, rays.ctypes.data, len(rays), mode, post, refill, hits.ctypes.data,
-                             st.ctypes.data)
+    host_bvh.hb_cast_batched(h, rays.ctypes.data, len(rays), mode, post, refill, node_steps,
+                             hits.ctypes.data, st.ctypes.data)
     return hits, st
 
 
-@pytest.mark.parametrize("post,refill", [(0, 4), (8, 12), (16, 8), (24, 24), (32, 1)])
-def test_batched_traversal_matches(host_bvh, oracle, post, refill):
-    """The GPU kernels' batched traversal (node and triangle phases chosen per warp, postponed
-    triangle groups, refill of idle lanes), simulated for one warp: closest hits bit-exact
-    against brute force for every phase threshold, any-hit occlusion identical, and the same
-    node and triangle work as the one-lane traversal up to the culling it defers."""
+@pytest.mark.parametrize("post,refill,node_steps", [(0, 4, 3), (8, 12, 3), (16, 8, 1), (24, 24, 2),
+                                                    (32, 1, 3), (12, 6, 4)])
+def test_batched_traversal_matches(host_bvh, oracle, post, refill, node_steps):
+    """The GPU kernels' batched traversal (node and triangle phases chosen per warp, up to
+    node_steps node visits per phase, postponed triangle groups, refill of idle lanes),
+    simulated for one warp: closest hits bit-exact against brute force for every phase threshold,
+    any-hit occlusion identical, and at least the node and triangle work of the one-lane
+    traversal (the deferred triangle tests only delay culling)."""
     from wayland_b200 import scenes
     sc = scenes.displaced_sphere(subdiv=24)
     h, V, I = host_build(host_bvh, sc.V, sc.I)
@@ -102,11 +104,11 @@ def test_batched_traversal_matches(host_bvh, oracle, post, refill):
     sec["org"] = (prim["org"][ok] + prim["dir"][ok] * hit["t"][ok][:, None]).astype(np.float32)
     rays = np.concatenate([prim, sec, axis_rays(500, 19)])
     ref = oracle.cast_bruteforce(V, I, rays, 0)
-    got, st = host_cast_batched(host_bvh, h, rays, 0, post, refill)
+    got, st = host_cast_batched(host_bvh, h, rays, 0, post, refill, node_steps)
     assert np.array_equal(got.view(np.uint32).reshape(-1, 4), ref.view(np.uint32).reshape(-1, 4))
     _, st1 = host_cast(host_bvh, h, rays, 0)
     assert st[0] >= st1[0] and st[1] >= st1[1]
     anyr = oracle.cast_bruteforce(V, I, rays, 1)
-    anyg, _ = host_cast_batched(host_bvh, h, rays, 1, post, refill)
+    anyg, _ = host_cast_batched(host_bvh, h, rays, 1, post, refill, node_steps)
     assert np.array_equal(anyg["prim"] == 0xFFFFFFFF, anyr["prim"] == 0xFFFFFFFF)
     host_bvh.hb_destroy(h)
