@@ -424,11 +424,17 @@ WL_API int wl_debug_rng(wl_context *ctx, uint32_t rng, uint64_t seed, const uint
  * allocation's implicit device synchronisation would stall the frame.
  *  - At most WL_NOALLOC_MAX_PATHS paths are in flight per wave; larger renders run in more
  *    waves. params->wave_paths above that limit is rejected with WL_ERR_INVALID_ARG.
- *  - The first call on a device looks up the array's device address (cudaGetSymbolAddress);
- *    make that first call before any stream capture.
+ *  - wl_context_create looks up the array's device address (cudaGetSymbolAddress) with the
+ *    context's device current and keeps it in the context. CUDA loads the array's module, and
+ *    so reserves the array, at that lookup; wl_render_noalloc itself never does. Kernel code
+ *    that CUDA has not loaded yet (lazy loading) loads on its first launch: run one wl_render
+ *    first, or set CUDA_MODULE_LOADING=EAGER, where even that must not happen mid-run.
  *  - All calls on a device share the one array and its contents persist between calls. Calls
- *    whose work overlaps on the GPU (other streams, other threads) race on it and must not
- *    overlap.
+ *    whose work overlaps on the GPU (other streams, other threads, other contexts on the same
+ *    device) race on it and must not overlap.
+ *  - flags: only WL_RENDER_SORT_MATERIALS; other flags are rejected with WL_ERR_INVALID_ARG.
+ *    The render uses the context's launch shapes (wl_autotune / wl_set_tune) but always sizes
+ *    its own waves, and it restores the caller's current device before returning.
  *  - No render statistics are recorded (wl_render_get_stats keeps the last wl_render's). */
 #define WL_NOALLOC_MAX_PATHS 65536u
 #define WL_NOALLOC_SCRATCH_BYTES (192u * WL_NOALLOC_MAX_PATHS + 512u)

@@ -15,7 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB_ORACLE = os.path.join(HERE, "_build", "liboracle.so")
 LIB_REF = os.path.join(HERE, "_ref", "libwlref.so")
-REF_TREE = "/root/reference"
+# the reference source tree (only the oracle recipes read it); WL_REFERENCE_ROOT overrides it
+REF_TREE = os.environ.get("WL_REFERENCE_ROOT", "/root/reference")
 
 ORACLE_FLAGS = ["-O2", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", "-fopenmp",
                 "-shared", "-fPIC"]

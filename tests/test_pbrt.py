@@ -9,7 +9,8 @@ import pytest
 from wayland_b200 import pbrt
 from pbrt_fixture import write_scene
 
-REF_CBOX = "/root/reference/scene/cornell-box/cbox.pbrt"
+REF_CBOX = os.path.join(os.environ.get("WL_REFERENCE_ROOT", "/root/reference"),
+                        "scene", "cornell-box", "cbox.pbrt")
 
 
 def test_synthetic_scene(tmp_path):

@@ -46,13 +46,13 @@ def test_noalloc_matches_render_twice(own_ctx):
     assert ref.mean() > 0.01
     for call in range(2):
         film = wl.Film(ctx, 320, 240, fp64=True)
-        if call == 1:
-            torch.cuda.synchronize()
-            free_before = torch.cuda.mem_get_info()[0]
+        # the context reserved the scratch when it was created: neither the first call nor the
+        # second changes the device's free memory
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
         noalloc(ctx, scene, cam, p, film)
         ctx.sync()
-        if call == 1:
-            assert torch.cuda.mem_get_info()[0] == free_before
+        assert torch.cuda.mem_get_info()[0] == free_before, f"call {call} allocated"
         got = film.download()
         assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), f"call {call}"
         assert np.array_equal(film.download64().view(np.uint64), ref64.view(np.uint64))
@@ -74,3 +74,11 @@ def test_noalloc_fast_mode_and_limit(own_ctx):
     big = wl.render_params(96, 64, 4, wave_paths=_abi.NOALLOC_MAX_PATHS + 1)
     with pytest.raises(wl.WlError, match="INVALID_ARG.*static scratch limit"):
         noalloc(ctx, scene, cam, big, b)
+    # flags it cannot honour are refused rather than ignored
+    for flag in (_abi.RENDER_GRAPH, _abi.RENDER_TRAVERSAL_STATS):
+        with pytest.raises(wl.WlError, match="INVALID_ARG.*SORT_MATERIALS"):
+            noalloc(ctx, scene, cam, wl.render_params(96, 64, 4, flags=flag), b)
+    # the caller's current device is the same after the call
+    torch.cuda.set_device(0)
+    noalloc(ctx, scene, cam, p, b)
+    assert torch.cuda.current_device() == 0

@@ -90,6 +90,9 @@ struct wl_context {
     size_t jobs_cap = 0;
     uint16_t *d_slot_job = nullptr;
     size_t slot_job_cap = 0;
+    // device address of wl_render_noalloc's static scratch array, looked up when the context is
+    // created (loading the array's module is what reserves it, so that no later call does)
+    void *noalloc_base = nullptr;
 };
 
 struct wl_scene {
@@ -361,6 +364,11 @@ int wl_context_create(int device, wl_context **out) {
         cudaEventCreate(&c->ev_total[1]) != cudaSuccess) {
         wl_context_destroy(c);
         return fail(WL_ERR_OOM, "context allocation failed");
+    }
+    std::string err;
+    if (noalloc_scratch_address(&c->noalloc_base, err) != WL_OK) {
+        wl_context_destroy(c);
+        return fail(WL_ERR_CUDA, err);
     }
     *out = c;
     return WL_OK;
@@ -1386,7 +1394,8 @@ int wl_nrc_train_step(wl_nrc *n, const float *d_in, const float *d_target, uint3
     ARG(n && d_in && d_target, "null argument");
     ARG(count > 0 && count <= nrc_max_samples(n->net), "count out of range");
     CK(cudaSetDevice(n->ctx->device));
-    nrc_train_raw(n->net, d_in, d_target, count, n->ctx->stream);
+    if (nrc_train_raw(n->net, d_in, d_target, count, n->ctx->stream) != WL_OK)
+        return fail(WL_ERR_OOM, "radiance-cache training scratch could not be allocated");
     CK(cudaGetLastError());
     if (loss) {
         CK(cudaMemcpyAsync(loss, nrc_loss_ptr(n->net), 4, cudaMemcpyDeviceToHost, n->ctx->stream));
@@ -1399,7 +1408,8 @@ int wl_nrc_mlp_gradients(wl_nrc *n, const float *d_in, const float *d_target, ui
     ARG(n && d_in && d_target && grad, "null argument");
     ARG(count > 0 && count <= nrc_max_samples(n->net), "count out of range");
     CK(cudaSetDevice(n->ctx->device));
-    nrc_gradients_raw(n->net, d_in, d_target, count, n->ctx->stream);
+    if (nrc_gradients_raw(n->net, d_in, d_target, count, n->ctx->stream) != WL_OK)
+        return fail(WL_ERR_OOM, "radiance-cache training scratch could not be allocated");
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(grad, nrc_weight_grad(n->net), WL_NRC_WEIGHTS * 4, cudaMemcpyDeviceToHost, n->ctx->stream));
     CK(cudaStreamSynchronize(n->ctx->stream));
@@ -1568,7 +1578,8 @@ int wl_render_nrc(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_ren
             CK(cudaGetLastError());
         }
         // clamp the sample count to the buffer and train one step on the frame's samples
-        nrc_train_collected(n->net, s->d_mats, st);
+        if (nrc_train_collected(n->net, s->d_mats, st) != WL_OK)
+            return fail(WL_ERR_OOM, "radiance-cache training scratch could not be allocated");
         CK(cudaGetLastError());
     }
     if (f) f->f.frames64 += p->spp;
@@ -1727,11 +1738,11 @@ int wl_debug_rng(wl_context *c, uint32_t rng, uint64_t seed, const uint32_t *d_p
 
 namespace wl {
 // Resolves the handles of a render call for wl_render_noalloc (noalloc.cu): the same argument
-// checks as wl_render, then the device scene, the film and the stream. Allocates nothing.
+// checks as wl_render, then the device scene, the film, the stream, the context's launch shapes
+// and its scratch address. Allocates nothing.
 int noalloc_render_inputs(wl_context *c, wl_scene *s, const wl_camera *cam,
-                          const wl_render_params *p, wl_film *f, DevScene *sc, Film **film,
-                          cudaStream_t *stream, int *device) {
-    ARG(c && s && cam && p && f && sc && film && stream && device, "null argument");
+                          const wl_render_params *p, wl_film *f, NoallocCall *out) {
+    ARG(c && s && cam && p && f && out, "null argument");
     ARG(s->ctx == c && f->ctx == c, "scene and film must belong to the context");
     if (!s->built) return fail(WL_ERR_NOT_BUILT, "bvh not built");
     ARG(p->width == f->f.W && p->height == f->f.H, "film size differs from the render size");
@@ -1742,12 +1753,18 @@ int noalloc_render_inputs(wl_context *c, wl_scene *s, const wl_camera *cam,
     ARG(p->math <= WL_MATH_STRICT, "bad math mode");
     ARG(p->lights <= WL_LIGHTS_POWER, "bad light selection");
     ARG(p->rr_prob > 0.0f && p->rr_prob <= 1.0f, "rr_prob must be in (0, 1]");
+    ARG((p->flags & ~(uint32_t)WL_RENDER_SORT_MATERIALS) == 0,
+        "wl_render_noalloc supports only the WL_RENDER_SORT_MATERIALS flag");
     ARG(finite3(cam->pos) && finite3(cam->look_at) && finite3(cam->up) && finite3(cam->right),
         "non-finite camera");
-    *sc = dev_scene(s);
-    *film = &f->f;
-    *stream = c->stream;
-    *device = c->device;
+    if (!c->noalloc_base) return fail(WL_ERR_CUDA, "wl_render_noalloc: no scratch address");
+    out->sc = dev_scene(s);
+    out->film = &f->f;
+    out->stream = c->stream;
+    out->device = c->device;
+    out->tune_extend = c->tune_extend;
+    out->tune_shadow = c->tune_shadow;
+    out->scratch = c->noalloc_base;
     return WL_OK;
 }
 void noalloc_fail(const std::string &msg) { g_err = msg; }

@@ -5,15 +5,13 @@
 // are the same as wl_render's (pt_fast.cu / pt_strict.cu / traverse.cu); only where the
 // queues live differs, so the images are identical.
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include "wl_internal.h"
 
 namespace wl {
 int noalloc_render_inputs(wl_context *c, wl_scene *s, const wl_camera *cam,
-                          const wl_render_params *p, wl_film *f, DevScene *sc, Film **film,
-                          cudaStream_t *stream, int *device);
+                          const wl_render_params *p, wl_film *f, NoallocCall *out);
 void noalloc_fail(const std::string &msg);
 }  // namespace wl
 
@@ -27,31 +25,6 @@ static_assert(PER_PATH * MAX_PATHS + 512 == WL_NOALLOC_SCRATCH_BYTES, "scratch l
 
 // The scratch: every GPU that loads this library holds it until the process exits.
 static __device__ __align__(256) unsigned char g_wave_scratch[WL_NOALLOC_SCRATCH_BYTES];
-
-constexpr int MAX_DEVICES = 64;
-std::mutex g_mu;
-void *g_addr[MAX_DEVICES] = {};
-
-// Host code cannot use g_wave_scratch's name as a device address: look the address up once per
-// device, with that device current.
-int scratch_address(int device, void **out) {
-    if (device < 0 || device >= MAX_DEVICES) {
-        noalloc_fail("wl_render_noalloc: device index out of range");
-        return WL_ERR_INVALID_ARG;
-    }
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_addr[device]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_wave_scratch);
-        if (e != cudaSuccess || !p) {
-            noalloc_fail(std::string("wl_render_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-            return WL_ERR_CUDA;
-        }
-        g_addr[device] = p;
-    }
-    *out = g_addr[device];
-    return WL_OK;
-}
 
 // Same arrays as the allocated queues, carved out of the static scratch for MAX_PATHS slots.
 Queues carve(void *base) {
@@ -79,36 +52,61 @@ Queues carve(void *base) {
     return q;
 }
 
+// Restores the caller's current device when a call returns.
+struct DeviceRestore {
+    int prev = -1;
+    DeviceRestore() {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    }
+    ~DeviceRestore() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
+int cuda_fail(cudaError_t e) {
+    noalloc_fail(std::string("wl_render_noalloc: ") + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? WL_ERR_OOM : WL_ERR_CUDA;
+}
+
 }  // namespace
+
+namespace wl {
+// Host code cannot use g_wave_scratch's name as a device address: wl_context_create calls this
+// with the context's device current and keeps the address for the context's life. Loading the
+// module that holds the array (CUDA loads modules lazily) is what reserves its memory, so it
+// happens here, at context creation, and never inside wl_render_noalloc.
+int noalloc_scratch_address(void **out, std::string &err) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_wave_scratch);
+    if (e != cudaSuccess || !p) {
+        err = std::string("wl_render_noalloc scratch: cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+        return WL_ERR_CUDA;
+    }
+    *out = p;
+    return WL_OK;
+}
+}  // namespace wl
 
 extern "C" int wl_render_noalloc(wl_context *ctx, wl_scene *scene, const wl_camera *cam,
                                  const wl_render_params *p, wl_film *film) {
-    DevScene sc;
-    Film *f = nullptr;
-    cudaStream_t st = nullptr;
-    int device = 0;
-    int rc = noalloc_render_inputs(ctx, scene, cam, p, film, &sc, &f, &st, &device);
+    NoallocCall nc{};
+    int rc = noalloc_render_inputs(ctx, scene, cam, p, film, &nc);
     if (rc != WL_OK) return rc;
     if (p->wave_paths > MAX_PATHS) {
         noalloc_fail("wl_render_noalloc: wave_paths " + std::to_string(p->wave_paths) +
                      " exceeds the static scratch limit of " + std::to_string(MAX_PATHS) + " paths");
         return WL_ERR_INVALID_ARG;
     }
-    cudaError_t e = cudaSetDevice(device);
-    if (e != cudaSuccess) {
-        noalloc_fail(std::string("wl_render_noalloc: ") + cudaGetErrorString(e));
-        return WL_ERR_CUDA;
-    }
-    void *base = nullptr;
-    rc = scratch_address(device, &base);
-    if (rc != WL_OK) return rc;
-    Queues q = carve(base);
+    DeviceRestore restore;
+    cudaError_t e = cudaSetDevice(nc.device);
+    if (e != cudaSuccess) return cuda_fail(e);
+    const DevScene &sc = nc.sc;
+    Film *f = nc.film;
+    cudaStream_t st = nc.stream;
+    Queues q = carve(nc.scratch);
     // the array keeps the previous call's contents: zero the counters and sums
     e = cudaMemsetAsync(q.counters, 0, 512, st);
-    if (e != cudaSuccess) {
-        noalloc_fail(std::string("wl_render_noalloc: ") + cudaGetErrorString(e));
-        return WL_ERR_CUDA;
-    }
+    if (e != cudaSuccess) return cuda_fail(e);
     const uint32_t npix = p->width * p->height;
     const uint64_t total = (uint64_t)npix * p->spp;
     uint64_t want = p->wave_paths ? p->wave_paths : MAX_PATHS;
@@ -137,20 +135,18 @@ extern "C" int wl_render_noalloc(wl_context *ctx, wl_scene *scene, const wl_came
         else fast::launch_generate(wp, q, st);
         int in = 0;
         for (uint32_t b = 0; b < p->max_depth; b++) {
-            launch_extend(sc, q, in, false, st);
-            cudaMemsetAsync(q.counters + (in ^ 1), 0, sizeof(uint32_t), st);
-            cudaMemsetAsync(q.counters + 2, 0, sizeof(uint32_t), st);
+            launch_extend(sc, q, in, false, st, nc.tune_extend);
+            e = cudaMemsetAsync(q.counters + (in ^ 1), 0, sizeof(uint32_t), st);
+            if (e == cudaSuccess) e = cudaMemsetAsync(q.counters + 2, 0, sizeof(uint32_t), st);
+            if (e != cudaSuccess) return cuda_fail(e);
             if (strict_math) strict::launch_shade(wp, sc, q, in, st);
             else fast::launch_shade(wp, sc, q, in, st);
-            launch_shadow(sc, q, false, st);
+            launch_shadow(sc, q, false, st, nc.tune_shadow);
             in ^= 1;
         }
         strict::launch_film(wp, q, *f, st);
         e = cudaGetLastError();
-        if (e != cudaSuccess) {
-            noalloc_fail(std::string("wl_render_noalloc: ") + cudaGetErrorString(e));
-            return WL_ERR_CUDA;
-        }
+        if (e != cudaSuccess) return cuda_fail(e);
     }
     f->frames64 += p->spp;
     return WL_OK;

@@ -178,27 +178,31 @@ void nrc_forward_raw(NrcNet *n, const float *in, float *out, uint32_t count, cud
 
 // Forward + backward + weight gradients for `count` rows (raw inputs) or for the samples
 // collected on the device (enc, count read from counters[0]). Leaves the MLP gradient in w_grad
-// and the grid gradient in grid.grad; the loss in n->loss[0].
-static void nrc_gradients(NrcNet *n, bool enc, const wl_disney *mats, const float *in,
-                          const float *target, uint32_t count, cudaStream_t s) {
+// and the grid gradient in grid.grad; the loss in n->loss[0]. Returns WL_ERR_OOM (and launches
+// nothing) when the tile scratch for a raw batch larger than it cannot grow.
+static int nrc_gradients(NrcNet *n, bool enc, const wl_disney *mats, const float *in,
+                         const float *target, uint32_t count, cudaStream_t s) {
     if (!enc && count > n->raw_cap) {
         // raw batches larger than the sample buffer: grow the tile scratch
         cudaStreamSynchronize(s);
         if (n->tiles) cudaFree(n->tiles);
         n->tiles = nullptr;
+        n->raw_cap = 0;
         if (cudaMalloc(&n->tiles, ((size_t)count + 127) / 128 * 32768) != cudaSuccess) {
             n->tiles = nullptr;
-            n->raw_cap = 0;
-            return;
+            cudaGetLastError();  // the failed allocation is reported by the status, not left pending
+            return WL_ERR_OOM;
         }
         n->raw_cap = count;
     }
+    if (!n->tiles) return WL_ERR_OOM;
     if (enc)
         nrc_tc_train(n->w, n->grid, mats, n->samples, n->counters, n->max_samples, nullptr, nullptr,
                      n->w_grad, n->loss, n->counters + 2, n->tiles, n->gin, s);
     else
         nrc_tc_train(n->w, n->grid, mats, nullptr, nullptr, count, in, target, n->w_grad, n->loss,
                      n->counters + 2, n->tiles, nullptr, s);
+    return WL_OK;
 }
 
 static void nrc_adam(NrcNet *n, bool grid, cudaStream_t s) {
@@ -212,19 +216,21 @@ static void nrc_adam(NrcNet *n, bool grid, cudaStream_t s) {
                                                  n->grid_count, n->lr, b1, b2, 1e-15f, c1, c2, 1);
 }
 
-void nrc_train_raw(NrcNet *n, const float *in, const float *target, uint32_t count, cudaStream_t s) {
-    nrc_gradients(n, false, nullptr, in, target, count, s);
-    nrc_adam(n, false, s);
+int nrc_train_raw(NrcNet *n, const float *in, const float *target, uint32_t count, cudaStream_t s) {
+    int rc = nrc_gradients(n, false, nullptr, in, target, count, s);
+    if (rc == WL_OK) nrc_adam(n, false, s);
+    return rc;
 }
 
-void nrc_gradients_raw(NrcNet *n, const float *in, const float *target, uint32_t count,
-                       cudaStream_t s) {
-    nrc_gradients(n, false, nullptr, in, target, count, s);
+int nrc_gradients_raw(NrcNet *n, const float *in, const float *target, uint32_t count,
+                      cudaStream_t s) {
+    return nrc_gradients(n, false, nullptr, in, target, count, s);
 }
 
-void nrc_train_collected(NrcNet *n, const wl_disney *mats, cudaStream_t s) {
-    nrc_gradients(n, true, mats, nullptr, nullptr, 0, s);
-    nrc_adam(n, true, s);
+int nrc_train_collected(NrcNet *n, const wl_disney *mats, cudaStream_t s) {
+    int rc = nrc_gradients(n, true, mats, nullptr, nullptr, 0, s);
+    if (rc == WL_OK) nrc_adam(n, true, s);
+    return rc;
 }
 
 int nrc_reserve_queries(NrcNet *n, uint32_t rows) {

@@ -261,6 +261,18 @@ struct TraceTune {
     uint32_t refill = 12;
     uint32_t postpone = 12;  // triangle phase when >= postpone/32 of the busy lanes hold triangles
 };
+// wl_render_noalloc (noalloc.cu): what a call needs from the handles (api.cu
+// noalloc_render_inputs) and the device address of the static scratch array, looked up for the
+// current device when a context is created.
+struct NoallocCall {
+    DevScene sc;
+    Film *film;
+    cudaStream_t stream;
+    int device;
+    TraceTune tune_extend, tune_shadow;
+    void *scratch;
+};
+int noalloc_scratch_address(void **out, std::string &err);
 void launch_extend(const DevScene &sc, const Queues &q, int in, bool stats, cudaStream_t s,
                    const TraceTune &t = TraceTune{}, const BatchView &bv = BatchView{},
                    bool zero_fetch = true);
@@ -306,10 +318,10 @@ int nrc_create(const wl_nrc_params &p, const float *bbox_lo, const float *bbox_h
                uint32_t max_samples, cudaStream_t s, NrcNet **out, std::string &err);
 void nrc_free(NrcNet *n);
 void nrc_forward_raw(NrcNet *n, const float *in, float *out, uint32_t count, cudaStream_t s);
-void nrc_train_raw(NrcNet *n, const float *in, const float *target, uint32_t count, cudaStream_t s);
-void nrc_gradients_raw(NrcNet *n, const float *in, const float *target, uint32_t count,
+int nrc_train_raw(NrcNet *n, const float *in, const float *target, uint32_t count, cudaStream_t s);
+int nrc_gradients_raw(NrcNet *n, const float *in, const float *target, uint32_t count,
                        cudaStream_t s);
-void nrc_train_collected(NrcNet *n, const wl_disney *mats, cudaStream_t s);
+int nrc_train_collected(NrcNet *n, const wl_disney *mats, cudaStream_t s);
 void nrc_query(NrcNet *n, const wl_disney *mats, const NrcVertex *q, const uint32_t *nq,
                float4 *rad, uint32_t max_q, cudaStream_t s);
 void nrc_collect(NrcNet *n, NrcWaveBuffers b, const Queues &q, uint32_t tcount, cudaStream_t s);

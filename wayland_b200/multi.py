@@ -37,7 +37,8 @@ def film_sum_tensor(film):
     _, sum64, _ = film.device_ptrs()
     if not sum64:
         raise ValueError("the film has no FP64 sum (create it with fp64=True)")
-    return torch.as_tensor(_DeviceArray(sum64, (film.height, film.width, 3), "<f8"), device="cuda")
+    return torch.as_tensor(_DeviceArray(sum64, (film.height, film.width, 3), "<f8"),
+                           device=f"cuda:{film.ctx.device}")
 
 
 def allreduce_mean(sums, frames, group=None):
