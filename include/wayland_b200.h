@@ -408,7 +408,55 @@ WL_API int wl_nrc_mlp_gradients(wl_nrc *nrc, const float *d_in, const float *d_t
 /* MLP weights as FP32 (17408 floats: W0..W3 64x64 then W4 16x64, row = output), host. */
 WL_API int wl_nrc_get_weights(wl_nrc *nrc, float *w);
 WL_API int wl_nrc_set_weights(wl_nrc *nrc, const float *w);
+/* Counters of the last frame. Returns WL_ERR_TIMEOUT (once; the error is then cleared) when a
+ * tensor-core wait of the cache's kernels gave up since the last call: every such wait polls
+ * its mbarrier a bounded number of times, then the kernel records the error, drains its
+ * in-flight tensor-core work, frees its tensor memory and returns. */
 WL_API int wl_nrc_stats(wl_nrc *nrc, uint32_t *train_samples, uint32_t *queries, float *loss);
+/* Polls of a tensor-core wait before it gives up (default WL_NRC_WAIT_POLLS). 0 makes every
+ * such wait give up at once: the hook that tests of the timeout path use. */
+#define WL_NRC_WAIT_POLLS 4194304u
+WL_API int wl_nrc_set_wait_limit(wl_nrc *nrc, uint32_t polls);
+
+/* A surface vertex as the cache sees it (64 bytes): position, material index, outgoing
+ * direction (unit, pointing away from the surface), shading normal, and for a training sample
+ * the target radiance in extra[0..2]. */
+typedef struct wl_nrc_vertex {
+    float pos[3];
+    uint32_t material;
+    float wo[3];
+    float pad0;
+    float n[3];
+    float pad1;
+    float extra[4];
+} wl_nrc_vertex;
+/* The hash grid's shape and the box that positions are normalised to:
+ * p_norm = clamp((p - lo) * inv_ext, 0, 1) per axis. */
+typedef struct wl_nrc_grid_desc {
+    uint32_t levels, log2_table, base_resolution;
+    float per_level_scale;
+    float lo[3];
+    float inv_ext[3];
+} wl_nrc_grid_desc;
+/* The grid's FP32 master parameters, levels x 2^log2_table x 2 floats (host); params may be
+ * NULL. wl_nrc_set_grid also refreshes the FP16 copy the encoding gathers. */
+WL_API int wl_nrc_get_grid(wl_nrc *nrc, wl_nrc_grid_desc *desc, float *params);
+WL_API int wl_nrc_set_grid(wl_nrc *nrc, const float *params);
+/* The cache's prediction for n vertices (device pointers): rgb[4 i .. 4 i + 2] = max(MLP output,
+ * 0) for vertex i, rgb[4 i + 3] = 0, through the render's query path (hash-grid encode into
+ * tensor-core operand tiles, tcgen05 MLP). */
+WL_API int wl_nrc_query(wl_nrc *nrc, const wl_nrc_vertex *d_vertices, uint32_t n, float *d_rgb);
+/* Parity access: the 64 encoded inputs of each vertex as the query pass stores them (bfloat16,
+ * returned as floats, n x 64) and, when d_corners is not NULL, the table entry of each level's
+ * 8 cell corners (n x levels x 8; corner k: bit 0 +x, bit 1 +y, bit 2 +z). Device pointers. */
+WL_API int wl_nrc_debug_encode(wl_nrc *nrc, const wl_nrc_vertex *d_vertices, uint32_t n,
+                               float *d_features, uint32_t *d_corners);
+/* Parity access: the gradients of one training step on n samples (device vertices, targets in
+ * extra), computed by the render's training path (encode, fused tensor-core forward and
+ * backward, grid scatter) without applying them: w_grad (17408 floats), grid_grad (as
+ * wl_nrc_get_grid's params) and the loss, all host; any may be NULL. n <= 131072. */
+WL_API int wl_nrc_sample_gradients(wl_nrc *nrc, const wl_nrc_vertex *d_samples, uint32_t n,
+                                   float *w_grad, float *grid_grad, float *loss);
 
 /* Random streams for parity tests: the first `count` uniforms of the stream of each listed
  * pixel at `frame` (count floats per pixel, pixel-major). Device pointers. */

@@ -134,3 +134,32 @@ def test_self_training_matches_full_paths(ctx):
     s.close()
     for m in means:
         assert abs(m - ref) < 0.1 * ref, (means, ref)
+
+
+def test_wait_timeout_reported(ctx):
+    """A tensor-core wait that gives up is reported, and the cache keeps working: with the wait
+    limit at 0 polls every mbarrier wait of the forward kernel gives up at once; the kernel
+    records the error, drains the tensor-core work it issued, frees its tensor memory and
+    returns; wl_nrc_stats returns WL_ERR_TIMEOUT once. With the limit restored the next forward
+    pass is correct again."""
+    sc = scenes.cornell_box(16, 16)
+    s = wl.Scene(ctx, sc)
+    c = wl.RadianceCache(ctx, s, log2_table=12)
+    x, _ = batch(1024, 5)
+    out = torch.zeros((1024, 4), dtype=torch.float32, device="cuda")
+    dx = dev(x)
+    c.set_wait_limit(0)
+    c.forward(dx.data_ptr(), out.data_ptr(), 1024)
+    ctx.sync()
+    with pytest.raises(wl.WlError, match="TIMEOUT"):
+        c.stats()
+    c.stats()  # reported once
+    c.set_wait_limit(wl._abi.NRC_WAIT_POLLS)
+    c.forward(dx.data_ptr(), out.data_ptr(), 1024)
+    ctx.sync()
+    ref, _ = nrc_oracle.forward(c.weights(), x)
+    err = np.abs(out.cpu().numpy()[:, :3] - ref[:, :3]) / (np.abs(ref[:, :3]) + 1e-2)
+    assert err.max() < 2e-2
+    c.stats()
+    c.close()
+    s.close()

@@ -126,6 +126,33 @@ def test_fast_mode_relmse(ctx, oracle):
     assert oracle.relmse(img2, ref2) < 5 * FAST_RELMSE_TOL
 
 
+BENCH_FAST_TOL = 1e-2
+
+
+def test_fast_mode_bench_scene(ctx, oracle):
+    """The benchmark's own arithmetic on the benchmark's own scene: the 1,997,130-triangle
+    displaced sphere with its 4 lights and environment 0.1, depth 16, MIS, TEA+LCG, fast math,
+    binned-SAH BVH, at 96x54 x 16 spp (the bench's 1920x1080 view at 1/20 scale) against the FP64
+    oracle with the same random streams. relMSE below BENCH_FAST_TOL, and below a tenth of the
+    relMSE of an independent 16-spp render (other frames) against the same oracle image: the
+    fast-math deviation is far below the Monte-Carlo noise of an image at the same spp."""
+    sc = scenes.displaced_sphere(96, 54, 16, 16)
+    assert sc.num_tris == 1997130
+    s = wl.Scene(ctx, sc, bvh_kind=wl.BVH_SAH)
+    p = wl.render_params(96, 54, 16, math=wl.MATH_FAST, max_depth=16, env=sc.env)
+    img, _, _, _ = gpu_render(ctx, sc, p, scene=s)
+    _, ref64, _ = oracle.render(sc, ocam(sc), oparams(p), prec=1, want64=True)
+    q = wl.render_params(96, 54, 16, math=wl.MATH_FAST, max_depth=16, env=sc.env, first_frame=1000)
+    other, _, _, _ = gpu_render(ctx, sc, q, scene=s)
+    rel = oracle.relmse(img, ref64)
+    noise = oracle.relmse(other, ref64)
+    print(f"bench scene fast vs FP64 oracle relMSE {rel:.3e}, independent render {noise:.3e}")
+    assert ref64.mean() > 0.01
+    assert rel < BENCH_FAST_TOL, rel
+    assert rel < 0.1 * noise, (rel, noise)
+    s.close()
+
+
 @pytest.mark.parametrize("rng", [wl.RNG_TEA_LCG, wl.RNG_PCG32])
 def test_rng_streams(ctx, oracle, rng):
     pix = np.array([0, 1, 77, 65535, 1 << 20, 2073599], np.uint32)

@@ -315,6 +315,47 @@ class RadianceCache:
         _abi.check("wl_nrc_stats", self.lib.wl_nrc_stats(self.handle, C.byref(a), C.byref(b), C.byref(l)))
         return {"train_samples": a.value, "queries": b.value, "loss": l.value}
 
+    def set_wait_limit(self, polls):
+        """mbarrier polls before a tensor-core wait gives up (0: at once; a test hook)."""
+        _abi.check("wl_nrc_set_wait_limit", self.lib.wl_nrc_set_wait_limit(self.handle, polls))
+
+    def grid(self, with_params=True):
+        """(descriptor dict, FP32 master parameters (levels, 2^log2_table, 2) or None)."""
+        d = _abi.NrcGridDesc()
+        _abi.check("wl_nrc_get_grid", self.lib.wl_nrc_get_grid(self.handle, C.byref(d), None))
+        desc = {"levels": d.levels, "log2_table": d.log2_table, "base_resolution": d.base_resolution,
+                "per_level_scale": d.per_level_scale, "lo": list(d.lo), "inv_ext": list(d.inv_ext)}
+        if not with_params:
+            return desc, None
+        params = np.empty((d.levels, 1 << d.log2_table, 2), np.float32)
+        _abi.check("wl_nrc_get_grid", self.lib.wl_nrc_get_grid(self.handle, None, _p(params)))
+        return desc, params
+
+    def set_grid(self, params):
+        params = np.ascontiguousarray(params, np.float32)
+        _abi.check("wl_nrc_set_grid", self.lib.wl_nrc_set_grid(self.handle, _p(params)))
+
+    def query(self, d_vertices, n, d_rgb):
+        """Cache predictions for n device wl_nrc_vertex records into d_rgb (n x 4 floats)."""
+        _abi.check("wl_nrc_query", self.lib.wl_nrc_query(self.handle, C.c_void_p(d_vertices), n,
+                                                         C.c_void_p(d_rgb)))
+
+    def debug_encode(self, d_vertices, n, d_features, d_corners=None):
+        _abi.check("wl_nrc_debug_encode", self.lib.wl_nrc_debug_encode(
+            self.handle, C.c_void_p(d_vertices), n, C.c_void_p(d_features),
+            C.c_void_p(d_corners) if d_corners else None))
+
+    def sample_gradients(self, d_samples, n):
+        """(loss, weight gradient (17408,), grid gradient (levels, 2^log2_table, 2)) of one
+        training step on n device samples, not applied."""
+        desc, _ = self.grid(with_params=False)
+        gw = np.empty(_abi.NRC_WEIGHTS, np.float32)
+        gg = np.empty((desc["levels"], 1 << desc["log2_table"], 2), np.float32)
+        loss = C.c_float()
+        _abi.check("wl_nrc_sample_gradients", self.lib.wl_nrc_sample_gradients(
+            self.handle, C.c_void_p(d_samples), n, _p(gw), _p(gg), C.byref(loss)))
+        return loss.value, gw, gg
+
     def close(self):
         if getattr(self, "handle", None):
             self.lib.wl_nrc_destroy(self.handle)

@@ -116,6 +116,17 @@ assert RAY_DTYPE.itemsize == 32 and HIT_DTYPE.itemsize == 16
 # Every symbol include/wayland_b200.h declares, with its ctypes signature.
 _P = C.c_void_p
 _U32 = C.c_uint32
+class NrcGridDesc(C.Structure):
+    _fields_ = [("levels", C.c_uint32), ("log2_table", C.c_uint32), ("base_resolution", C.c_uint32),
+                ("per_level_scale", C.c_float), ("lo", C.c_float * 3), ("inv_ext", C.c_float * 3)]
+
+
+# wl_nrc_vertex (64 bytes) as a numpy record
+NRC_VERTEX_DTYPE = np.dtype([("pos", np.float32, 3), ("material", np.uint32), ("wo", np.float32, 3),
+                             ("pad0", np.float32), ("n", np.float32, 3), ("pad1", np.float32),
+                             ("extra", np.float32, 4)])
+
+
 SIGNATURES = {
     "wl_context_create": (C.c_int, [C.c_int, C.POINTER(_P)]),
     "wl_context_destroy": (C.c_int, [_P]),
@@ -163,8 +174,15 @@ SIGNATURES = {
     "wl_nrc_set_weights": (C.c_int, [_P, _P]),
     "wl_nrc_stats": (C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_float)]),
     "wl_render_ao": (C.c_int, [_P, _P, C.POINTER(Camera), C.POINTER(AoParams), _P]),
+    "wl_nrc_set_wait_limit": (C.c_int, [_P, _U32]),
+    "wl_nrc_get_grid": (C.c_int, [_P, C.POINTER(NrcGridDesc), _P]),
+    "wl_nrc_set_grid": (C.c_int, [_P, _P]),
+    "wl_nrc_query": (C.c_int, [_P, _P, _U32, _P]),
+    "wl_nrc_debug_encode": (C.c_int, [_P, _P, _U32, _P, _P]),
+    "wl_nrc_sample_gradients": (C.c_int, [_P, _P, _U32, _P, _P, C.POINTER(C.c_float)]),
 }
 NOALLOC_MAX_PATHS = 65536
+NRC_WAIT_POLLS = 4194304
 
 
 class WlError(RuntimeError):

@@ -13,6 +13,7 @@
 
 #include "wl_bvh.cuh"
 #include "wl_internal.h"
+#include "wl_nrc.cuh"
 
 using namespace wl;
 
@@ -1444,7 +1445,95 @@ int wl_nrc_stats(wl_nrc *n, uint32_t *samples, uint32_t *queries, float *loss) {
     if (samples) *samples = cnt[0] < nrc_max_samples(n->net) ? cnt[0] : nrc_max_samples(n->net);
     if (queries) *queries = q;
     if (loss) *loss = l;
-    if (cnt[2]) return fail(WL_ERR_TIMEOUT, "radiance-cache tensor-core wait timed out");
+    if (cnt[2]) {
+        // reported once: the word is cleared for the calls that follow
+        nrc_clear_error(n->net, n->ctx->stream);
+        CK(cudaStreamSynchronize(n->ctx->stream));
+        return fail(WL_ERR_TIMEOUT, "radiance-cache tensor-core wait timed out");
+    }
+    return WL_OK;
+}
+
+int wl_nrc_set_wait_limit(wl_nrc *n, uint32_t polls) {
+    ARG(n, "null argument");
+    nrc_set_wait_polls(n->net, polls);
+    return WL_OK;
+}
+
+static_assert(sizeof(wl_nrc_vertex) == sizeof(NrcVertex), "wl_nrc_vertex mirrors NrcVertex");
+static_assert(NRC_WAIT_POLLS == WL_NRC_WAIT_POLLS, "one default wait limit");
+
+int wl_nrc_get_grid(wl_nrc *n, wl_nrc_grid_desc *d, float *params) {
+    ARG(n, "null argument");
+    CK(cudaSetDevice(n->ctx->device));
+    const NrcGrid g = nrc_grid(n->net);
+    if (d) {
+        d->levels = g.levels;
+        d->log2_table = g.log2T;
+        d->base_resolution = g.base;
+        d->per_level_scale = g.scale;
+        for (int k = 0; k < 3; k++) {
+            d->lo[k] = g.lo[k];
+            d->inv_ext[k] = g.inv_ext[k];
+        }
+    }
+    if (params) {
+        CK(cudaMemcpyAsync(params, g.params, nrc_grid_count(n->net) * 4, cudaMemcpyDeviceToHost, n->ctx->stream));
+        CK(cudaStreamSynchronize(n->ctx->stream));
+    }
+    return WL_OK;
+}
+
+int wl_nrc_set_grid(wl_nrc *n, const float *params) {
+    ARG(n && params, "null argument");
+    CK(cudaSetDevice(n->ctx->device));
+    const NrcGrid g = nrc_grid(n->net);
+    CK(cudaMemcpyAsync(g.params, params, nrc_grid_count(n->net) * 4, cudaMemcpyHostToDevice, n->ctx->stream));
+    nrc_grid_changed(n->net, n->ctx->stream);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(n->ctx->stream));
+    return WL_OK;
+}
+
+int wl_nrc_query(wl_nrc *n, const wl_nrc_vertex *v, uint32_t count, float *rgb) {
+    ARG(n && v && rgb, "null argument");
+    ARG(((uintptr_t)v & 15) == 0 && ((uintptr_t)rgb & 15) == 0, "buffers must be 16-byte aligned");
+    if (count == 0) return WL_OK;
+    CK(cudaSetDevice(n->ctx->device));
+    int rc = nrc_query_vertices(n->net, n->scene->d_mats, reinterpret_cast<const NrcVertex *>(v), count,
+                                reinterpret_cast<float4 *>(rgb), n->ctx->stream);
+    if (rc != WL_OK) return fail(rc, "radiance-cache query buffers could not be allocated");
+    CK(cudaGetLastError());
+    return WL_OK;
+}
+
+int wl_nrc_debug_encode(wl_nrc *n, const wl_nrc_vertex *v, uint32_t count, float *feat, uint32_t *corners) {
+    ARG(n && v && feat, "null argument");
+    ARG(((uintptr_t)v & 15) == 0, "vertices must be 16-byte aligned");
+    if (count == 0) return WL_OK;
+    CK(cudaSetDevice(n->ctx->device));
+    int rc = nrc_encode_vertices(n->net, n->scene->d_mats, reinterpret_cast<const NrcVertex *>(v), count, feat,
+                                 corners, n->ctx->stream);
+    if (rc != WL_OK) return fail(rc, "radiance-cache encode failed");
+    return WL_OK;
+}
+
+int wl_nrc_sample_gradients(wl_nrc *n, const wl_nrc_vertex *v, uint32_t count, float *w_grad, float *grid_grad,
+                            float *loss) {
+    ARG(n && v, "null argument");
+    ARG(((uintptr_t)v & 15) == 0, "samples must be 16-byte aligned");
+    ARG(count > 0 && count <= nrc_max_samples(n->net), "count out of range");
+    CK(cudaSetDevice(n->ctx->device));
+    cudaStream_t st = n->ctx->stream;
+    int rc = nrc_sample_gradients(n->net, n->scene->d_mats, reinterpret_cast<const NrcVertex *>(v), count, st);
+    if (rc != WL_OK) return fail(rc, "radiance-cache gradients failed");
+    CK(cudaGetLastError());
+    if (w_grad) CK(cudaMemcpyAsync(w_grad, nrc_weight_grad(n->net), WL_NRC_WEIGHTS * 4, cudaMemcpyDeviceToHost, st));
+    if (grid_grad)
+        CK(cudaMemcpyAsync(grid_grad, nrc_grid(n->net).grad, nrc_grid_count(n->net) * 4, cudaMemcpyDeviceToHost, st));
+    if (loss) CK(cudaMemcpyAsync(loss, nrc_loss_ptr(n->net), 4, cudaMemcpyDeviceToHost, st));
+    nrc_zero_grid_grad(n->net, st);
+    CK(cudaStreamSynchronize(st));
     return WL_OK;
 }
 

@@ -34,6 +34,58 @@ __global__ void k_adam(float *p, float *g, float *m, float *v, size_t count, flo
     }
 }
 
+// Adam on the hash grid's FP32 master parameters, two features (one entry) per step, writing
+// the FP16 copy that the encoding gathers; the gradient is consumed (zeroed).
+__global__ void k_adam_grid(float2 *p, __half2 *feat, float2 *g, float2 *m, float2 *v, size_t entries,
+                            float lr, float b1, float b2, float eps, float c1, float c2) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < entries;
+         i += (size_t)gridDim.x * blockDim.x) {
+        float2 gi = g[i], mi = m[i], vi = v[i], pi = p[i];
+        mi.x = b1 * mi.x + (1.0f - b1) * gi.x;
+        mi.y = b1 * mi.y + (1.0f - b1) * gi.y;
+        vi.x = b2 * vi.x + (1.0f - b2) * gi.x * gi.x;
+        vi.y = b2 * vi.y + (1.0f - b2) * gi.y * gi.y;
+        pi.x -= lr * (mi.x / c1) / (sqrtf(vi.x / c2) + eps);
+        pi.y -= lr * (mi.y / c1) / (sqrtf(vi.y / c2) + eps);
+        m[i] = mi;
+        v[i] = vi;
+        p[i] = pi;
+        feat[i] = __floats2half2_rn(pi.x, pi.y);
+        g[i] = make_float2(0.0f, 0.0f);
+    }
+}
+
+// FP16 copy of the grid's master parameters.
+__global__ void k_grid_to_half(const float2 *p, __half2 *feat, size_t entries) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < entries;
+         i += (size_t)gridDim.x * blockDim.x) {
+        float2 x = p[i];
+        feat[i] = __floats2half2_rn(x.x, x.y);
+    }
+}
+
+// Parity access (wl_nrc_query, wl_nrc_debug_encode, wl_nrc_sample_gradients): caller vertices
+// copied into the cache's own records. As queries, extra = (1, 1, 1, row) so that the query pass
+// writes each row's prediction to out[row]; as samples, extra holds the target. count[0] = n.
+__global__ void k_nrc_load(const NrcVertex *in, NrcVertex *out, uint32_t n, int as_query, uint32_t *count) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) count[0] = n;
+    if (i >= n) return;
+    NrcVertex v = in[i];
+    if (as_query) v.extra = make_float4(1.0f, 1.0f, 1.0f, __uint_as_float(i));
+    out[i] = v;
+}
+
+// Every vertex's entry index of corner k of level l at idx[(i * levels + l) * 8 + k].
+__global__ void k_nrc_corners(NrcGrid g, const NrcVertex *v, uint32_t n, uint32_t *idx) {
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t i = t / (g.levels * 8u), r = t % (g.levels * 8u);
+    if (i >= n) return;
+    float w;
+    float3 pn = grid_normalise(g, v[i].pos_mat);
+    idx[t] = grid_corner(g, pn, r / 8u, (int)(r % 8u), w);
+}
+
 // Training samples of the wave: for every recorded vertex of a training path, the radiance
 // the rest of the path brought back, divided by the throughput that reached the vertex.
 __global__ void k_nrc_targets(NrcWaveBuffers b, const Queues q, uint32_t tcount) {
@@ -87,6 +139,9 @@ struct NrcNet {
     float lr = 1e-2f;
     uint32_t step = 0;
     int grid_blocks = 0;
+    NrcVertex *dbg_v = nullptr;  // caller vertices of the parity entry points
+    uint32_t dbg_cap = 0;
+    uint32_t wait_polls = NRC_WAIT_POLLS;
 };
 
 static void *nrc_alloc(size_t bytes, cudaError_t &e) {
@@ -97,8 +152,9 @@ static void *nrc_alloc(size_t bytes, cudaError_t &e) {
 
 void nrc_free(NrcNet *n) {
     if (!n) return;
-    void *ps[] = {n->grid.params, n->grid.grad, n->grid_m, n->grid_v, n->w, n->w_grad, n->w_m, n->w_v,
-                  n->loss, n->counters, n->samples, n->tiles, n->gin, n->q_tiles};
+    void *ps[] = {n->grid.params, n->grid.feat, n->grid.grad, n->grid_m, n->grid_v, n->w, n->w_grad,
+                  n->w_m, n->w_v, n->loss, n->counters, n->samples, n->tiles, n->gin, n->q_tiles,
+                  n->dbg_v};
     for (void *p : ps)
         if (p) cudaFree(p);
     delete n;
@@ -120,6 +176,7 @@ int nrc_create(const wl_nrc_params &p, const float *bbox_lo, const float *bbox_h
     }
     n->grid_count = (size_t)p.levels * ((size_t)1 << p.log2_table) * 2;
     n->grid.params = (float *)nrc_alloc(n->grid_count * 4, e);
+    n->grid.feat = (__half2 *)nrc_alloc(n->grid_count * 2, e);
     n->grid.grad = (float *)nrc_alloc(n->grid_count * 4, e);
     n->grid_m = (float *)nrc_alloc(n->grid_count * 4, e);
     n->grid_v = (float *)nrc_alloc(n->grid_count * 4, e);
@@ -158,6 +215,11 @@ int nrc_create(const wl_nrc_params &p, const float *bbox_lo, const float *bbox_h
     if (e == cudaSuccess) e = cudaMemsetAsync(n->w_v, 0, NRC_WEIGHTS * 4, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(n->w_grad, 0, NRC_WEIGHTS * 4, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(n->counters, 0, 64, s);
+    if (e == cudaSuccess) {
+        k_grid_to_half<<<1024, 256, 0, s>>>(reinterpret_cast<const float2 *>(n->grid.params), n->grid.feat,
+                                            n->grid_count / 2);
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
         err = std::string("nrc init: ") + cudaGetErrorString(e);
@@ -173,7 +235,7 @@ int nrc_create(const wl_nrc_params &p, const float *bbox_lo, const float *bbox_h
 }
 
 void nrc_forward_raw(NrcNet *n, const float *in, float *out, uint32_t count, cudaStream_t s) {
-    nrc_tc_forward_raw(n->w, in, out, count, n->counters + 2, s);
+    nrc_tc_forward_raw(n->w, in, out, count, n->counters + 2, n->wait_polls, s);
 }
 
 // Forward + backward + weight gradients for `count` rows (raw inputs) or for the samples
@@ -198,10 +260,10 @@ static int nrc_gradients(NrcNet *n, bool enc, const wl_disney *mats, const float
     if (!n->tiles) return WL_ERR_OOM;
     if (enc)
         nrc_tc_train(n->w, n->grid, mats, n->samples, n->counters, n->max_samples, nullptr, nullptr,
-                     n->w_grad, n->loss, n->counters + 2, n->tiles, n->gin, s);
+                     n->w_grad, n->loss, n->counters + 2, n->wait_polls, n->tiles, n->gin, s);
     else
         nrc_tc_train(n->w, n->grid, mats, nullptr, nullptr, count, in, target, n->w_grad, n->loss,
-                     n->counters + 2, n->tiles, nullptr, s);
+                     n->counters + 2, n->wait_polls, n->tiles, nullptr, s);
     return WL_OK;
 }
 
@@ -212,8 +274,10 @@ static void nrc_adam(NrcNet *n, bool grid, cudaStream_t s) {
     k_adam<<<(NRC_WEIGHTS + 255) / 256, 256, 0, s>>>(n->w, n->w_grad, n->w_m, n->w_v, NRC_WEIGHTS,
                                                     n->lr, b1, b2, 1e-8f, c1, c2, 1);
     if (grid)
-        k_adam<<<n->grid_blocks * 4, 256, 0, s>>>(n->grid.params, n->grid.grad, n->grid_m, n->grid_v,
-                                                 n->grid_count, n->lr, b1, b2, 1e-15f, c1, c2, 1);
+        k_adam_grid<<<n->grid_blocks * 4, 256, 0, s>>>(
+            reinterpret_cast<float2 *>(n->grid.params), n->grid.feat, reinterpret_cast<float2 *>(n->grid.grad),
+            reinterpret_cast<float2 *>(n->grid_m), reinterpret_cast<float2 *>(n->grid_v), n->grid_count / 2,
+            n->lr, b1, b2, 1e-15f, c1, c2);
 }
 
 int nrc_train_raw(NrcNet *n, const float *in, const float *target, uint32_t count, cudaStream_t s) {
@@ -249,7 +313,7 @@ int nrc_reserve_queries(NrcNet *n, uint32_t rows) {
 void nrc_query(NrcNet *n, const wl_disney *mats, const NrcVertex *q, const uint32_t *nq,
                float4 *rad, uint32_t max_q, cudaStream_t s) {
     if (max_q > n->q_cap) max_q = n->q_cap;  // the render reserved the query rows beforehand
-    nrc_tc_query(n->w, n->grid, mats, q, nq, rad, max_q, n->counters + 2, n->q_tiles, s);
+    nrc_tc_query(n->w, n->grid, mats, q, nq, rad, max_q, n->counters + 2, n->wait_polls, n->q_tiles, s);
 }
 
 void nrc_collect(NrcNet *n, NrcWaveBuffers b, const Queues &q, uint32_t tcount, cudaStream_t s) {
@@ -258,6 +322,88 @@ void nrc_collect(NrcNet *n, NrcWaveBuffers b, const Queues &q, uint32_t tcount, 
     b.max_samples = n->max_samples;
     if (tcount) k_nrc_targets<<<(tcount + 127) / 128, 128, 0, s>>>(b, q, tcount);
 }
+
+// ---- parity access -----------------------------------------------------------------------
+static int nrc_load(const NrcVertex *v, uint32_t count, bool as_query, NrcVertex *dst, uint32_t *cnt,
+                    cudaStream_t s) {
+    k_nrc_load<<<(count + 255) / 256 + 1, 256, 0, s>>>(v, dst, count, as_query ? 1 : 0, cnt);
+    return cudaGetLastError() == cudaSuccess ? WL_OK : WL_ERR_CUDA;
+}
+
+static int nrc_dbg_reserve(NrcNet *n, uint32_t count) {
+    if (n->dbg_cap >= count && n->dbg_v) return WL_OK;
+    if (n->dbg_v) cudaFree(n->dbg_v);
+    n->dbg_v = nullptr;
+    n->dbg_cap = 0;
+    if (cudaMalloc(&n->dbg_v, sizeof(NrcVertex) * (size_t)count) != cudaSuccess) {
+        cudaGetLastError();
+        return WL_ERR_OOM;
+    }
+    n->dbg_cap = count;
+    return WL_OK;
+}
+
+NrcGrid nrc_grid(NrcNet *n) { return n->grid; }
+size_t nrc_grid_count(NrcNet *n) { return n->grid_count; }
+
+void nrc_grid_changed(NrcNet *n, cudaStream_t s) {
+    k_grid_to_half<<<1024, 256, 0, s>>>(reinterpret_cast<const float2 *>(n->grid.params), n->grid.feat,
+                                        n->grid_count / 2);
+}
+
+// The render's query path (encode into tiles, tensor-core MLP) on caller vertices: out[i] =
+// (max(o, 0) for outputs 0..2, 0) for vertex i.
+int nrc_query_vertices(NrcNet *n, const wl_disney *mats, const NrcVertex *v, uint32_t count, float4 *out,
+                       cudaStream_t s) {
+    int rc = nrc_dbg_reserve(n, count);
+    if (rc == WL_OK) rc = nrc_reserve_queries(n, count);
+    if (rc != WL_OK) return rc;
+    cudaMemsetAsync(out, 0, sizeof(float4) * (size_t)count, s);
+    rc = nrc_load(v, count, true, n->dbg_v, n->counters + 4, s);
+    if (rc != WL_OK) return rc;
+    nrc_tc_query(n->w, n->grid, mats, n->dbg_v, n->counters + 4, out, count, n->counters + 2, n->wait_polls,
+                 n->q_tiles, s);
+    return WL_OK;
+}
+
+// The encoded inputs of caller vertices as the query pass stores them (bfloat16 tiles), read
+// back into rows of 64 floats; corners (optional): entry index of every level's 8 corners.
+int nrc_encode_vertices(NrcNet *n, const wl_disney *mats, const NrcVertex *v, uint32_t count, float *feat,
+                        uint32_t *corners, cudaStream_t s) {
+    int rc = nrc_dbg_reserve(n, count);
+    if (rc == WL_OK) rc = nrc_reserve_queries(n, count);
+    if (rc != WL_OK) return rc;
+    rc = nrc_load(v, count, true, n->dbg_v, n->counters + 4, s);
+    if (rc != WL_OK) return rc;
+    nrc_tc_encode_rows(n->grid, mats, n->dbg_v, n->counters + 4, count, n->q_tiles, feat, s);
+    if (corners) {
+        uint64_t threads = (uint64_t)count * n->grid.levels * 8u;
+        k_nrc_corners<<<(uint32_t)((threads + 255) / 256), 256, 0, s>>>(n->grid, n->dbg_v, count, corners);
+    }
+    return cudaGetLastError() == cudaSuccess ? WL_OK : WL_ERR_CUDA;
+}
+
+// One training step's gradients on caller samples (targets in extra.xyz), as the render's
+// training path computes them (encode, fused tensor-core forward/backward, grid scatter),
+// without the Adam step: w_grad and the grid gradient are left on the device for the caller to
+// read; the grid gradient must be zeroed afterwards (nrc_zero_grid_grad).
+int nrc_sample_gradients(NrcNet *n, const wl_disney *mats, const NrcVertex *v, uint32_t count,
+                         cudaStream_t s) {
+    if (count > n->max_samples) return WL_ERR_INVALID_ARG;
+    cudaMemsetAsync(n->grid.grad, 0, n->grid_count * 4, s);
+    int rc = nrc_load(v, count, false, n->samples, n->counters, s);
+    if (rc != WL_OK) return rc;
+    rc = nrc_gradients(n, true, mats, nullptr, nullptr, 0, s);
+    return rc;
+}
+
+void nrc_zero_grid_grad(NrcNet *n, cudaStream_t s) {
+    cudaMemsetAsync(n->grid.grad, 0, n->grid_count * 4, s);
+    cudaMemsetAsync(n->counters, 0, sizeof(uint32_t), s);
+}
+
+void nrc_set_wait_polls(NrcNet *n, uint32_t polls) { n->wait_polls = polls; }
+void nrc_clear_error(NrcNet *n, cudaStream_t s) { cudaMemsetAsync(n->counters + 2, 0, sizeof(uint32_t), s); }
 
 float *nrc_weights(NrcNet *n) { return n->w; }
 float *nrc_weight_grad(NrcNet *n) { return n->w_grad; }

@@ -19,7 +19,7 @@ namespace {
 
 constexpr int TC_THREADS = 128;
 constexpr uint32_t TMEM_COLS = 64;
-constexpr uint32_t WAIT_LIMIT = 1u << 22;
+constexpr uint32_t WAIT_LIMIT = NRC_WAIT_POLLS;
 // shared-memory layout (bytes)
 constexpr uint32_t SM_W = 0;                        // W0..W3, 8 KB each
 constexpr uint32_t SM_W4 = 4 * 8192;                // W4 (16 x 64), 2 KB
@@ -66,8 +66,11 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
                  : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
-    for (uint32_t it = 0; it < WAIT_LIMIT; it++) {
+// Polls the mbarrier phase at most `polls` times (WAIT_LIMIT by default; wl_nrc_set_wait_limit
+// lowers it for the tests of the timeout path). The waits that drain in-flight tensor-core work
+// before tensor memory is released always use WAIT_LIMIT.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase, uint32_t polls = WAIT_LIMIT) {
+    for (uint32_t it = 0; it < polls; it++) {
         uint32_t ok;
         asm volatile(
             "{\n\t"
@@ -124,7 +127,7 @@ template <int MODE>
 __global__ void __launch_bounds__(TC_THREADS) k_mlp_tc(const float *w, NrcGrid g, const wl_disney *mats,
                                                         const NrcVertex *q, const uint32_t *nq,
                                                         float4 *rad, const float *in, float *out,
-                                                        uint32_t n_raw, uint32_t *err,
+                                                        uint32_t n_raw, uint32_t *err, uint32_t polls,
                                                         const uint8_t *tiles = nullptr) {
     extern __shared__ __align__(1024) uint8_t smem[];
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
@@ -191,7 +194,7 @@ __global__ void __launch_bounds__(TC_THREADS) k_mlp_tc(const float *w, NrcGrid g
                     mma_bf16(tmem, sdesc(aA + ks * 256u), sdesc(wB + ks * 256u), id, ks > 0 ? 1u : 0u);
                 mma_commit(bar);
             }
-            bool got = mbar_wait(bar, phase);
+            bool got = mbar_wait(bar, phase, polls);
             phase ^= 1u;
             ok = __syncthreads_and(got) != 0;
             tc_after_sync();
@@ -300,8 +303,8 @@ __device__ __forceinline__ void store_t(uint8_t *tile, uint32_t k, uint32_t r, f
     *reinterpret_cast<__nv_bfloat16 *>(tile + kmaj128(k, r)) = __float2bfloat16_rn(x);
 }
 
-__device__ __forceinline__ bool tc_step(uint32_t bar, uint32_t &phase) {
-    bool got = mbar_wait(bar, phase);
+__device__ __forceinline__ bool tc_step(uint32_t bar, uint32_t &phase, uint32_t polls) {
+    bool got = mbar_wait(bar, phase, polls);
     phase ^= 1u;
     bool ok = __syncthreads_and(got) != 0;
     tc_after_sync();
@@ -378,7 +381,7 @@ template <int MODE>
 __global__ void __launch_bounds__(TR_THREADS, 1)
     k_train_tc(const float *w, const NrcVertex *samples, const uint32_t *n_ptr, uint32_t n_fixed,
                const float *target, const uint8_t *tiles, float *gin_out, float *w_grad,
-               float *loss, uint32_t *err) {
+               float *loss, uint32_t *err, uint32_t polls) {
     extern __shared__ __align__(1024) uint8_t smem[];
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const uint32_t r = tid & 127u, h = tid >> 7;
@@ -451,7 +454,7 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
                              ks > 0 ? 1u : 0u);
                 mma_commit(bar);
             }
-            ok = tc_step(bar, phase);
+            ok = tc_step(bar, phase, polls);
             if (!ok) break;
             if (l < 4) {
                 float a[32];
@@ -503,7 +506,7 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
                          sdesc_s(sAT + 4u * 16384u + ks * 256u, 2048u), ID64, (any || ks > 0) ? 1u : 0u);
             mma_commit(bar);
         }
-        ok = tc_step(bar, phase);
+        ok = tc_step(bar, phase, polls);
         for (int l = 3; l >= 0 && ok; l--) {
             // dZ_l = dA_{l+1} masked by the activation of layer l
             float d[32];
@@ -528,7 +531,7 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
                              sdesc_s(sAT + l * 16384u + ks * 256u, 2048u), ID64, (any || ks > 0) ? 1u : 0u);
                 mma_commit(bar);
             }
-            ok = tc_step(bar, phase);
+            ok = tc_step(bar, phase, polls);
         }
         if (!ok) break;
         // ---- input gradient of the grid features (levels [8h, 8h + 8)), scattered into the grid
@@ -590,27 +593,44 @@ int tc_grid(const void *k) {
 }  // namespace
 
 void nrc_tc_forward_raw(const float *w, const float *in, float *out, uint32_t n, uint32_t *err,
-                        cudaStream_t s) {
+                        uint32_t polls, cudaStream_t s) {
     static int grid = tc_grid((const void *)k_mlp_tc<0>);
     uint32_t tiles = (n + TC_THREADS - 1) / TC_THREADS;
     uint32_t blocks = tiles < (uint32_t)grid ? tiles : (uint32_t)grid;
     if (blocks == 0) return;
     k_mlp_tc<0><<<blocks, TC_THREADS, SM_BYTES, s>>>(w, NrcGrid{}, nullptr, nullptr, nullptr, nullptr,
-                                                      in, out, n, err);
+                                                      in, out, n, err, polls);
 }
 
 // Cache queries: encoded into tiles by a many-CTA kernel (the grid gathers are latency-bound),
 // then the tensor-core MLP over the tiles. tiles: 16 KB per 128 queries (max_q rows).
 void nrc_tc_query(const float *w, const NrcGrid &g, const wl_disney *mats, const NrcVertex *q,
-                  const uint32_t *nq, float4 *rad, uint32_t max_q, uint32_t *err, uint8_t *tiles,
-                  cudaStream_t s) {
+                  const uint32_t *nq, float4 *rad, uint32_t max_q, uint32_t *err, uint32_t polls,
+                  uint8_t *tiles, cudaStream_t s) {
     static int grid = tc_grid((const void *)k_mlp_tc<2>);
     uint32_t ntiles = (max_q + TC_THREADS - 1) / TC_THREADS;
     if (ntiles == 0) return;
     k_encode_tiles<1, false><<<ntiles, 256, 0, s>>>(g, mats, q, nq, max_q, nullptr, tiles);
     uint32_t blocks = ntiles < (uint32_t)grid ? ntiles : (uint32_t)grid;
     k_mlp_tc<2><<<blocks, TC_THREADS, SM_BYTES, s>>>(w, g, mats, q, nq, rad, nullptr, nullptr, 0, err,
-                                                     tiles);
+                                                     polls, tiles);
+}
+
+// Rows of 64 floats read back from the query pass's bfloat16 tiles (parity access).
+__global__ void k_tiles_to_rows(const uint8_t *tiles, uint32_t n, float *rows) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = t >> 6, k = t & 63u;
+    if (i >= n) return;
+    const uint8_t *tile = tiles + (size_t)(i >> 7) * 16384u;
+    rows[(size_t)i * 64u + k] = __bfloat162float(*reinterpret_cast<const __nv_bfloat16 *>(tile + kmaj(i & 127u, k)));
+}
+
+void nrc_tc_encode_rows(const NrcGrid &g, const wl_disney *mats, const NrcVertex *v, const uint32_t *n_ptr,
+                        uint32_t count, uint8_t *tiles, float *rows, cudaStream_t s) {
+    uint32_t ntiles = (count + TC_THREADS - 1) / TC_THREADS;
+    if (ntiles == 0) return;
+    k_encode_tiles<1, false><<<ntiles, 256, 0, s>>>(g, mats, v, n_ptr, count, nullptr, tiles);
+    k_tiles_to_rows<<<(uint32_t)(((uint64_t)count * 64u + 255) / 256), 256, 0, s>>>(tiles, count, rows);
 }
 
 // Gradients of one training step into w_grad (zeroed here) and the grid gradient; loss (zeroed
@@ -618,8 +638,8 @@ void nrc_tc_query(const float *w, const NrcGrid &g, const wl_disney *mats, const
 // rows; gin: 32 floats per row.
 void nrc_tc_train(const float *w, const NrcGrid &g, const wl_disney *mats, const NrcVertex *samples,
                   const uint32_t *n_ptr, uint32_t n_max, const float *in, const float *target,
-                  float *w_grad, float *loss, uint32_t *err, uint8_t *tiles, float *gin,
-                  cudaStream_t s) {
+                  float *w_grad, float *loss, uint32_t *err, uint32_t polls, uint8_t *tiles,
+                  float *gin, cudaStream_t s) {
     static int sms = [] {
         int dev = 0, v = 0;
         cudaGetDevice(&dev);
@@ -638,13 +658,13 @@ void nrc_tc_train(const float *w, const NrcGrid &g, const wl_disney *mats, const
     if (samples) {
         k_encode_tiles<1><<<tiles_n, 256, 0, s>>>(g, mats, samples, n_ptr, n_max, nullptr, tiles);
         k_train_tc<1><<<blocks, TR_THREADS, TS_BYTES, s>>>(w, samples, n_ptr, n_max, nullptr, tiles, gin,
-                                                           w_grad, loss, err);
+                                                           w_grad, loss, err, polls);
         uint64_t threads = (uint64_t)n_max * 16u;
         k_grid_scatter<<<(uint32_t)((threads + 255) / 256), 256, 0, s>>>(g, samples, n_ptr, n_max, gin);
     } else {
         k_encode_tiles<0><<<tiles_n, 256, 0, s>>>(g, mats, nullptr, nullptr, n_max, in, tiles);
         k_train_tc<0><<<blocks, TR_THREADS, TS_BYTES, s>>>(w, nullptr, nullptr, n_max, target, tiles,
-                                                           nullptr, w_grad, loss, err);
+                                                           nullptr, w_grad, loss, err, polls);
     }
 }
 

@@ -332,15 +332,34 @@ uint32_t *nrc_counters(NrcNet *n);
 uint32_t nrc_max_samples(NrcNet *n);
 // nrc_tc.cu (tensor-core inference)
 struct NrcGrid;
+// err: the cache's error word (set when a tensor-core wait gives up); polls: mbarrier polls
+// before a wait gives up (NRC_WAIT_POLLS unless a test lowered it)
+constexpr uint32_t NRC_WAIT_POLLS = 1u << 22;
 void nrc_tc_forward_raw(const float *w, const float *in, float *out, uint32_t n, uint32_t *err,
-                        cudaStream_t s);
+                        uint32_t polls, cudaStream_t s);
 void nrc_tc_query(const float *w, const NrcGrid &g, const wl_disney *mats, const NrcVertex *q,
-                  const uint32_t *nq, float4 *rad, uint32_t max_q, uint32_t *err, uint8_t *tiles,
-                  cudaStream_t s);
+                  const uint32_t *nq, float4 *rad, uint32_t max_q, uint32_t *err, uint32_t polls,
+                  uint8_t *tiles, cudaStream_t s);
 int nrc_reserve_queries(NrcNet *n, uint32_t rows);
+// parity access (nrc.cu): grid parameters, the query and encode passes on caller vertices, and
+// one training step's gradients on caller samples
+NrcGrid nrc_grid(NrcNet *n);
+size_t nrc_grid_count(NrcNet *n);
+void nrc_grid_changed(NrcNet *n, cudaStream_t s);
+int nrc_query_vertices(NrcNet *n, const wl_disney *mats, const NrcVertex *v, uint32_t count, float4 *out,
+                       cudaStream_t s);
+int nrc_encode_vertices(NrcNet *n, const wl_disney *mats, const NrcVertex *v, uint32_t count, float *feat,
+                        uint32_t *corners, cudaStream_t s);
+int nrc_sample_gradients(NrcNet *n, const wl_disney *mats, const NrcVertex *v, uint32_t count,
+                         cudaStream_t s);
+void nrc_zero_grid_grad(NrcNet *n, cudaStream_t s);
+void nrc_tc_encode_rows(const NrcGrid &g, const wl_disney *mats, const NrcVertex *v, const uint32_t *n_ptr,
+                        uint32_t count, uint8_t *tiles, float *rows, cudaStream_t s);
 void nrc_tc_train(const float *w, const NrcGrid &g, const wl_disney *mats, const NrcVertex *samples,
                   const uint32_t *n_ptr, uint32_t n_max, const float *in, const float *target,
-                  float *w_grad, float *loss, uint32_t *err, uint8_t *tiles, float *gin,
-                  cudaStream_t s);
+                  float *w_grad, float *loss, uint32_t *err, uint32_t polls, uint8_t *tiles,
+                  float *gin, cudaStream_t s);
+void nrc_set_wait_polls(NrcNet *n, uint32_t polls);
+void nrc_clear_error(NrcNet *n, cudaStream_t s);
 
 }  // namespace wl

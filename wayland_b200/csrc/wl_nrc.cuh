@@ -15,6 +15,7 @@
 // products accumulate in FP32.
 #pragma once
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include "wl_disney.cuh"
 #include "wl_internal.h"
@@ -28,12 +29,16 @@ constexpr int NRC_HIDDEN_MATS = 4;  // 64x64 matrices before the output layer
 constexpr int NRC_WEIGHTS = NRC_HIDDEN_MATS * NRC_HID * NRC_IN + NRC_OUT * NRC_HID;  // 17408
 constexpr int NRC_MAX_LEVELS = 16;
 
+// The grid's parameters: FP32 master values (what Adam updates) and their FP16 copy (what the
+// encoding gathers: 4 bytes per entry, 2 features), and the FP32 gradient, each
+// [levels][2^log2T][2 features].
 struct NrcGrid {
     uint32_t levels, log2T, base;
     float scale;
     float lo[3], inv_ext[3];
-    float *params;   // [levels][2^log2T][2]
-    float *grad;     // same shape
+    float *params;
+    __half2 *feat;
+    float *grad;
 };
 
 __host__ __device__ __forceinline__ float bf16r(float x) {
@@ -100,22 +105,31 @@ __device__ __forceinline__ void sh16(float x, float y, float z, float *o) {
     o[15] = 0.59004358992664352f * x * (-xx + 3.0f * yy);
 }
 
+// Corner k (bit 0: +x, bit 1: +y, bit 2: +z) of the level-l cell around pn: its entry index
+// and trilinear weight.
+__device__ __forceinline__ uint32_t grid_corner(const NrcGrid &g, float3 pn, uint32_t l, int k, float &w) {
+    uint32_t res = grid_res(g, l);
+    GridCell c = grid_cell(g, pn, res);
+    uint32_t dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
+    w = (dx ? c.fx : 1.0f - c.fx) * (dy ? c.fy : 1.0f - c.fy) * (dz ? c.fz : 1.0f - c.fz);
+    return grid_index(g, res, c.cx + dx, c.cy + dy, c.cz + dz);
+}
+
 // Hash-grid features of levels [l0, l0 + 8): x[0..15] (rounded to bfloat16).
 __device__ __forceinline__ void nrc_grid_features(const NrcGrid &g, float3 pn, uint32_t l0, float *x) {
-    const uint32_t F = 2;
     for (uint32_t j = 0; j < 8; j++) {
         const uint32_t l = l0 + j;
         float f0 = 0.0f, f1 = 0.0f;
         if (l < g.levels) {
             uint32_t res = grid_res(g, l);
             GridCell c = grid_cell(g, pn, res);
-            const float *tab = g.params + (size_t)l * ((size_t)1 << g.log2T) * F;
+            const __half2 *tab = g.feat + (size_t)l * ((size_t)1 << g.log2T);
 #pragma unroll
             for (int k = 0; k < 8; k++) {
                 uint32_t dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
                 float w = (dx ? c.fx : 1.0f - c.fx) * (dy ? c.fy : 1.0f - c.fy) * (dz ? c.fz : 1.0f - c.fz);
                 uint32_t idx = grid_index(g, res, c.cx + dx, c.cy + dy, c.cz + dz);
-                float2 e = *reinterpret_cast<const float2 *>(tab + (size_t)idx * F);
+                float2 e = __half22float2(tab[idx]);
                 f0 += w * e.x;
                 f1 += w * e.y;
             }
