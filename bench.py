@@ -28,10 +28,16 @@ sys.path.insert(0, ROOT)
 
 W, H, SPP, DEPTH = 1920, 1080, 64, 16
 METRIC = "Mpaths/s"
-# DRAM bytes (read + write) per extend ray of this workload: 45.64 GB over the 16 extend launches
-# of one step (one wave) in the ncu launch list of
-# profiles/launches_plain_pt_displaced_sphere_1920x1080x64spp.md, / 298.3 M rays per step
+# DRAM bytes (read + write) per extend ray of this workload, from an ncu launch list of the same
+# command (dram__bytes_read.sum + dram__bytes_write.sum over the 16 extend launches of one step,
+# divided by the step's extend rays); CUDA events cannot count DRAM bytes, so the bench scales
+# this figure by its own rays and labels the number as taken from that capture
 EXTEND_DRAM_BYTES_PER_RAY = 153.0
+TRAFFIC_SOURCE = ("ncu launch list of this workload: 45.34 GB of DRAM over the 16 extend launches "
+                  "of one step / 298.3 M extend rays = 153 B per ray, times this run's rays")
+# The CPU legs time the same fixed pixel sample: CPU_ROWS rows of the 1920x1080 image around its
+# centre, at the full 64 spp
+CPU_ROWS = 32
 WORKLOAD = "plain PT at scale: displaced icosphere 1,997,120 tris + ground, 4 quad lights + env 0.1, 1920x1080, 64 spp, depth 16, FP32"
 
 
@@ -143,27 +149,27 @@ class CpuPT:
                                    self.threads, self.film.ctypes.data, None, lo, hi)
         return time.perf_counter() - t
 
-    def calibrate(self, target_s):
-        mid = (H // 2) * W
-        dt = self.run(mid, mid + 4 * W)
-        rate = 4 * W / max(dt, 1e-6)
-        self.npx = int(min(max(rate * target_s, W), H * W // 2))
-
-    def sample(self):
-        """Returns (Mpaths/s, description) for one timed sample."""
-        lo = (H // 2) * W - self.npx // 2
-        dt = self.run(lo, lo + self.npx)
-        desc = (f"{self.npx} pixels ({self.npx / W:.1f} rows around the image centre) x {SPP} spp "
-                f"= {self.npx * SPP} paths in {dt:.1f} s")
+    def sample(self, rows=CPU_ROWS):
+        """Times the fixed sample (rows x W pixels around the image centre at SPP samples per
+        pixel); returns (Mpaths/s, seconds, description)."""
+        npx = rows * W
+        lo = (H // 2) * W - npx // 2
+        dt = self.run(lo, lo + npx)
+        desc = (f"{npx} pixels ({rows} rows around the image centre) x {SPP} spp "
+                f"= {npx * SPP} paths in {dt:.2f} s on {self.threads} threads")
         if self.kind == "reference":
             desc += " (PathTracing.cu as compiled: depth cap 25, background 0)"
-        return self.npx * SPP / dt / 1e6, desc
+        return npx * SPP / dt / 1e6, dt, desc
 
     def close(self):
         self.lib.lib.or_bvh_destroy(self.bvh)
 
 
 def reference_arm(args):
+    """The reference's own CPU implementation of the path (PathTracing.cu compiled on the host
+    over an emulation of its OptiX calls) on all host cores. Each step renders the same fixed
+    pixel sample of the bench frame (CPU_ROWS centre rows at 64 spp, about 3.9 M paths), so
+    ms_per_step is the time of the sample actually rendered, not of a full frame."""
     rank = env_int("RANK", 0)
     if rank != 0:
         return 0
@@ -171,20 +177,24 @@ def reference_arm(args):
     scene = scenes.displaced_sphere(W, H, SPP, DEPTH)
     threads = os.cpu_count() or 1
     cpu = CpuPT(scene, threads)
-    cpu.calibrate(args.ref_step_s)
-    vals, desc = [], ""
+    vals, secs, desc = [], [], ""
     for step in range(args.warmup + args.steps):
-        v, desc = cpu.sample()
+        v, dt, desc = cpu.sample()
         if step >= args.warmup:
             vals.append(v)
+            secs.append(dt)
     cpu.close()
     value = float(statistics.mean(vals))
+    npx = CPU_ROWS * W
     line = {"metric": METRIC, "value": round(value, 4), "unit": METRIC, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(W * H * SPP / (value * 1e6) * 1e3, 1),
+            "ms_per_step": round(1e3 * float(statistics.mean(secs)), 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": WORKLOAD, "device": "host CPU", "threads": threads},
+            "config": {"workload": WORKLOAD, "device": "host CPU", "threads": threads,
+                       "sampled": True, "sample_pixels": npx, "sample_paths": npx * SPP,
+                       "sample": f"{CPU_ROWS} rows around the centre of the 1920x1080 frame, 64 spp; "
+                                 "a step renders this sample, not the full frame"},
             "cpu_baseline": {"value": round(value, 4), "unit": METRIC, "cores": threads,
                              "kind": cpu.kind, "sample": desc},
             "e2e": {"value": round(value, 4), "unit": METRIC, "h2d_bytes_per_step": 0,
@@ -297,37 +307,81 @@ def raycast_microbench(wl, torch, ctx, sc, scene, stream):
     return out
 
 
-def graph_leg(wl, torch, ctx, sc, scene, stream, frames=16):
+def graph_leg(wl, torch, ctx, sc, scene, stream, repeats=12, frames=4):
     """Progressive rendering, 1 spp per call at 1920x1080 on the benchmark scene: device time per
-    call with direct launches and with every wave replayed as one CUDA graph."""
+    call with direct launches and with every wave replayed as one CUDA graph. The two modes
+    alternate in blocks of `frames` calls, `repeats` blocks each; the median block time per
+    frame is reported (and the spread), so that drift on a shared machine hits both modes."""
     cam = scene.camera_struct()
+    modes = (("launches", 0), ("graph", wl._abi.RENDER_GRAPH))
+    films = {name: wl.Film(ctx, W, H) for name, _ in modes}
+    times = {name: [] for name, _ in modes}
+    frame = {name: 0 for name, _ in modes}
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    for rep in range(repeats + 1):  # block 0 of each mode is warm-up (first launches, capture)
+        for name, flags in modes:
+            p = wl.render_params(W, H, 1, max_depth=DEPTH, env=scene.env, flags=flags)
+            ctx.sync()
+            e0.record(stream)
+            for _ in range(frames):
+                p.first_frame = frame[name]
+                frame[name] += 1
+                wl.render(ctx, sc, cam, p, films[name])
+            e1.record(stream)
+            e1.synchronize()
+            if rep:
+                times[name].append(e0.elapsed_time(e1) / frames)
     out = {}
+    for name, _ in modes:
+        t = sorted(times[name])
+        out[name] = {"ms_per_frame": round(statistics.median(t), 3), "min": round(t[0], 3),
+                     "max": round(t[-1], 3), "repeats": repeats, "frames_per_repeat": frames}
+        films[name].close()
+    out["graph_over_launches"] = round(out["graph"]["ms_per_frame"] / out["launches"]["ms_per_frame"], 4)
+    return out
+
+
+def cornell_leg(wl, torch, ctx, repeats=20):
+    """Configuration 1: the procedural Cornell box (36 triangles), 256x256 x 16 spp, depth 8,
+    NEE+MIS, PCG32 seed 0, FP32 fast math: one render of 1,048,576 paths, the case dominated by
+    per-launch overhead. Median device time of `repeats` renders, with direct launches and with
+    CUDA-graph replay."""
+    from wayland_b200 import scenes
+    sc = scenes.cornell_box(256, 256, 16, 8)
+    s = wl.Scene(ctx, sc, bvh_kind=BVH_KIND[0])
+    cam = sc.camera_struct()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    out = {"scene": f"Cornell box {sc.num_tris} tris, 256x256, 16 spp, depth 8, PCG32 seed 0"}
+    paths = 256 * 256 * 16
     for name, flags in (("launches", 0), ("graph", wl._abi.RENDER_GRAPH)):
-        film = wl.Film(ctx, W, H)
-        p = wl.render_params(W, H, 1, max_depth=DEPTH, env=scene.env, flags=flags)
-        for f in range(3):
-            p.first_frame = f
-            wl.render(ctx, sc, cam, p, film)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        ctx.sync()
-        t0 = time.perf_counter()
-        e0.record(stream)
-        for f in range(frames):
-            p.first_frame = 3 + f
-            wl.render(ctx, sc, cam, p, film)
-        e1.record(stream)
-        e1.synchronize()
-        out[name] = {"ms_per_frame": round(e0.elapsed_time(e1) / frames, 3),
-                     "host_ms_per_call": round((time.perf_counter() - t0) * 1e3 / frames, 3)}
+        film = wl.Film(ctx, 256, 256)
+        t = []
+        for rep in range(repeats + 2):
+            p = wl.render_params(256, 256, 16, max_depth=8, rng=wl.RNG_PCG32, seed=0,
+                                 first_frame=16 * rep, flags=flags)
+            ctx.sync()
+            e0.record(stream)
+            wl.render(ctx, s, cam, p, film)
+            e1.record(stream)
+            e1.synchronize()
+            if rep >= 2:
+                t.append(e0.elapsed_time(e1))
+        ms = statistics.median(t)
+        out[name] = {"ms": round(ms, 3), "mpaths_s": round(paths / ms / 1e3, 1)}
         film.close()
+    s.close()
     return out
 
 
 def batch_leg(wl, torch, ctx, stream, jobs=64):
     """Configuration 3: 64 procedural scenes (scenes.batch_scene: triangles lognormal in [10K, 5M],
-    resolution, spp, depth and 1-8 lights drawn per scene), rendered one wl_render call per scene
-    and as one wl_render_batch. Device time; Mpaths/s = all jobs' W x H x spp / time."""
+    resolution, spp, depth and 1-8 lights drawn per scene), rendered one wl_render call per scene,
+    as one wl_render_batch, and as one wl_render_batch replayed as a single CUDA graph
+    (WL_RENDER_GRAPH; captured on the first round, replayed on the timed second round). Device
+    time; Mpaths/s = all jobs' W x H x spp / time."""
     from wayland_b200 import scenes
     datas = [scenes.batch_scene(i) for i in range(jobs)]
     objs = [wl.Scene(ctx, d, bvh_kind=BVH_KIND[0]) for d in datas]
@@ -337,12 +391,16 @@ def batch_leg(wl, torch, ctx, stream, jobs=64):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     out = {"jobs": jobs, "triangles": int(sum(d.num_tris for d in datas)), "paths": int(paths)}
-    for mode in ("separate", "batch", "separate", "batch"):  # second round timed
+    gparams = [wl.render_params(d.width, d.height, d.spp, max_depth=d.max_depth, flags=wl._abi.RENDER_GRAPH)
+               for d in datas]
+    for mode in ("separate", "batch", "batch_graph") * 2:  # second round timed
         films = [wl.Film(ctx, d.width, d.height) for d in datas]
         ctx.sync()
         e0.record(stream)
         if mode == "batch":
             wl.render_batch(ctx, objs, cams, params, films)
+        elif mode == "batch_graph":
+            wl.render_batch(ctx, objs, cams, gparams, films)
         else:
             for o, c, p, f in zip(objs, cams, params, films):
                 wl.render(ctx, o, c, p, f)
@@ -355,15 +413,18 @@ def batch_leg(wl, torch, ctx, stream, jobs=64):
     for o in objs:
         o.close()
     out["batch_gain"] = round(out["separate"]["ms"] / out["batch"]["ms"], 3)
+    out["batch_graph_gain"] = round(out["separate"]["ms"] / out["batch_graph"]["ms"], 3)
     return out
 
 
-def bdpt_ao_leg(wl, torch, ctx, res=512, spp=256, oracle_spp=4096, ao_res=(512, 256)):
+def bdpt_ao_leg(wl, torch, ctx, res=1024, spp=256, oracle_spp=4096, ao_res=(512, 256)):
     """Configuration 5: the glass-sphere caustic scene (158,420 sphere triangles + plane + a
-    0.05-wide quad light). BDPT with subpaths of at most 10 vertices: samples/s at res x res x
-    spp, and relMSE of that image against an FP64 film of oracle_spp BDPT samples (seeds
-    disjoint). AO: 4 camera samples x 32 occlusion rays of radius 0.1 per pixel at ao_res (about
-    2^24 rays). Device time with CUDA events on the library's stream."""
+    0.05-wide quad light), roughness 0.05. BDPT with subpaths of at most 10 vertices: samples/s
+    at res x res x spp, and the relMSE of that image against an independent estimate of the same
+    image, the plain path tracer's FP64 film of oracle_spp samples per pixel (other seeds) with
+    paths of up to 20 vertices (what an eye and a light subpath of 10 vertices each can join);
+    the oracle's own noise floor is reported beside it (relMSE of its two halves / 4). AO: 4 camera samples x 32 occlusion rays of radius 0.1 per pixel at ao_res
+    (about 2^24 rays). Device time with CUDA events on the library's stream."""
     from wayland_b200 import scenes
     sc = scenes.glass_sphere(res, res)
     scene = wl.Scene(ctx, sc, bvh_kind=BVH_KIND[0])
@@ -386,24 +447,34 @@ def bdpt_ao_leg(wl, torch, ctx, res=512, spp=256, oracle_spp=4096, ao_res=(512, 
     st = ctx.stats()
     img = film.download64()
     film.close()
-    ref = wl.Film(ctx, res, res, fp64=True)
-    done = 0
+    # independent oracle: plain path tracer (NEE + MIS, unbiased Russian roulette, paths of up to
+    # 20 vertices), FP64 film, two halves of disjoint frames
     t0 = time.perf_counter()
-    while done < oracle_spp:
-        k = min(512, oracle_spp - done)
-        wl.render(ctx, scene, cam, wl.render_params(res, res, k, strategy=wl.STRATEGY_BDPT, max_depth=10,
-                                                    first_frame=20000000 + done), ref)
-        done += k
-    r64 = ref.download64()
+    halves = []
+    for h in range(2):
+        ref = wl.Film(ctx, res, res, fp64=True)
+        done = 0
+        while done < oracle_spp // 2:
+            k = min(256, oracle_spp // 2 - done)
+            wl.render(ctx, scene, cam, wl.render_params(res, res, k, max_depth=20,
+                                                        first_frame=20000000 + h * oracle_spp + done), ref)
+            done += k
+        halves.append(ref.download64())
+        ref.close()
     oracle_s = time.perf_counter() - t0
-    ref.close()
-    rel = float(((img - r64) ** 2 / (r64 * r64 + 1e-2)).mean())
+    r64 = 0.5 * (halves[0] + halves[1])
+
+    def rel(a, b):
+        return float(((a - b) ** 2 / (b * b + 1e-2)).mean())
+
     samples = res * res * spp
     out = {"scene": f"glass sphere {sc.num_tris} tris, roughness 0.05, {res}x{res}, subpaths <= 10 vertices",
            "spp": spp, "ms": round(ms, 1), "msamples_s": round(samples / ms / 1e3, 2),
            "closest_hit_rays_per_sample": round(st["segments"] / samples, 3),
            "connection_rays_per_sample": round(st["shadow_rays"] / samples, 3),
-           "relmse_vs_fp64": rel, "oracle": f"{oracle_spp} spp BDPT, FP64 film ({oracle_s:.1f} s)"}
+           "relmse_vs_pt_oracle": rel(img, r64),
+           "oracle": f"plain path tracer, {oracle_spp} spp, FP64 film, depth 20 ({oracle_s:.1f} s)",
+           "oracle_noise_floor": rel(halves[0], halves[1]) / 4}
     # ambient occlusion, radius 0.1
     aw, ah = ao_res
     afilm = wl.Film(ctx, aw, ah)
@@ -424,30 +495,38 @@ def bdpt_ao_leg(wl, torch, ctx, res=512, spp=256, oracle_spp=4096, ao_res=(512, 
     return out
 
 
-def nrc_convergence(wl, torch, ctx, res=(480, 270), oracle_spp=16384, target=1e-2,
+def nrc_convergence(wl, torch, ctx, res=(1920, 1080), oracle_spp=8192, target=1e-2,
                     budget_s=60.0, chunk=4, warmup_frames=16):
-    """Time to relMSE <= target against an FP64-accumulated high-spp render, for the plain path
-    tracer and for the radiance-cache path tracer, on the door-slit room (about 500K triangles,
-    mostly indirect light). relMSE = mean over pixels and channels of (I - R)^2 / (R^2 + 1e-2).
-    Times are device time of the render calls (CUDA events on the library's stream); the cache's
-    time includes its warm-up frames (training only, no image) from a fresh cache."""
+    """Configuration 4: time to relMSE <= target against an FP64-accumulated high-spp render, for
+    the plain path tracer and for the radiance-cache path tracer (1 spp per frame), on the
+    door-slit room (about 500K triangles, mostly indirect light) at 1920x1080. relMSE = mean over
+    pixels and channels of (I - R)^2 / (R^2 + 1e-2). Times are device time of the render calls
+    (CUDA events on the library's stream); the cache's time includes its warm-up frames
+    (training only, no image) from a fresh cache. The oracle is rendered in two halves of
+    disjoint frames; relMSE(half A, half B) / 4 is its own noise floor."""
     from wayland_b200 import scenes
     W_, H_ = res
     sc = scenes.door_slit_room(W_, H_)
     scene = wl.Scene(ctx, sc, bvh_kind=BVH_KIND[0])
     cam = sc.camera_struct()
     stream = torch.cuda.ExternalStream(ctx.stream)
-    # oracle: FP64 film, plain path tracer, fast math
-    ref_film = wl.Film(ctx, W_, H_, fp64=True)
+    # oracle: FP64 films of two halves of disjoint frames, plain path tracer, fast math
     t0 = time.perf_counter()
-    done = 0
-    while done < oracle_spp:
-        k = min(1024, oracle_spp - done)
-        wl.render(ctx, scene, cam, wl.render_params(W_, H_, k, first_frame=1000000 + done,
-                                                    max_depth=16), ref_film)
-        done += k
-    ref = torch.from_numpy(ref_film.download64()).cuda()
+    halves = []
+    for h in range(2):
+        hf = wl.Film(ctx, W_, H_, fp64=True)
+        done = 0
+        while done < oracle_spp // 2:
+            k = min(512, oracle_spp // 2 - done)
+            wl.render(ctx, scene, cam, wl.render_params(W_, H_, k, first_frame=1000000 + h * oracle_spp + done,
+                                                        max_depth=16), hf)
+            done += k
+        halves.append(torch.from_numpy(hf.download64()).cuda())
+        hf.close()
+    ref = 0.5 * (halves[0] + halves[1])
     oracle_s = time.perf_counter() - t0
+    noise_floor = float(((halves[0] - halves[1]) ** 2 / (ref * ref + 1e-2)).mean()) / 4
+    del halves
 
     def relmse(img):
         x = torch.from_numpy(img).cuda().double()
@@ -492,12 +571,16 @@ def nrc_convergence(wl, torch, ctx, res=(480, 270), oracle_spp=16384, target=1e-
             curve.append((spp, round(t_dev, 4), err))
             if err <= target or t_dev > budget_s:
                 break
+        extra = {}
         if cache is not None:
+            st = cache.stats()
+            extra = {"train_samples_last_frame": st["train_samples"], "queries_last_frame": st["queries"]}
             cache.close()
         film.close()
         reached = curve[-1][2] <= target
         return {"reached": reached, "seconds": curve[-1][1] if reached else None, "spp": curve[-1][0],
-                "final_relmse": curve[-1][2], "curve": curve[:: max(1, len(curve) // 12)]}
+                "ms_per_frame": round(1e3 * curve[-1][1] / (curve[-1][0] + (warmup_frames if cache is not None else 0)), 3),
+                "final_relmse": curve[-1][2], "curve": curve[:: max(1, len(curve) // 12)], **extra}
 
     plain = run("plain")
     nrc = run("nrc")
@@ -505,10 +588,63 @@ def nrc_convergence(wl, torch, ctx, res=(480, 270), oracle_spp=16384, target=1e-
     scene.close()
     out = {"scene": f"door-slit room {sc.num_tris} tris, {W_}x{H_}, depth 16, fast math",
            "oracle": f"{oracle_spp} spp, FP64 film, plain path tracer ({oracle_s:.1f} s)",
+           "oracle_noise_floor": noise_floor,
+           "cache": "hash grid 16 levels x 2^19 entries x 2 FP16 features, MLP 64-64-64-64-64-16 BF16 "
+                    "(FP32 accumulation), 2^14 training paths per frame",
            "target_relmse": target, "plain": plain, "nrc": nrc}
     if plain["seconds"] and nrc["seconds"]:
         out["nrc_time_fraction"] = round(nrc["seconds"] / plain["seconds"], 4)
     return out
+
+
+def nrc_kernels(wl, torch, ctx, queries=1920 * 1080, samples=1 << 16, repeats=10):
+    """FLOP roofline of the radiance cache's tensor-core kernels at 1080p batch sizes, through the
+    public entry points (device buffers, CUDA events on the library's stream, median of repeats):
+    the MLP forward on `queries` rows (wl_nrc_mlp_forward: the query pass's tcgen05 MLP kernel
+    alone, 34,816 FLOP per row) and one training step on `samples` rows (wl_nrc_train_step:
+    operand tiles, the fused forward/backward tcgen05 kernel, Adam; 104,448 FLOP per row),
+    against the measured sustained BF16 peak."""
+    from wayland_b200 import scenes
+    sc = scenes.cornell_box(16, 16)
+    s = wl.Scene(ctx, sc)
+    c = wl.RadianceCache(ctx, s)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+    x = torch.rand((queries, 64), device="cuda", generator=g) * 2 - 1
+    out = torch.empty((queries, 4), device="cuda")
+    t = torch.rand((samples, 4), device="cuda", generator=g)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+
+    def med(fn):
+        ts = []
+        for r in range(repeats + 2):
+            ctx.sync()
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            if r >= 2:
+                ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    ms_q = med(lambda: c.forward(x.data_ptr(), out.data_ptr(), queries))
+    ms_t = med(lambda: c.lib.wl_nrc_train_step(c.handle, wl._abi.C.c_void_p(x.data_ptr()),
+                                               wl._abi.C.c_void_p(t.data_ptr()), samples, None))
+    c.close()
+    s.close()
+    pk = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peak = pk.get("bf16_tflops_sustained", 1400.0)
+    kind = "measured sustained" if "bf16_tflops_sustained" in pk else "fallback sustained"
+    fq = queries * 34816 / (ms_q * 1e-3) / 1e12
+    ft = samples * 104448 / (ms_t * 1e-3) / 1e12
+    return {"mlp_query": {"rows": queries, "ms": round(ms_q, 4), "tflops": round(fq, 1),
+                          "frac": round(fq / peak, 4)},
+            "train_step": {"rows": samples, "ms": round(ms_t, 4), "tflops": round(ft, 1),
+                           "frac": round(ft / peak, 4)},
+            "peak_tflops": peak, "peak_kind": kind, "bound": "tensor"}
 
 
 def main():
@@ -517,8 +653,6 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--ref-step-s", type=float, default=8.0, help="CPU seconds per reference step")
-    ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-raycast", action="store_true")
     ap.add_argument("--math", default="fast", choices=["fast", "strict"])
@@ -529,7 +663,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--bdpt-only", action="store_true", help="only the BDPT + AO leg (prints its JSON)")
-    ap.add_argument("--nrc-res", default="960x540", help="resolution of the radiance-cache comparison")
+    ap.add_argument("--nrc-res", default="1920x1080", help="resolution of the radiance-cache comparison")
     ap.add_argument("--nrc-oracle-spp", type=int, default=8192)
     ap.add_argument("--nrc-budget-s", type=float, default=60.0)
     ap.add_argument("--tune", default=None,
@@ -564,8 +698,10 @@ def main():
     if args.nrc_only:
         ctx = wl.Context(local)
         w_, h_ = (int(v) for v in args.nrc_res.split("x"))
-        print(json.dumps(nrc_convergence(wl, torch, ctx, res=(w_, h_), oracle_spp=args.nrc_oracle_spp,
-                                         budget_s=args.nrc_budget_s)), flush=True)
+        r = nrc_convergence(wl, torch, ctx, res=(w_, h_), oracle_spp=args.nrc_oracle_spp,
+                            budget_s=args.nrc_budget_s)
+        r["kernels"] = nrc_kernels(wl, torch, ctx)
+        print(json.dumps(r), flush=True)
         ctx.close()
         return 0
     if world > 1:
@@ -678,6 +814,7 @@ def main():
             "roofline": {"bound": "hbm", "kernel": "k_extend (closest-hit traversal)",
                          "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "traffic_source": TRAFFIC_SOURCE if traffic is not None else None,
                          "peak_kind": peak_kind,
                          "bytes_per_ray": round(b_ray, 1),
                          "algorithmic_bytes_per_launch": round(segs * b_ray / ext_launches),
@@ -703,6 +840,7 @@ def main():
             line["raycast"] = raycast_microbench(wl, torch, ctx, sc, scene, stream)
         if world == 1:
             line["progressive_1spp"] = graph_leg(wl, torch, ctx, sc, scene, stream)
+            line["cornell_config1"] = cornell_leg(wl, torch, ctx)
         if world == 1 and not args.no_batch:
             line["batch"] = batch_leg(wl, torch, ctx, stream)
         if world == 1 and not args.no_bdpt:
@@ -714,11 +852,11 @@ def main():
             line["time_to_relmse"] = nrc_convergence(wl, torch, ctx, res=(w_, h_),
                                                      oracle_spp=args.nrc_oracle_spp,
                                                      budget_s=args.nrc_budget_s)
+            line["time_to_relmse"]["kernels"] = nrc_kernels(wl, torch, ctx)
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             cpu = CpuPT(scene, threads)
-            cpu.calibrate(args.cpu_sample_s)
-            v, desc = cpu.sample()
+            v, _, desc = cpu.sample()
             cpu.close()
             line["cpu_baseline"] = {"value": round(v, 4), "unit": METRIC, "cores": threads,
                                     "kind": cpu.kind, "sample": desc}

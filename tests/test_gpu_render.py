@@ -326,6 +326,28 @@ def test_batch_matches_separate_renders(ctx):
             assert np.array_equal(bits(f.download()), bits(r))
         for f in films:
             f.close()
+        # WL_RENDER_GRAPH: the whole batch is one captured graph, replayed by a second call with
+        # other frames (the jobs table changes, the graph does not); both equal separate renders
+        for shift in (0, 11):
+            gparams, gfilms, grefs = [], [], []
+            for (sc, _), s, p in zip(jobs, objs, params):
+                q = wl.render_params(p.width, p.height, p.spp, math=wl.MATH_STRICT, env=sc.env,
+                                     max_depth=p.max_depth, rng=p.rng, seed=p.seed,
+                                     strategy=p.strategy, first_frame=p.first_frame + shift,
+                                     flags=wl._abi.RENDER_GRAPH)
+                gparams.append(q)
+                gfilms.append(wl.Film(ctx, sc.width, sc.height))
+                rf = wl.Film(ctx, sc.width, sc.height)
+                r = wl.render_params(p.width, p.height, p.spp, math=wl.MATH_STRICT, env=sc.env,
+                                     max_depth=p.max_depth, rng=p.rng, seed=p.seed,
+                                     strategy=p.strategy, first_frame=p.first_frame + shift)
+                wl.render(ctx, s, sc.camera_struct(), r, rf)
+                grefs.append(rf.download())
+                rf.close()
+            wl.render_batch(ctx, objs, [sc.camera_struct() for sc, _ in jobs], gparams, gfilms)
+            for f, r in zip(gfilms, grefs):
+                assert np.array_equal(bits(f.download()), bits(r))
+                f.close()
         for s in objs:
             s.close()
     finally:

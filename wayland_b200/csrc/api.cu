@@ -65,16 +65,16 @@ struct wl_context {
     BdptWave bd{};          // bidirectional wave buffers (allocated by the first BDPT render)
     void *bd_block = nullptr;
     bool events_on = true;  // per-launch timing events (off while a wave is captured)
-    // CUDA graphs of one wave (WL_RENDER_GRAPH): per-wave (base, first_frame) pairs, the replay
-    // counter and the current pair read by the kernels; a few instantiated graphs keyed by every
-    // argument they captured
-    uint64_t *d_dyn_all = nullptr;
-    size_t dyn_cap = 0;
-    uint32_t *d_dyn_ctr = nullptr;
+    // CUDA graphs (WL_RENDER_GRAPH): the (first sample, first frame) pair that a captured wave's
+    // kernels read, set by the wave's first node; a few instantiated graphs keyed by every
+    // argument they captured, each with its template (for that node's per-replay arguments)
     uint64_t *d_dyn_cur = nullptr;
     struct GraphEntry {
         std::vector<uint8_t> key;
+        cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
+        cudaGraphNode_t begin = nullptr;  // the k_wave_begin node (null for a batch graph)
+        uint32_t launches = 0;            // kernels of one replay
         uint64_t used = 0;
     };
     GraphEntry graphs[4];
@@ -386,10 +386,11 @@ int wl_context_destroy(wl_context *c) {
     if (c->bd_block) cudaFree(c->bd_block);
     if (c->d_jobs) cudaFree(c->d_jobs);
     if (c->d_slot_job) cudaFree(c->d_slot_job);
-    if (c->d_dyn_all) cudaFree(c->d_dyn_all);
-    if (c->d_dyn_ctr) cudaFree(c->d_dyn_ctr);
-    for (auto &g : c->graphs)
+    if (c->d_dyn_cur) cudaFree(c->d_dyn_cur);
+    for (auto &g : c->graphs) {
         if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+    }
     if (c->d_misc) cudaFree(c->d_misc);
     if (c->d_cast_counts) cudaFree(c->d_cast_counts);
     for (auto &v : c->ev)
@@ -882,63 +883,77 @@ template <class T> static void key_add(std::vector<uint8_t> &k, const T &v) {
     k.insert(k.end(), p, p + sizeof(T));
 }
 
-// The instantiated graph of one wave whose captured arguments are `key`: reused when an equal
-// key was captured before, else captured from `issue` (which enqueues work on the context's
-// stream, and on its side stream only between a fork from and a join back to the main stream)
-// into the least recently used entry.
+// The graph entry whose captured arguments are `key`: reused when an equal key was captured
+// before, else captured from `issue` (which enqueues work on the context's stream, and on its
+// side stream only between a fork from and a join back to the main stream, and returns the
+// kernels it launched) into the least recently used entry. With `wave_begin`, the graph's one
+// root node is the k_wave_begin kernel whose arguments each replay sets.
 template <class F>
-static int wave_graph(wl_context *c, const std::vector<uint8_t> &key, F issue, cudaGraphExec_t *out) {
+static int cached_graph(wl_context *c, const std::vector<uint8_t> &key, bool wave_begin, F issue,
+                        wl_context::GraphEntry **out) {
     c->graph_clock++;
     for (auto &g : c->graphs)
         if (g.exec && g.key == key) {
             g.used = c->graph_clock;
-            *out = g.exec;
+            *out = &g;
             return WL_OK;
         }
     auto *slot = &c->graphs[0];
     for (auto &g : c->graphs)
         if (!g.exec || g.used < slot->used) slot = &g;
-    if (slot->exec) {
-        cudaGraphExecDestroy(slot->exec);
-        slot->exec = nullptr;
-    }
+    if (slot->exec) cudaGraphExecDestroy(slot->exec);
+    if (slot->graph) cudaGraphDestroy(slot->graph);
+    *slot = wl_context::GraphEntry{};
     cudaGraph_t graph = nullptr;
     const bool ev = c->events_on;
     c->events_on = false;
     CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-    issue();
+    const uint32_t launches = issue();
     cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
     c->events_on = ev;
-    if (e != cudaSuccess) return fail(WL_ERR_CUDA, std::string("wave capture: ") + cudaGetErrorString(e));
-    e = cudaGraphInstantiate(&slot->exec, graph, 0);
-    cudaGraphDestroy(graph);
-    if (e != cudaSuccess) {
-        slot->exec = nullptr;
-        return fail(WL_ERR_CUDA, std::string("wave graph: ") + cudaGetErrorString(e));
+    if (e != cudaSuccess) return fail(WL_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    cudaGraphNode_t begin = nullptr;
+    if (wave_begin) {
+        cudaGraphNode_t roots[2];
+        size_t nroots = 2;
+        cudaGraphNodeType type = cudaGraphNodeTypeEmpty;
+        e = cudaGraphGetRootNodes(graph, roots, &nroots);
+        if (e == cudaSuccess && nroots == 1) e = cudaGraphNodeGetType(roots[0], &type);
+        if (e != cudaSuccess || nroots != 1 || type != cudaGraphNodeTypeKernel) {
+            cudaGraphDestroy(graph);
+            return fail(WL_ERR_CUDA, "graph capture: the wave's first node is not its begin kernel");
+        }
+        begin = roots[0];
     }
+    e = cudaGraphInstantiate(&slot->exec, graph, 0);
+    if (e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        slot->exec = nullptr;
+        return fail(WL_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    }
+    slot->graph = graph;
+    slot->begin = begin;
+    slot->launches = launches;
     slot->key = key;
     slot->used = c->graph_clock;
-    *out = slot->exec;
+    *out = slot;
     return WL_OK;
 }
 
 extern "C" {
 
-// Device copies of every wave's (first sample, first frame) for graph replays.
-static int upload_dyn(wl_context *c, const std::vector<uint64_t> &dyn) {
-    if (!c->d_dyn_ctr) {
-        CK(cudaMalloc(&c->d_dyn_ctr, 64));
-        c->d_dyn_cur = reinterpret_cast<uint64_t *>(reinterpret_cast<char *>(c->d_dyn_ctr) + 16);
-    }
-    if (c->dyn_cap < dyn.size()) {
-        if (c->d_dyn_all) cudaFree(c->d_dyn_all);
-        c->d_dyn_all = nullptr;
-        CK(cudaMalloc(&c->d_dyn_all, dyn.size() * sizeof(uint64_t)));
-        c->dyn_cap = dyn.size();
-    }
-    CK(cudaMemcpyAsync(c->d_dyn_all, dyn.data(), dyn.size() * sizeof(uint64_t), cudaMemcpyHostToDevice,
-                       c->stream));
-    CK(cudaMemsetAsync(c->d_dyn_ctr, 0, sizeof(uint32_t), c->stream));
+// Replays a captured wave for the wave starting at sample `base` of frame `frame`: the begin
+// node's arguments are set on the instantiated graph (later replays are unaffected by earlier
+// ones: the arguments are captured at launch), then the graph is launched on the stream.
+static int replay_wave(wl_context *c, wl_context::GraphEntry *g, uint64_t base, uint64_t frame) {
+    cudaKernelNodeParams kp{};
+    CK(cudaGraphKernelNodeGetParams(g->begin, &kp));
+    uint64_t *cur = c->d_dyn_cur;
+    void *args[3] = {&base, &frame, &cur};
+    kp.kernelParams = args;
+    kp.extra = nullptr;
+    CK(cudaGraphExecKernelNodeSetParams(g->exec, g->begin, &kp));
+    CK(cudaGraphLaunch(g->exec, c->stream));
     return WL_OK;
 }
 
@@ -1066,15 +1081,7 @@ int wl_render(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_
     uint32_t launches = 0, waves = 0;
     const bool strict_math = p->math == WL_MATH_STRICT;
     const bool graph = (p->flags & WL_RENDER_GRAPH) != 0 && !tstats;
-    if (graph) {
-        std::vector<uint64_t> dyn;
-        for (uint64_t base = 0; base < total; base += wave) {
-            dyn.push_back(base);
-            dyn.push_back(p->first_frame);
-        }
-        int rc2 = upload_dyn(c, dyn);
-        if (rc2 != WL_OK) return rc2;
-    }
+    if (graph && !c->d_dyn_cur) CK(cudaMalloc(&c->d_dyn_cur, 2 * sizeof(uint64_t)));
     for (uint64_t base = 0; base < total; base += wave) {
         wp.base = base;
         wp.count = (uint32_t)((total - base) < wave ? (total - base) : wave);
@@ -1082,32 +1089,38 @@ int wl_render(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_
             launches += bdpt ? bdpt_wave(c, wp, sc, f->f, strict_math, tstats)
                              : pt_wave(c, wp, sc, f->f, p->max_depth, strict_math, tstats);
         } else {
+            // every wave of this shape (and every later call with the same arguments) replays
+            // one captured graph; the wave's first sample and frame are the begin node's
+            // arguments, and the film's sample count (host only) is not part of the key
             WaveParams gp = wp;
             gp.base = 0;
             gp.first_frame = 0;
             gp.dyn = c->d_dyn_cur;
+            Film fk = f->f;
+            fk.frames64 = 0;
             std::vector<uint8_t> key;
+            key_add(key, (uint32_t)1);  // a single-scene wave
             key_add(key, gp);
             key_add(key, sc);
-            key_add(key, f->f);
+            key_add(key, fk);
             key_add(key, c->q);
             key_add(key, c->bd);
             key_add(key, p->max_depth);
             key_add(key, (uint32_t)(bdpt * 2 + strict_math));
             key_add(key, c->tune_extend);
             key_add(key, c->tune_shadow);
-            uint32_t nl = 0;
-            cudaGraphExec_t exec = nullptr;
-            cudaEvent_t fk, jn;  // the wave's fork / join events exist before the capture
-            fork_join(c, p->max_depth ? p->max_depth - 1 : 0, fk, jn);
-            int rc2 = wave_graph(c, key, [&] {
-                strict::launch_wave_begin(c->d_dyn_all, c->d_dyn_ctr, c->d_dyn_cur, st);
-                nl = bdpt ? bdpt_wave(c, gp, sc, f->f, strict_math, false)
-                          : pt_wave(c, gp, sc, f->f, p->max_depth, strict_math, false);
-            }, &exec);
+            cudaEvent_t fe, je;  // the wave's fork / join events exist before the capture
+            fork_join(c, p->max_depth ? p->max_depth - 1 : 0, fe, je);
+            wl_context::GraphEntry *g = nullptr;
+            int rc2 = cached_graph(c, key, true, [&]() -> uint32_t {
+                strict::launch_wave_begin(0, 0, c->d_dyn_cur, st);
+                return 1 + (bdpt ? bdpt_wave(c, gp, sc, f->f, strict_math, false)
+                                 : pt_wave(c, gp, sc, f->f, p->max_depth, strict_math, false));
+            }, &g);
             if (rc2 != WL_OK) return rc2;
-            CK(cudaGraphLaunch(exec, st));
-            launches += nl ? nl + 1 : 0;
+            rc2 = replay_wave(c, g, base, p->first_frame);
+            if (rc2 != WL_OK) return rc2;
+            launches += g->launches;
         }
         waves++;
         CK(cudaGetLastError());
@@ -1135,6 +1148,7 @@ int wl_render_batch(wl_context *c, uint32_t n, wl_scene *const *scenes, const wl
     uint64_t total = 0;
     uint32_t maxd = 0;
     bool sort_batch = false;  // any job with WL_RENDER_SORT_MATERIALS sorts every shade pass
+    bool graph = false;       // any job with WL_RENDER_GRAPH replays the batch as one graph
     const uint32_t math = params[0].math;
     for (uint32_t j = 0; j < n; j++) {
         wl_scene *s = scenes[j];
@@ -1170,6 +1184,7 @@ int wl_render_batch(wl_context *c, uint32_t n, wl_scene *const *scenes, const wl
         wp.has_env = (p->env[0] != 0.f || p->env[1] != 0.f || p->env[2] != 0.f) ? 1u : 0u;
         wp.sort_materials = (p->flags & WL_RENDER_SORT_MATERIALS) ? 1u : 0u;
         if (wp.sort_materials) sort_batch = true;
+        if (p->flags & WL_RENDER_GRAPH) graph = true;
         J.sc = dev_scene(s);
         J.film = f->f;
         J.off = total;
@@ -1200,48 +1215,81 @@ int wl_render_batch(wl_context *c, uint32_t n, wl_scene *const *scenes, const wl
     CK(cudaEventRecord(c->ev_total[0], st));
     const bool strict_math = math == WL_MATH_STRICT;
     const DevScene sc0 = jobs[0].sc;
-    uint32_t launches = 0, waves = 0;
-    for (uint64_t base = 0; base < total; base += wave) {
-        const uint32_t count = (uint32_t)((total - base) < wave ? (total - base) : wave);
-        BatchView bv{c->d_jobs, n, base, c->d_slot_job};
-        rec(c, 3, true);
-        if (strict_math) strict::launch_generate_batch(bv, c->q, count, st);
-        else fast::launch_generate_batch(bv, c->q, count, st);
-        rec(c, 3, false);
-        // the shadow pass of bounce b overlaps the extension rays of bounce b + 1 (as pt_wave)
-        cudaEvent_t join_prev = nullptr;
-        int in = 0;
-        for (uint32_t b = 0; b < maxd; b++) {
-            rec(c, 0, true);
-            launch_extend(sc0, c->q, in, false, st, c->tune_extend, bv);
-            rec(c, 0, false);
+    uint32_t waves = 0;
+    for (uint64_t base = 0; base < total; base += wave) waves++;
+    // All waves of the batch. The kernels read the jobs from the device table uploaded above,
+    // so a captured batch replays for any jobs of the same sample counts and depth.
+    auto issue = [&]() -> uint32_t {
+        uint32_t launches = 0;
+        for (uint64_t base = 0; base < total; base += wave) {
+            const uint32_t count = (uint32_t)((total - base) < wave ? (total - base) : wave);
+            BatchView bv{c->d_jobs, n, base, c->d_slot_job};
+            rec(c, 3, true);
+            if (strict_math) strict::launch_generate_batch(bv, c->q, count, st);
+            else fast::launch_generate_batch(bv, c->q, count, st);
+            rec(c, 3, false);
+            // the shadow pass of bounce b overlaps the extension rays of bounce b + 1, and one
+            // reset launch per bounce zeroes the counters (as pt_wave)
+            cudaEvent_t join_prev = nullptr;
+            launch_reset_counters(c->q.counters, (1u << 6) | (1u << 7), st);
+            int in = 0;
+            for (uint32_t b = 0; b < maxd; b++) {
+                rec(c, 0, true);
+                launch_extend(sc0, c->q, in, false, st, c->tune_extend, bv, false);
+                rec(c, 0, false);
+                if (join_prev) cudaStreamWaitEvent(st, join_prev, 0);
+                launch_reset_counters(c->q.counters, (1u << (in ^ 1)) | (1u << 2) | (1u << 6) | (1u << 7), st);
+                rec(c, 1, true);
+                if (strict_math) strict::launch_shade_batch(bv, c->q, in, sort_batch, st);
+                else fast::launch_shade_batch(bv, c->q, in, sort_batch, st);
+                rec(c, 1, false);
+                cudaEvent_t fk, jn;
+                fork_join(c, b, fk, jn);
+                cudaEventRecord(fk, st);
+                cudaStreamWaitEvent(c->side, fk, 0);
+                rec(c, 2, true, c->side);
+                launch_shadow(sc0, c->q, false, c->side, c->tune_shadow, bv, false);
+                rec(c, 2, false, c->side);
+                cudaEventRecord(jn, c->side);
+                join_prev = jn;
+                in ^= 1;
+                launches += 4;
+            }
             if (join_prev) cudaStreamWaitEvent(st, join_prev, 0);
-            cudaMemsetAsync(c->q.counters + (in ^ 1), 0, sizeof(uint32_t), st);
-            cudaMemsetAsync(c->q.counters + 2, 0, sizeof(uint32_t), st);
-            rec(c, 1, true);
-            if (strict_math) strict::launch_shade_batch(bv, c->q, in, sort_batch, st);
-            else fast::launch_shade_batch(bv, c->q, in, sort_batch, st);
-            rec(c, 1, false);
-            cudaEvent_t fk, jn;
-            fork_join(c, b, fk, jn);
-            cudaEventRecord(fk, st);
-            cudaStreamWaitEvent(c->side, fk, 0);
-            rec(c, 2, true, c->side);
-            launch_shadow(sc0, c->q, false, c->side, c->tune_shadow, bv);
-            rec(c, 2, false, c->side);
-            cudaEventRecord(jn, c->side);
-            join_prev = jn;
-            in ^= 1;
+            rec(c, 3, true);
+            strict::launch_film_batch(bv, c->q, count, st);
+            rec(c, 3, false);
             launches += 3;
         }
-        if (join_prev) cudaStreamWaitEvent(st, join_prev, 0);
-        rec(c, 3, true);
-        strict::launch_film_batch(bv, c->q, count, st);
-        rec(c, 3, false);
-        launches += 2;
-        waves++;
-        CK(cudaGetLastError());
+        return launches;
+    };
+    uint32_t launches = 0;
+    if (graph) {
+        // one graph for the whole batch (WL_RENDER_GRAPH in any job's flags)
+        std::vector<uint8_t> key;
+        key_add(key, (uint32_t)2);  // a batch
+        key_add(key, total);
+        key_add(key, wave);
+        key_add(key, n);
+        key_add(key, maxd);
+        key_add(key, (uint32_t)(sort_batch * 2 + strict_math));
+        key_add(key, sc0);
+        key_add(key, c->q);
+        key_add(key, c->d_jobs);
+        key_add(key, c->d_slot_job);
+        key_add(key, c->tune_extend);
+        key_add(key, c->tune_shadow);
+        cudaEvent_t fe, je;  // the batch's fork / join events exist before the capture
+        fork_join(c, maxd ? maxd - 1 : 0, fe, je);
+        wl_context::GraphEntry *g = nullptr;
+        rc = cached_graph(c, key, false, issue, &g);
+        if (rc != WL_OK) return rc;
+        CK(cudaGraphLaunch(g->exec, st));
+        launches = g->launches;
+    } else {
+        launches = issue();
     }
+    CK(cudaGetLastError());
     CK(cudaEventRecord(c->ev_total[1], st));
     for (uint32_t j = 0; j < n; j++) films[j]->f.frames64 += params[j].spp;
     c->stats = wl_render_stats{};

@@ -260,14 +260,14 @@ __global__ void k_debug_rng(uint32_t mode, uint64_t seed, const uint32_t *pixels
     for (uint32_t k = 0; k < count; k++) out[(size_t)i * count + k] = r.next();
 }
 
-__global__ void k_wave_begin(const uint64_t *all, uint32_t *ctr, uint64_t *cur) {
-    uint32_t w = *ctr;
-    cur[0] = all[2 * (size_t)w];
-    cur[1] = all[2 * (size_t)w + 1];
-    *ctr = w + 1;
+// First node of a captured wave: the wave's first sample index and first frame, which the
+// host sets as this node's arguments before every replay (cudaGraphExecKernelNodeSetParams).
+__global__ void k_wave_begin(uint64_t base, uint64_t frame, uint64_t *cur) {
+    cur[0] = base;
+    cur[1] = frame;
 }
-void launch_wave_begin(const uint64_t *all, uint32_t *ctr, uint64_t *cur, cudaStream_t s) {
-    k_wave_begin<<<1, 1, 0, s>>>(all, ctr, cur);
+void launch_wave_begin(uint64_t base, uint64_t frame, uint64_t *cur, cudaStream_t s) {
+    k_wave_begin<<<1, 1, 0, s>>>(base, frame, cur);
 }
 
 void launch_film(const WaveParams &wp, const Queues &q, const Film &f, cudaStream_t s) {

@@ -243,8 +243,9 @@ void launch_film_batch(const BatchView &bv, const Queues &q, uint32_t count, cud
 void launch_emit_cdf(const float *V, const uint4 *tri, const uint32_t *emit_tri,
                      const uint32_t *emit_light, uint32_t n, DevLight *lights, uint32_t nLight,
                      double *cdf, double *chunk, cudaStream_t s);
-// graph replays: cur = all[2 w], all[2 w + 1] for the w-th replay (counter ctr)
-void launch_wave_begin(const uint64_t *all, uint32_t *ctr, uint64_t *cur, cudaStream_t s);
+// graph replays: the first node of a captured wave writes (base, frame) to cur, the WaveParams
+// dyn pointer the wave's kernels read
+void launch_wave_begin(uint64_t base, uint64_t frame, uint64_t *cur, cudaStream_t s);
 void launch_bdpt_connections(const WaveParams &wp, const BdptWave &bw, cudaStream_t s);
 void launch_bdpt_film(const WaveParams &wp, const DevScene &sc, const Queues &q, const BdptWave &bw,
                       const Film &f, cudaStream_t s);
