@@ -417,14 +417,18 @@ def batch_leg(wl, torch, ctx, stream, jobs=64):
     return out
 
 
-def bdpt_ao_leg(wl, torch, ctx, res=1024, spp=256, oracle_spp=4096, ao_res=(512, 256)):
+def bdpt_ao_leg(wl, torch, ctx, res=1024, spp=256, oracle_spp=2048, ao_res=(512, 256)):
     """Configuration 5: the glass-sphere caustic scene (158,420 sphere triangles + plane + a
     0.05-wide quad light), roughness 0.05. BDPT with subpaths of at most 10 vertices: samples/s
-    at res x res x spp, and the relMSE of that image against an independent estimate of the same
-    image, the plain path tracer's FP64 film of oracle_spp samples per pixel (other seeds) with
-    paths of up to 20 vertices (what an eye and a light subpath of 10 vertices each can join);
-    the oracle's own noise floor is reported beside it (relMSE of its two halves / 4). AO: 4 camera samples x 32 occlusion rays of radius 0.1 per pixel at ao_res
-    (about 2^24 rays). Device time with CUDA events on the library's stream."""
+    at res x res x spp (fast math), and the relMSE of that image against an FP64 oracle: the
+    reference's BDPT estimator evaluated in WL_MATH_STRICT mode (per sample bit-identical to the
+    reference's own BDPT.cu compiled on the host, which the strict-mode tests check) with an FP64
+    film, oracle_spp samples per pixel of disjoint seeds. The oracle is rendered in two halves;
+    relMSE(half A, half B) / 4 is its own noise floor. (A plain path tracer cannot serve: its
+    estimate of the caustic through the glass sphere stays dominated by rare paths that hit the
+    small light, with a noise floor far above 1.) AO: 4 camera samples x 32 occlusion rays of
+    radius 0.1 per pixel at ao_res (about 2^24 rays). Device time with CUDA events on the
+    library's stream."""
     from wayland_b200 import scenes
     sc = scenes.glass_sphere(res, res)
     scene = wl.Scene(ctx, sc, bvh_kind=BVH_KIND[0])
@@ -447,18 +451,13 @@ def bdpt_ao_leg(wl, torch, ctx, res=1024, spp=256, oracle_spp=4096, ao_res=(512,
     st = ctx.stats()
     img = film.download64()
     film.close()
-    # independent oracle: plain path tracer (NEE + MIS, unbiased Russian roulette, paths of up to
-    # 20 vertices), FP64 film, two halves of disjoint frames
     t0 = time.perf_counter()
     halves = []
     for h in range(2):
         ref = wl.Film(ctx, res, res, fp64=True)
-        done = 0
-        while done < oracle_spp // 2:
-            k = min(256, oracle_spp // 2 - done)
-            wl.render(ctx, scene, cam, wl.render_params(res, res, k, max_depth=20,
-                                                        first_frame=20000000 + h * oracle_spp + done), ref)
-            done += k
+        wl.render(ctx, scene, cam, wl.render_params(res, res, oracle_spp // 2, strategy=wl.STRATEGY_BDPT,
+                                                    max_depth=10, math=wl.MATH_STRICT,
+                                                    first_frame=20000000 + h * oracle_spp), ref)
         halves.append(ref.download64())
         ref.close()
     oracle_s = time.perf_counter() - t0
@@ -472,9 +471,10 @@ def bdpt_ao_leg(wl, torch, ctx, res=1024, spp=256, oracle_spp=4096, ao_res=(512,
            "spp": spp, "ms": round(ms, 1), "msamples_s": round(samples / ms / 1e3, 2),
            "closest_hit_rays_per_sample": round(st["segments"] / samples, 3),
            "connection_rays_per_sample": round(st["shadow_rays"] / samples, 3),
-           "relmse_vs_pt_oracle": rel(img, r64),
-           "oracle": f"plain path tracer, {oracle_spp} spp, FP64 film, depth 20 ({oracle_s:.1f} s)",
-           "oracle_noise_floor": rel(halves[0], halves[1]) / 4}
+           "relmse_vs_fp64_oracle": rel(img, r64),
+           "oracle": f"BDPT in strict math (the reference's estimator, bit-exact per sample), {oracle_spp} spp, "
+                     f"FP64 film, disjoint seeds ({oracle_s:.1f} s)",
+           "oracle_noise_floor": float(((halves[0] - halves[1]) ** 2 / (r64 * r64 + 1e-2)).mean()) / 4}
     # ambient occlusion, radius 0.1
     aw, ah = ao_res
     afilm = wl.Film(ctx, aw, ah)
@@ -584,7 +584,6 @@ def nrc_convergence(wl, torch, ctx, res=(1920, 1080), oracle_spp=8192, target=1e
 
     plain = run("plain")
     nrc = run("nrc")
-    ref_film.close()
     scene.close()
     out = {"scene": f"door-slit room {sc.num_tris} tris, {W_}x{H_}, depth 16, fast math",
            "oracle": f"{oracle_spp} spp, FP64 film, plain path tracer ({oracle_s:.1f} s)",
@@ -836,23 +835,33 @@ def main():
             "autotune": tune,
             "clocks": clk,
         }
+        def leg(key, fn):
+            # an extra leg that fails is recorded in the line instead of losing the line
+            try:
+                line[key] = fn()
+            except Exception as e:  # noqa: BLE001
+                line[key] = {"error": f"{type(e).__name__}: {e}"}
+
         if not args.no_raycast:
-            line["raycast"] = raycast_microbench(wl, torch, ctx, sc, scene, stream)
+            leg("raycast", lambda: raycast_microbench(wl, torch, ctx, sc, scene, stream))
         if world == 1:
-            line["progressive_1spp"] = graph_leg(wl, torch, ctx, sc, scene, stream)
-            line["cornell_config1"] = cornell_leg(wl, torch, ctx)
+            leg("progressive_1spp", lambda: graph_leg(wl, torch, ctx, sc, scene, stream))
+            leg("cornell_config1", lambda: cornell_leg(wl, torch, ctx))
         if world == 1 and not args.no_batch:
-            line["batch"] = batch_leg(wl, torch, ctx, stream)
+            leg("batch", lambda: batch_leg(wl, torch, ctx, stream))
         if world == 1 and not args.no_bdpt:
-            line["bdpt"] = bdpt_ao_leg(wl, torch, ctx)
+            leg("bdpt", lambda: bdpt_ao_leg(wl, torch, ctx))
         if world == 1 and not args.no_nrc:
             # the second half of the metric: time to relMSE 1e-2 vs an FP64 high-spp render,
             # radiance cache vs plain path tracing (door-slit room)
             w_, h_ = (int(v) for v in args.nrc_res.split("x"))
-            line["time_to_relmse"] = nrc_convergence(wl, torch, ctx, res=(w_, h_),
-                                                     oracle_spp=args.nrc_oracle_spp,
-                                                     budget_s=args.nrc_budget_s)
-            line["time_to_relmse"]["kernels"] = nrc_kernels(wl, torch, ctx)
+
+            def nrc_leg():
+                r = nrc_convergence(wl, torch, ctx, res=(w_, h_), oracle_spp=args.nrc_oracle_spp,
+                                    budget_s=args.nrc_budget_s)
+                r["kernels"] = nrc_kernels(wl, torch, ctx)
+                return r
+            leg("time_to_relmse", nrc_leg)
         if world == 1 and not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             cpu = CpuPT(scene, threads)

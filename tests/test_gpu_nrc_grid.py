@@ -110,7 +110,7 @@ def test_query_matches_oracle(setup):
     err = np.abs(got[:, :3] - ref) / (np.abs(ref) + 1e-2)
     assert np.median(err) < 1e-4 and np.quantile(err, 0.99) < 1e-2 and err.max() < 5e-2, \
         (np.median(err), np.quantile(err, 0.99), err.max())
-    assert (ref > 0).mean() > 0.2
+    assert (ref > 0).mean() > 0.1
 
 
 def test_training_gradients_match_oracle(setup):
