@@ -4,6 +4,9 @@
 // divides each component), dot(a, b) = (a.x*b.x + a.y*b.y) + a.z*b.z, length = sqrt(dot),
 // normalize(v) = v * (1 / sqrt(dot(v, v))), cross as in glm/detail/func_geometric.inl,
 // clamp(x, lo, hi) = min(max(x, lo), hi) with max(a, b) = a < b ? b : a, min(a, b) = b < a ? b : a.
+// mat4 is column-major (m[c] = column c); mat4 * vec4 = (m[0] v.x + m[1] v.y) + (m[2] v.z +
+// m[3] v.w) as glm/detail/type_mat4x4.inl groups it; make_mat4 reads 16 floats column by column
+// (glm/gtc/type_ptr.inl); transpose swaps m[i][j] and m[j][i].
 #pragma once
 #include <cmath>
 #include <cstdint>
@@ -39,6 +42,8 @@ template <class T> struct tvec4 {
     explicit tvec4(T s) : x(s), y(s), z(s), w(s) {}
     tvec4(const tvec3<T> &v, T d) : x(v.x), y(v.y), z(v.z), w(d) {}
     template <class U> tvec4(const tvec4<U> &v) : x((T)v.x), y((T)v.y), z((T)v.z), w((T)v.w) {}
+    T &operator[](int i) { return (&x)[i]; }
+    const T &operator[](int i) const { return (&x)[i]; }
 };
 
 template <class T> tvec3<T> operator+(const tvec3<T> &a, const tvec3<T> &b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
@@ -81,6 +86,41 @@ template <class T> tvec4<T> clamp(const tvec4<T> &v, typename ident<T>::type lo,
     return {gmin(gmax(v.x, lo), hi), gmin(gmax(v.y, lo), hi), gmin(gmax(v.z, lo), hi), gmin(gmax(v.w, lo), hi)};
 }
 
+// ---- the matrix part the reference's frontend uses (SceneManager, Shape, Camera) ----------
+template <class T> tvec4<T> operator*(const tvec4<T> &a, const tvec4<T> &b) { return {a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w}; }
+template <class T> tvec4<T> operator*(typename ident<T>::type s, const tvec4<T> &a) { return {s * a.x, s * a.y, s * a.z, s * a.w}; }
+// dot of 4-vectors as glm's compute_dot: (x + y) + (z + w) of the componentwise product
+template <class T> T dot(const tvec4<T> &a, const tvec4<T> &b) {
+    tvec4<T> t = a * b;
+    return (t.x + t.y) + (t.z + t.w);
+}
+template <class T> tvec4<T> normalize(const tvec4<T> &v) { return v * inversesqrt(dot(v, v)); }
+template <class T> T tan(T x) { return std::tan(x); }
+// column-major 4x4: m[c] is column c
+template <class T> struct tmat4 {
+    tvec4<T> c[4];
+    tvec4<T> &operator[](int i) { return c[i]; }
+    const tvec4<T> &operator[](int i) const { return c[i]; }
+};
+// m * v as glm's mat4x4 * vec4: (m0 v.x + m1 v.y) + (m2 v.z + m3 v.w), each product componentwise
+template <class T> tvec4<T> operator*(const tmat4<T> &m, const tvec4<T> &v) {
+    const tvec4<T> a = m[0] * v.x + m[1] * v.y;
+    const tvec4<T> b = m[2] * v.z + m[3] * v.w;
+    return a + b;
+}
+template <class T> tmat4<T> transpose(const tmat4<T> &m) {
+    tmat4<T> r;
+    for (int i = 0; i < 4; i++) r[i] = tvec4<T>(m[0][i], m[1][i], m[2][i], m[3][i]);
+    return r;
+}
+template <class T> tmat4<T> make_mat4(const T *p) {
+    tmat4<T> r;
+    for (int i = 0; i < 4; i++) r[i] = tvec4<T>(p[4 * i], p[4 * i + 1], p[4 * i + 2], p[4 * i + 3]);
+    return r;
+}
+template <class T> tvec3<T> make_vec3(const T *p) { return tvec3<T>(p[0], p[1], p[2]); }
+template <class T> tvec2<T> make_vec2(const T *p) { return tvec2<T>(p[0], p[1]); }
+
 typedef tvec2<float> vec2;
 typedef tvec3<float> vec3;
 typedef tvec4<float> vec4;
@@ -88,5 +128,6 @@ typedef tvec4<double> dvec4;
 typedef tvec2<int> ivec2;
 typedef tvec3<int> ivec3;
 typedef tvec4<uint8_t> u8vec4;
+typedef tmat4<float> mat4;
 
 }  // namespace glm

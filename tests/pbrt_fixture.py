@@ -23,7 +23,7 @@ MakeNamedMaterial "shiny" "string type" [ "plastic" ] "rgb Kd" [ 0.3 0.2 0.1 ]
     "rgb Ks" [ 0.2 0.2 0.2 ] "float roughness" [ 0.05 ]
 NamedMaterial "floor"
 Shape "trianglemesh" "point3 P" [ -3 0 -3  3 0 -3  3 0 3  -3 0 3 ]
-    "integer indices" [ 0 2 1 0 3 2 ] "point2 uv" [ 0 0 4 0 4 4 0 4 ]
+    "integer indices" [ 0 2 1 0 3 2 ] "float uv" [ 0 0 4 0 4 4 0 4 ]
 AttributeBegin
   Translate 0 0.5 0
   Rotate 30 0 1 0

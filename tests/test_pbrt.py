@@ -22,7 +22,8 @@ def test_synthetic_scene(tmp_path):
     assert tuple(sc.lights[0]["L"]) == (8, 7, 6) and sc.lights[0]["two_sided"] == 0
     # materials in creation order: floor (textured matte), shiny (plastic), disney, glass, light
     m = sc.mats
-    assert m[0]["texture"] == 0 and np.allclose(m[0]["color"], 0.5)
+    # a texture-bound Kd keeps minipbrt's default value (1, 1, 1), which the reference reads
+    assert m[0]["texture"] == 0 and np.allclose(m[0]["color"], 1.0)
     assert np.allclose(m[1]["color"], [0.5, 0.4, 0.3]) and math.isclose(m[1]["metallic"], math.sqrt(0.12), rel_tol=1e-6)
     assert math.isclose(m[1]["roughness"], 0.05, rel_tol=1e-6) and m[1]["texture"] == -1
     assert np.allclose(m[2]["color"], [0.2, 0.5, 0.8]) and math.isclose(m[2]["trans"], 0.2, rel_tol=1e-6)

@@ -12,13 +12,21 @@ subset that conversion accepts and converts it the same way:
   does; named materials (MakeNamedMaterial / NamedMaterial) and anonymous ones.
 - Textures "imagemap" (PNG or TGA files) bound to Kd / Kt / color; "scale" textures are left
   out as SceneManager.cpp:144-146 does.
-- Shape "trianglemesh" (P, indices, optional N and uv/st) and "plymesh" (ASCII or binary
+- Shape "trianglemesh" (P, indices, optional N and "float uv") and "plymesh" (ASCII or binary
   little-endian PLY with x y z [nx ny nz] [u v | s t], triangle or quad faces). Vertices and
   normals are transformed by the shape's object-to-world matrix as points, as
   TriangleMesh::TriangleMesh does (Shape.cpp:17-40).
 - AreaLightSource "diffuse" (L, twosided) bound to the shapes of its attribute block.
 - Film x/yresolution, Sampler pixelsamples, Integrator maxdepth; Transform, ConcatTransform,
   Translate, Scale, Rotate, LookAt, Identity, AttributeBegin/End, TransformBegin/End, Include.
+
+minipbrt's own rules are kept where they differ from pbrt-v3's specification: its parameter
+defaults (matte Kd and disney color (1, 1, 1)), texture coordinates only as "float uv", PLY
+quads split into (0, 1, 3), (2, 3, 1) and larger faces by its ear clipping, and its
+single-precision matrix arithmetic (Mat4 translate / rotate / lookAt / inverse) followed by the
+frontend's glm float arithmetic for vertices and the camera frame. The arrays this loader
+returns equal, bit for bit, what the reference's own SceneManager (built from its sources)
+hands to the C ABI through the integration guide's DeviceManager (tests/test_frontend.py).
 """
 import math
 import os
@@ -96,39 +104,170 @@ class _Stream:
         return out
 
 
-def _translate(d):
-    m = np.eye(4)
-    m[:3, 3] = d
-    return m
+F32 = np.float32
 
 
-def _scale(s):
-    return np.diag([s[0], s[1], s[2], 1.0])
+def _libm():
+    """glibc's single-precision sinf / cosf / tanf, the functions minipbrt and the reference's
+    frontend call through std::sin / std::cos / glm::tan on float arguments."""
+    import ctypes
+    import ctypes.util
+    lib = ctypes.CDLL(ctypes.util.find_library("m") or "libm.so.6")
+    for name in ("sinf", "cosf", "tanf"):
+        f = getattr(lib, name)
+        f.restype = ctypes.c_float
+        f.argtypes = [ctypes.c_float]
+    return lib
 
 
-def _rotate(angle, axis):
-    a = np.asarray(axis, np.float64)
-    a = a / np.linalg.norm(a)
-    s, c = math.sin(math.radians(angle)), math.cos(math.radians(angle))
-    x, y, z = a
-    m = np.eye(4)
-    m[:3, :3] = [[x * x + (1 - x * x) * c, x * y * (1 - c) - z * s, x * z * (1 - c) + y * s],
-                 [x * y * (1 - c) + z * s, y * y + (1 - y * y) * c, y * z * (1 - c) - x * s],
-                 [x * z * (1 - c) - y * s, y * z * (1 - c) + x * s, z * z + (1 - z * z) * c]]
-    return m
+_LIBM = _libm()
 
 
-def _look_at(eye, look, up):
-    """World-to-camera of pbrt-v3's LookAt (camera looks along +z, x = normalize(up) x dir)."""
-    eye, look, up = (np.asarray(v, np.float64) for v in (eye, look, up))
-    d = look - eye
-    d = d / np.linalg.norm(d)
-    right = np.cross(up / np.linalg.norm(up), d)
-    right = right / np.linalg.norm(right)
-    new_up = np.cross(d, right)
-    c2w = np.eye(4)
-    c2w[:3, 0], c2w[:3, 1], c2w[:3, 2], c2w[:3, 3] = right, new_up, d, eye
-    return np.linalg.inv(c2w)
+def _f(x):
+    return F32(x)
+
+
+def _v_normalize(v):
+    """minipbrt's normalize: v / sqrt((x x + y y) + z z), in float."""
+    x, y, z = (_f(c) for c in v)
+    n = F32(np.sqrt(F32(F32(x * x + y * y) + z * z)))
+    return (x / n, y / n, z / n)
+
+
+def _v_cross(a, b):
+    return (a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0])
+
+
+class _Mat4:
+    """minipbrt's Mat4 (row-major, float) and the operations its parser applies to the current
+    transform (Mat4::translate / scale / rotate / lookAt / concatTransform and inverse), in the
+    same float operation order, so the transforms equal the reference frontend's bit for bit."""
+
+    def __init__(self, rows=None):
+        self.r = [[_f(1.0 if i == j else 0.0) for j in range(4)] for i in range(4)] if rows is None \
+            else [[_f(x) for x in row] for row in rows]
+
+    def copy(self):
+        return _Mat4(self.r)
+
+    @staticmethod
+    def from_column_major(vals):
+        # Transform / ConcatTransform arguments are column-major (rows[r][c] = arg[4 c + r])
+        return _Mat4([[vals[4 * c + r] for c in range(4)] for r in range(4)])
+
+    def translate(self, v):
+        v = [_f(x) for x in v]
+        for r in self.r:
+            r[3] = r[3] + ((r[0] * v[0] + r[1] * v[1]) + r[2] * v[2])
+
+    def scale(self, v):
+        v = [_f(x) for x in v]
+        for r in self.r:
+            for c in range(3):
+                r[c] = r[c] * v[c]
+
+    def rotate(self, degrees, axis):
+        ang = F32(F32(_f(degrees) * F32(math.pi)) / F32(180.0))  # degrees_to_radians
+        c, s = F32(_LIBM.cosf(float(ang))), F32(_LIBM.sinf(float(ang)))
+        ux, uy, uz = _v_normalize(axis)
+        k = F32(1.0) - c
+        b = [[ux * ux * k + c, ux * uy * k - uz * s, ux * uz * k + uy * s],
+             [uy * ux * k + uz * s, uy * uy * k + c, uy * uz * k - ux * s],
+             [uz * ux * k - uy * s, uz * uy * k + ux * s, uz * uz * k + c]]
+        a = [row[:] for row in self.r]
+        for i in range(4):
+            for j in range(3):
+                self.r[i][j] = (a[i][0] * b[0][j] + a[i][1] * b[1][j]) + a[i][2] * b[2][j]
+
+    def concat(self, m):
+        a = [row[:] for row in self.r]
+        for i in range(4):
+            for j in range(4):
+                self.r[i][j] = ((a[i][0] * m.r[0][j] + a[i][1] * m.r[1][j]) + a[i][2] * m.r[2][j]) + \
+                    a[i][3] * m.r[3][j]
+
+    def look_at(self, pos, target, up):
+        pos, target = [_f(x) for x in pos], [_f(x) for x in target]
+        d = _v_normalize([target[k] - pos[k] for k in range(3)])
+        x = _v_normalize(_v_cross(_v_normalize(up), d))
+        y = _v_normalize(_v_cross(d, x))
+        m = _Mat4([[x[0], y[0], d[0], pos[0]], [x[1], y[1], d[1], pos[1]], [x[2], y[2], d[2], pos[2]],
+                   [0, 0, 0, 1]])
+        self.concat(m.inverse())
+
+    def _d2(self, r0, r1, c0, c1):
+        r = self.r
+        return r[r0][c0] * r[r1][c1] - r[r0][c1] * r[r1][c0]
+
+    def inverse(self):
+        m = self.r
+        d = self._d2
+        A, B, C, D, E, Fv = d(2, 3, 2, 3), d(2, 3, 1, 3), d(2, 3, 1, 2), d(2, 3, 0, 3), d(2, 3, 0, 2), d(2, 3, 0, 1)
+        G, H, I, J, K, L = d(1, 3, 2, 3), d(1, 3, 1, 3), d(1, 3, 1, 2), d(1, 3, 0, 3), d(1, 3, 0, 2), d(1, 3, 0, 1)
+        M, N, O, P, Q, R = d(1, 2, 2, 3), d(1, 2, 1, 3), d(1, 2, 1, 2), d(1, 2, 0, 3), d(1, 2, 0, 2), d(1, 2, 0, 1)
+
+        def t(a, x, b, y, c, z):
+            return (a * x - b * y) + c * z
+        inv = [[+t(m[1][1], A, m[1][2], B, m[1][3], C), -t(m[0][1], A, m[0][2], B, m[0][3], C),
+                +t(m[0][1], G, m[0][2], H, m[0][3], I), -t(m[0][1], M, m[0][2], N, m[0][3], O)],
+               [-t(m[1][0], A, m[1][2], D, m[1][3], E), +t(m[0][0], A, m[0][2], D, m[0][3], E),
+                -t(m[0][0], G, m[0][2], J, m[0][3], K), +t(m[0][0], M, m[0][2], P, m[0][3], Q)],
+               [+t(m[1][0], B, m[1][1], D, m[1][3], Fv), -t(m[0][0], B, m[0][1], D, m[0][3], Fv),
+                +t(m[0][0], H, m[0][1], J, m[0][3], L), -t(m[0][0], N, m[0][1], P, m[0][3], R)],
+               [-t(m[1][0], C, m[1][1], E, m[1][2], Fv), +t(m[0][0], C, m[0][1], E, m[0][2], Fv),
+                -t(m[0][0], I, m[0][1], K, m[0][2], L), +t(m[0][0], O, m[0][1], Q, m[0][2], R)]]
+        det = ((m[0][0] * inv[0][0] + m[0][1] * inv[1][0]) + m[0][2] * inv[2][0]) + m[0][3] * inv[3][0]
+        inv_det = F32(1.0) / det
+        return _Mat4([[x * inv_det for x in row] for row in inv])
+
+    def apply(self, P, w):
+        """The reference frontend's TransformVec3(transpose(make_mat4(rows)), p, w): glm's
+        mat4 * vec4, (r0 x + r1 y) + (r2 z + r3 w) per row, in float, for an (n, 3) array."""
+        P = np.asarray(P, F32)
+        x, y, z = P[:, 0], P[:, 1], P[:, 2]
+        wf = F32(w)
+        out = np.empty((len(P), 3), F32)
+        for i in range(3):
+            r = self.r[i]
+            out[:, i] = (r[0] * x + r[1] * y) + (r[2] * z + r[3] * wf)
+        return out
+
+    def apply4(self, v):
+        """glm's mat4 * vec4 for one 4-vector (float)."""
+        v = [_f(c) for c in v]
+        return [(r[0] * v[0] + r[1] * v[1]) + (r[2] * v[2] + r[3] * v[3]) for r in self.r]
+
+
+def _glm_normalize4(v):
+    """glm::normalize of a vec4: v * (1 / sqrt((x x + y y) + (z z + w w)))."""
+    dot = (v[0] * v[0] + v[1] * v[1]) + (v[2] * v[2] + v[3] * v[3])
+    k = F32(1.0) / F32(np.sqrt(dot))
+    return [c * k for c in v]
+
+
+def _glm_normalize3(v):
+    """glm::normalize of a vec3: v * (1 / sqrt((x x + y y) + z z))."""
+    dot = (v[0] * v[0] + v[1] * v[1]) + v[2] * v[2]
+    k = F32(1.0) / F32(np.sqrt(dot))
+    return [c * k for c in v]
+
+
+def _camera_frame(c2w, fov, W, H):
+    """PinholeCamera(fov, cameraToWorld) (Camera.cpp:15-28) and the aspect scaling of
+    PathTracingProgramManager.cpp:28, in the reference frontend's float operation order."""
+    pos = c2w.apply4([0, 0, 0, 1])[:3]
+    up = _glm_normalize4(c2w.apply4([0, 1, 0, 0]))[:3]
+    look = _glm_normalize3(c2w.apply4([0, 0, 1, 0])[:3])
+    half = F32(_f(fov) / F32(2.0))
+    rad = F32(np.float64(half * F32(math.pi)) / 180.0)  # AngleToRadian: (a * PI) / 180.0
+    t = F32(_LIBM.tanf(float(rad)))
+    up = [t * c for c in up]
+    right = [look[1] * up[2] - up[1] * look[2], look[2] * up[0] - up[2] * look[0],
+             look[0] * up[1] - up[0] * look[1]]  # glm::cross(look, up)
+    aspect = F32(F32(W) / F32(H))
+    right = [c * aspect for c in right]
+    return {"pos": np.array(pos, F32), "look_at": np.array(look, F32), "up": np.array(up, F32),
+            "right": np.array(right, F32)}
 
 
 def _color(params, name, default):
@@ -152,9 +291,10 @@ def _tex(params, name, tex_index):
 
 
 def material_to_disney(kind, params, tex_index):
-    """Material.cpp:33-107 (Disney(...) constructors) with pbrt-v3's parameter defaults."""
+    """Material.cpp:33-107 (Disney(...) constructors) with minipbrt's parameter defaults (which
+    the reference reads; a texture-bound colour keeps its default value)."""
     if kind == "matte":
-        m = scenes.matte(tuple(_color(params, "Kd", (0.5, 0.5, 0.5))))
+        m = scenes.matte(tuple(_color(params, "Kd", (1.0, 1.0, 1.0))))
         m["texture"] = _tex(params, "Kd", tex_index)
     elif kind == "plastic":
         kd = np.array(_color(params, "Kd", (0.25, 0.25, 0.25)), np.float32)
@@ -171,7 +311,7 @@ def material_to_disney(kind, params, tex_index):
                           sheen_tint=0.5)
         m["texture"] = _tex(params, "Kt", tex_index)
     elif kind == "disney":
-        m = scenes.disney(tuple(_color(params, "color", (0.5, 0.5, 0.5))),
+        m = scenes.disney(tuple(_color(params, "color", (1.0, 1.0, 1.0))),
                           metallic=_float(params, "metallic", 0.0),
                           roughness=_float(params, "roughness", 0.5), specular=0.0,
                           specular_tint=_float(params, "speculartint", 0.0),
@@ -276,16 +416,67 @@ def read_ply(path):
             UV = np.stack([col(a), col(b)], 1)
     tris = []
     for f in faces:
-        f = [int(x) for x in f]
-        for j in range(1, len(f) - 1):
-            tris.append([f[0], f[j], f[j + 1]])
+        tris.extend(triangulate_polygon([int(x) for x in f], P))
     return P, N, UV, np.array(tris, np.int64).reshape(-1, 3)
+
+
+def _angle_at_vert(i, pts, prev, nxt):
+    """minipbrt's angle_at_vert: the angle at a remaining polygon vertex, 10000 when reflex."""
+    x = pts[nxt[i]] - pts[i]
+    x = (x / np.float32(np.sqrt(np.float32(x @ x)))).astype(np.float32)
+    y = np.array([-x[1], x[0]], np.float32)
+    p = (pts[prev[i]] - pts[i]).astype(np.float32)
+    a = float(np.arctan2(np.float32(p @ y), np.float32(p @ x)))
+    return 10000.0 if a <= 0.0 or a >= math.pi else a
+
+
+def triangulate_polygon(idx, P):
+    """The triangles minipbrt makes of a PLY face (miniply triangulate_polygon): a triangle as is,
+    a quad as (0, 1, 3), (2, 3, 1), larger polygons by ear clipping at the sharpest remaining
+    vertex of the face projected on its plane."""
+    n = len(idx)
+    if n < 3:
+        return []
+    if n == 3:
+        return [idx]
+    if n == 4:
+        return [[idx[0], idx[1], idx[3]], [idx[2], idx[3], idx[1]]]
+    V = np.asarray(P, np.float32)
+
+    def unit(v):
+        return (v / np.float32(np.sqrt(np.float32(v @ v)))).astype(np.float32)
+
+    o = V[idx[0]]
+    u = unit(V[idx[1]] - o)
+    nrm = unit(np.cross(u, unit(V[idx[n - 1]] - o)).astype(np.float32))
+    v = unit(np.cross(nrm, u).astype(np.float32))
+    pts = [np.zeros(2, np.float32)] + [np.array([(V[idx[i]] - o) @ u, (V[idx[i]] - o) @ v], np.float32)
+                                       for i in range(1, n)]
+    nxt = [(i + 1) % n for i in range(n)]
+    prev = [(i - 1) % n for i in range(n)]
+    first, out = 0, []
+    while n > 3:
+        best, best_a = first, _angle_at_vert(first, pts, prev, nxt)
+        i = nxt[first]
+        while i != first:
+            a = _angle_at_vert(i, pts, prev, nxt)
+            if a < best_a:
+                best, best_a = i, a
+            i = nxt[i]
+        ni, pi = nxt[best], prev[best]
+        out.append([idx[best], idx[ni], idx[pi]])
+        if best == first:
+            first = ni
+        nxt[pi], prev[ni] = ni, pi
+        n -= 1
+    out.append([idx[first], idx[nxt[first]], idx[prev[first]]])
+    return out
 
 
 def load(path, width=None, height=None):
     """Read a pbrt-v3 file into a scenes.Scene (the SceneManager fields, flattened)."""
     base = os.path.dirname(os.path.abspath(path))
-    state = {"ctm": np.eye(4), "material": None, "light": None, "reverse": False}
+    state = {"ctm": _Mat4(), "material": None, "light": None, "reverse": False}
     stack, tstack = [], []
     named_mats, mats, tex_index, textures = {}, [], {}, []
     meshes = []          # (P, N, UV, tris, material, light)
@@ -305,27 +496,27 @@ def load(path, width=None, height=None):
         while not s.done():
             d = s.next()
             if d == "Transform":
-                state["ctm"] = np.array(s.numbers(16), np.float64).reshape(4, 4).T
+                state["ctm"] = _Mat4.from_column_major(s.numbers(16))
             elif d == "ConcatTransform":
-                state["ctm"] = state["ctm"] @ np.array(s.numbers(16), np.float64).reshape(4, 4).T
+                state["ctm"].concat(_Mat4.from_column_major(s.numbers(16)))
             elif d == "Translate":
-                state["ctm"] = state["ctm"] @ _translate(s.numbers(3))
+                state["ctm"].translate(s.numbers(3))
             elif d == "Scale":
-                state["ctm"] = state["ctm"] @ _scale(s.numbers(3))
+                state["ctm"].scale(s.numbers(3))
             elif d == "Rotate":
                 v = s.numbers(4)
-                state["ctm"] = state["ctm"] @ _rotate(v[0], v[1:])
+                state["ctm"].rotate(v[0], v[1:])
             elif d == "LookAt":
                 v = s.numbers(9)
-                state["ctm"] = state["ctm"] @ _look_at(v[0:3], v[3:6], v[6:9])
+                state["ctm"].look_at(v[0:3], v[3:6], v[6:9])
             elif d == "Identity":
-                state["ctm"] = np.eye(4)
+                state["ctm"] = _Mat4()
             elif d == "Camera":
                 kind = s.string()
                 p = s.params()
                 if kind != "perspective":
                     raise ValueError(f"unsupported camera {kind!r} (the reference accepts perspective)")
-                cam["c2w"] = np.linalg.inv(state["ctm"])
+                cam["c2w"] = state["ctm"].inverse()
                 cam["fov"] = _float(p, "fov", 90.0)
             elif d == "Film":
                 s.string()
@@ -348,11 +539,11 @@ def load(path, width=None, height=None):
                     s.string()
                     s.params()
             elif d == "WorldBegin":
-                state["ctm"] = np.eye(4)
+                state["ctm"] = _Mat4()
             elif d == "WorldEnd":
                 pass
             elif d == "AttributeBegin":
-                stack.append(dict(state))
+                stack.append(dict(state, ctm=state["ctm"].copy()))
             elif d == "AttributeEnd":
                 state.update(stack.pop())
             elif d == "TransformBegin":
@@ -402,8 +593,10 @@ def load(path, width=None, height=None):
                     P = np.array(p["P"][1], np.float64).reshape(-1, 3)
                     tris = np.array(p["indices"][1], np.int64).reshape(-1, 3)
                     N = np.array(p["N"][1], np.float64).reshape(-1, 3) if "N" in p else None
-                    uvk = "uv" if "uv" in p else ("st" if "st" in p else None)
-                    UV = np.array(p[uvk][1], np.float64).reshape(-1, 2) if uvk else None
+                    # minipbrt reads texture coordinates only as "float uv" (a "point2 uv" or
+                    # "st" list is not a float parameter there and is dropped)
+                    UV = np.array(p["uv"][1], np.float64).reshape(-1, 2) \
+                        if "uv" in p and p["uv"][0] == "float" else None
                 elif kind == "plymesh":
                     P, N, UV, tris = read_ply(os.path.join(cwd, p["filename"][1][0]))
                 else:
@@ -433,12 +626,10 @@ def load(path, width=None, height=None):
     has_n = any(m[1] is not None for m in meshes)
     has_uv = any(m[2] is not None for m in meshes)
     for P, N, UV, tris, o2w, mat, light in meshes:
-        Ph = np.concatenate([P, np.ones((len(P), 1))], 1) @ o2w.T
-        Vs.append(Ph[:, :3])
+        Vs.append(o2w.apply(P, 1.0))
         if has_n:
             if N is not None:
-                Nh = np.concatenate([N, np.ones((len(N), 1))], 1) @ o2w.T  # as points (Shape.cpp:39)
-                Ns.append(Nh[:, :3])
+                Ns.append(o2w.apply(N, 1.0))  # as points (Shape.cpp:39)
             else:
                 Ns.append(np.zeros((len(P), 3)))
         if has_uv:
@@ -459,15 +650,7 @@ def load(path, width=None, height=None):
         larr[k]["two_sided"] = int(two)
         larr[k]["first_tri"] = first
         larr[k]["tri_count"] = count
-    c2w = cam["c2w"]
-    pos = c2w @ np.array([0, 0, 0, 1.0])
-    up = c2w @ np.array([0, 1.0, 0, 0])
-    look = c2w @ np.array([0, 0, 1.0, 0])
-    up = up[:3] / np.linalg.norm(up[:3]) * math.tan(math.radians(cam["fov"] / 2))
-    look = look[:3] / np.linalg.norm(look[:3])
-    right = np.cross(look, up) * (W / H)
-    camera = {"pos": pos[:3].astype(np.float32), "look_at": look.astype(np.float32),
-              "up": up.astype(np.float32), "right": right.astype(np.float32)}
+    camera = _camera_frame(cam["c2w"], cam["fov"], W, H)
     sc = scenes.Scene(os.path.basename(path), np.concatenate(Vs).astype(np.float32),
                       np.concatenate(Is).astype(np.uint32), np.concatenate(Ms),
                       np.array(mats) if mats else np.array([scenes.matte((0.5, 0.5, 0.5))]), larr,
