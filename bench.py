@@ -574,7 +574,9 @@ def nrc_convergence(wl, torch, ctx, res=(1920, 1080), oracle_spp=8192, target=1e
         extra = {}
         if cache is not None:
             st = cache.stats()
-            extra = {"train_samples_last_frame": st["train_samples"], "queries_last_frame": st["queries"]}
+            mq, mt = cache.kernel_times()
+            extra = {"train_samples_last_frame": st["train_samples"], "queries_last_frame": st["queries"],
+                     "kernel_ms_last_frame": {"mlp_query": round(mq, 4), "train_step": round(mt, 4)}}
             cache.close()
         film.close()
         reached = curve[-1][2] <= target
@@ -596,54 +598,51 @@ def nrc_convergence(wl, torch, ctx, res=(1920, 1080), oracle_spp=8192, target=1e
     return out
 
 
-def nrc_kernels(wl, torch, ctx, queries=1920 * 1080, samples=1 << 16, repeats=10):
-    """FLOP roofline of the radiance cache's tensor-core kernels at 1080p batch sizes, through the
-    public entry points (device buffers, CUDA events on the library's stream, median of repeats):
-    the MLP forward on `queries` rows (wl_nrc_mlp_forward: the query pass's tcgen05 MLP kernel
-    alone, 34,816 FLOP per row) and one training step on `samples` rows (wl_nrc_train_step:
-    operand tiles, the fused forward/backward tcgen05 kernel, Adam; 104,448 FLOP per row),
-    against the measured sustained BF16 peak."""
+def nrc_kernels(wl, torch, ctx, queries=1920 * 1080, samples=1 << 16, repeats=10, in_situ=None):
+    """FLOP roofline of the radiance cache's tensor-core kernels at 1080p batch sizes: the query
+    MLP on `queries` rows (34,816 FLOP per row) and the fused training step on `samples` rows
+    (104,448 FLOP per row), through wl_nrc_mlp_forward / wl_nrc_train_step on device buffers;
+    each kernel's own device time comes from wl_nrc_kernel_times (CUDA events around the
+    tensor-core launch alone; median of repeats). in_situ: (queries, samples, ms_query, ms_train)
+    of the last frame of a real 1080p cache render, reported beside it. Against the measured
+    sustained BF16 peak."""
     from wayland_b200 import scenes
     sc = scenes.cornell_box(16, 16)
     s = wl.Scene(ctx, sc)
     c = wl.RadianceCache(ctx, s)
-    stream = torch.cuda.ExternalStream(ctx.stream)
     g = torch.Generator(device="cuda")
     g.manual_seed(0)
     x = torch.rand((queries, 64), device="cuda", generator=g) * 2 - 1
     out = torch.empty((queries, 4), device="cuda")
     t = torch.rand((samples, 4), device="cuda", generator=g)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-
-    def med(fn):
-        ts = []
-        for r in range(repeats + 2):
-            ctx.sync()
-            e0.record(stream)
-            fn()
-            e1.record(stream)
-            e1.synchronize()
-            if r >= 2:
-                ts.append(e0.elapsed_time(e1))
-        return statistics.median(ts)
-
-    ms_q = med(lambda: c.forward(x.data_ptr(), out.data_ptr(), queries))
-    ms_t = med(lambda: c.lib.wl_nrc_train_step(c.handle, wl._abi.C.c_void_p(x.data_ptr()),
-                                               wl._abi.C.c_void_p(t.data_ptr()), samples, None))
+    tq, tt = [], []
+    for r in range(repeats + 2):
+        c.forward(x.data_ptr(), out.data_ptr(), queries)
+        c.lib.wl_nrc_train_step(c.handle, wl._abi.C.c_void_p(x.data_ptr()), wl._abi.C.c_void_p(t.data_ptr()),
+                                samples, None)
+        mq, mt = c.kernel_times()
+        if r >= 2:
+            tq.append(mq)
+            tt.append(mt)
     c.close()
     s.close()
     pk = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
         os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
     peak = pk.get("bf16_tflops_sustained", 1400.0)
     kind = "measured sustained" if "bf16_tflops_sustained" in pk else "fallback sustained"
-    fq = queries * 34816 / (ms_q * 1e-3) / 1e12
-    ft = samples * 104448 / (ms_t * 1e-3) / 1e12
-    return {"mlp_query": {"rows": queries, "ms": round(ms_q, 4), "tflops": round(fq, 1),
-                          "frac": round(fq / peak, 4)},
-            "train_step": {"rows": samples, "ms": round(ms_t, 4), "tflops": round(ft, 1),
-                           "frac": round(ft / peak, 4)},
-            "peak_tflops": peak, "peak_kind": kind, "bound": "tensor"}
+
+    def entry(rows, ms, flop_per_row):
+        tf = rows * flop_per_row / (ms * 1e-3) / 1e12 if ms > 0 else 0.0
+        return {"rows": int(rows), "ms": round(ms, 4), "tflops": round(tf, 1), "frac": round(tf / peak, 4)}
+
+    outd = {"mlp_query": entry(queries, statistics.median(tq), 34816),
+            "train_step": entry(samples, statistics.median(tt), 104448),
+            "peak_tflops": peak, "peak_kind": kind, "bound": "tensor",
+            "timing": "wl_nrc_kernel_times: CUDA events around the tensor-core kernel alone"}
+    if in_situ:
+        nq, ns, mq, mt = in_situ
+        outd["render_last_frame"] = {"mlp_query": entry(nq, mq, 34816), "train_step": entry(ns, mt, 104448)}
+    return outd
 
 
 def main():
@@ -699,7 +698,10 @@ def main():
         w_, h_ = (int(v) for v in args.nrc_res.split("x"))
         r = nrc_convergence(wl, torch, ctx, res=(w_, h_), oracle_spp=args.nrc_oracle_spp,
                             budget_s=args.nrc_budget_s)
-        r["kernels"] = nrc_kernels(wl, torch, ctx)
+        n = r["nrc"]
+        ins = (n["queries_last_frame"], n["train_samples_last_frame"], n["kernel_ms_last_frame"]["mlp_query"],
+               n["kernel_ms_last_frame"]["train_step"]) if "kernel_ms_last_frame" in n else None
+        r["kernels"] = nrc_kernels(wl, torch, ctx, in_situ=ins)
         print(json.dumps(r), flush=True)
         ctx.close()
         return 0
@@ -859,7 +861,12 @@ def main():
             def nrc_leg():
                 r = nrc_convergence(wl, torch, ctx, res=(w_, h_), oracle_spp=args.nrc_oracle_spp,
                                     budget_s=args.nrc_budget_s)
-                r["kernels"] = nrc_kernels(wl, torch, ctx)
+                n = r["nrc"]
+                ins = None
+                if "kernel_ms_last_frame" in n:
+                    ins = (n["queries_last_frame"], n["train_samples_last_frame"],
+                           n["kernel_ms_last_frame"]["mlp_query"], n["kernel_ms_last_frame"]["train_step"])
+                r["kernels"] = nrc_kernels(wl, torch, ctx, in_situ=ins)
                 return r
             leg("time_to_relmse", nrc_leg)
         if world == 1 and not args.no_cpu_baseline:

@@ -413,6 +413,11 @@ WL_API int wl_nrc_set_weights(wl_nrc *nrc, const float *w);
  * its mbarrier a bounded number of times, then the kernel records the error, drains its
  * in-flight tensor-core work, frees its tensor memory and returns. */
 WL_API int wl_nrc_stats(wl_nrc *nrc, uint32_t *train_samples, uint32_t *queries, float *loss);
+/* Device time (ms, CUDA events) of the last launch of the cache's tensor-core kernels: the query
+ * MLP (wl_render_nrc's query pass, wl_nrc_query, wl_nrc_mlp_forward) and the fused training step
+ * (wl_render_nrc's training, wl_nrc_train_step, wl_nrc_mlp_gradients, wl_nrc_sample_gradients),
+ * without the encoding kernels around them; 0 for a kernel that has not run. Synchronises. */
+WL_API int wl_nrc_kernel_times(wl_nrc *nrc, float *ms_query_mlp, float *ms_train);
 /* Polls of a tensor-core wait before it gives up (default WL_NRC_WAIT_POLLS). 0 makes every
  * such wait give up at once: the hook that tests of the timeout path use. */
 #define WL_NRC_WAIT_POLLS 4194304u

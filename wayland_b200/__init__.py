@@ -315,6 +315,12 @@ class RadianceCache:
         _abi.check("wl_nrc_stats", self.lib.wl_nrc_stats(self.handle, C.byref(a), C.byref(b), C.byref(l)))
         return {"train_samples": a.value, "queries": b.value, "loss": l.value}
 
+    def kernel_times(self):
+        """(ms of the last query-MLP kernel, ms of the last training kernel), device time."""
+        a, b = C.c_float(), C.c_float()
+        _abi.check("wl_nrc_kernel_times", self.lib.wl_nrc_kernel_times(self.handle, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def set_wait_limit(self, polls):
         """mbarrier polls before a tensor-core wait gives up (0: at once; a test hook)."""
         _abi.check("wl_nrc_set_wait_limit", self.lib.wl_nrc_set_wait_limit(self.handle, polls))

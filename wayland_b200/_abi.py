@@ -175,6 +175,7 @@ SIGNATURES = {
     "wl_nrc_stats": (C.c_int, [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_float)]),
     "wl_render_ao": (C.c_int, [_P, _P, C.POINTER(Camera), C.POINTER(AoParams), _P]),
     "wl_nrc_set_wait_limit": (C.c_int, [_P, _U32]),
+    "wl_nrc_kernel_times": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "wl_nrc_get_grid": (C.c_int, [_P, C.POINTER(NrcGridDesc), _P]),
     "wl_nrc_set_grid": (C.c_int, [_P, _P]),
     "wl_nrc_query": (C.c_int, [_P, _P, _U32, _P]),

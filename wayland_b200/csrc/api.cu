@@ -1434,7 +1434,8 @@ int wl_nrc_destroy(wl_nrc *n) {
 int wl_nrc_mlp_forward(wl_nrc *n, const float *d_in, float *d_out, uint32_t count) {
     ARG(n && d_in && d_out, "null argument");
     CK(cudaSetDevice(n->ctx->device));
-    nrc_forward_raw(n->net, d_in, d_out, count, n->ctx->stream);
+    if (nrc_forward_raw(n->net, d_in, d_out, count, n->ctx->stream) != WL_OK)
+        return fail(WL_ERR_OOM, "radiance-cache tile scratch could not be allocated");
     CK(cudaGetLastError());
     return WL_OK;
 }
@@ -1477,6 +1478,8 @@ int wl_nrc_set_weights(wl_nrc *n, const float *w) {
     ARG(n && w, "null argument");
     CK(cudaSetDevice(n->ctx->device));
     CK(cudaMemcpyAsync(nrc_weights(n->net), w, WL_NRC_WEIGHTS * 4, cudaMemcpyHostToDevice, n->ctx->stream));
+    nrc_weights_changed(n->net, n->ctx->stream);
+    CK(cudaGetLastError());
     CK(cudaStreamSynchronize(n->ctx->stream));
     return WL_OK;
 }
@@ -1499,6 +1502,13 @@ int wl_nrc_stats(wl_nrc *n, uint32_t *samples, uint32_t *queries, float *loss) {
         CK(cudaStreamSynchronize(n->ctx->stream));
         return fail(WL_ERR_TIMEOUT, "radiance-cache tensor-core wait timed out");
     }
+    return WL_OK;
+}
+
+int wl_nrc_kernel_times(wl_nrc *n, float *ms_query, float *ms_train) {
+    ARG(n && ms_query && ms_train, "null argument");
+    CK(cudaSetDevice(n->ctx->device));
+    if (nrc_kernel_times(n->net, ms_query, ms_train) != WL_OK) return fail(WL_ERR_CUDA, "kernel timing events");
     return WL_OK;
 }
 

@@ -139,6 +139,10 @@ struct NrcNet {
     float lr = 1e-2f;
     uint32_t step = 0;
     int grid_blocks = 0;
+    uint8_t *w_img = nullptr;     // bfloat16 operand image of the weights (nrc_tc_weight_image)
+    float *w_part = nullptr;      // per-CTA partial weight gradients of the training kernel
+    cudaEvent_t ev_q[2] = {nullptr, nullptr}, ev_t[2] = {nullptr, nullptr};
+    bool ran_q = false, ran_t = false;
     NrcVertex *dbg_v = nullptr;  // caller vertices of the parity entry points
     uint32_t dbg_cap = 0;
     uint32_t wait_polls = NRC_WAIT_POLLS;
@@ -154,9 +158,11 @@ void nrc_free(NrcNet *n) {
     if (!n) return;
     void *ps[] = {n->grid.params, n->grid.feat, n->grid.grad, n->grid_m, n->grid_v, n->w, n->w_grad,
                   n->w_m, n->w_v, n->loss, n->counters, n->samples, n->tiles, n->gin, n->q_tiles,
-                  n->dbg_v};
+                  n->dbg_v, n->w_img, n->w_part};
     for (void *p : ps)
         if (p) cudaFree(p);
+    for (cudaEvent_t e : {n->ev_q[0], n->ev_q[1], n->ev_t[0], n->ev_t[1]})
+        if (e) cudaEventDestroy(e);
     delete n;
 }
 
@@ -181,6 +187,10 @@ int nrc_create(const wl_nrc_params &p, const float *bbox_lo, const float *bbox_h
     n->grid_m = (float *)nrc_alloc(n->grid_count * 4, e);
     n->grid_v = (float *)nrc_alloc(n->grid_count * 4, e);
     n->w = (float *)nrc_alloc(NRC_WEIGHTS * 4, e);
+    n->w_img = (uint8_t *)nrc_alloc(NRC_WEIGHT_IMAGE_BYTES, e);
+    n->w_part = (float *)nrc_alloc((size_t)nrc_tc_train_ctas() * NRC_WEIGHTS * 4, e);
+    for (cudaEvent_t *ev : {&n->ev_q[0], &n->ev_q[1], &n->ev_t[0], &n->ev_t[1]})
+        if (e == cudaSuccess) e = cudaEventCreate(ev);
     n->w_grad = (float *)nrc_alloc(NRC_WEIGHTS * 4, e);
     n->w_m = (float *)nrc_alloc(NRC_WEIGHTS * 4, e);
     n->w_v = (float *)nrc_alloc(NRC_WEIGHTS * 4, e);
@@ -218,6 +228,7 @@ int nrc_create(const wl_nrc_params &p, const float *bbox_lo, const float *bbox_h
     if (e == cudaSuccess) {
         k_grid_to_half<<<1024, 256, 0, s>>>(reinterpret_cast<const float2 *>(n->grid.params), n->grid.feat,
                                             n->grid_count / 2);
+        nrc_tc_weight_image(n->w, n->w_img, s);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -234,9 +245,15 @@ int nrc_create(const wl_nrc_params &p, const float *bbox_lo, const float *bbox_h
     return WL_OK;
 }
 
-void nrc_forward_raw(NrcNet *n, const float *in, float *out, uint32_t count, cudaStream_t s) {
-    nrc_tc_forward_raw(n->w, in, out, count, n->counters + 2, n->wait_polls, s);
+// Raw rows through the query kernel: the rows are converted into the query tile scratch first.
+int nrc_forward_raw(NrcNet *n, const float *in, float *out, uint32_t count, cudaStream_t s) {
+    if (nrc_reserve_queries(n, count) != WL_OK) return WL_ERR_OOM;
+    nrc_tc_forward_raw(n->w_img, in, out, count, n->q_tiles, n->counters + 2, n->wait_polls, s, n->ev_q);
+    n->ran_q = count > 0;
+    return WL_OK;
 }
+
+void nrc_weights_changed(NrcNet *n, cudaStream_t s) { nrc_tc_weight_image(n->w, n->w_img, s); }
 
 // Forward + backward + weight gradients for `count` rows (raw inputs) or for the samples
 // collected on the device (enc, count read from counters[0]). Leaves the MLP gradient in w_grad
@@ -259,11 +276,12 @@ static int nrc_gradients(NrcNet *n, bool enc, const wl_disney *mats, const float
     }
     if (!n->tiles) return WL_ERR_OOM;
     if (enc)
-        nrc_tc_train(n->w, n->grid, mats, n->samples, n->counters, n->max_samples, nullptr, nullptr,
-                     n->w_grad, n->loss, n->counters + 2, n->wait_polls, n->tiles, n->gin, s);
+        nrc_tc_train(n->w_img, n->grid, mats, n->samples, n->counters, n->max_samples, nullptr, nullptr,
+                     n->w_grad, n->w_part, n->loss, n->counters + 2, n->wait_polls, n->tiles, n->gin, s, n->ev_t);
     else
-        nrc_tc_train(n->w, n->grid, mats, nullptr, nullptr, count, in, target, n->w_grad, n->loss,
-                     n->counters + 2, n->wait_polls, n->tiles, nullptr, s);
+        nrc_tc_train(n->w_img, n->grid, mats, nullptr, nullptr, count, in, target, n->w_grad, n->w_part, n->loss,
+                     n->counters + 2, n->wait_polls, n->tiles, nullptr, s, n->ev_t);
+    n->ran_t = true;
     return WL_OK;
 }
 
@@ -273,6 +291,7 @@ static void nrc_adam(NrcNet *n, bool grid, cudaStream_t s) {
     float c1 = 1.0f - std::pow(b1, (float)n->step), c2 = 1.0f - std::pow(b2, (float)n->step);
     k_adam<<<(NRC_WEIGHTS + 255) / 256, 256, 0, s>>>(n->w, n->w_grad, n->w_m, n->w_v, NRC_WEIGHTS,
                                                     n->lr, b1, b2, 1e-8f, c1, c2, 1);
+    nrc_tc_weight_image(n->w, n->w_img, s);
     if (grid)
         k_adam_grid<<<n->grid_blocks * 4, 256, 0, s>>>(
             reinterpret_cast<float2 *>(n->grid.params), n->grid.feat, reinterpret_cast<float2 *>(n->grid.grad),
@@ -313,7 +332,8 @@ int nrc_reserve_queries(NrcNet *n, uint32_t rows) {
 void nrc_query(NrcNet *n, const wl_disney *mats, const NrcVertex *q, const uint32_t *nq,
                float4 *rad, uint32_t max_q, cudaStream_t s) {
     if (max_q > n->q_cap) max_q = n->q_cap;  // the render reserved the query rows beforehand
-    nrc_tc_query(n->w, n->grid, mats, q, nq, rad, max_q, n->counters + 2, n->wait_polls, n->q_tiles, s);
+    nrc_tc_query(n->w_img, n->grid, mats, q, nq, rad, max_q, n->counters + 2, n->wait_polls, n->q_tiles, s, n->ev_q);
+    n->ran_q = max_q > 0;
 }
 
 void nrc_collect(NrcNet *n, NrcWaveBuffers b, const Queues &q, uint32_t tcount, cudaStream_t s) {
@@ -361,8 +381,9 @@ int nrc_query_vertices(NrcNet *n, const wl_disney *mats, const NrcVertex *v, uin
     cudaMemsetAsync(out, 0, sizeof(float4) * (size_t)count, s);
     rc = nrc_load(v, count, true, n->dbg_v, n->counters + 4, s);
     if (rc != WL_OK) return rc;
-    nrc_tc_query(n->w, n->grid, mats, n->dbg_v, n->counters + 4, out, count, n->counters + 2, n->wait_polls,
-                 n->q_tiles, s);
+    nrc_tc_query(n->w_img, n->grid, mats, n->dbg_v, n->counters + 4, out, count, n->counters + 2, n->wait_polls,
+                 n->q_tiles, s, n->ev_q);
+    n->ran_q = count > 0;
     return WL_OK;
 }
 
@@ -403,6 +424,21 @@ void nrc_zero_grid_grad(NrcNet *n, cudaStream_t s) {
 }
 
 void nrc_set_wait_polls(NrcNet *n, uint32_t polls) { n->wait_polls = polls; }
+
+int nrc_kernel_times(NrcNet *n, float *ms_query, float *ms_train) {
+    *ms_query = *ms_train = 0.0f;
+    if (n->ran_q) {
+        if (cudaEventSynchronize(n->ev_q[1]) != cudaSuccess ||
+            cudaEventElapsedTime(ms_query, n->ev_q[0], n->ev_q[1]) != cudaSuccess)
+            return WL_ERR_CUDA;
+    }
+    if (n->ran_t) {
+        if (cudaEventSynchronize(n->ev_t[1]) != cudaSuccess ||
+            cudaEventElapsedTime(ms_train, n->ev_t[0], n->ev_t[1]) != cudaSuccess)
+            return WL_ERR_CUDA;
+    }
+    return WL_OK;
+}
 void nrc_clear_error(NrcNet *n, cudaStream_t s) { cudaMemsetAsync(n->counters + 2, 0, sizeof(uint32_t), s); }
 
 float *nrc_weights(NrcNet *n) { return n->w; }

@@ -1,13 +1,14 @@
-// nrc_tc.cu - radiance-cache MLP inference on the 5th-generation tensor cores (sm_100a).
+// nrc_tc.cu - the radiance cache's MLP on the 5th-generation tensor cores (sm_100a): the query
+// pass (inference) and the fused training step.
 //
-// One CTA of 128 threads (4 warps) processes tiles of 128 rows. The bfloat16 weights and the
-// current activation tile live in shared memory in the canonical K-major layout without
-// swizzle (8-row x 16-byte core matrices; adjacent K core matrices 128 B apart, adjacent 8-row
-// groups 1024 B apart). Per layer, one thread issues four tcgen05.mma (M=128, N=64 or 16,
-// K=16, bf16 x bf16 -> fp32) accumulating in tensor memory and commits them to an mbarrier;
-// every warp then reads its 32 rows back with tcgen05.ld (thread t owns row t), applies ReLU,
-// rounds to bfloat16 and writes the next layer's input tile. Waits on the mbarrier are bounded:
-// a timeout sets the error word, waits once more, frees the tensor memory and returns.
+// Operands are bfloat16 tiles in shared memory in the canonical K-major layout without swizzle
+// (8-row x 16-byte core matrices; adjacent K core matrices 128 B apart, adjacent 8-row groups
+// 1024 B apart for 64 columns). One thread issues tcgen05.mma (M=128, N=64 or 16, K=16,
+// bf16 x bf16 -> fp32 in tensor memory) and commits them to an mbarrier; the accumulators are
+// read back with tcgen05.ld (thread t of a warpgroup owns row t). Input tiles and the weights
+// (a bfloat16 image refreshed after every weight update) are copied into shared memory with
+// cp.async.bulk. Every wait is bounded: a wait that gives up sets the error word, the kernel
+// drains what it has in flight (with the full limit), frees its tensor memory and returns.
 #include <cuda_bf16.h>
 
 #include "wl_internal.h"
@@ -18,15 +19,7 @@ namespace wl {
 namespace {
 
 constexpr int TC_THREADS = 128;
-constexpr uint32_t TMEM_COLS = 64;
 constexpr uint32_t WAIT_LIMIT = NRC_WAIT_POLLS;
-// shared-memory layout (bytes)
-constexpr uint32_t SM_W = 0;                        // W0..W3, 8 KB each
-constexpr uint32_t SM_W4 = 4 * 8192;                // W4 (16 x 64), 2 KB
-constexpr uint32_t SM_A = SM_W4 + 2048;             // activation tile 128 x 64, 16 KB
-constexpr uint32_t SM_BAR = SM_A + 16384;           // mbarrier
-constexpr uint32_t SM_TMEM = SM_BAR + 8;            // tensor-memory address
-constexpr uint32_t SM_BYTES = SM_TMEM + 8;
 
 // byte offset of element (r, k) in a K-major tile with 64 columns
 __device__ __forceinline__ uint32_t kmaj(uint32_t r, uint32_t k) {
@@ -121,126 +114,192 @@ __device__ __forceinline__ void store_row(uint8_t *tile, uint32_t r, const float
     }
 }
 
-// MODE 0: raw rows in[n][64] -> out[n][4]. MODE 1: cache queries of the render loop, encoded
-// here. MODE 2: the same queries, encoded beforehand into 16 KB tiles (k_encode_tiles).
-template <int MODE>
-__global__ void __launch_bounds__(TC_THREADS) k_mlp_tc(const float *w, NrcGrid g, const wl_disney *mats,
-                                                        const NrcVertex *q, const uint32_t *nq,
-                                                        float4 *rad, const float *in, float *out,
-                                                        uint32_t n_raw, uint32_t *err, uint32_t polls,
-                                                        const uint8_t *tiles = nullptr) {
-    extern __shared__ __align__(1024) uint8_t smem[];
-    const uint32_t tid = threadIdx.x, warp = tid >> 5;
-    const uint32_t bar = smem_u32(smem + SM_BAR);
-    // weights -> bfloat16 K-major tiles
-    for (uint32_t i = tid; i < (uint32_t)NRC_WEIGHTS; i += TC_THREADS) {
-        uint32_t l = i / 4096u, rem = i % 4096u;
-        uint32_t r = rem / 64u, k = rem % 64u;
-        uint8_t *base = l < 4 ? smem + SM_W + l * 8192u : smem + SM_W4;
-        *reinterpret_cast<__nv_bfloat16 *>(base + kmaj(r, k)) = __float2bfloat16_rn(w[i]);
+// bfloat16 image of the MLP weights in the tensor-core operand layout, built once per weight
+// update (k_weight_image) and bulk-copied into shared memory by every CTA: W_0..W_3 (8 KB each)
+// and W_4 (2 KB) K-major with row = output (the B operand of the forward layers), then the same
+// matrices transposed, row = input (the B operand of the backward products).
+constexpr uint32_t WI_FWD = 4 * 8192 + 2048;        // 34,816 bytes
+constexpr uint32_t WI_BYTES = 2 * WI_FWD;
+
+__global__ void k_weight_image(const float *w, uint8_t *img) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (uint32_t)NRC_WEIGHTS) return;
+    const uint32_t l = i / 4096u, rem = i % 4096u, o = rem / 64u, k = rem % 64u;
+    const __nv_bfloat16 b = __float2bfloat16_rn(w[i]);
+    if (l < 4) {
+        *reinterpret_cast<__nv_bfloat16 *>(img + l * 8192u + kmaj(o, k)) = b;
+        *reinterpret_cast<__nv_bfloat16 *>(img + WI_FWD + l * 8192u + kmaj(k, o)) = b;
+    } else {
+        *reinterpret_cast<__nv_bfloat16 *>(img + 4 * 8192u + kmaj(o, k)) = b;
+        // W_4^T: 64 x 16 with 16 columns (8-row groups 256 B apart)
+        *reinterpret_cast<__nv_bfloat16 *>(img + WI_FWD + 4 * 8192u + ((k >> 3) * 256u + (o >> 3) * 128u +
+                                                                        (k & 7u) * 16u + (o & 7u) * 2u)) = b;
     }
+}
+
+// Bulk copy (cp.async.bulk, no tensor map, no multicast) of `bytes` from global memory into this
+// CTA's shared memory, completing on the mbarrier at `bar` (which this call arms with the byte
+// count). Both addresses 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ void named_sync(uint32_t id, uint32_t threads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
+// The query MLP: a persistent kernel, one CTA per SM, QC independent chains of 128 threads
+// (warpgroups) per CTA. Each chain runs its own 128-row tiles through the five layers with its own
+// 64 tensor-memory columns, mbarriers and two input buffers, so that while one chain converts a
+// layer's accumulators (tcgen05.ld, ReLU, bfloat16, st.shared) the tensor core executes the
+// others' MMAs. The next tile of a chain is bulk-copied into its second buffer while the current
+// one is computed; the weights are bulk-copied once per CTA from the bfloat16 image.
+// MODE 0: outputs to out[i][0..3] (raw rows, encoded into tiles by k_encode_tiles<0, false>).
+// MODE 2: cache queries of the render loop: rad[slot] += extra.xyz * max(o, 0).
+constexpr int QC = 4;
+constexpr uint32_t QS_A = WI_FWD + 1024;                    // tiles, 1024-aligned
+constexpr uint32_t QS_BAR = QS_A + 2 * QC * 16384u;         // per chain: mma, load0, load1; + weights
+constexpr uint32_t QS_TMEM = QS_BAR + (3 * QC + 1) * 8u;
+constexpr uint32_t QS_BYTES = QS_TMEM + 16;
+constexpr uint32_t QS_TMEM_COLS = 64u * QC;
+static_assert(QS_TMEM_COLS == 256u, "tensor-memory allocations are powers of two");
+
+// AND of a predicate over the 128 threads of a chain (a barrier of the chain's own id; also a
+// barrier for them)
+__device__ __forceinline__ bool chain_and(uint32_t id, bool v) {
+    uint32_t res;
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p, q;\n\t"
+        "setp.ne.u32 q, %1, 0;\n\t"
+        "bar.red.and.pred p, %2, 128, q;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t"
+        "}\n"
+        : "=r"(res)
+        : "r"((uint32_t)v), "r"(id)
+        : "memory");
+    return res != 0;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(128 * QC, 1)
+    k_mlp_q(const uint8_t *wimg, const uint8_t *tiles, const uint32_t *nq, uint32_t n_fixed, const NrcVertex *q,
+            float4 *rad, float *out, uint32_t *err, uint32_t polls) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, chain = tid >> 7, r = tid & 127u;
+    const uint32_t cbar = 1u + chain;  // the chain's named barrier (0 is the CTA's)
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + QS_BAR);
+    const uint32_t mbar = smem_u32(bars + 3 * chain);
+    const uint32_t lbar[2] = {smem_u32(bars + 3 * chain + 1), smem_u32(bars + 3 * chain + 2)};
+    const uint32_t wbar = smem_u32(bars + 3 * QC);
+    uint8_t *bufs[2] = {smem + QS_A + (2 * chain) * 16384u, smem + QS_A + (2 * chain + 1) * 16384u};
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        for (int k = 0; k < 3 * QC + 1; k++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bars + k)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(smem + SM_TMEM)),
-                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(smem + QS_TMEM)),
+                     "r"(QS_TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
     }
-    fence_async_smem();
     tc_before_sync();
     __syncthreads();
     tc_after_sync();
-    const uint32_t tmem = *reinterpret_cast<volatile uint32_t *>(smem + SM_TMEM);
-    const uint32_t lane_base = (warp * 32u) << 16;
-    const uint32_t n = MODE == 0 ? n_raw : *nq;
-    const uint32_t aA = smem_u32(smem + SM_A);
-    uint32_t phase = 0;
-    bool ok = true;
-    for (uint32_t tile = blockIdx.x * TC_THREADS; tile < n && ok; tile += gridDim.x * TC_THREADS) {
-        const uint32_t i = tile + tid;
-        const bool valid = i < n;
-        NrcVertex v;
-        if (MODE == 2) {
-            const uint4 *src = reinterpret_cast<const uint4 *>(tiles + (size_t)(tile / 128u) * 16384u);
-            uint4 *dst = reinterpret_cast<uint4 *>(smem + SM_A);
-            for (uint32_t k = tid; k < 1024u; k += TC_THREADS) dst[k] = src[k];
-            if (valid) v.extra = q[i].extra;
-        } else {
-            float x[NRC_IN];
-            if (valid) {
-                if (MODE == 0) {
-                    for (int k = 0; k < NRC_IN; k++) x[k] = in[(size_t)i * NRC_IN + k];
-                } else {
-                    v = q[i];
-                    nrc_encode(g, mats, v, x);
-                }
-            } else {
-                for (int k = 0; k < NRC_IN; k++) x[k] = 0.0f;
-            }
-            store_row(smem + SM_A, tid, x);
+    const uint32_t tmem0 = *reinterpret_cast<volatile uint32_t *>(smem + QS_TMEM);
+    const uint32_t tmem = tmem0 + 64u * chain;
+    const uint32_t lane_base = ((warp & 3u) * 32u) << 16;
+    const uint32_t n = MODE == 2 ? min(*nq, n_fixed) : n_fixed;
+    const uint32_t ntiles = (n + 127u) / 128u;
+    const uint32_t stride = gridDim.x * QC;
+    uint32_t t = blockIdx.x * QC + chain;
+    // state every thread of a chain keeps identically (its decisions are chain-wide)
+    bool pending[2] = {t < ntiles, false};  // a bulk copy into buffer b is in flight
+    bool mma_inflight = false;
+    uint32_t mph = 0, lph[2] = {0, 0};
+    if (tid == 0) bulk_load(smem_u32(smem), wimg, WI_FWD, wbar);
+    if (r == 0 && pending[0]) bulk_load(smem_u32(bufs[0]), tiles + (size_t)t * 16384u, 16384u, lbar[0]);
+    const bool wok = __syncthreads_and(mbar_wait(wbar, 0, polls)) != 0;
+    bool ok = wok;
+    for (uint32_t k = 0; t < ntiles && ok; t += stride, k++) {
+        const uint32_t b = k & 1u;
+        if (!chain_and(cbar, mbar_wait(lbar[b], lph[b], polls))) {
+            ok = false;
+            break;
         }
-        fence_async_smem();
-        tc_before_sync();
-        __syncthreads();
-        tc_after_sync();
-        for (int layer = 0; layer < 5 && ok; layer++) {
-            const uint32_t wB = smem_u32(smem + (layer < 4 ? SM_W + layer * 8192u : SM_W4));
+        pending[b] = false;
+        lph[b] ^= 1u;
+        if (t + stride < ntiles) {
+            if (r == 0) bulk_load(smem_u32(bufs[b ^ 1u]), tiles + (size_t)(t + stride) * 16384u, 16384u, lbar[b ^ 1u]);
+            pending[b ^ 1u] = true;
+        }
+        const uint32_t aA = smem_u32(bufs[b]);
+        for (int layer = 0; layer < 5; layer++) {
+            const uint32_t wB = smem_u32(smem + (layer < 4 ? layer * 8192u : 4 * 8192u));
             const uint32_t id = layer < 4 ? idesc(64, 128) : idesc(16, 128);
-            if (tid == 0) {
+            if (r == 0) {
+                tc_after_sync();
 #pragma unroll
                 for (uint32_t ks = 0; ks < 4; ks++)
                     mma_bf16(tmem, sdesc(aA + ks * 256u), sdesc(wB + ks * 256u), id, ks > 0 ? 1u : 0u);
-                mma_commit(bar);
+                mma_commit(mbar);
             }
-            bool got = mbar_wait(bar, phase, polls);
-            phase ^= 1u;
-            ok = __syncthreads_and(got) != 0;
+            mma_inflight = true;
+            if (!chain_and(cbar, mbar_wait(mbar, mph, polls))) {
+                ok = false;
+                break;
+            }
+            mma_inflight = false;
+            mph ^= 1u;
             tc_after_sync();
-            if (!ok) break;
             if (layer < 4) {
                 float h[NRC_HID];
 #pragma unroll
                 for (int c = 0; c < 4; c++) tmem_ld16(tmem + lane_base + 16u * c, h + 16 * c);
                 tmem_wait_ld();
 #pragma unroll
-                for (int k = 0; k < NRC_HID; k++) h[k] = fmaxf(h[k], 0.0f);
-                store_row(smem + SM_A, tid, h);
+                for (int j = 0; j < NRC_HID; j++) h[j] = fmaxf(h[j], 0.0f);
+                store_row(bufs[b], r, h);
                 fence_async_smem();
             } else {
                 float o[16];
                 tmem_ld16(tmem + lane_base, o);
                 tmem_wait_ld();
-                if (valid) {
+                const uint32_t i = t * 128u + r;
+                if (i < n) {
                     if (MODE == 0) {
-                        for (int c = 0; c < 4; c++) out[(size_t)i * 4 + c] = o[c];
+                        *reinterpret_cast<float4 *>(out + (size_t)i * 4) = make_float4(o[0], o[1], o[2], o[3]);
                     } else {
-                        uint32_t slot = __float_as_uint(v.extra.w);
-                        float4 r = rad[slot];
-                        r.x += v.extra.x * fmaxf(o[0], 0.0f);
-                        r.y += v.extra.y * fmaxf(o[1], 0.0f);
-                        r.z += v.extra.z * fmaxf(o[2], 0.0f);
-                        rad[slot] = r;
+                        const float4 e = q[i].extra;
+                        const uint32_t slot = __float_as_uint(e.w);
+                        float4 v = rad[slot];
+                        v.x += e.x * fmaxf(o[0], 0.0f);
+                        v.y += e.y * fmaxf(o[1], 0.0f);
+                        v.z += e.z * fmaxf(o[2], 0.0f);
+                        rad[slot] = v;
                     }
                 }
             }
             tc_before_sync();
-            __syncthreads();
-            tc_after_sync();
+            named_sync(cbar, 128u);
         }
     }
     if (!ok) {
-        if (tid == 0) atomicExch(err, 1u);
-        // let the tensor-core work still in flight (the phase that timed out) finish before the
-        // memory is released
-        mbar_wait(bar, phase ^ 1u);
+        if (r == 0) atomicExch(err, 1u);
+        // drain what this chain still has in flight (the weights' copy for chain 0, its MMAs, its
+        // bulk copies) with the full wait limit before shared and tensor memory are released
+        if (!wok && tid == 0) mbar_wait(wbar, 0);
+        if (mma_inflight) mbar_wait(mbar, mph);
+        for (int b = 0; b < 2; b++)
+            if (pending[b]) mbar_wait(lbar[b], lph[b]);
     }
     tc_before_sync();
     __syncthreads();
     tc_after_sync();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem0), "r"(QS_TMEM_COLS));
 }
 
 // ---------------------------------------------------------------------------------------
@@ -269,9 +328,12 @@ constexpr uint32_t TS_T0 = TS_W4T + 2048;       // A_0, A_2, A_4
 constexpr uint32_t TS_T1 = TS_T0 + 16384;       // A_1, A_3, then dZ
 constexpr uint32_t TS_DZT = TS_T1 + 16384;      // dZ^T, 64 x 128 (its M=128 read spans 32 KB)
 constexpr uint32_t TS_AT = TS_DZT + 16384;      // A_0^T..A_4^T, 64 x 128 each
-constexpr uint32_t TS_BAR = TS_AT + 5 * 16384;
-constexpr uint32_t TS_TMEM = TS_BAR + 8;
+constexpr uint32_t TS_BAR = TS_AT + 5 * 16384;   // MMA completion
+constexpr uint32_t TS_WBAR = TS_BAR + 8;          // the weights' bulk copy
+constexpr uint32_t TS_LBAR = TS_BAR + 16;         // each tile's bulk copy
+constexpr uint32_t TS_TMEM = TS_BAR + 24;
 constexpr uint32_t TS_BYTES = TS_TMEM + 8;
+static_assert(TS_WT == TS_W + WI_FWD && TS_W4T + 2048 == TS_W + WI_BYTES, "the weight image's layout");
 
 // K-major tiles with 16 and 128 columns (core matrices 8 rows x 16 bytes)
 __device__ __forceinline__ uint32_t kmaj16(uint32_t r, uint32_t k) {
@@ -379,28 +441,20 @@ __global__ void __launch_bounds__(256) k_grid_scatter(NrcGrid g, const NrcVertex
 // (count on the device), encoded here; the input gradient goes to the hash grid.
 template <int MODE>
 __global__ void __launch_bounds__(TR_THREADS, 1)
-    k_train_tc(const float *w, const NrcVertex *samples, const uint32_t *n_ptr, uint32_t n_fixed,
-               const float *target, const uint8_t *tiles, float *gin_out, float *w_grad,
+    k_train_tc(const uint8_t *wimg, const NrcVertex *samples, const uint32_t *n_ptr, uint32_t n_fixed,
+               const float *target, const uint8_t *tiles, float *gin_out, float *w_part,
                float *loss, uint32_t *err, uint32_t polls) {
     extern __shared__ __align__(1024) uint8_t smem[];
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const uint32_t r = tid & 127u, h = tid >> 7;
-    const uint32_t bar = smem_u32(smem + TS_BAR);
-    for (uint32_t i = tid; i < (uint32_t)NRC_WEIGHTS; i += TR_THREADS) {
-        uint32_t l = i / 4096u, rem = i % 4096u;
-        uint32_t o = rem / 64u, k = rem % 64u;
-        __nv_bfloat16 b = __float2bfloat16_rn(w[i]);
-        if (l < 4) {
-            *reinterpret_cast<__nv_bfloat16 *>(smem + TS_W + l * 8192u + kmaj(o, k)) = b;
-            *reinterpret_cast<__nv_bfloat16 *>(smem + TS_WT + l * 8192u + kmaj(k, o)) = b;
-        } else {
-            *reinterpret_cast<__nv_bfloat16 *>(smem + TS_W4 + kmaj(o, k)) = b;
-            *reinterpret_cast<__nv_bfloat16 *>(smem + TS_W4T + kmaj16(k, o)) = b;
-        }
-    }
+    const uint32_t bar = smem_u32(smem + TS_BAR), wbar = smem_u32(smem + TS_WBAR), lbar = smem_u32(smem + TS_LBAR);
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(wbar) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(lbar) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        // the weights and their transposes, one bulk copy of the bfloat16 image
+        bulk_load(smem_u32(smem + TS_W), wimg, WI_BYTES, wbar);
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(smem + TS_TMEM)),
@@ -416,23 +470,30 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
     const uint32_t sT0 = smem_u32(smem + TS_T0), sT1 = smem_u32(smem + TS_T1);
     const uint32_t sAT = smem_u32(smem + TS_AT), sDZT = smem_u32(smem + TS_DZT);
     const uint32_t sW = smem_u32(smem + TS_W), sWT = smem_u32(smem + TS_WT);
-    uint32_t phase = 0;
-    bool ok = true, any = false;
+    uint32_t phase = 0, lphase = 0;
+    bool wok = __syncthreads_and(mbar_wait(wbar, 0, polls)) != 0;
+    bool ok = wok, any = false, lpending = false;
     float lsum = 0.0f;
     for (uint32_t tile = blockIdx.x * 128u; tile < n && ok; tile += gridDim.x * 128u) {
         const uint32_t i = tile + r;
         const bool valid = i < n;
-        // ---- inputs: the encoded tile and its transpose (k_encode_tiles), 32 KB
+        // ---- inputs: the encoded tile and its transpose (k_encode_tiles), 32 KB in two bulk copies
         float t3[3] = {0.f, 0.f, 0.f};
-        {
-            const uint4 *src = reinterpret_cast<const uint4 *>(tiles + (size_t)(tile / 128u) * 32768u);
-            uint4 *dA = reinterpret_cast<uint4 *>(smem + TS_T0);
-            uint4 *dT = reinterpret_cast<uint4 *>(smem + TS_AT);
-            for (uint32_t k = tid; k < 1024u; k += TR_THREADS) {
-                dA[k] = src[k];
-                dT[k] = src[1024u + k];
-            }
+        if (tid == 0) {
+            const uint8_t *src = tiles + (size_t)(tile / 128u) * 32768u;
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(lbar), "r"(32768u) : "memory");
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                         ::"r"(smem_u32(smem + TS_T0)), "l"(src), "r"(16384u), "r"(lbar) : "memory");
+            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                         ::"r"(smem_u32(smem + TS_AT)), "l"(src + 16384u), "r"(16384u), "r"(lbar) : "memory");
         }
+        lpending = true;
+        if (__syncthreads_and(mbar_wait(lbar, lphase, polls)) == 0) {
+            ok = false;
+            break;
+        }
+        lpending = false;
+        lphase ^= 1u;
         if (valid && h == 0) {
             if (MODE == 1) {
                 float4 e = samples[i].extra;
@@ -550,23 +611,34 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
         __syncthreads();
         tc_after_sync();
     }
-    if (ok && any && r < 64u) {
-        // dW_l rows (outputs) r, columns [32h, 32h + 32)
+    // this CTA's dW_l rows (outputs) r, columns [32h, 32h + 32), into its own partial gradient
+    // (summed over the CTAs in a fixed order by k_wgrad_reduce; zeros when it had no tile)
+    if (r < 64u) {
+        float *part = w_part + (size_t)blockIdx.x * NRC_WEIGHTS;
         for (uint32_t l = 0; l < 5; l++) {
             float a[32];
-            tmem_ld16(tmem + lane + 128u + 64u * l + 32u * h, a);
-            tmem_ld16(tmem + lane + 128u + 64u * l + 32u * h + 16u, a + 16);
-            tmem_wait_ld();
+            if (ok && any) {
+                tmem_ld16(tmem + lane + 128u + 64u * l + 32u * h, a);
+                tmem_ld16(tmem + lane + 128u + 64u * l + 32u * h + 16u, a + 16);
+                tmem_wait_ld();
+            } else {
+                for (int k = 0; k < 32; k++) a[k] = 0.0f;
+            }
             const uint32_t rows = l < 4 ? 64u : 16u;
-            if (r < rows)
-                for (int k = 0; k < 32; k++) atomicAdd(w_grad + l * 4096u + r * 64u + 32u * h + k, a[k]);
+            if (r < rows) {
+                float4 *dst = reinterpret_cast<float4 *>(part + l * 4096u + r * 64u + 32u * h);
+                for (int k = 0; k < 8; k++) dst[k] = make_float4(a[4 * k], a[4 * k + 1], a[4 * k + 2], a[4 * k + 3]);
+            }
         }
     }
     for (int off = 16; off > 0; off >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, off);
     if ((tid & 31u) == 0 && lsum != 0.0f) atomicAdd(loss, lsum);
     if (!ok) {
         if (tid == 0) atomicExch(err, 1u);
-        mbar_wait(bar, phase ^ 1u);
+        // drain the copies and MMAs still in flight with the full wait limit
+        if (!wok) mbar_wait(wbar, 0);
+        else if (lpending) mbar_wait(lbar, lphase);
+        else mbar_wait(bar, phase ^ 1u);
     }
     tc_before_sync();
     __syncthreads();
@@ -575,45 +647,51 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TR_TMEM_COLS));
 }
 
-int tc_grid(const void *k) {
-    int dev = 0, sms = 0, per = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_BYTES);
-    cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, TC_THREADS, SM_BYTES);
-    // 4 CTAs per SM fit by shared memory (4 x 51 KB), registers and tensor memory (4 x 64
-    // columns); launch that many even where the occupancy query reports fewer (CTAs that do not
-    // fit wait for a free slot; they never wait on one another)
-    if (per < 4) per = 4;
-    if (per > 4) per = 4;
-    return sms * per;
+// CTAs of the query kernel: one per SM, at most one per QC tiles.
+template <int MODE> uint32_t q_blocks(uint32_t ntiles) {
+    static int sms = [] {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        cudaFuncSetAttribute(k_mlp_q<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)QS_BYTES);
+        cudaFuncSetAttribute(k_mlp_q<MODE>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+        return v;
+    }();
+    const uint32_t want = (ntiles + QC - 1) / QC;
+    return want < (uint32_t)sms ? want : (uint32_t)sms;
 }
 
 }  // namespace
 
-void nrc_tc_forward_raw(const float *w, const float *in, float *out, uint32_t n, uint32_t *err,
-                        uint32_t polls, cudaStream_t s) {
-    static int grid = tc_grid((const void *)k_mlp_tc<0>);
-    uint32_t tiles = (n + TC_THREADS - 1) / TC_THREADS;
-    uint32_t blocks = tiles < (uint32_t)grid ? tiles : (uint32_t)grid;
-    if (blocks == 0) return;
-    k_mlp_tc<0><<<blocks, TC_THREADS, SM_BYTES, s>>>(w, NrcGrid{}, nullptr, nullptr, nullptr, nullptr,
-                                                      in, out, n, err, polls);
+void nrc_tc_weight_image(const float *w, uint8_t *img, cudaStream_t s) {
+    k_weight_image<<<(NRC_WEIGHTS + 255) / 256, 256, 0, s>>>(w, img);
+}
+
+// Raw rows in[n][64] -> out[n][4]: the rows converted into operand tiles (16 KB per 128 rows),
+// then the query kernel over them.
+void nrc_tc_forward_raw(const uint8_t *wimg, const float *in, float *out, uint32_t n, uint8_t *tiles,
+                        uint32_t *err, uint32_t polls, cudaStream_t s, const cudaEvent_t *ev) {
+    const uint32_t ntiles = (n + 127u) / 128u;
+    if (ntiles == 0) return;
+    k_encode_tiles<0, false><<<ntiles, 256, 0, s>>>(NrcGrid{}, nullptr, nullptr, nullptr, n, in, tiles);
+    if (ev) cudaEventRecord(ev[0], s);
+    k_mlp_q<0><<<q_blocks<0>(ntiles), 128 * QC, QS_BYTES, s>>>(wimg, tiles, nullptr, n, nullptr, nullptr, out,
+                                                             err, polls);
+    if (ev) cudaEventRecord(ev[1], s);
 }
 
 // Cache queries: encoded into tiles by a many-CTA kernel (the grid gathers are latency-bound),
 // then the tensor-core MLP over the tiles. tiles: 16 KB per 128 queries (max_q rows).
-void nrc_tc_query(const float *w, const NrcGrid &g, const wl_disney *mats, const NrcVertex *q,
+void nrc_tc_query(const uint8_t *wimg, const NrcGrid &g, const wl_disney *mats, const NrcVertex *q,
                   const uint32_t *nq, float4 *rad, uint32_t max_q, uint32_t *err, uint32_t polls,
-                  uint8_t *tiles, cudaStream_t s) {
-    static int grid = tc_grid((const void *)k_mlp_tc<2>);
-    uint32_t ntiles = (max_q + TC_THREADS - 1) / TC_THREADS;
+                  uint8_t *tiles, cudaStream_t s, const cudaEvent_t *ev) {
+    const uint32_t ntiles = (max_q + 127u) / 128u;
     if (ntiles == 0) return;
     k_encode_tiles<1, false><<<ntiles, 256, 0, s>>>(g, mats, q, nq, max_q, nullptr, tiles);
-    uint32_t blocks = ntiles < (uint32_t)grid ? ntiles : (uint32_t)grid;
-    k_mlp_tc<2><<<blocks, TC_THREADS, SM_BYTES, s>>>(w, g, mats, q, nq, rad, nullptr, nullptr, 0, err,
-                                                     polls, tiles);
+    if (ev) cudaEventRecord(ev[0], s);
+    k_mlp_q<2><<<q_blocks<2>(ntiles), 128 * QC, QS_BYTES, s>>>(wimg, tiles, nq, max_q, q, rad, nullptr, err,
+                                                             polls);
+    if (ev) cudaEventRecord(ev[1], s);
 }
 
 // Rows of 64 floats read back from the query pass's bfloat16 tiles (parity access).
@@ -636,10 +714,17 @@ void nrc_tc_encode_rows(const NrcGrid &g, const wl_disney *mats, const NrcVertex
 // Gradients of one training step into w_grad (zeroed here) and the grid gradient; loss (zeroed
 // here) receives the mean relative L2 loss. Raw rows when samples is null. tiles: 32 KB per 128
 // rows; gin: 32 floats per row.
-void nrc_tc_train(const float *w, const NrcGrid &g, const wl_disney *mats, const NrcVertex *samples,
-                  const uint32_t *n_ptr, uint32_t n_max, const float *in, const float *target,
-                  float *w_grad, float *loss, uint32_t *err, uint32_t polls, uint8_t *tiles,
-                  float *gin, cudaStream_t s) {
+// Sum of the training kernel's per-CTA partial weight gradients, CTA by CTA in a fixed order
+// (so that the gradient does not depend on scheduling).
+__global__ void k_wgrad_reduce(const float *part, uint32_t nparts, float *w_grad) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (uint32_t)NRC_WEIGHTS) return;
+    float acc = 0.0f;
+    for (uint32_t p = 0; p < nparts; p++) acc += part[(size_t)p * NRC_WEIGHTS + i];
+    w_grad[i] = acc;
+}
+
+uint32_t nrc_tc_train_ctas() {
     static int sms = [] {
         int dev = 0, v = 0;
         cudaGetDevice(&dev);
@@ -650,22 +735,37 @@ void nrc_tc_train(const float *w, const NrcGrid &g, const wl_disney *mats, const
         cudaFuncSetAttribute(k_train_tc<1>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
         return v;
     }();
-    cudaMemsetAsync(w_grad, 0, NRC_WEIGHTS * sizeof(float), s);
+    return (uint32_t)sms;
+}
+
+void nrc_tc_train(const uint8_t *wimg, const NrcGrid &g, const wl_disney *mats, const NrcVertex *samples,
+                  const uint32_t *n_ptr, uint32_t n_max, const float *in, const float *target,
+                  float *w_grad, float *w_part, float *loss, uint32_t *err, uint32_t polls, uint8_t *tiles,
+                  float *gin, cudaStream_t s, const cudaEvent_t *ev) {
+    const uint32_t sms = nrc_tc_train_ctas();
     cudaMemsetAsync(loss, 0, sizeof(float), s);
     uint32_t tiles_n = (n_max + 127u) / 128u;
-    uint32_t blocks = tiles_n < (uint32_t)sms ? tiles_n : (uint32_t)sms;
-    if (blocks == 0) return;
+    uint32_t blocks = tiles_n < sms ? tiles_n : sms;
+    if (blocks == 0) {
+        cudaMemsetAsync(w_grad, 0, NRC_WEIGHTS * sizeof(float), s);
+        return;
+    }
     if (samples) {
         k_encode_tiles<1><<<tiles_n, 256, 0, s>>>(g, mats, samples, n_ptr, n_max, nullptr, tiles);
-        k_train_tc<1><<<blocks, TR_THREADS, TS_BYTES, s>>>(w, samples, n_ptr, n_max, nullptr, tiles, gin,
-                                                           w_grad, loss, err, polls);
+        if (ev) cudaEventRecord(ev[0], s);
+        k_train_tc<1><<<blocks, TR_THREADS, TS_BYTES, s>>>(wimg, samples, n_ptr, n_max, nullptr, tiles, gin,
+                                                           w_part, loss, err, polls);
+        if (ev) cudaEventRecord(ev[1], s);
         uint64_t threads = (uint64_t)n_max * 16u;
         k_grid_scatter<<<(uint32_t)((threads + 255) / 256), 256, 0, s>>>(g, samples, n_ptr, n_max, gin);
     } else {
         k_encode_tiles<0><<<tiles_n, 256, 0, s>>>(g, mats, nullptr, nullptr, n_max, in, tiles);
-        k_train_tc<0><<<blocks, TR_THREADS, TS_BYTES, s>>>(w, nullptr, nullptr, n_max, target, tiles,
-                                                           nullptr, w_grad, loss, err, polls);
+        if (ev) cudaEventRecord(ev[0], s);
+        k_train_tc<0><<<blocks, TR_THREADS, TS_BYTES, s>>>(wimg, nullptr, nullptr, n_max, target, tiles,
+                                                           nullptr, w_part, loss, err, polls);
+        if (ev) cudaEventRecord(ev[1], s);
     }
+    k_wgrad_reduce<<<(NRC_WEIGHTS + 255) / 256, 256, 0, s>>>(w_part, blocks, w_grad);
 }
 
 }  // namespace wl

@@ -318,7 +318,8 @@ struct NrcNet;
 int nrc_create(const wl_nrc_params &p, const float *bbox_lo, const float *bbox_hi,
                uint32_t max_samples, cudaStream_t s, NrcNet **out, std::string &err);
 void nrc_free(NrcNet *n);
-void nrc_forward_raw(NrcNet *n, const float *in, float *out, uint32_t count, cudaStream_t s);
+int nrc_forward_raw(NrcNet *n, const float *in, float *out, uint32_t count, cudaStream_t s);
+void nrc_weights_changed(NrcNet *n, cudaStream_t s);
 int nrc_train_raw(NrcNet *n, const float *in, const float *target, uint32_t count, cudaStream_t s);
 int nrc_gradients_raw(NrcNet *n, const float *in, const float *target, uint32_t count,
                        cudaStream_t s);
@@ -336,11 +337,16 @@ struct NrcGrid;
 // err: the cache's error word (set when a tensor-core wait gives up); polls: mbarrier polls
 // before a wait gives up (NRC_WAIT_POLLS unless a test lowered it)
 constexpr uint32_t NRC_WAIT_POLLS = 1u << 22;
-void nrc_tc_forward_raw(const float *w, const float *in, float *out, uint32_t n, uint32_t *err,
-                        uint32_t polls, cudaStream_t s);
-void nrc_tc_query(const float *w, const NrcGrid &g, const wl_disney *mats, const NrcVertex *q,
+// the bfloat16 operand image of the MLP weights (NRC_WEIGHT_IMAGE_BYTES), rebuilt after every
+// weight update; the query kernel and the training kernel copy it into shared memory
+constexpr uint32_t NRC_WEIGHT_IMAGE_BYTES = 2u * (4u * 8192u + 2048u);
+void nrc_tc_weight_image(const float *w, uint8_t *img, cudaStream_t s);
+// ev (optional): two events recorded around the tensor-core kernel alone
+void nrc_tc_forward_raw(const uint8_t *wimg, const float *in, float *out, uint32_t n, uint8_t *tiles,
+                        uint32_t *err, uint32_t polls, cudaStream_t s, const cudaEvent_t *ev);
+void nrc_tc_query(const uint8_t *wimg, const NrcGrid &g, const wl_disney *mats, const NrcVertex *q,
                   const uint32_t *nq, float4 *rad, uint32_t max_q, uint32_t *err, uint32_t polls,
-                  uint8_t *tiles, cudaStream_t s);
+                  uint8_t *tiles, cudaStream_t s, const cudaEvent_t *ev);
 int nrc_reserve_queries(NrcNet *n, uint32_t rows);
 // parity access (nrc.cu): grid parameters, the query and encode passes on caller vertices, and
 // one training step's gradients on caller samples
@@ -356,10 +362,14 @@ int nrc_sample_gradients(NrcNet *n, const wl_disney *mats, const NrcVertex *v, u
 void nrc_zero_grid_grad(NrcNet *n, cudaStream_t s);
 void nrc_tc_encode_rows(const NrcGrid &g, const wl_disney *mats, const NrcVertex *v, const uint32_t *n_ptr,
                         uint32_t count, uint8_t *tiles, float *rows, cudaStream_t s);
-void nrc_tc_train(const float *w, const NrcGrid &g, const wl_disney *mats, const NrcVertex *samples,
+// the training kernel's CTAs (one per SM): w_part holds one partial weight gradient per CTA
+uint32_t nrc_tc_train_ctas();
+void nrc_tc_train(const uint8_t *wimg, const NrcGrid &g, const wl_disney *mats, const NrcVertex *samples,
                   const uint32_t *n_ptr, uint32_t n_max, const float *in, const float *target,
-                  float *w_grad, float *loss, uint32_t *err, uint32_t polls, uint8_t *tiles,
-                  float *gin, cudaStream_t s);
+                  float *w_grad, float *w_part, float *loss, uint32_t *err, uint32_t polls, uint8_t *tiles,
+                  float *gin, cudaStream_t s, const cudaEvent_t *ev);
+// device time of the last query / training tensor-core kernel (ms; 0 when none ran)
+int nrc_kernel_times(NrcNet *n, float *ms_query, float *ms_train);
 void nrc_set_wait_polls(NrcNet *n, uint32_t polls);
 void nrc_clear_error(NrcNet *n, cudaStream_t s);
 
