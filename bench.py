@@ -585,7 +585,9 @@ def nrc_convergence(wl, torch, ctx, res=(1920, 1080), oracle_spp=8192, target=1e
                 "final_relmse": curve[-1][2], "curve": curve[:: max(1, len(curve) // 12)], **extra}
 
     plain = run("plain")
+    torch.cuda.nvtx.range_push("nrc")  # the window a profiler can select (--nvtx-include nrc/)
     nrc = run("nrc")
+    torch.cuda.nvtx.range_pop()
     scene.close()
     out = {"scene": f"door-slit room {sc.num_tris} tris, {W_}x{H_}, depth 16, fast math",
            "oracle": f"{oracle_spp} spp, FP64 film, plain path tracer ({oracle_s:.1f} s)",
