@@ -205,10 +205,11 @@ def reference_arm(args):
     return 0
 
 
-def raycast_microbench(wl, torch, ctx, sc, scene, stream):
+def raycast_microbench(wl, torch, ctx, sc, scene, stream, tune=None):
     """2^24 coherent primary rays (4096 x 4096 view), 2^24 cosine-distributed bounce rays from
     the primary hit points and 2^24 any-hit shadow rays from the same points to uniform points of
-    random lights; Mrays/s and traversal counts."""
+    random lights; Mrays/s and traversal counts. The shadow rays are also timed with the other
+    any-hit child order (far to near against near to far) under `shadow_other_order`."""
     n_side = 4096
     dev = torch.device("cuda")
     cam = {k: torch.tensor(np.asarray(scene.camera[k], np.float32), device=dev) for k in scene.camera}
@@ -295,6 +296,20 @@ def raycast_microbench(wl, torch, ctx, sc, scene, stream):
     nodes_s, tris_s = sc.cast_stats(srays.data_ptr(), n, wl.CAST_ANY)
     t_bounce = timed(brays)
     nodes_b, tris_b = sc.cast_stats(brays.data_ptr(), n)
+    other = None
+    if tune is not None:
+        flipped = dict(tune)
+        flipped.pop("fixed", None)
+        flipped["shadow_far_first"] = 0 if tune.get("shadow_far_first") else 1
+        ctx.set_tune(flipped)
+        t_o = timed(srays, mode=wl.CAST_ANY)
+        n_o, tr_o = sc.cast_stats(srays.data_ptr(), n, wl.CAST_ANY)
+        restore = dict(tune)
+        restore.pop("fixed", None)
+        ctx.set_tune(restore)
+        other = {"shadow_far_first": flipped["shadow_far_first"], "ms": round(t_o, 3),
+                 "mrays_s": round(n / t_o / 1e3, 1), "nodes_per_ray": round(n_o / n, 2),
+                 "tris_per_ray": round(tr_o / n, 2)}
     out = {}
     for name, t, nn, tt in (("primary", t_primary, nodes_p, tris_p), ("bounce", t_bounce, nodes_b, tris_b),
                             ("shadow", t_shadow, nodes_s, tris_s)):
@@ -304,6 +319,8 @@ def raycast_microbench(wl, torch, ctx, sc, scene, stream):
                      "nodes_per_ray": round(nodes_per, 2), "tris_per_ray": round(tris_per, 2),
                      "algorithmic_gbs": round(n * bytes_per / (t * 1e-3) / 1e9, 1)}
     out["primary_hit_fraction"] = round(float(ok.float().mean()), 4)
+    if other is not None:
+        out["shadow_other_order"] = other
     return out
 
 
@@ -475,6 +492,37 @@ def bdpt_ao_leg(wl, torch, ctx, res=1024, spp=256, oracle_spp=2048, ao_res=(512,
            "oracle": f"BDPT in strict math (the reference's estimator, bit-exact per sample), {oracle_spp} spp, "
                      f"FP64 film, disjoint seeds ({oracle_s:.1f} s)",
            "oracle_noise_floor": float(((halves[0] - halves[1]) ** 2 / (r64 * r64 + 1e-2)).mean()) / 4}
+    # the radiance cache on the camera subpaths: BDPT over the paths of at most cache_t vertices
+    # after the camera, the cache's prediction at the cache_t-th eye vertex for the longer ones;
+    # trained online (path-traced training paths every frame), warm-up frames without an image
+    # included in the time
+    # the cache at the second eye vertex: deeper cache vertices on this scene sit mostly in the
+    # glass, where the path-traced training targets of caustic light are too noisy (measured at
+    # 512^2 x 64 spp against the same oracle: relMSE 0.042 at the 2nd vertex, 0.046 at the 3rd,
+    # 0.52 at the 4th, 6.4 at the 5th)
+    cache_t, warm = 2, 16
+    cache = wl.RadianceCache(ctx, scene, query_depth=cache_t)
+    cp = wl.render_params(res, res, warm, strategy=wl.STRATEGY_BDPT, max_depth=10, first_frame=30000000)
+    cache.reserve(cp)
+    cfilm = wl.Film(ctx, res, res, fp64=True)
+    ctx.sync()
+    e0.record(stream)
+    wl.render_nrc(ctx, scene, cam, cp, cache, None)
+    wl.render_nrc(ctx, scene, cam, wl.render_params(res, res, spp, strategy=wl.STRATEGY_BDPT, max_depth=10),
+                  cache, cfilm)
+    e1.record(stream)
+    e1.synchronize()
+    cms = e0.elapsed_time(e1)
+    cimg = cfilm.download64()
+    cst = cache.stats()
+    cfilm.close()
+    cache.close()
+    out["with_cache"] = {"cache_vertex": cache_t, "warmup_frames": warm, "spp": spp, "ms": round(cms, 1),
+                         "msamples_s": round(samples / cms / 1e3, 2), "relmse_vs_fp64_oracle": rel(cimg, r64),
+                         "train_samples_last_frame": cst["train_samples"],
+                         "note": "paths of at most cache_t vertices after the camera by BDPT, longer ones by "
+                                 "the cache at the cache_t-th eye vertex; time includes the warm-up frames "
+                                 "and every frame's training step"}
     # ambient occlusion, radius 0.1
     aw, ah = ao_res
     afilm = wl.Film(ctx, aw, ah)
@@ -847,7 +895,7 @@ def main():
                 line[key] = {"error": f"{type(e).__name__}: {e}"}
 
         if not args.no_raycast:
-            leg("raycast", lambda: raycast_microbench(wl, torch, ctx, sc, scene, stream))
+            leg("raycast", lambda: raycast_microbench(wl, torch, ctx, sc, scene, stream, tune))
         if world == 1:
             leg("progressive_1spp", lambda: graph_leg(wl, torch, ctx, sc, scene, stream))
             leg("cornell_config1", lambda: cornell_leg(wl, torch, ctx))

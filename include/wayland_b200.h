@@ -353,6 +353,8 @@ typedef struct wl_tune_result {
     float ms_tuned;             /* wave-size render with the chosen shape */
     uint32_t extend_postpone, shadow_postpone;  /* triangle phase when at least this many
                                                    32nds of a warp's busy lanes hold triangles */
+    uint32_t shadow_far_first;  /* 1: any-hit passes (shadow, connection and wl_cast_rays any-hit
+                                   rays) visit a node's children far to near; 0: near to far */
 } wl_tune_result;
 /* Times renders of (scene, camera, params with spp reduced) for candidate shapes by coordinate
  * descent and keeps the fastest in the context for later renders of every program: wave sizes
@@ -380,7 +382,7 @@ typedef struct wl_nrc_params {
     float per_level_scale;      /* resolution growth per level (1.38) */
     uint32_t train_paths;       /* training paths per frame (2^14; ~2^16 samples) */
     uint32_t query_depth;       /* surface vertex where other paths query the cache (2) */
-    float learning_rate;        /* Adam step size (1e-2) */
+    float learning_rate;        /* Adam step size (1e-2; 0 leaves the network as it is) */
     uint32_t seed;              /* initialisation */
     uint32_t train_extra;       /* training-path vertices past query_depth (3; 0 = full paths) */
 } wl_nrc_params;
@@ -394,7 +396,16 @@ WL_API int wl_nrc_destroy(wl_nrc *nrc);
  * without rendering or training. */
 WL_API int wl_nrc_reserve(wl_context *ctx, wl_nrc *nrc, const wl_render_params *params);
 /* Render params->spp frames with the cache (query, then train on the frame's samples). With
- * film == NULL the frames train the cache and leave no image (warm-up). */
+ * film == NULL the frames train the cache and leave no image (warm-up).
+ * params->strategy == WL_STRATEGY_BDPT puts the cache on the bidirectional program's camera
+ * subpaths (BDPT.cu:230-345 ends them instead): each frame renders one sample per pixel by
+ * BDPT over the paths of at most t = query_depth vertices after the camera (eye subpaths of t
+ * vertices, light subpaths of t - 1, the connections whose paths have at most t vertices, with
+ * the plain program's MIS weights), and every longer path is the cache's prediction at the
+ * eye subpath's t-th vertex times its throughput. The frame then trains the cache on
+ * path-traced (MIS) training paths of every (width x height / train_paths)-th pixel with their
+ * own random streams. Uniform light selection only; params->max_depth bounds the training
+ * paths. */
 WL_API int wl_render_nrc(wl_context *ctx, wl_scene *scene, const wl_camera *camera,
                          const wl_render_params *params, wl_nrc *nrc, wl_film *film);
 /* Network access for tests: inputs are n x 64 feature rows (FP32, device), outputs n x 4. */

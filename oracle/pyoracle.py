@@ -288,17 +288,18 @@ class Oracle:
         del keep
         return film, f64, rays
 
-    def render_bdpt(self, scene, cam, params, prec=0, threads=0, film=None, want64=False):
+    def render_bdpt(self, scene, cam, params, prec=0, threads=0, film=None, want64=False, max_len=0):
         """Bidirectional path tracer (BDPT.cu:42-567); returns (film_rgb[H,W,3] f32, film64 or
-        None, rays)."""
+        None, rays). max_len > 0 keeps only the paths of at most max_len vertices after the
+        camera (or_render_bdpt_len)."""
         W, H = params.width, params.height
         film = np.zeros((H, W, 3), np.float32) if film is None else film
         f64 = np.zeros((H, W, 3), np.float64) if want64 else None
         b = self.bvh_for(scene)
         keep, osc = make_or_scene(scene)
-        self.lib.or_render_bdpt.restype = C.c_uint64
-        rays = self.lib.or_render_bdpt(C.byref(osc), b.handle, C.byref(cam), C.byref(params), prec,
-                                       threads, ptr(film), ptr(f64))
+        self.lib.or_render_bdpt_len.restype = C.c_uint64
+        rays = self.lib.or_render_bdpt_len(C.byref(osc), b.handle, C.byref(cam), C.byref(params),
+                                           C.c_uint32(max_len), prec, threads, ptr(film), ptr(f64))
         del keep
         return film, f64, rays
 

@@ -1584,20 +1584,30 @@ template <class T> V3<T> bd_contribution(const SceneView &sv, const BdVertex<T> 
 }
 
 // One sample of __raygen__RenderFrame (BDPT.cu:522-560): the value added to the film.
+// max_len > 0 restricts the estimator to the paths of at most max_len vertices after the
+// camera (eye subpaths of max_len vertices, light subpaths of max_len - 1, connections with
+// i + j + 2 <= max_len): the bidirectional part of a render whose radiance cache takes the
+// longer paths (wl_render_nrc with WL_STRATEGY_BDPT).
 template <class T>
 V3<T> bd_sample(const SceneView &sv, const wl_camera &cam, const wl_render_params &P, uint32_t px,
-                uint32_t py, uint32_t frame, uint64_t &rays) {
+                uint32_t py, uint32_t frame, uint64_t &rays, uint32_t max_len = 0) {
     uint32_t pixel = P.width * py + px;
     Rng rng = make_rng(P.rng, P.seed, pixel, frame);
     BdVertex<T> E[WL_BDPT_MAX_VERTICES], Lp[WL_BDPT_MAX_VERTICES];
     V3<T> radiance(T(0));
-    uint32_t ne = bd_eye(sv, cam, P, px, py, rng, E, radiance, rays);
+    wl_render_params PE = P, PL = P;
+    if (max_len) {
+        PE.max_depth = max_len;
+        PL.max_depth = max_len > 1 ? max_len - 1 : 1;
+    }
+    uint32_t ne = bd_eye(sv, cam, PE, px, py, rng, E, radiance, rays);
     V3<T> out = V3<T>(T(0)) + radiance;
     if (ne == 0 || sv.s->nLight == 0) return out;
-    uint32_t nl = bd_light(sv, P, rng, Lp, rays);
+    uint32_t nl = bd_light(sv, PL, rng, Lp, rays);
     V3<T> conn(T(0));
     for (uint32_t i = 0; i < ne; ++i) {
         for (uint32_t j = 0; j < nl; ++j) {
+            if (max_len && i + j + 2 > max_len) continue;
             const BdVertex<T> &e = E[i], &l = Lp[j];
             V3<T> vis = l.pos - e.pos;
             T dist = length(vis);
@@ -1801,6 +1811,12 @@ uint64_t or_render_ao(const or_scene *scene, void *bvh, const wl_camera *cam,
 uint64_t or_render_bdpt(const or_scene *scene, void *bvh, const wl_camera *cam,
                         const wl_render_params *p, int prec, int threads, float *film_rgb,
                         double *film64) {
+    return or_render_bdpt_len(scene, bvh, cam, p, 0, prec, threads, film_rgb, film64);
+}
+
+uint64_t or_render_bdpt_len(const or_scene *scene, void *bvh, const wl_camera *cam,
+                            const wl_render_params *p, uint32_t max_len, int prec, int threads,
+                            float *film_rgb, double *film64) {
     SceneView sv;
     sv.s = scene;
     sv.bvh = (const OBvh *)bvh;
@@ -1823,10 +1839,10 @@ uint64_t or_render_bdpt(const or_scene *scene, void *bvh, const wl_camera *cam,
             uint32_t f = p->first_frame + s;
             double r[3];
             if (prec == 0) {
-                V3<float> o = bd_sample<float>(sv, *cam, *p, px, py, f, rays);
+                V3<float> o = bd_sample<float>(sv, *cam, *p, px, py, f, rays, max_len);
                 r[0] = o.x; r[1] = o.y; r[2] = o.z;
             } else {
-                V3<double> o = bd_sample<double>(sv, *cam, *p, px, py, f, rays);
+                V3<double> o = bd_sample<double>(sv, *cam, *p, px, py, f, rays, max_len);
                 r[0] = o.x; r[1] = o.y; r[2] = o.z;
             }
             // a sample that is not finite contributes 0 (the reference would keep a NaN in its

@@ -93,6 +93,12 @@ uint64_t or_render_ao(const or_scene *scene, void *bvh, const wl_camera *cam,
 uint64_t or_render_bdpt(const or_scene *scene, void *bvh, const wl_camera *cam,
                         const wl_render_params *p, int prec, int threads, float *film_rgb,
                         double *film64);
+/* The same restricted to the paths of at most max_len vertices after the camera (0: no
+ * restriction): eye subpaths of max_len vertices, light subpaths of max_len - 1, connections
+ * (i, j) with i + j + 2 <= max_len. */
+uint64_t or_render_bdpt_len(const or_scene *scene, void *bvh, const wl_camera *cam,
+                            const wl_render_params *p, uint32_t max_len, int prec, int threads,
+                            float *film_rgb, double *film64);
 
 /* relMSE = mean over pixels and channels of (I - R)^2 / (R^2 + eps) */
 double or_relmse(const float *img, const double *ref, uint64_t n, double eps);

@@ -145,7 +145,8 @@ void hb_export(void *p, uint64_t *morton, uint32_t *sorted, int *left, int *righ
     }
 }
 
-// rays: 8 floats each (org, tmin, dir, tmax); hits: 4 words (t, prim, u, v)
+// rays: 8 floats each (org, tmin, dir, tmax); hits: 4 words (t, prim, u, v). mode 0: closest
+// hit, 1: any hit, 2: any hit visiting children far to near
 void hb_cast(void *p, const float *rays, uint32_t n, uint32_t mode, float *hits, uint64_t *stats) {
     HostBvh *b = (HostBvh *)p;
     uint64_t cn = 0, ct = 0;
@@ -158,6 +159,10 @@ void hb_cast(void *p, const float *rays, uint32_t n, uint32_t mode, float *hits,
         } else if (mode == 1) {
             traverse<true, true>((const float4 *)b->nodes.data(), b->tris.data(), r[0], r[1], r[2],
                                  r[4], r[5], r[6], r[3], r[7], res, &a, &c);
+            if (res.prim != INVALID) res.prim = 0;
+        } else if (mode == 2) {
+            traverse<true, true, true>((const float4 *)b->nodes.data(), b->tris.data(), r[0], r[1], r[2],
+                                       r[4], r[5], r[6], r[3], r[7], res, &a, &c);
             if (res.prim != INVALID) res.prim = 0;
         } else {
             traverse<false, true>((const float4 *)b->nodes.data(), b->tris.data(), r[0], r[1], r[2],
@@ -176,13 +181,13 @@ void hb_cast(void *p, const float *rays, uint32_t n, uint32_t mode, float *hits,
 // The batched traversal of the GPU kernels (trav_node / trav_tri with the warp's phase choice
 // and refill of idle lanes), played for one simulated 32-lane warp in lock step. post: the
 // triangle-phase threshold in 32nds of the busy lanes; refill: idle lanes that trigger a fetch;
-// node_steps: node visits per lane in a node phase.
+// node_steps: node visits per lane in a node phase. mode 2: any hit, children far to near.
 void hb_cast_batched(void *p, const float *rays, uint32_t n, uint32_t mode, uint32_t post,
                      uint32_t refill, uint32_t node_steps, float *hits, uint64_t *stats) {
     HostBvh *b = (HostBvh *)p;
     const float4 *nodes = (const float4 *)b->nodes.data();
     const float4 *tris = b->tris.data();
-    const bool any = mode == 1;
+    const bool any = mode != 0, far = mode == 2;
     std::vector<TravState> st(32);
     std::vector<uint2> stack(32 * (size_t)TRAV_STACK);
     bool active[32] = {}, exhausted[32] = {}, has_t[32], can_n[32], fin[32];
@@ -212,6 +217,7 @@ void hb_cast_batched(void *p, const float *rays, uint32_t n, uint32_t mode, uint
                 if (next < n) {
                     const float *r = rays + 8 * (size_t)next;
                     trav_init(st[l], r[0], r[1], r[2], r[4], r[5], r[6], r[3], r[7]);
+                    if (far) trav_root<true>(st[l]);
                     my[l] = next++;
                     active[l] = true;
                     busy |= 1u << l;
@@ -245,9 +251,13 @@ void hb_cast_batched(void *p, const float *rays, uint32_t n, uint32_t mode, uint
             // a node phase: up to node_steps visits per lane (the kernels' NODE_STEPS)
             for (int l = 0; l < 32; l++) {
                 const ArrayStack stk{stack.data() + (size_t)l * TRAV_STACK};
-                if (can_n[l]) trav_node<true>(st[l], stk, nodes, &cn);
+                auto visit = [&]() {
+                    if (far) trav_node<true, true>(st[l], stk, nodes, &cn);
+                    else trav_node<true>(st[l], stk, nodes, &cn);
+                };
+                if (can_n[l]) visit();
                 for (uint32_t k = 1; k < node_steps; k++)
-                    if (active[l] && trav_can_node(st[l])) trav_node<true>(st[l], stk, nodes, &cn);
+                    if (active[l] && trav_can_node(st[l])) visit();
             }
         }
         for (int l = 0; l < 32; l++) {

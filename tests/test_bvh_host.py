@@ -55,6 +55,8 @@ def test_closest_hit_bitexact(host_bvh, oracle, name, V, I):
     anyg, _ = host_cast(host_bvh, h, rays, 1)
     anyr = oracle.cast_bruteforce(V, I, rays, 1)
     assert np.array_equal(anyg["prim"] == po.np.uint32(0xFFFFFFFF), anyr["prim"] == 0xFFFFFFFF)
+    anyf, _ = host_cast(host_bvh, h, rays, 2)  # children far to near
+    assert np.array_equal(anyf["prim"] == po.np.uint32(0xFFFFFFFF), anyr["prim"] == 0xFFFFFFFF)
     host_bvh.hb_destroy(h)
 
 
@@ -111,4 +113,7 @@ def test_batched_traversal_matches(host_bvh, oracle, post, refill, node_steps):
     anyr = oracle.cast_bruteforce(V, I, rays, 1)
     anyg, _ = host_cast_batched(host_bvh, h, rays, 1, post, refill, node_steps)
     assert np.array_equal(anyg["prim"] == 0xFFFFFFFF, anyr["prim"] == 0xFFFFFFFF)
+    # any hit with children visited far to near (the shadow pass's tunable order): same answers
+    anyf, _ = host_cast_batched(host_bvh, h, rays, 2, post, refill, node_steps)
+    assert np.array_equal(anyf["prim"] == 0xFFFFFFFF, anyr["prim"] == 0xFFFFFFFF)
     host_bvh.hb_destroy(h)

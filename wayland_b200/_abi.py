@@ -78,7 +78,8 @@ class TuneResult(C.Structure):
                 ("extend_refill", C.c_uint32), ("shadow_ctas_per_sm", C.c_uint32),
                 ("shadow_refill", C.c_uint32), ("candidates", C.c_uint32), ("spp", C.c_uint32),
                 ("ms_default", C.c_float), ("ms_tuned", C.c_float),
-                ("extend_postpone", C.c_uint32), ("shadow_postpone", C.c_uint32)]
+                ("extend_postpone", C.c_uint32), ("shadow_postpone", C.c_uint32),
+                ("shadow_far_first", C.c_uint32)]
 
 
 class RenderStats(C.Structure):

@@ -241,6 +241,7 @@ int ensure_bdpt(wl_context *c, uint32_t cap, uint32_t maxv) {
     BdptWave &b = c->bd;
     if (c->bd_block && b.cap >= cap && b.maxv >= maxv) {
         b.maxv = maxv;  // the vertex arrays keep their allocated stride (cap)
+        b.maxl = maxv;
         return WL_OK;
     }
     if (c->bd_block) {
@@ -259,6 +260,7 @@ int ensure_bdpt(wl_context *c, uint32_t cap, uint32_t maxv) {
     b = BdptWave{};
     b.cap = cap;
     b.maxv = maxv;
+    b.maxl = maxv;
     float4 **vs[10] = {&b.eye.a, &b.eye.b, &b.eye.c, &b.eye.d, &b.eye.e,
                        &b.lit.a, &b.lit.b, &b.lit.c, &b.lit.d, &b.lit.e};
     for (auto v : vs) { *v = (float4 *)p; p += vtx; }
@@ -680,7 +682,7 @@ int wl_cast_rays(wl_scene *s, const wl_ray *d_rays, wl_hit *d_hits, uint32_t n, 
     ARG(((uintptr_t)d_rays & 15) == 0 && ((uintptr_t)d_hits & 15) == 0, "buffers must be 16-byte aligned");
     CK(cudaSetDevice(s->ctx->device));
     const TraceTune &tt = mode == WL_CAST_ANY ? s->ctx->tune_shadow : s->ctx->tune_extend;
-    launch_cast(dev_scene(s), d_rays, d_hits, n, mode, s->ctx->d_misc, tt.postpone, s->ctx->stream);
+    launch_cast(dev_scene(s), d_rays, d_hits, n, mode, s->ctx->d_misc, tt.postpone, tt.far_first, s->ctx->stream);
     CK(cudaGetLastError());
     return WL_OK;
 }
@@ -714,7 +716,7 @@ int wl_cast_rays_stats(wl_scene *s, const wl_ray *d_rays, uint32_t n, uint32_t m
     if (!s->built) return fail(WL_ERR_NOT_BUILT, "bvh not built");
     CK(cudaSetDevice(s->ctx->device));
     launch_cast_stats(dev_scene(s), d_rays, n, mode, s->ctx->d_cast_counts, s->ctx->d_misc,
-                      s->ctx->stream);
+                      mode == WL_CAST_ANY ? s->ctx->tune_shadow.far_first : 0u, s->ctx->stream);
     CK(cudaGetLastError());
     unsigned long long h[2];
     CK(cudaMemcpyAsync(h, s->ctx->d_cast_counts, sizeof(h), cudaMemcpyDeviceToHost, s->ctx->stream));
@@ -960,11 +962,15 @@ static int replay_wave(wl_context *c, wl_context::GraphEntry *g, uint64_t base, 
 // One wave of the bidirectional path tracer (BDPT.cu:522-560 for wp.count samples): eye
 // subpaths, light subpaths, connections, connection rays, film. Returns the launches issued.
 // Event categories: 0 closest-hit passes, 1 vertex and connection kernels, 2 connection rays,
-// 3 the rest.
+// 3 the rest. With a radiance cache (bw.queries set, cache non-null), the last eye vertices'
+// queries are answered into the samples' eye-path radiance before the film.
+struct BdCache {
+    NrcNet *net;
+    const wl_disney *mats;
+};
 static uint32_t bdpt_wave(wl_context *c, const WaveParams &wp, const DevScene &sc, const Film &film,
-                          bool strict_math, bool tstats) {
+                          bool strict_math, bool tstats, const BdptWave &bw, const BdCache *cache = nullptr) {
     cudaStream_t st = c->stream;
-    BdptWave &bw = c->bd;
     uint32_t launches = 0;
     rec(c, 3, true);
     if (strict_math) strict::launch_bdpt_eye_gen(wp, c->q, bw, st);
@@ -991,7 +997,7 @@ static uint32_t bdpt_wave(wl_context *c, const WaveParams &wp, const DevScene &s
     rec(c, 1, false);
     launches++;
     in = 0;
-    for (uint32_t d = 2; d <= bw.maxv; d++) {
+    for (uint32_t d = 2; d <= bw.maxl; d++) {
         rec(c, 0, true);
         launch_extend(sc, c->q, in, tstats, st, c->tune_extend);
         rec(c, 0, false);
@@ -1014,6 +1020,10 @@ static uint32_t bdpt_wave(wl_context *c, const WaveParams &wp, const DevScene &s
     rec(c, 2, true);
     launch_connection_rays(sc, c->q, bw, tstats, st, c->tune_shadow);
     rec(c, 2, false);
+    if (cache && bw.queries) {
+        nrc_query(cache->net, cache->mats, bw.queries, bw.n_queries, c->q.st_rad, wp.count, st);
+        launches += 2;
+    }
     rec(c, 3, true);
     strict::launch_bdpt_film(wp, sc, c->q, bw, film, st);
     rec(c, 3, false);
@@ -1086,7 +1096,7 @@ int wl_render(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_
         wp.base = base;
         wp.count = (uint32_t)((total - base) < wave ? (total - base) : wave);
         if (!graph) {
-            launches += bdpt ? bdpt_wave(c, wp, sc, f->f, strict_math, tstats)
+            launches += bdpt ? bdpt_wave(c, wp, sc, f->f, strict_math, tstats, c->bd)
                              : pt_wave(c, wp, sc, f->f, p->max_depth, strict_math, tstats);
         } else {
             // every wave of this shape (and every later call with the same arguments) replays
@@ -1114,7 +1124,7 @@ int wl_render(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_
             wl_context::GraphEntry *g = nullptr;
             int rc2 = cached_graph(c, key, true, [&]() -> uint32_t {
                 strict::launch_wave_begin(0, 0, c->d_dyn_cur, st);
-                return 1 + (bdpt ? bdpt_wave(c, gp, sc, f->f, strict_math, false)
+                return 1 + (bdpt ? bdpt_wave(c, gp, sc, f->f, strict_math, false, c->bd)
                                  : pt_wave(c, gp, sc, f->f, p->max_depth, strict_math, false));
             }, &g);
             if (rc2 != WL_OK) return rc2;
@@ -1391,7 +1401,7 @@ int wl_nrc_create(wl_context *c, wl_scene *s, const wl_nrc_params *p, wl_nrc **o
     ARG(p->levels >= 1 && p->levels <= 16, "levels must be in [1, 16]");
     ARG(p->log2_table >= 8 && p->log2_table <= 24, "log2_table must be in [8, 24]");
     ARG(p->base_resolution >= 2 && p->per_level_scale >= 1.0f && p->per_level_scale <= 4.0f, "bad grid resolution");
-    ARG(p->train_paths >= 1 && p->query_depth >= 1 && p->learning_rate > 0.f, "bad training parameters");
+    ARG(p->train_paths >= 1 && p->query_depth >= 1 && p->learning_rate >= 0.f, "bad training parameters");
     CK(cudaSetDevice(c->device));
     std::vector<float> V(3 * (size_t)s->nV);
     float lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
@@ -1638,6 +1648,128 @@ int wl_nrc_reserve(wl_context *c, wl_nrc *n, const wl_render_params *p) {
     return nrc_prepare(c, n, p, wave, stride);
 }
 
+// One path-tracing wave of wl_render_nrc: camera rays, bounces (the shadow pass of bounce b
+// overlapping the extension rays of bounce b + 1, one reset launch per bounce zeroing the
+// counters, as pt_wave), then the cache's answers to the wave's queries and the training
+// samples of its training paths, then the film (f non-null).
+static int nrc_pt_wave(wl_context *c, wl_nrc *n, const WaveParams &wp, const NrcWaveBuffers &nb,
+                       const DevScene &sc, bool strict_math, uint32_t tcount, const wl_film *f) {
+    cudaStream_t st = c->stream;
+    CK(cudaMemsetAsync(n->n_queries, 0, 4, st));
+    if (tcount) CK(cudaMemsetAsync(n->rec_count, 0, sizeof(uint32_t) * tcount, st));
+    if (strict_math) strict::launch_generate(wp, c->q, st);
+    else fast::launch_generate(wp, c->q, st);
+    int in = 0;
+    // every path has ended by vertex train_end when training paths end at the cache
+    const uint32_t bounces = nb.train_end && nb.train_end < wp.max_depth ? nb.train_end : wp.max_depth;
+    cudaEvent_t join_prev = nullptr;
+    launch_reset_counters(c->q.counters, (1u << 6) | (1u << 7), st);
+    for (uint32_t b = 0; b < bounces; b++) {
+        launch_extend(sc, c->q, in, false, st, c->tune_extend, BatchView{}, false);
+        if (join_prev) CK(cudaStreamWaitEvent(st, join_prev, 0));
+        launch_reset_counters(c->q.counters, (1u << (in ^ 1)) | (1u << 2) | (1u << 6) | (1u << 7), st);
+        if (strict_math) strict::launch_shade_nrc(wp, sc, c->q, in, nb, st);
+        else fast::launch_shade_nrc(wp, sc, c->q, in, nb, st);
+        cudaEvent_t fk, jn;
+        fork_join(c, b, fk, jn);
+        CK(cudaEventRecord(fk, st));
+        CK(cudaStreamWaitEvent(c->side, fk, 0));
+        launch_shadow(sc, c->q, false, c->side, c->tune_shadow, BatchView{}, false);
+        CK(cudaEventRecord(jn, c->side));
+        join_prev = jn;
+        in ^= 1;
+    }
+    if (join_prev) CK(cudaStreamWaitEvent(st, join_prev, 0));
+    nrc_query(n->net, n->scene->d_mats, n->queries, n->n_queries, c->q.st_rad, wp.count, st);
+    nrc_collect(n->net, nb, c->q, tcount, st);
+    if (f) strict::launch_film(wp, c->q, f->f, st);
+    CK(cudaGetLastError());
+    return WL_OK;
+}
+
+// Cache buffers of a wave whose training paths are the samples g of the frame with
+// g % stride == first_g % stride.
+static NrcWaveBuffers nrc_wave_buffers(const wl_nrc *n, uint32_t stride, uint64_t first_g, uint32_t max_depth) {
+    NrcWaveBuffers nb{};
+    nb.query_depth = n->p.query_depth;
+    nb.train_stride = stride;
+    nb.first_g = first_g;
+    nb.max_depth = max_depth;
+    nb.train_end = n->p.train_extra ? n->p.query_depth + n->p.train_extra : 0u;
+    nb.queries = n->queries;
+    nb.n_queries = n->n_queries;
+    nb.rec_v = n->rec_v; nb.rec_tr = n->rec_tr; nb.rec_rb = n->rec_rb;
+    nb.rec_count = n->rec_count; nb.rec_slot = n->rec_slot;
+    return nb;
+}
+
+// Bidirectional frames with the cache on the camera subpaths. Each frame renders one sample
+// per pixel by BDPT restricted to paths of at most t = query_depth vertices after the camera
+// (eye subpaths of t vertices, light subpaths of t - 1, connections with i + j + 2 <= t): for
+// those paths the estimator, its strategies and MIS weights are the plain BDPT's. Every longer
+// path continues some eye subpath past its t-th vertex, and the cache's prediction of the
+// radiance leaving that vertex towards the previous one, times the subpath's throughput, stands
+// for all of them. Then the frame trains the cache on path-traced training paths (every
+// stride-th pixel, own random streams) as wl_render_nrc does for the path tracer.
+static int nrc_bdpt_frames(wl_context *c, wl_scene *s, const wl_render_params *p, wl_nrc *n, wl_film *f,
+                           WaveParams wp, uint64_t wave, uint32_t stride) {
+    cudaStream_t st = c->stream;
+    const bool strict_math = p->math == WL_MATH_STRICT;
+    const uint32_t npix = wp.npix;
+    uint32_t t = n->p.query_depth < 1 ? 1 : n->p.query_depth;
+    if (t > WL_BDPT_MAX_VERTICES) t = WL_BDPT_MAX_VERTICES;
+    uint64_t bwave = auto_bdpt_wave(c, t);
+    if (bwave > wave) bwave = wave;
+    int rc = ensure_bdpt(c, (uint32_t)bwave, t);
+    if (rc != WL_OK) return rc;
+    BdptWave bw = c->bd;
+    bw.maxv = t;
+    bw.maxl = t > 1 ? t - 1 : 1;
+    bw.max_len = t;
+    bw.queries = n->queries;
+    bw.n_queries = n->n_queries;
+    const BdCache cache{n->net, s->d_mats};
+    DevScene sc = dev_scene(s);
+    uint32_t *ncnt = nrc_counters(n->net);
+    for (uint32_t fr = 0; fr < p->spp; fr++) {
+        const uint32_t frame = p->first_frame + fr;
+        if (f) {
+            WaveParams bp = wp;
+            bp.first_frame = frame;
+            bp.strategy = WL_STRATEGY_BDPT;
+            for (uint64_t base = 0; base < npix; base += bwave) {
+                bp.base = base;
+                bp.count = (uint32_t)((npix - base) < bwave ? (npix - base) : bwave);
+                CK(cudaMemsetAsync(n->n_queries, 0, 4, st));
+                bdpt_wave(c, bp, sc, f->f, strict_math, false, bw, &cache);
+            }
+        }
+        // training paths of this frame (path traced with MIS, decorrelated from the image's
+        // samples by their frame number): pixels offset, offset + stride, ...
+        const uint32_t offset = (uint32_t)(splitmix64(frame * 0x9E3779B97F4A7C15ULL + n->p.seed) % stride);
+        const uint32_t tcount = (npix - 1 - offset) / stride + 1;
+        // as many training paths per wave as the training records hold
+        const uint32_t chunk = n->t_cap - 2 < (uint32_t)wave ? n->t_cap - 2 : (uint32_t)wave;
+        WaveParams tp = wp;
+        tp.strategy = WL_STRATEGY_MIS;
+        tp.first_frame = frame ^ 0x80000000u;
+        tp.gstride = stride;
+        CK(cudaMemsetAsync(ncnt, 0, 8, st));
+        for (uint32_t done = 0; done < tcount; done += chunk) {
+            tp.base = offset + (uint64_t)done * stride;
+            tp.count = tcount - done < chunk ? tcount - done : chunk;
+            rc = nrc_pt_wave(c, n, tp, nrc_wave_buffers(n, stride, tp.base, p->max_depth), sc, strict_math,
+                             tp.count, nullptr);
+            if (rc != WL_OK) return rc;
+        }
+        if (nrc_train_collected(n->net, s->d_mats, st) != WL_OK)
+            return fail(WL_ERR_OOM, "radiance-cache training scratch could not be allocated");
+        CK(cudaGetLastError());
+    }
+    if (f) f->f.frames64 += p->spp;
+    return WL_OK;
+}
+
 int wl_render_nrc(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_render_params *p,
                   wl_nrc *n, wl_film *f) {
     ARG(c && s && cam && p && n, "null argument");
@@ -1645,8 +1777,10 @@ int wl_render_nrc(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_ren
     if (!s->built) return fail(WL_ERR_NOT_BUILT, "bvh not built");
     ARG(!f || (p->width == f->f.W && p->height == f->f.H), "film size differs from the render size");
     ARG(p->spp > 0 && p->max_depth > 0 && p->max_depth <= 1024, "bad spp or max_depth");
-    ARG(p->strategy <= WL_STRATEGY_MIS && p->rng <= WL_RNG_PCG32 && p->math <= WL_MATH_STRICT, "bad params");
+    ARG(p->strategy <= WL_STRATEGY_BDPT && p->rng <= WL_RNG_PCG32 && p->math <= WL_MATH_STRICT, "bad params");
     ARG(p->lights <= WL_LIGHTS_POWER, "bad light selection");
+    ARG(p->strategy != WL_STRATEGY_BDPT || p->lights == WL_LIGHTS_UNIFORM,
+        "the bidirectional program samples lights uniformly (BDPT.cu:341-366)");
     ARG(finite3(cam->pos) && finite3(cam->look_at) && finite3(cam->up) && finite3(cam->right), "non-finite camera");
     CK(cudaSetDevice(c->device));
     c->stats_pending = false;
@@ -1667,6 +1801,7 @@ int wl_render_nrc(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_ren
     }
     wp.has_env = (p->env[0] != 0.f || p->env[1] != 0.f || p->env[2] != 0.f) ? 1u : 0u;
     wp.sort_materials = (p->flags & WL_RENDER_SORT_MATERIALS) ? 1u : 0u;
+    if (p->strategy == WL_STRATEGY_BDPT) return nrc_bdpt_frames(c, s, p, n, f, wp, wave, stride);
     DevScene sc = dev_scene(s);
     cudaStream_t st = c->stream;
     const bool strict_math = p->math == WL_MATH_STRICT;
@@ -1682,47 +1817,8 @@ int wl_render_nrc(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_ren
             wp.count = (uint32_t)((npix - base) < wave ? (npix - base) : wave);
             uint64_t first_g = base + ((offset + stride - (base % stride)) % stride);
             uint32_t tcount = first_g < base + wp.count ? (uint32_t)((base + wp.count - 1 - first_g) / stride + 1) : 0;
-            NrcWaveBuffers nb{};
-            nb.query_depth = n->p.query_depth;
-            nb.train_stride = stride;
-            nb.first_g = first_g;
-            nb.max_depth = p->max_depth;
-            nb.train_end = n->p.train_extra ? n->p.query_depth + n->p.train_extra : 0u;
-            nb.queries = n->queries;
-            nb.n_queries = n->n_queries;
-            nb.rec_v = n->rec_v; nb.rec_tr = n->rec_tr; nb.rec_rb = n->rec_rb;
-            nb.rec_count = n->rec_count; nb.rec_slot = n->rec_slot;
-            CK(cudaMemsetAsync(n->n_queries, 0, 4, st));
-            if (tcount) CK(cudaMemsetAsync(n->rec_count, 0, sizeof(uint32_t) * tcount, st));
-            if (strict_math) strict::launch_generate(wp, c->q, st);
-            else fast::launch_generate(wp, c->q, st);
-            int in = 0;
-            // every path has ended by vertex train_end when training paths end at the cache
-            const uint32_t bounces = nb.train_end && nb.train_end < p->max_depth ? nb.train_end : p->max_depth;
-            // the shadow pass of bounce b overlaps the extension rays of bounce b + 1, and one
-            // reset launch per bounce zeroes the counters (as pt_wave)
-            cudaEvent_t join_prev = nullptr;
-            launch_reset_counters(c->q.counters, (1u << 6) | (1u << 7), st);
-            for (uint32_t b = 0; b < bounces; b++) {
-                launch_extend(sc, c->q, in, false, st, c->tune_extend, BatchView{}, false);
-                if (join_prev) CK(cudaStreamWaitEvent(st, join_prev, 0));
-                launch_reset_counters(c->q.counters, (1u << (in ^ 1)) | (1u << 2) | (1u << 6) | (1u << 7), st);
-                if (strict_math) strict::launch_shade_nrc(wp, sc, c->q, in, nb, st);
-                else fast::launch_shade_nrc(wp, sc, c->q, in, nb, st);
-                cudaEvent_t fk, jn;
-                fork_join(c, b, fk, jn);
-                CK(cudaEventRecord(fk, st));
-                CK(cudaStreamWaitEvent(c->side, fk, 0));
-                launch_shadow(sc, c->q, false, c->side, c->tune_shadow, BatchView{}, false);
-                CK(cudaEventRecord(jn, c->side));
-                join_prev = jn;
-                in ^= 1;
-            }
-            if (join_prev) CK(cudaStreamWaitEvent(st, join_prev, 0));
-            nrc_query(n->net, s->d_mats, n->queries, n->n_queries, c->q.st_rad, wp.count, st);
-            nrc_collect(n->net, nb, c->q, tcount, st);
-            if (f) strict::launch_film(wp, c->q, f->f, st);
-            CK(cudaGetLastError());
+            rc = nrc_pt_wave(c, n, wp, nrc_wave_buffers(n, stride, first_g, p->max_depth), sc, strict_math, tcount, f);
+            if (rc != WL_OK) return rc;
         }
         // clamp the sample count to the buffer and train one step on the frame's samples
         if (nrc_train_collected(n->net, s->d_mats, st) != WL_OK)
@@ -1812,6 +1908,16 @@ int wl_autotune(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_rende
             }
         t = bt;
     }
+    if (rc == WL_OK) {
+        // any-hit child order: far to near against near to far
+        TraceTune &t = c->tune_shadow;
+        const TraceTune bt = t;
+        t.far_first = bt.far_first ? 0u : 1u;
+        float ms = 0.f;
+        rc = timed(q, ms);
+        if (rc == WL_OK && ms < best) best = ms;
+        else t = bt;
+    }
     const uint32_t posts[] = {4u, 8u, 12u, 16u, 20u};
     for (int pass = 0; pass < 2 && rc == WL_OK; pass++) {
         TraceTune &t = pass == 0 ? c->tune_extend : c->tune_shadow;
@@ -1842,6 +1948,7 @@ int wl_autotune(wl_context *c, wl_scene *s, const wl_camera *cam, const wl_rende
     out->shadow_refill = c->tune_shadow.refill;
     out->extend_postpone = c->tune_extend.postpone;
     out->shadow_postpone = c->tune_shadow.postpone;
+    out->shadow_far_first = c->tune_shadow.far_first;
     out->candidates = candidates;
     out->ms_default = ms_default;
     out->ms_tuned = ms_tuned;
@@ -1861,6 +1968,7 @@ int wl_set_tune(wl_context *c, const wl_tune_result *t) {
     ARG(ok_refill(t->extend_refill) && ok_refill(t->shadow_refill), "refill must be 4, 6, 8, 12, 16 or 24");
     ARG(t->extend_postpone <= 32 && t->shadow_postpone <= 32, "postpone must be in [0, 32]");
     ARG(t->wave_paths == 0 || (t->wave_paths >= 1024 && t->wave_paths <= (1u << 27)), "wave_paths out of range");
+    ARG(t->shadow_far_first <= 1, "shadow_far_first must be 0 or 1");
     c->tune_wave = t->wave_paths;
     c->tune_extend.ctas_per_sm = t->extend_ctas_per_sm;
     c->tune_extend.refill = t->extend_refill;
@@ -1868,6 +1976,7 @@ int wl_set_tune(wl_context *c, const wl_tune_result *t) {
     c->tune_shadow.refill = t->shadow_refill;
     c->tune_extend.postpone = t->extend_postpone;
     c->tune_shadow.postpone = t->shadow_postpone;
+    c->tune_shadow.far_first = t->shadow_far_first;
     return WL_OK;
 }
 

@@ -226,9 +226,10 @@ __global__ void __launch_bounds__(PT) k_bd_eye(WaveParams wp, DevScene sc, Queue
     const uint32_t cap = bw.cap;
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
         uint32_t i = base + threadIdx.x;
-        bool push = false;
+        bool push = false, query = false;
         uint32_t slot = 0;
         v3 npos, ndir;
+        BdV e;
         if (i < n) {
             slot = q.ray_slot[in][i];
             float4 h = q.hit[i];
@@ -236,7 +237,6 @@ __global__ void __launch_bounds__(PT) k_bd_eye(WaveParams wp, DevScene sc, Queue
             v3 org = f4xyz(q.ray_o[in][i]), dir = f4xyz(q.ray_d[in][i]);
             if (__float_as_uint(h.y) != INVALID) {
                 const uint32_t v = depth - 1;
-                BdV e;
                 uint32_t lid;
                 bd_surface(sc, h, org, dir, e, lid);
                 e.wi = -dir;
@@ -291,6 +291,9 @@ __global__ void __launch_bounds__(PT) k_bd_eye(WaveParams wp, DevScene sc, Queue
                     q.st_rng[slot] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
                     npos = e.pos;
                     push = depth < bw.maxv;
+                    // with a radiance cache, the last eye vertex asks the cache for the radiance
+                    // of the paths longer than bw.max_len that continue from it
+                    query = bw.queries != nullptr && depth == bw.maxv;
                 }
             }
         }
@@ -299,6 +302,17 @@ __global__ void __launch_bounds__(PT) k_bd_eye(WaveParams wp, DevScene sc, Queue
             q.ray_o[out][pos] = make_float4(npos.x, npos.y, npos.z, wp.eps);
             q.ray_d[out][pos] = make_float4(ndir.x, ndir.y, ndir.z, 1e30f);
             q.ray_slot[out][pos] = slot;
+        }
+        if (bw.queries != nullptr) {
+            uint32_t qpos = warp_append(query, bw.n_queries);
+            if (query) {
+                NrcVertex rv;
+                rv.pos_mat = make_float4(e.pos.x, e.pos.y, e.pos.z, __uint_as_float(e.id));
+                rv.wo = make_float4(e.wi.x, e.wi.y, e.wi.z, 0.f);
+                rv.n = make_float4(e.ns.x, e.ns.y, e.ns.z, 0.f);
+                rv.extra = make_float4(e.tput.x, e.tput.y, e.tput.z, __uint_as_float(slot));
+                bw.queries[qpos] = rv;
+            }
         }
         uint32_t nv = __popc(__ballot_sync(0xffffffffu, i < n));
         if ((threadIdx.x & 31) == 0 && nv) atomicAdd(&q.totals[0], (unsigned long long)nv);
@@ -357,7 +371,7 @@ __global__ void __launch_bounds__(PT) k_bd_light_gen(WaveParams wp, DevScene sc,
             bd_store(bw.lit, cap, 0, slot, l);
             bw.n_light[slot] = 1;
             q.st_rng[slot] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
-            push = bw.maxv > 1;
+            push = bw.maxl > 1;
         }
         uint32_t pos = warp_append(push, &q.counters[0]);
         if (push) {
@@ -415,7 +429,7 @@ __global__ void __launch_bounds__(PT) k_bd_light(WaveParams wp, DevScene sc, Que
                     }
                     bd_store(bw.lit, cap, vi, slot, v);
                     bw.n_light[slot] = depth;
-                    if (depth < bw.maxv) {  // no random number is used after the light subpath
+                    if (depth < bw.maxl) {  // no random number is used after the light subpath
                         Rng rng = bd_rng(wp, q, slot);
                         Mat m = load_mat(sc.mats + v.id);
                         ndir = normalize(sample_disney(m, v.ns, v.wi, rng));
@@ -452,28 +466,32 @@ __global__ void __launch_bounds__(PT) k_bd_connect(WaveParams wp, DevScene sc, Q
             uint32_t c = t - bw.conn_first[slot];
             uint32_t nl = bw.n_light[slot];
             uint32_t i = c / nl, j = c - (c / nl) * nl;
-            BdV e = bd_load(bw.eye, cap, i, slot), l = bd_load(bw.lit, cap, j, slot);
-            vis = l.pos - e.pos;
-            float dist = length(vis);
-            vis = vis / dist;
             bw.conn_val[t] = make_float4(0.f, 0.f, 0.f, 0.f);
-            const bool l_is_light = (l.id & BD_LIGHT) != 0;
-            bool facing = true;
-            if (l_is_light && !sc.lights[l.id & ~BD_LIGHT].two_sided && dot(l.ns, vis) > 0.0f) facing = false;
-            if (facing) {
-                Mat me = load_mat(sc.mats + e.id);
-                v3 fe = eval_disney(me, e.ns, e.ng, e.wi, vis, v3(1.f));
-                v3 cv = e.tput * fe * fabsf(dot(e.ns, vis)) * fabsf(dot(l.ns, vis)) * l.tput / (dist * dist);
-                if (!l_is_light) {
-                    Mat ml = load_mat(sc.mats + l.id);
-                    cv = cv * eval_disney(ml, l.ns, l.ng, -vis, l.wi, v3(1.f));
-                }
-                if (cv.x + cv.y + cv.z > 1e-10f) {
-                    float lp0 = bw.lit.d[slot].w;  // light vertex pdf_light
-                    val = cv * bd_mis(sc, bw, slot, (int)i, (int)j, lp0);
-                    org = e.pos;
-                    tmax = dist * (1.0f - wp.eps);
-                    push = true;
+            // with a radiance cache, a path longer than max_len (i + j + 2 vertices after the
+            // camera) is the cache's at the last eye vertex
+            if (bw.max_len == 0 || i + j + 2 <= bw.max_len) {
+                BdV e = bd_load(bw.eye, cap, i, slot), l = bd_load(bw.lit, cap, j, slot);
+                vis = l.pos - e.pos;
+                float dist = length(vis);
+                vis = vis / dist;
+                const bool l_is_light = (l.id & BD_LIGHT) != 0;
+                bool facing = true;
+                if (l_is_light && !sc.lights[l.id & ~BD_LIGHT].two_sided && dot(l.ns, vis) > 0.0f) facing = false;
+                if (facing) {
+                    Mat me = load_mat(sc.mats + e.id);
+                    v3 fe = eval_disney(me, e.ns, e.ng, e.wi, vis, v3(1.f));
+                    v3 cv = e.tput * fe * fabsf(dot(e.ns, vis)) * fabsf(dot(l.ns, vis)) * l.tput / (dist * dist);
+                    if (!l_is_light) {
+                        Mat ml = load_mat(sc.mats + l.id);
+                        cv = cv * eval_disney(ml, l.ns, l.ng, -vis, l.wi, v3(1.f));
+                    }
+                    if (cv.x + cv.y + cv.z > 1e-10f) {
+                        float lp0 = bw.lit.d[slot].w;  // light vertex pdf_light
+                        val = cv * bd_mis(sc, bw, slot, (int)i, (int)j, lp0);
+                        org = e.pos;
+                        tmax = dist * (1.0f - wp.eps);
+                        push = true;
+                    }
                 }
             }
         }

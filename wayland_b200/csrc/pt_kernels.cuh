@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(PT) k_generate(WaveParams wp, Queues q) {
         q.counters[2] = 0;
     }
     if (i >= wp.count) return;
-    uint64_t g = wp.base + i;
+    uint64_t g = wp.base + (uint64_t)i * (wp.gstride > 1u ? wp.gstride : 1u);
     uint32_t pixel = (uint32_t)(g % wp.npix);
     uint32_t frame = wp.first_frame + (uint32_t)(g / wp.npix);
     uint32_t px = pixel % wp.W, py = pixel / wp.W;
@@ -147,7 +147,8 @@ __device__ __forceinline__ void shade_lane(const WaveParams &wp, const DevScene 
             v3 thr = f4xyz(thr4), term = f4xyz(term4), rad = f4xyz(rad4);
             float last_pdf = thr4.w;
             uint32_t depth = __float_as_uint(term4.w);
-            uint64_t g = wp.base + slot;
+            // a cache training wave traces every gstride-th sample only
+            uint64_t g = wp.base + (NRC && wp.gstride > 1u ? (uint64_t)slot * wp.gstride : (uint64_t)slot);
             Rng rng;
             rng.mode = wp.rng;
             rng.pixel = (uint32_t)(g % wp.npix);
@@ -309,7 +310,11 @@ __device__ __forceinline__ void shade_lane(const WaveParams &wp, const DevScene 
                                 sh_d = vis;
                                 sh_tmax = dist * (1.0f - wp.eps);
                                 new_o = hit_pos;
-                                push_shadow = true;
+                                // a light sample of exactly zero (the BSDF has no lobe towards
+                                // the light, or the throughput is zero) adds +0 whether or not
+                                // its ray is occluded, so its ray is not traced; NaN samples
+                                // still are
+                                push_shadow = !(ld.x == 0.0f && ld.y == 0.0f && ld.z == 0.0f);
                             }
                         }
                         // Russian roulette (PathTracing.cu:130-138)

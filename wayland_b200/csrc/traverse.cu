@@ -69,7 +69,7 @@ struct SplitStack {
 // lanes holding triangles are at least post/32 of the busy lanes (or no lane can visit a node),
 // kept up while that holds; otherwise a node phase of up to NODE_STEPS node visits per lane.
 // Returns true for a lane whose ray finished.
-template <bool ANY, bool STATS>
+template <bool ANY, bool STATS, bool FAR>
 __device__ __forceinline__ bool warp_trav(bool active, uint32_t busy, uint32_t post, TravState &st,
                                           const SplitStack &stack, const float4 *__restrict__ nodes,
                                           const float4 *__restrict__ tris, uint32_t &cn, uint32_t &ct) {
@@ -86,13 +86,13 @@ __device__ __forceinline__ bool warp_trav(bool active, uint32_t busy, uint32_t p
             tm = __ballot_sync(0xffffffffu, has_t);
         } while (tm && (!nm || (uint32_t)__popc(tm) * 32u >= need));
     } else {
-        if (can_n) trav_node<STATS>(st, stack, nodes, &cn);
+        if (can_n) trav_node<STATS, FAR>(st, stack, nodes, &cn);
         // up to NODE_STEPS node visits per node phase for lanes that still can: fewer loop
         // votes per node visit (a lane that parked triangles sits the rest out); 3 measured best
         // against 1, 2 and 4 (784, 810-819, 826, 801 Mpaths/s)
 #pragma unroll
         for (int k = 1; k < NODE_STEPS; k++)
-            if (active && trav_can_node(st)) trav_node<STATS>(st, stack, nodes, &cn);
+            if (active && trav_can_node(st)) trav_node<STATS, FAR>(st, stack, nodes, &cn);
     }
     return active && (fin || trav_done(st));
 }
@@ -101,11 +101,12 @@ __device__ __forceinline__ bool warp_trav(bool active, uint32_t busy, uint32_t p
 // written to q.hit with the triangle's leaf index in place of its id. MODE 1: any hit of the shadow queue; an unoccluded ray adds its light
 // sample to the path radiance. MODE 2: any hit of the bidirectional connection rays (passed as
 // the shadow queue); an unoccluded ray stores its value as the result of its connection
-// (EvalContri's visibility ray, BDPT.cu:460-467).
-template <int MODE, bool STATS, int REFILL>
+// (EvalContri's visibility ray, BDPT.cu:460-467). FAR (any hit only): children far to near.
+template <int MODE, bool STATS, int REFILL, bool FAR>
 __global__ void __launch_bounds__(TT, TRACE_MIN_CTAS) k_trace(DevScene sc, Queues q, int in, uint32_t *fetch,
                                               BatchView bv, uint32_t post) {
     constexpr bool ANY = MODE != 0;
+    static_assert(ANY || !FAR, "closest hits are found near to far");
     const uint32_t n = MODE == 0 ? q.counters[in] : q.counters[2];
     const float4 *ro = MODE == 0 ? q.ray_o[in] : q.sh_o;
     const float4 *rd = MODE == 0 ? q.ray_d[in] : q.sh_d;
@@ -129,6 +130,7 @@ __global__ void __launch_bounds__(TT, TRACE_MIN_CTAS) k_trace(DevScene sc, Queue
                 if (r < n) {
                     float4 o = ro[r], d = rd[r];
                     trav_init(st, o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w);
+                    if (FAR) trav_root<FAR>(st);
                     if (bv.jobs) {
                         uint32_t slot = MODE == 0 ? q.ray_slot[in][r] : __float_as_uint(q.sh_l[r].w);
                         const DevScene &js = bv.jobs[bv.slot_job[slot]].sc;
@@ -144,7 +146,7 @@ __global__ void __launch_bounds__(TT, TRACE_MIN_CTAS) k_trace(DevScene sc, Queue
             busy = __ballot_sync(0xffffffffu, active);
         }
         if (busy == 0) break;
-        if (warp_trav<ANY, STATS>(active, busy, post, st, stack, nodes, tris, cn, ct)) {
+        if (warp_trav<ANY, STATS, FAR>(active, busy, post, st, stack, nodes, tris, cn, ct)) {
             active = false;
             if (MODE == 0) {
                 // the hit by leaf index (INVALID on a miss): shading reads the leaf-ordered records
@@ -167,9 +169,9 @@ __global__ void __launch_bounds__(TT, TRACE_MIN_CTAS) k_trace(DevScene sc, Queue
 }
 
 // wl_cast_rays: the same persistent batched traversal over an array of 32-byte wl_ray records
-// (refill threshold 12).
+// (refill threshold 12; any hits in the shadow pass's child order).
 constexpr int CAST_REFILL = 12;
-template <bool ANY>
+template <bool ANY, bool FAR>
 __global__ void __launch_bounds__(TT, TRACE_MIN_CTAS) k_cast(DevScene sc, const float4 *rays, float4 *hits,
                                               uint32_t n, uint32_t *fetch, uint32_t post) {
     const uint32_t lane = threadIdx.x & 31;
@@ -191,6 +193,7 @@ __global__ void __launch_bounds__(TT, TRACE_MIN_CTAS) k_cast(DevScene sc, const 
                 if (r < n) {
                     float4 o = rays[2 * (size_t)r], d = rays[2 * (size_t)r + 1];
                     trav_init(st, o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w);
+                    if (FAR) trav_root<FAR>(st);
                     my = r;
                     active = true;
                 } else {
@@ -200,7 +203,7 @@ __global__ void __launch_bounds__(TT, TRACE_MIN_CTAS) k_cast(DevScene sc, const 
             busy = __ballot_sync(0xffffffffu, active);
         }
         if (busy == 0) break;
-        if (warp_trav<ANY, false>(active, busy, post, st, stack, sc.nodes, sc.tris, cn, ct)) {
+        if (warp_trav<ANY, false, FAR>(active, busy, post, st, stack, sc.nodes, sc.tris, cn, ct)) {
             active = false;
             uint32_t prim = st.res.prim;
             if (ANY && prim != INVALID) prim = 0;
@@ -217,7 +220,7 @@ __global__ void k_cast_empty(const float4 *rays, float4 *hits, uint32_t n) {
 
 __global__ void __launch_bounds__(TT) k_cast_stats(DevScene sc, const wl_ray *rays, uint32_t n,
                                                     uint32_t mode, unsigned long long *counts,
-                                                    uint32_t *fetch) {
+                                                    uint32_t *fetch, uint32_t far_first) {
     unsigned long long a = 0, b = 0;
     while (true) {
         uint32_t base = warp_fetch(fetch);
@@ -228,7 +231,10 @@ __global__ void __launch_bounds__(TT) k_cast_stats(DevScene sc, const wl_ray *ra
             float4 o = rp[0], d = rp[1];
             TraceResult r;
             uint32_t cn = 0, ct = 0;
-            if (mode == WL_CAST_ANY)
+            if (mode == WL_CAST_ANY && far_first)
+                traverse<true, true, true>(sc.nodes, sc.tris, o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w, r,
+                                           &cn, &ct);
+            else if (mode == WL_CAST_ANY)
                 traverse<true, true>(sc.nodes, sc.tris, o.x, o.y, o.z, d.x, d.y, d.z, o.w, d.w, r,
                                      &cn, &ct);
             else
@@ -260,10 +266,10 @@ int grid_for(const void *kernel, uint32_t ctas_per_sm = 0) {
     return sms * per;
 }
 
-template <int MODE, bool STATS, int R>
+template <int MODE, bool STATS, int R, bool FAR>
 void trace_launch(const DevScene &sc, const Queues &q, int in, uint32_t *fetch, uint32_t ctas,
                   uint32_t post, const BatchView &bv, cudaStream_t s) {
-    static int full = grid_for((const void *)k_trace<MODE, STATS, R>);
+    static int full = grid_for((const void *)k_trace<MODE, STATS, R, FAR>);
     int grid = full;
     if (ctas) {
         int dev = 0, sms = 0;
@@ -271,20 +277,28 @@ void trace_launch(const DevScene &sc, const Queues &q, int in, uint32_t *fetch, 
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         if ((int)ctas * sms < full) grid = (int)ctas * sms;
     }
-    k_trace<MODE, STATS, R><<<grid, TT, 0, s>>>(sc, q, in, fetch, bv, post);
+    k_trace<MODE, STATS, R, FAR><<<grid, TT, 0, s>>>(sc, q, in, fetch, bv, post);
 }
 
+template <int MODE, bool STATS, bool FAR>
+void trace_dispatch_order(const DevScene &sc, const Queues &q, int in, uint32_t *fetch, const TraceTune &t,
+                          const BatchView &bv, cudaStream_t s) {
+    switch (t.refill) {
+    case 4: trace_launch<MODE, STATS, 4, FAR>(sc, q, in, fetch, t.ctas_per_sm, t.postpone, bv, s); break;
+    case 6: trace_launch<MODE, STATS, 6, FAR>(sc, q, in, fetch, t.ctas_per_sm, t.postpone, bv, s); break;
+    case 8: trace_launch<MODE, STATS, 8, FAR>(sc, q, in, fetch, t.ctas_per_sm, t.postpone, bv, s); break;
+    case 16: trace_launch<MODE, STATS, 16, FAR>(sc, q, in, fetch, t.ctas_per_sm, t.postpone, bv, s); break;
+    case 24: trace_launch<MODE, STATS, 24, FAR>(sc, q, in, fetch, t.ctas_per_sm, t.postpone, bv, s); break;
+    default: trace_launch<MODE, STATS, 12, FAR>(sc, q, in, fetch, t.ctas_per_sm, t.postpone, bv, s); break;
+    }
+}
+
+// Closest hits always visit children near to far; any-hit passes far to near when t.far_first.
 template <int MODE, bool STATS>
 void trace_dispatch(const DevScene &sc, const Queues &q, int in, uint32_t *fetch, const TraceTune &t,
                     const BatchView &bv, cudaStream_t s) {
-    switch (t.refill) {
-    case 4: trace_launch<MODE, STATS, 4>(sc, q, in, fetch, t.ctas_per_sm, t.postpone, bv, s); break;
-    case 6: trace_launch<MODE, STATS, 6>(sc, q, in, fetch, t.ctas_per_sm, t.postpone, bv, s); break;
-    case 8: trace_launch<MODE, STATS, 8>(sc, q, in, fetch, t.ctas_per_sm, t.postpone, bv, s); break;
-    case 16: trace_launch<MODE, STATS, 16>(sc, q, in, fetch, t.ctas_per_sm, t.postpone, bv, s); break;
-    case 24: trace_launch<MODE, STATS, 24>(sc, q, in, fetch, t.ctas_per_sm, t.postpone, bv, s); break;
-    default: trace_launch<MODE, STATS, 12>(sc, q, in, fetch, t.ctas_per_sm, t.postpone, bv, s); break;
-    }
+    if (MODE != 0 && t.far_first) trace_dispatch_order<MODE, STATS, MODE != 0>(sc, q, in, fetch, t, bv, s);
+    else trace_dispatch_order<MODE, STATS, false>(sc, q, in, fetch, t, bv, s);
 }
 
 }  // namespace
@@ -331,8 +345,8 @@ void launch_connection_rays(const DevScene &sc, const Queues &q, const BdptWave 
 }
 
 void launch_cast(const DevScene &sc, const wl_ray *rays, wl_hit *hits, uint32_t n, uint32_t mode,
-                 uint32_t *fetch, uint32_t post, cudaStream_t s) {
-    static int grid = grid_for((const void *)k_cast<false>);
+                 uint32_t *fetch, uint32_t post, uint32_t far_first, cudaStream_t s) {
+    static int grid = grid_for((const void *)k_cast<false, false>);
     const float4 *r = reinterpret_cast<const float4 *>(rays);
     float4 *h = reinterpret_cast<float4 *>(hits);
     if (!sc.has_bvh) {
@@ -340,16 +354,17 @@ void launch_cast(const DevScene &sc, const wl_ray *rays, wl_hit *hits, uint32_t 
         return;
     }
     cudaMemsetAsync(fetch, 0, sizeof(uint32_t), s);
-    if (mode == WL_CAST_ANY) k_cast<true><<<grid, TT, 0, s>>>(sc, r, h, n, fetch, post);
-    else k_cast<false><<<grid, TT, 0, s>>>(sc, r, h, n, fetch, post);
+    if (mode == WL_CAST_ANY && far_first) k_cast<true, true><<<grid, TT, 0, s>>>(sc, r, h, n, fetch, post);
+    else if (mode == WL_CAST_ANY) k_cast<true, false><<<grid, TT, 0, s>>>(sc, r, h, n, fetch, post);
+    else k_cast<false, false><<<grid, TT, 0, s>>>(sc, r, h, n, fetch, post);
 }
 
 void launch_cast_stats(const DevScene &sc, const wl_ray *rays, uint32_t n, uint32_t mode,
-                       unsigned long long *counts, uint32_t *fetch, cudaStream_t s) {
+                       unsigned long long *counts, uint32_t *fetch, uint32_t far_first, cudaStream_t s) {
     static int grid = grid_for((const void *)k_cast_stats);
     cudaMemsetAsync(fetch, 0, sizeof(uint32_t), s);
     cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), s);
-    k_cast_stats<<<grid, TT, 0, s>>>(sc, rays, n, mode, counts, fetch);
+    k_cast_stats<<<grid, TT, 0, s>>>(sc, rays, n, mode, counts, fetch, far_first);
 }
 
 }  // namespace wl

@@ -409,9 +409,24 @@ WL_HD void trav_init(TravState &s, float ox, float oy, float oz, float dx, float
     s.ok = true;
 }
 
+// Visiting order of a node's internal children: slot XOR octant is near to far (the slots are
+// assigned by octant); FAR (any-hit rays only, where the order cannot change the answer)
+// visits them far to near by XOR with the opposite octant.
+template <bool FAR>
+WL_HD uint32_t visit_order(const TravState &s) {
+    return FAR ? (s.oct ^ 7u) : s.oct;
+}
+// The root as the only child of the first group, at the bit of slot 0 in visiting order.
+template <bool FAR>
+WL_HD void trav_root(TravState &s) {
+    s.ng = make_uint2(0u, (1u << (24 + visit_order<FAR>(s))) | 1u);
+}
+
 // Loads the node at np and tests the ray against its children's boxes. Returns the node's
 // group of hit internal children (child base; hit bits in [24, 32) ordered by slot XOR
-// octant; imask in [0, 8)) in ng and its group of hit triangles (triangle base, hit bits) in tg.
+// visit_order; imask in [0, 8)) in ng and its group of hit triangles (triangle base, hit bits)
+// in tg.
+template <bool FAR = false>
 WL_HD void node_test(const TravState &s, const float4 *__restrict__ np, uint2 &ng, uint2 &tg) {
     float4 n0 = ldg4(np), n1 = ldg4(np + 1), n2 = ldg4(np + 2), n3 = ldg4(np + 3), n4 = ldg4(np + 4);
     uint32_t ew = as_uint(n0.w);
@@ -458,11 +473,12 @@ WL_HD void node_test(const TravState &s, const float4 *__restrict__ np, uint2 &n
         // triangles on bits [offset, offset + count)
         if (tn <= XMUL(tf, grow)) hits |= (meta >> 5) << (meta & 31u);
     }
-    // internal hits from slot order to visiting order (bit c -> bit c XOR octant)
+    // internal hits from slot order to visiting order (bit c -> bit c XOR order)
     uint32_t ih = hits >> 24;
-    if (s.oct & 1u) ih = ((ih & 0x55u) << 1) | ((ih >> 1) & 0x55u);
-    if (s.oct & 2u) ih = ((ih & 0x33u) << 2) | ((ih >> 2) & 0x33u);
-    if (s.oct & 4u) ih = ((ih & 0x0fu) << 4) | ((ih >> 4) & 0x0fu);
+    const uint32_t ord = visit_order<FAR>(s);
+    if (ord & 1u) ih = ((ih & 0x55u) << 1) | ((ih >> 1) & 0x55u);
+    if (ord & 2u) ih = ((ih & 0x33u) << 2) | ((ih >> 2) & 0x33u);
+    if (ord & 4u) ih = ((ih & 0x0fu) << 4) | ((ih >> 4) & 0x0fu);
     ng = make_uint2(as_uint(n1.x), (ih << 24) | imask);
     tg = make_uint2(as_uint(n1.y), hits & 0x00ffffffu);
 }
@@ -494,20 +510,20 @@ WL_HD bool tri_test_next(TravState &s, const float4 *__restrict__ tris) {
 // One step: visit the nearest pending child node (if the current group has one), test the
 // triangles of its hit leaves, and pop the stack when the group is exhausted. Returns true when
 // the ray is finished (stack empty, or an any-hit found).
-template <bool ANY, bool STATS>
+template <bool ANY, bool STATS, bool FAR = false>
 WL_HD bool trav_step(TravState &s, uint2 *stack, const float4 *__restrict__ nodes,
                      const float4 *__restrict__ tris, uint32_t *n_nodes, uint32_t *n_tris) {
     if (s.ng.y & 0xff000000u) {
         int k = lowest_bit(s.ng.y >> 24);
         s.ng.y &= ~(1u << (24 + k));
-        uint32_t slot = (uint32_t)k ^ s.oct;
+        uint32_t slot = (uint32_t)k ^ visit_order<FAR>(s);
         uint32_t node = s.ng.x + popcount(s.ng.y & 0xffu & ((1u << slot) - 1u));
         if (s.ng.y & 0xff000000u) {
             if (s.sp < TRAV_STACK) stack[s.sp++] = s.ng;
             else s.ok = false;
         }
         if (STATS) (*n_nodes)++;
-        node_test(s, nodes + 5 * (size_t)node, s.ng, s.tg);
+        node_test<FAR>(s, nodes + 5 * (size_t)node, s.ng, s.tg);
     }
     while (s.tg.y) {
         if (STATS) (*n_tris)++;
@@ -549,12 +565,12 @@ struct ArrayStack {
 
 // Node step (requires trav_can_node): pop the stack when the current group is exhausted, then
 // visit the group's nearest pending child. Stack: put(i, v) / get(i) of entry i.
-template <bool STATS, class Stack>
+template <bool STATS, bool FAR = false, class Stack>
 WL_HD void trav_node(TravState &s, const Stack &stack, const float4 *__restrict__ nodes, uint32_t *n_nodes) {
     if (!(s.ng.y & 0xff000000u)) s.ng = stack.get(--s.sp);
     int k = lowest_bit(s.ng.y >> 24);
     s.ng.y &= ~(1u << (24 + k));
-    uint32_t slot = (uint32_t)k ^ s.oct;
+    uint32_t slot = (uint32_t)k ^ visit_order<FAR>(s);
     uint32_t node = s.ng.x + popcount(s.ng.y & 0xffu & ((1u << slot) - 1u));
     if (s.ng.y & 0xff000000u) {
         if (s.sp < TRAV_STACK) stack.put(s.sp++, s.ng);
@@ -562,7 +578,7 @@ WL_HD void trav_node(TravState &s, const Stack &stack, const float4 *__restrict_
     }
     if (STATS) (*n_nodes)++;
     uint2 tg;
-    node_test(s, nodes + 5 * (size_t)node, s.ng, tg);
+    node_test<FAR>(s, nodes + 5 * (size_t)node, s.ng, tg);
     if (tg.y) {
         if (s.tg.y == 0) s.tg = tg;
         else s.tq = tg;
@@ -582,17 +598,19 @@ WL_HD bool trav_tri(TravState &s, const float4 *__restrict__ tris, uint32_t *n_t
     return ANY && hit;
 }
 
-// ANY: stop at the first hit (shadow rays). STATS: count node visits and triangle tests.
-// Returns false if the traversal stack overflowed (cannot happen when the tree depth is
-// <= TRAV_STACK, which the build checks).
-template <bool ANY, bool STATS>
+// ANY: stop at the first hit (shadow rays). STATS: count node visits and triangle tests. FAR
+// (with ANY): children far to near. Returns false if the traversal stack overflowed (cannot
+// happen when the tree depth is <= TRAV_STACK, which the build checks).
+template <bool ANY, bool STATS, bool FAR = false>
 WL_HD bool traverse(const float4 *__restrict__ nodes, const float4 *__restrict__ tris, float ox,
                     float oy, float oz, float dx, float dy, float dz, float tmin, float tmax,
                     TraceResult &res, uint32_t *n_nodes, uint32_t *n_tris) {
+    static_assert(ANY || !FAR, "closest hits are found near to far");
     TravState s;
     uint2 stack[TRAV_STACK];
     trav_init(s, ox, oy, oz, dx, dy, dz, tmin, tmax);
-    while (!trav_step<ANY, STATS>(s, stack, nodes, tris, n_nodes, n_tris)) {
+    trav_root<FAR>(s);
+    while (!trav_step<ANY, STATS, FAR>(s, stack, nodes, tris, n_nodes, n_tris)) {
     }
     res = s.res;
     return s.ok;

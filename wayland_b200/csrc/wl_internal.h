@@ -94,9 +94,17 @@ struct BdVerts {
 // One wave of bidirectional samples: slot i is sample (base + i) like the path tracer's waves.
 // Connections are numbered in slot order and, within a slot, in the reference's loop order
 // (eye vertex i outer, light vertex j inner): connection t of slot s is conn_first[s] + i nl + j.
+struct NrcVertex;
 struct BdptWave {
     uint32_t cap;        // slots
-    uint32_t maxv;       // subpath vertex cap
+    uint32_t maxv;       // eye-subpath vertex cap (and the vertex arrays' depth)
+    uint32_t maxl;       // light-subpath vertex cap (<= maxv)
+    // 0, or the longest path (vertices after the camera, the light's included) that the
+    // connections and eye-path light hits account for: the radiance cache takes the longer
+    // paths at eye vertex maxv (queries != null)
+    uint32_t max_len;
+    NrcVertex *queries;  // cache queries of the eye subpaths' last vertices (null: no cache)
+    uint32_t *n_queries;
     BdVerts eye, lit;    // [maxv][cap] each
     uint32_t *n_eye, *n_light;  // stored vertices per slot
     uint32_t *conn_count;       // n_eye * n_light per slot
@@ -136,6 +144,9 @@ struct WaveParams {
     // graph replays: the wave's first sample index and first frame come from device memory
     // (dyn[0], dyn[1]) instead of base / first_frame, so one captured wave serves every wave
     const uint64_t *dyn;
+    // 0 or 1: slot i is sample base + i. k > 1 (radiance-cache training waves, which trace
+    // only every k-th sample): slot i is sample base + i k
+    uint32_t gstride;
 };
 
 #ifdef __CUDACC__
@@ -261,6 +272,7 @@ struct TraceTune {
     uint32_t ctas_per_sm = 0;
     uint32_t refill = 12;
     uint32_t postpone = 12;  // triangle phase when >= postpone/32 of the busy lanes hold triangles
+    uint32_t far_first = 0;  // any-hit passes: visit children far to near
 };
 // wl_render_noalloc (noalloc.cu): what a call needs from the handles (api.cu
 // noalloc_render_inputs) and the device address of the static scratch array, looked up for the
@@ -284,9 +296,9 @@ void launch_reset_counters(uint32_t *counters, uint32_t mask, cudaStream_t s);
 void launch_connection_rays(const DevScene &sc, const Queues &q, const BdptWave &bw, bool stats,
                             cudaStream_t s, const TraceTune &t = TraceTune{});
 void launch_cast(const DevScene &sc, const wl_ray *rays, wl_hit *hits, uint32_t n, uint32_t mode,
-                 uint32_t *fetch, uint32_t postpone, cudaStream_t s);
+                 uint32_t *fetch, uint32_t postpone, uint32_t far_first, cudaStream_t s);
 void launch_cast_stats(const DevScene &sc, const wl_ray *rays, uint32_t n, uint32_t mode,
-                       unsigned long long *counts, uint32_t *fetch, cudaStream_t s);
+                       unsigned long long *counts, uint32_t *fetch, uint32_t far_first, cudaStream_t s);
 
 // bvh_build.cu
 struct BvhBuild {
