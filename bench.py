@@ -710,6 +710,8 @@ def main():
     ap.add_argument("--no-bdpt", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="skip the progressive 1-spp launches/graph leg")
+    ap.add_argument("--no-cornell", action="store_true", help="skip the Cornell-box configuration leg")
     ap.add_argument("--bdpt-only", action="store_true", help="only the BDPT + AO leg (prints its JSON)")
     ap.add_argument("--nrc-res", default="1920x1080", help="resolution of the radiance-cache comparison")
     ap.add_argument("--nrc-oracle-spp", type=int, default=8192)
@@ -896,8 +898,9 @@ def main():
 
         if not args.no_raycast:
             leg("raycast", lambda: raycast_microbench(wl, torch, ctx, sc, scene, stream, tune))
-        if world == 1:
+        if world == 1 and not args.no_graph:
             leg("progressive_1spp", lambda: graph_leg(wl, torch, ctx, sc, scene, stream))
+        if world == 1 and not args.no_cornell:
             leg("cornell_config1", lambda: cornell_leg(wl, torch, ctx))
         if world == 1 and not args.no_batch:
             leg("batch", lambda: batch_leg(wl, torch, ctx, stream))

@@ -318,21 +318,28 @@ __global__ void __launch_bounds__(128 * QC, 1)
 // Tensor memory: columns 0-63 forward D, 64-127 backward D, 128 + 64 l the dW_l accumulators.
 constexpr int TR_THREADS = 256;
 constexpr uint32_t TR_TMEM_COLS = 512;
-constexpr uint32_t TS_DYT = 0;                  // dY^T, 16 x 128 (its M=128 read spans 32 KB)
-constexpr uint32_t TS_DY = 4096;                // dY, 128 x 16
-constexpr uint32_t TS_W = 8192;                 // W_0..W_3 (row = output), 8 KB each
+// Transposed tiles that the kernel writes itself (row = feature, 128 samples along K) keep
+// their K-adjacent core matrices 144 bytes apart instead of 128, so that the 32 samples one warp
+// stores for a feature land in 4 different groups of banks (128 would put all four 16-byte
+// pieces in banks 0-3: a 4-way conflict on every store); 8-row groups are then 2304 bytes apart.
+constexpr uint32_t TP_LBO = 144, TP_SBO = 16 * TP_LBO;
+constexpr uint32_t TP_TILE = 8 * TP_SBO;           // 64 x 128, 18,432 bytes
+constexpr uint32_t TS_DYT = 0;                  // dY^T, 16 x 128 (its M=128 read spans 36 KB)
+constexpr uint32_t TS_DY = 2 * TP_SBO;          // dY, 128 x 16
+constexpr uint32_t TS_W = 9216;                 // W_0..W_3 (row = output), 8 KB each
 constexpr uint32_t TS_W4 = TS_W + 4 * 8192;     // W_4, 16 x 64
 constexpr uint32_t TS_WT = TS_W4 + 2048;        // W_0^T..W_3^T (row = input)
 constexpr uint32_t TS_W4T = TS_WT + 4 * 8192;   // W_4^T, 64 x 16
 constexpr uint32_t TS_T0 = TS_W4T + 2048;       // A_0, A_2, A_4
 constexpr uint32_t TS_T1 = TS_T0 + 16384;       // A_1, A_3, then dZ
-constexpr uint32_t TS_DZT = TS_T1 + 16384;      // dZ^T, 64 x 128 (its M=128 read spans 32 KB)
-constexpr uint32_t TS_AT = TS_DZT + 16384;      // A_0^T..A_4^T, 64 x 128 each
-constexpr uint32_t TS_BAR = TS_AT + 5 * 16384;   // MMA completion
+constexpr uint32_t TS_DZT = TS_T1 + 16384;      // dZ^T, 64 x 128 (its M=128 read spans 36 KB)
+constexpr uint32_t TS_AT = TS_DZT + TP_TILE;    // A_0^T (as copied, 128-byte K stride), A_1^T..A_4^T
+constexpr uint32_t TS_BAR = TS_AT + 16384 + 4 * TP_TILE;  // MMA completion
 constexpr uint32_t TS_WBAR = TS_BAR + 8;          // the weights' bulk copy
 constexpr uint32_t TS_LBAR = TS_BAR + 16;         // each tile's bulk copy
 constexpr uint32_t TS_TMEM = TS_BAR + 24;
 constexpr uint32_t TS_BYTES = TS_TMEM + 8;
+static_assert(TS_DY + 4096 <= TS_W && TS_BYTES <= 232448, "training kernel shared-memory layout");
 static_assert(TS_WT == TS_W + WI_FWD && TS_W4T + 2048 == TS_W + WI_BYTES, "the weight image's layout");
 
 // K-major tiles with 16 and 128 columns (core matrices 8 rows x 16 bytes)
@@ -342,9 +349,18 @@ __device__ __forceinline__ uint32_t kmaj16(uint32_t r, uint32_t k) {
 __device__ __forceinline__ uint32_t kmaj128(uint32_t r, uint32_t k) {
     return (r >> 3) * 2048u + (k >> 3) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
 }
-__device__ __forceinline__ uint64_t sdesc_s(uint32_t saddr, uint32_t sbo) {
-    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) |
+__device__ __forceinline__ uint64_t sdesc_s(uint32_t saddr, uint32_t sbo, uint32_t lbo = 128u) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(lbo >> 4) << 16) |
            ((uint64_t)(sbo >> 4) << 32) | (1ull << 46);
+}
+// element (row r, column k) of a transposed tile the training kernel writes (TP_LBO layout)
+__device__ __forceinline__ uint32_t kmajp(uint32_t r, uint32_t k) {
+    return (r >> 3) * TP_SBO + (k >> 3) * TP_LBO + (r & 7u) * 16u + (k & 7u) * 2u;
+}
+// A_l^T in shared memory: its address, and its descriptor at K step ks (16 samples)
+__device__ __forceinline__ uint32_t at_off(uint32_t l) { return l == 0 ? 0u : 16384u + (l - 1) * TP_TILE; }
+__device__ __forceinline__ uint64_t at_desc(uint32_t sAT, uint32_t l, uint32_t ks) {
+    return l == 0 ? sdesc_s(sAT + ks * 256u, 2048u) : sdesc_s(sAT + at_off(l) + ks * 2u * TP_LBO, TP_SBO, TP_LBO);
 }
 
 // 8 consecutive values (k0 multiple of 8) of row r of a 64-wide K-major tile, as bfloat16
@@ -363,6 +379,10 @@ __device__ __forceinline__ void store8(uint8_t *tile, uint32_t r, uint32_t k0, c
 // column k of a transposed 128-column tile (row = feature, column = sample r)
 __device__ __forceinline__ void store_t(uint8_t *tile, uint32_t k, uint32_t r, float x) {
     *reinterpret_cast<__nv_bfloat16 *>(tile + kmaj128(k, r)) = __float2bfloat16_rn(x);
+}
+// the same in a transposed tile of the training kernel's own (TP_LBO layout)
+__device__ __forceinline__ void store_tp(uint8_t *tile, uint32_t k, uint32_t r, float x) {
+    *reinterpret_cast<__nv_bfloat16 *>(tile + kmajp(k, r)) = __float2bfloat16_rn(x);
 }
 
 __device__ __forceinline__ bool tc_step(uint32_t bar, uint32_t &phase, uint32_t polls) {
@@ -532,8 +552,8 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
                 uint8_t *next = smem + ((l & 1u) ? TS_T0 : TS_T1);
 #pragma unroll
                 for (int c = 0; c < 4; c++) store8(next, r, 32 * h + 8 * c, a + 8 * c);
-                uint8_t *at = smem + TS_AT + (l + 1) * 16384u;
-                for (int k = 0; k < 32; k++) store_t(at, 32 * h + k, r, a[k]);
+                uint8_t *at = smem + TS_AT + at_off(l + 1);
+                for (int k = 0; k < 32; k++) store_tp(at, 32 * h + k, r, a[k]);
             } else if (h == 0) {
                 float o[16], d[16];
                 tmem_ld16(tmem + lane, o);
@@ -548,11 +568,20 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
                         d[c] = 2.0f * e / den * inv;
                     }
                 }
-                __nv_bfloat16 *dy = reinterpret_cast<__nv_bfloat16 *>(smem + TS_DY);
-                for (int c = 0; c < 16; c++) {
-                    dy[kmaj16(r, c) / 2] = __float2bfloat16_rn(d[c]);
-                    store_t(smem + TS_DYT, c, r, d[c]);
+                // dY row r: two 16-byte pieces of the 16-column tile
+                for (int c = 0; c < 2; c++) {
+                    __nv_bfloat162 p0 = __floats2bfloat162_rn(d[8 * c + 0], d[8 * c + 1]);
+                    __nv_bfloat162 p1 = __floats2bfloat162_rn(d[8 * c + 2], d[8 * c + 3]);
+                    __nv_bfloat162 p2 = __floats2bfloat162_rn(d[8 * c + 4], d[8 * c + 5]);
+                    __nv_bfloat162 p3 = __floats2bfloat162_rn(d[8 * c + 6], d[8 * c + 7]);
+                    uint4 u;
+                    u.x = *reinterpret_cast<uint32_t *>(&p0);
+                    u.y = *reinterpret_cast<uint32_t *>(&p1);
+                    u.z = *reinterpret_cast<uint32_t *>(&p2);
+                    u.w = *reinterpret_cast<uint32_t *>(&p3);
+                    *reinterpret_cast<uint4 *>(smem + TS_DY + kmaj16(r, 8 * c)) = u;
                 }
+                for (int c = 0; c < 16; c++) store_tp(smem + TS_DYT, c, r, d[c]);
             }
             smem_to_tc();
         }
@@ -563,8 +592,9 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
                      sdesc_s(smem_u32(smem + TS_W4T), 256u), ID64, 0u);
 #pragma unroll
             for (uint32_t ks = 0; ks < 8; ks++)
-                mma_bf16(tmem + 128u + 4u * 64u, sdesc_s(smem_u32(smem + TS_DYT) + ks * 256u, 2048u),
-                         sdesc_s(sAT + 4u * 16384u + ks * 256u, 2048u), ID64, (any || ks > 0) ? 1u : 0u);
+                mma_bf16(tmem + 128u + 4u * 64u,
+                         sdesc_s(smem_u32(smem + TS_DYT) + ks * 2u * TP_LBO, TP_SBO, TP_LBO),
+                         at_desc(sAT, 4u, ks), ID64, (any || ks > 0) ? 1u : 0u);
             mma_commit(bar);
         }
         ok = tc_step(bar, phase, polls);
@@ -579,7 +609,7 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
                 if (!((mask[l] >> k) & 1u)) d[k] = 0.0f;
 #pragma unroll
             for (int c = 0; c < 4; c++) store8(smem + TS_T1, r, 32 * h + 8 * c, d + 8 * c);
-            for (int k = 0; k < 32; k++) store_t(smem + TS_DZT, 32 * h + k, r, d[k]);
+            for (int k = 0; k < 32; k++) store_tp(smem + TS_DZT, 32 * h + k, r, d[k]);
             smem_to_tc();
             if (tid == 0) {
 #pragma unroll
@@ -588,8 +618,8 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
                              ks > 0 ? 1u : 0u);
 #pragma unroll
                 for (uint32_t ks = 0; ks < 8; ks++)
-                    mma_bf16(tmem + 128u + 64u * l, sdesc_s(sDZT + ks * 256u, 2048u),
-                             sdesc_s(sAT + l * 16384u + ks * 256u, 2048u), ID64, (any || ks > 0) ? 1u : 0u);
+                    mma_bf16(tmem + 128u + 64u * l, sdesc_s(sDZT + ks * 2u * TP_LBO, TP_SBO, TP_LBO),
+                             at_desc(sAT, (uint32_t)l, ks), ID64, (any || ks > 0) ? 1u : 0u);
                 mma_commit(bar);
             }
             ok = tc_step(bar, phase, polls);
