@@ -128,7 +128,7 @@ struct NrcNet {
     float *w = nullptr, *w_grad = nullptr, *w_m = nullptr, *w_v = nullptr;
     uint32_t max_samples = 0;
     float *loss = nullptr;
-    // training scratch: encoded input tiles (32 KB per 128 rows) and grid-feature gradients
+    // training scratch: encoded input tiles (16 KB per 128 rows) and grid-feature gradients
     uint8_t *tiles = nullptr;
     float *gin = nullptr;
     uint32_t raw_cap = 0;  // rows the scratch holds
@@ -195,7 +195,7 @@ int nrc_create(const wl_nrc_params &p, const float *bbox_lo, const float *bbox_h
     n->w_m = (float *)nrc_alloc(NRC_WEIGHTS * 4, e);
     n->w_v = (float *)nrc_alloc(NRC_WEIGHTS * 4, e);
     n->max_samples = max_samples;
-    n->tiles = (uint8_t *)nrc_alloc(((size_t)max_samples + 127) / 128 * 32768, e);
+    n->tiles = (uint8_t *)nrc_alloc(((size_t)max_samples + 127) / 128 * 16384, e);
     n->gin = (float *)nrc_alloc((size_t)max_samples * 32 * 4, e);
     n->raw_cap = max_samples;
     n->loss = (float *)nrc_alloc(16, e);
@@ -267,7 +267,7 @@ static int nrc_gradients(NrcNet *n, bool enc, const wl_disney *mats, const float
         if (n->tiles) cudaFree(n->tiles);
         n->tiles = nullptr;
         n->raw_cap = 0;
-        if (cudaMalloc(&n->tiles, ((size_t)count + 127) / 128 * 32768) != cudaSuccess) {
+        if (cudaMalloc(&n->tiles, ((size_t)count + 127) / 128 * 16384) != cudaSuccess) {
             n->tiles = nullptr;
             cudaGetLastError();  // the failed allocation is reported by the status, not left pending
             return WL_ERR_OOM;

@@ -116,25 +116,16 @@ __device__ __forceinline__ void store_row(uint8_t *tile, uint32_t r, const float
 
 // bfloat16 image of the MLP weights in the tensor-core operand layout, built once per weight
 // update (k_weight_image) and bulk-copied into shared memory by every CTA: W_0..W_3 (8 KB each)
-// and W_4 (2 KB) K-major with row = output (the B operand of the forward layers), then the same
-// matrices transposed, row = input (the B operand of the backward products).
+// and W_4 (2 KB) K-major with row = output. The forward layers read them as the B operand; the
+// backward products dA = dZ W read the same bytes MN-major (N = the inputs).
 constexpr uint32_t WI_FWD = 4 * 8192 + 2048;        // 34,816 bytes
-constexpr uint32_t WI_BYTES = 2 * WI_FWD;
+static_assert(WI_FWD == NRC_WEIGHT_IMAGE_BYTES, "the weight image's size");
 
 __global__ void k_weight_image(const float *w, uint8_t *img) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (uint32_t)NRC_WEIGHTS) return;
     const uint32_t l = i / 4096u, rem = i % 4096u, o = rem / 64u, k = rem % 64u;
-    const __nv_bfloat16 b = __float2bfloat16_rn(w[i]);
-    if (l < 4) {
-        *reinterpret_cast<__nv_bfloat16 *>(img + l * 8192u + kmaj(o, k)) = b;
-        *reinterpret_cast<__nv_bfloat16 *>(img + WI_FWD + l * 8192u + kmaj(k, o)) = b;
-    } else {
-        *reinterpret_cast<__nv_bfloat16 *>(img + 4 * 8192u + kmaj(o, k)) = b;
-        // W_4^T: 64 x 16 with 16 columns (8-row groups 256 B apart)
-        *reinterpret_cast<__nv_bfloat16 *>(img + WI_FWD + 4 * 8192u + ((k >> 3) * 256u + (o >> 3) * 128u +
-                                                                        (k & 7u) * 16u + (o & 7u) * 2u)) = b;
-    }
+    *reinterpret_cast<__nv_bfloat16 *>(img + l * 8192u + kmaj(o, k)) = __float2bfloat16_rn(w[i]);
 }
 
 // Bulk copy (cp.async.bulk, no tensor map, no multicast) of `bytes` from global memory into this
@@ -156,7 +147,7 @@ __device__ __forceinline__ void named_sync(uint32_t id, uint32_t threads) {
 // layer's accumulators (tcgen05.ld, ReLU, bfloat16, st.shared) the tensor core executes the
 // others' MMAs. The next tile of a chain is bulk-copied into its second buffer while the current
 // one is computed; the weights are bulk-copied once per CTA from the bfloat16 image.
-// MODE 0: outputs to out[i][0..3] (raw rows, encoded into tiles by k_encode_tiles<0, false>).
+// MODE 0: outputs to out[i][0..3] (raw rows, encoded into tiles by k_encode_tiles<0>).
 // MODE 2: cache queries of the render loop: rad[slot] += extra.xyz * max(o, 0).
 constexpr int QC = 4;
 constexpr uint32_t QS_A = WI_FWD + 1024;                    // tiles, 1024-aligned
@@ -315,52 +306,47 @@ __global__ void __launch_bounds__(128 * QC, 1)
 //             memory across all tiles of the CTA (M = 128 with the rows past the 64 (16) outputs
 //             unused), added to the global gradient once at the end
 //   grid      dA_0[:, 0:32] scattered into the hash grid's gradient
+// Every tile is stored once, K-major as the forward pass reads it (row = sample). The products
+// that contract over samples (dW) or over outputs (dA = dZ W) read the same bytes as MN-major
+// operands (instruction descriptor bits 15 / 16): in a K-major tile of 8-row x 16-byte core
+// matrices, 8 consecutive features of one sample are one 16-byte core-matrix row, which is the
+// MN-major core matrix (8 K-rows of 8 contiguous M or N elements) with the feature groups
+// (MN atoms) 128 bytes apart and the sample groups (K atoms) 1024 bytes apart.
+// Shared memory: the forward weight image (W_0..W_4, row = output), the five activation tiles
+// A_0..A_4 (dZ_l overwrites A_{l+1} once dW_{l+1} has read it) and dY.
 // Tensor memory: columns 0-63 forward D, 64-127 backward D, 128 + 64 l the dW_l accumulators.
 constexpr int TR_THREADS = 256;
 constexpr uint32_t TR_TMEM_COLS = 512;
-// Transposed tiles that the kernel writes itself (row = feature, 128 samples along K) keep
-// their K-adjacent core matrices 144 bytes apart instead of 128, so that the 32 samples one warp
-// stores for a feature land in 4 different groups of banks (128 would put all four 16-byte
-// pieces in banks 0-3: a 4-way conflict on every store); 8-row groups are then 2304 bytes apart.
-constexpr uint32_t TP_LBO = 144, TP_SBO = 16 * TP_LBO;
-constexpr uint32_t TP_TILE = 8 * TP_SBO;           // 64 x 128, 18,432 bytes
-constexpr uint32_t TS_DYT = 0;                  // dY^T, 16 x 128 (its M=128 read spans 36 KB)
-constexpr uint32_t TS_DY = 2 * TP_SBO;          // dY, 128 x 16
-constexpr uint32_t TS_W = 9216;                 // W_0..W_3 (row = output), 8 KB each
-constexpr uint32_t TS_W4 = TS_W + 4 * 8192;     // W_4, 16 x 64
-constexpr uint32_t TS_WT = TS_W4 + 2048;        // W_0^T..W_3^T (row = input)
-constexpr uint32_t TS_W4T = TS_WT + 4 * 8192;   // W_4^T, 64 x 16
-constexpr uint32_t TS_T0 = TS_W4T + 2048;       // A_0, A_2, A_4
-constexpr uint32_t TS_T1 = TS_T0 + 16384;       // A_1, A_3, then dZ
-constexpr uint32_t TS_DZT = TS_T1 + 16384;      // dZ^T, 64 x 128 (its M=128 read spans 36 KB)
-constexpr uint32_t TS_AT = TS_DZT + TP_TILE;    // A_0^T (as copied, 128-byte K stride), A_1^T..A_4^T
-constexpr uint32_t TS_BAR = TS_AT + 16384 + 4 * TP_TILE;  // MMA completion
+constexpr uint32_t TS_W = 0;                    // W_0..W_3 (row = output), 8 KB each, then W_4
+constexpr uint32_t TS_A = WI_FWD;               // A_0..A_4, 16 KB each (A_0 as bulk-copied)
+constexpr uint32_t TS_DY = TS_A + 5 * 16384;    // dY, 128 x 16
+// an M=128 MN-major read of dY (16 real rows) or of a dZ tile (64 real rows) spans up to 2 KB
+// more than the 128 x 16 (x 64) data; the rows past the real ones feed unused accumulator rows
+constexpr uint32_t TS_BAR = TS_DY + 4096 + 2048;  // MMA completion
 constexpr uint32_t TS_WBAR = TS_BAR + 8;          // the weights' bulk copy
 constexpr uint32_t TS_LBAR = TS_BAR + 16;         // each tile's bulk copy
 constexpr uint32_t TS_TMEM = TS_BAR + 24;
 constexpr uint32_t TS_BYTES = TS_TMEM + 8;
-static_assert(TS_DY + 4096 <= TS_W && TS_BYTES <= 232448, "training kernel shared-memory layout");
-static_assert(TS_WT == TS_W + WI_FWD && TS_W4T + 2048 == TS_W + WI_BYTES, "the weight image's layout");
+static_assert(TS_A % 1024 == 0 && TS_BYTES <= 232448, "training kernel shared-memory layout");
 
-// K-major tiles with 16 and 128 columns (core matrices 8 rows x 16 bytes)
+// K-major tile with 16 columns (core matrices 8 rows x 16 bytes, 8-row groups 256 B apart)
 __device__ __forceinline__ uint32_t kmaj16(uint32_t r, uint32_t k) {
     return (r >> 3) * 256u + (k >> 3) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
 }
-__device__ __forceinline__ uint32_t kmaj128(uint32_t r, uint32_t k) {
-    return (r >> 3) * 2048u + (k >> 3) * 128u + (r & 7u) * 16u + (k & 7u) * 2u;
-}
-__device__ __forceinline__ uint64_t sdesc_s(uint32_t saddr, uint32_t sbo, uint32_t lbo = 128u) {
+// shared-memory matrix descriptor, no swizzle: K-major (leading = K-atom stride, stride = 8-row
+// group stride) or MN-major (leading = K-atom stride, stride = MN-atom stride)
+__device__ __forceinline__ uint64_t sdesc_s(uint32_t saddr, uint32_t sbo, uint32_t lbo) {
     return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(lbo >> 4) << 16) |
            ((uint64_t)(sbo >> 4) << 32) | (1ull << 46);
 }
-// element (row r, column k) of a transposed tile the training kernel writes (TP_LBO layout)
-__device__ __forceinline__ uint32_t kmajp(uint32_t r, uint32_t k) {
-    return (r >> 3) * TP_SBO + (k >> 3) * TP_LBO + (r & 7u) * 16u + (k & 7u) * 2u;
+// a 64-wide K-major tile (A_l, dZ_l, W_l) read MN-major along its 64 columns, K step ks
+// (16 rows = two 8-row groups)
+__device__ __forceinline__ uint64_t mn64(uint32_t saddr, uint32_t ks) {
+    return sdesc_s(saddr + ks * 2048u, 128u, 1024u);
 }
-// A_l^T in shared memory: its address, and its descriptor at K step ks (16 samples)
-__device__ __forceinline__ uint32_t at_off(uint32_t l) { return l == 0 ? 0u : 16384u + (l - 1) * TP_TILE; }
-__device__ __forceinline__ uint64_t at_desc(uint32_t sAT, uint32_t l, uint32_t ks) {
-    return l == 0 ? sdesc_s(sAT + ks * 256u, 2048u) : sdesc_s(sAT + at_off(l) + ks * 2u * TP_LBO, TP_SBO, TP_LBO);
+// instruction descriptor with A and / or B MN-major
+__host__ __device__ constexpr uint32_t idesc_mn(uint32_t n, uint32_t m, bool a_mn, bool b_mn) {
+    return idesc(n, m) | (a_mn ? 1u << 15 : 0u) | (b_mn ? 1u << 16 : 0u);
 }
 
 // 8 consecutive values (k0 multiple of 8) of row r of a 64-wide K-major tile, as bfloat16
@@ -375,14 +361,6 @@ __device__ __forceinline__ void store8(uint8_t *tile, uint32_t r, uint32_t k0, c
     u.z = *reinterpret_cast<uint32_t *>(&p2);
     u.w = *reinterpret_cast<uint32_t *>(&p3);
     *reinterpret_cast<uint4 *>(tile + kmaj(r, k0)) = u;
-}
-// column k of a transposed 128-column tile (row = feature, column = sample r)
-__device__ __forceinline__ void store_t(uint8_t *tile, uint32_t k, uint32_t r, float x) {
-    *reinterpret_cast<__nv_bfloat16 *>(tile + kmaj128(k, r)) = __float2bfloat16_rn(x);
-}
-// the same in a transposed tile of the training kernel's own (TP_LBO layout)
-__device__ __forceinline__ void store_tp(uint8_t *tile, uint32_t k, uint32_t r, float x) {
-    *reinterpret_cast<__nv_bfloat16 *>(tile + kmajp(k, r)) = __float2bfloat16_rn(x);
 }
 
 __device__ __forceinline__ bool tc_step(uint32_t bar, uint32_t &phase, uint32_t polls) {
@@ -399,12 +377,11 @@ __device__ __forceinline__ void smem_to_tc() {
     tc_after_sync();
 }
 
-// Encoded inputs of a training step in the tensor-core operand layout, one 32 KB record per
-// 128 rows: the K-major tile (row = sample) and its transpose (row = feature). Thread (r, h)
-// encodes row r's columns [16h, 16h + 16) and [32 + 16h, 32 + 16h + 16): grid levels 8h..8h+7
-// and the direction (h = 0) or auxiliary (h = 1) features. Many CTAs per SM hide the grid
-// gathers' latency, which the tensor-core kernel (one CTA per SM) could not.
-template <int MODE, bool TRANSPOSE = true>
+// Encoded inputs in the tensor-core operand layout, one 16 KB K-major tile per 128 rows (row =
+// sample). Thread (r, h) encodes row r's columns [16h, 16h + 16) and [32 + 16h, 32 + 16h + 16):
+// grid levels 8h..8h+7 and the direction (h = 0) or auxiliary (h = 1) features. Many CTAs per SM
+// hide the grid gathers' latency, which the tensor-core kernels (one CTA per SM) could not.
+template <int MODE>
 __global__ void __launch_bounds__(256) k_encode_tiles(NrcGrid g, const wl_disney *mats,
                                                       const NrcVertex *samples, const uint32_t *n_ptr,
                                                       uint32_t n_fixed, const float *in, uint8_t *tiles) {
@@ -430,18 +407,11 @@ __global__ void __launch_bounds__(256) k_encode_tiles(NrcGrid g, const wl_disney
     } else {
         for (int k = 0; k < 32; k++) x[k] = 0.0f;
     }
-    uint8_t *A = tiles + (size_t)tile * (TRANSPOSE ? 32768u : 16384u);
+    uint8_t *A = tiles + (size_t)tile * 16384u;
     store8(A, r, 16 * h, x);
     store8(A, r, 16 * h + 8, x + 8);
     store8(A, r, 32 + 16 * h, x + 16);
     store8(A, r, 32 + 16 * h + 8, x + 24);
-    if (TRANSPOSE) {
-        uint8_t *AT = A + 16384u;
-        for (int k = 0; k < 16; k++) {
-            store_t(AT, 16 * h + k, r, x[k]);
-            store_t(AT, 32 + 16 * h + k, r, x[16 + k]);
-        }
-    }
 }
 
 // The hash-grid gradient: thread (sample, level) adds its two feature gradients, weighted
@@ -458,7 +428,7 @@ __global__ void __launch_bounds__(256) k_grid_scatter(NrcGrid g, const NrcVertex
 }
 
 // MODE 0: raw rows in[n][64], targets target[n][4]. MODE 1: the collected training samples
-// (count on the device), encoded here; the input gradient goes to the hash grid.
+// (count on the device), encoded by k_encode_tiles; the input gradient goes to the hash grid.
 template <int MODE>
 __global__ void __launch_bounds__(TR_THREADS, 1)
     k_train_tc(const uint8_t *wimg, const NrcVertex *samples, const uint32_t *n_ptr, uint32_t n_fixed,
@@ -473,8 +443,8 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(wbar) : "memory");
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(lbar) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        // the weights and their transposes, one bulk copy of the bfloat16 image
-        bulk_load(smem_u32(smem + TS_W), wimg, WI_BYTES, wbar);
+        // the weights, one bulk copy of the bfloat16 image (row = output)
+        bulk_load(smem_u32(smem + TS_W), wimg, WI_FWD, wbar);
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(smem + TS_TMEM)),
@@ -487,9 +457,8 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
     const uint32_t n = MODE == 1 ? min(*n_ptr, n_fixed) : n_fixed;
     const float inv = n ? 1.0f / (3.0f * (float)n) : 0.0f;
     const uint32_t ID64 = idesc(64, 128), ID16 = idesc(16, 128);
-    const uint32_t sT0 = smem_u32(smem + TS_T0), sT1 = smem_u32(smem + TS_T1);
-    const uint32_t sAT = smem_u32(smem + TS_AT), sDZT = smem_u32(smem + TS_DZT);
-    const uint32_t sW = smem_u32(smem + TS_W), sWT = smem_u32(smem + TS_WT);
+    const uint32_t ID_BMN = idesc_mn(64, 128, false, true), ID_ABMN = idesc_mn(64, 128, true, true);
+    const uint32_t sW = smem_u32(smem + TS_W), sA = smem_u32(smem + TS_A), sDY = smem_u32(smem + TS_DY);
     uint32_t phase = 0, lphase = 0;
     bool wok = __syncthreads_and(mbar_wait(wbar, 0, polls)) != 0;
     bool ok = wok, any = false, lpending = false;
@@ -497,16 +466,9 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
     for (uint32_t tile = blockIdx.x * 128u; tile < n && ok; tile += gridDim.x * 128u) {
         const uint32_t i = tile + r;
         const bool valid = i < n;
-        // ---- inputs: the encoded tile and its transpose (k_encode_tiles), 32 KB in two bulk copies
+        // ---- inputs: the encoded tile (k_encode_tiles), 16 KB in one bulk copy, into A_0
         float t3[3] = {0.f, 0.f, 0.f};
-        if (tid == 0) {
-            const uint8_t *src = tiles + (size_t)(tile / 128u) * 32768u;
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(lbar), "r"(32768u) : "memory");
-            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                         ::"r"(smem_u32(smem + TS_T0)), "l"(src), "r"(16384u), "r"(lbar) : "memory");
-            asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                         ::"r"(smem_u32(smem + TS_AT)), "l"(src + 16384u), "r"(16384u), "r"(lbar) : "memory");
-        }
+        if (tid == 0) bulk_load(sA, tiles + (size_t)(tile / 128u) * 16384u, 16384u, lbar);
         lpending = true;
         if (__syncthreads_and(mbar_wait(lbar, lphase, polls)) == 0) {
             ok = false;
@@ -526,12 +488,12 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
         // ---- forward
         uint32_t mask[4];
         for (uint32_t l = 0; l < 5 && ok; l++) {
-            const uint32_t sA = (l & 1u) ? sT1 : sT0;
-            const uint32_t sB = l < 4 ? sW + l * 8192u : smem_u32(smem + TS_W4);
+            const uint32_t sAl = sA + l * 16384u;
+            const uint32_t sB = sW + l * 8192u;  // W_4 follows W_3
             if (tid == 0) {
 #pragma unroll
                 for (uint32_t ks = 0; ks < 4; ks++)
-                    mma_bf16(tmem, sdesc(sA + ks * 256u), sdesc(sB + ks * 256u), l < 4 ? ID64 : ID16,
+                    mma_bf16(tmem, sdesc(sAl + ks * 256u), sdesc(sB + ks * 256u), l < 4 ? ID64 : ID16,
                              ks > 0 ? 1u : 0u);
                 mma_commit(bar);
             }
@@ -549,11 +511,9 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
                     m |= (a[k] > 0.0f ? 1u : 0u) << k;
                 }
                 mask[l] = m;
-                uint8_t *next = smem + ((l & 1u) ? TS_T0 : TS_T1);
+                uint8_t *next = smem + TS_A + (l + 1) * 16384u;
 #pragma unroll
                 for (int c = 0; c < 4; c++) store8(next, r, 32 * h + 8 * c, a + 8 * c);
-                uint8_t *at = smem + TS_AT + at_off(l + 1);
-                for (int k = 0; k < 32; k++) store_tp(at, 32 * h + k, r, a[k]);
             } else if (h == 0) {
                 float o[16], d[16];
                 tmem_ld16(tmem + lane, o);
@@ -581,25 +541,25 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
                     u.w = *reinterpret_cast<uint32_t *>(&p3);
                     *reinterpret_cast<uint4 *>(smem + TS_DY + kmaj16(r, 8 * c)) = u;
                 }
-                for (int c = 0; c < 16; c++) store_tp(smem + TS_DYT, c, r, d[c]);
             }
             smem_to_tc();
         }
         if (!ok) break;
-        // ---- backward, output layer: dA_4 = dY W_4, dW_4 += dY^T A_4
+        // ---- backward, output layer: dA_4 = dY W_4 (W_4 read MN-major: N = its 64 inputs,
+        // K = its 16 outputs), dW_4 += dY^T A_4 (dY MN-major: M = its 16 outputs, K = the
+        // samples, 8-row groups 256 B apart; A_4 MN-major)
         if (tid == 0) {
-            mma_bf16(tmem + 64u, sdesc_s(smem_u32(smem + TS_DY), 256u),
-                     sdesc_s(smem_u32(smem + TS_W4T), 256u), ID64, 0u);
+            mma_bf16(tmem + 64u, sdesc_s(sDY, 256u, 128u), sdesc_s(sW + 4u * 8192u, 128u, 1024u), ID_BMN, 0u);
 #pragma unroll
             for (uint32_t ks = 0; ks < 8; ks++)
-                mma_bf16(tmem + 128u + 4u * 64u,
-                         sdesc_s(smem_u32(smem + TS_DYT) + ks * 2u * TP_LBO, TP_SBO, TP_LBO),
-                         at_desc(sAT, 4u, ks), ID64, (any || ks > 0) ? 1u : 0u);
+                mma_bf16(tmem + 128u + 4u * 64u, sdesc_s(sDY + ks * 512u, 128u, 256u), mn64(sA + 4u * 16384u, ks),
+                         ID_ABMN, (any || ks > 0) ? 1u : 0u);
             mma_commit(bar);
         }
         ok = tc_step(bar, phase, polls);
         for (int l = 3; l >= 0 && ok; l--) {
-            // dZ_l = dA_{l+1} masked by the activation of layer l
+            // dZ_l = dA_{l+1} masked by the activation of layer l, into A_{l+1}'s tile (dW_{l+1}
+            // has read A_{l+1})
             float d[32];
             tmem_ld16(tmem + lane + 64u + 32u * h, d);
             tmem_ld16(tmem + lane + 64u + 32u * h + 16u, d + 16);
@@ -607,19 +567,21 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
 #pragma unroll
             for (int k = 0; k < 32; k++)
                 if (!((mask[l] >> k) & 1u)) d[k] = 0.0f;
+            const uint32_t sZ = sA + (uint32_t)(l + 1) * 16384u;
 #pragma unroll
-            for (int c = 0; c < 4; c++) store8(smem + TS_T1, r, 32 * h + 8 * c, d + 8 * c);
-            for (int k = 0; k < 32; k++) store_tp(smem + TS_DZT, 32 * h + k, r, d[k]);
+            for (int c = 0; c < 4; c++) store8(smem + TS_A + (l + 1) * 16384u, r, 32 * h + 8 * c, d + 8 * c);
             smem_to_tc();
             if (tid == 0) {
+                // dA_l = dZ_l W_l: dZ_l K-major, W_l MN-major (N = inputs, K = outputs)
 #pragma unroll
                 for (uint32_t ks = 0; ks < 4; ks++)
-                    mma_bf16(tmem + 64u, sdesc(sT1 + ks * 256u), sdesc(sWT + l * 8192u + ks * 256u), ID64,
+                    mma_bf16(tmem + 64u, sdesc(sZ + ks * 256u), mn64(sW + (uint32_t)l * 8192u, ks), ID_BMN,
                              ks > 0 ? 1u : 0u);
+                // dW_l += dZ_l^T A_l: both MN-major, K = the 128 samples
 #pragma unroll
                 for (uint32_t ks = 0; ks < 8; ks++)
-                    mma_bf16(tmem + 128u + 64u * l, sdesc_s(sDZT + ks * 2u * TP_LBO, TP_SBO, TP_LBO),
-                             at_desc(sAT, (uint32_t)l, ks), ID64, (any || ks > 0) ? 1u : 0u);
+                    mma_bf16(tmem + 128u + 64u * l, mn64(sZ, ks), mn64(sA + (uint32_t)l * 16384u, ks), ID_ABMN,
+                             (any || ks > 0) ? 1u : 0u);
                 mma_commit(bar);
             }
             ok = tc_step(bar, phase, polls);
@@ -703,7 +665,7 @@ void nrc_tc_forward_raw(const uint8_t *wimg, const float *in, float *out, uint32
                         uint32_t *err, uint32_t polls, cudaStream_t s, const cudaEvent_t *ev) {
     const uint32_t ntiles = (n + 127u) / 128u;
     if (ntiles == 0) return;
-    k_encode_tiles<0, false><<<ntiles, 256, 0, s>>>(NrcGrid{}, nullptr, nullptr, nullptr, n, in, tiles);
+    k_encode_tiles<0><<<ntiles, 256, 0, s>>>(NrcGrid{}, nullptr, nullptr, nullptr, n, in, tiles);
     if (ev) cudaEventRecord(ev[0], s);
     k_mlp_q<0><<<q_blocks<0>(ntiles), 128 * QC, QS_BYTES, s>>>(wimg, tiles, nullptr, n, nullptr, nullptr, out,
                                                              err, polls);
@@ -717,7 +679,7 @@ void nrc_tc_query(const uint8_t *wimg, const NrcGrid &g, const wl_disney *mats, 
                   uint8_t *tiles, cudaStream_t s, const cudaEvent_t *ev) {
     const uint32_t ntiles = (max_q + 127u) / 128u;
     if (ntiles == 0) return;
-    k_encode_tiles<1, false><<<ntiles, 256, 0, s>>>(g, mats, q, nq, max_q, nullptr, tiles);
+    k_encode_tiles<1><<<ntiles, 256, 0, s>>>(g, mats, q, nq, max_q, nullptr, tiles);
     if (ev) cudaEventRecord(ev[0], s);
     k_mlp_q<2><<<q_blocks<2>(ntiles), 128 * QC, QS_BYTES, s>>>(wimg, tiles, nq, max_q, q, rad, nullptr, err,
                                                              polls);
@@ -737,12 +699,12 @@ void nrc_tc_encode_rows(const NrcGrid &g, const wl_disney *mats, const NrcVertex
                         uint32_t count, uint8_t *tiles, float *rows, cudaStream_t s) {
     uint32_t ntiles = (count + TC_THREADS - 1) / TC_THREADS;
     if (ntiles == 0) return;
-    k_encode_tiles<1, false><<<ntiles, 256, 0, s>>>(g, mats, v, n_ptr, count, nullptr, tiles);
+    k_encode_tiles<1><<<ntiles, 256, 0, s>>>(g, mats, v, n_ptr, count, nullptr, tiles);
     k_tiles_to_rows<<<(uint32_t)(((uint64_t)count * 64u + 255) / 256), 256, 0, s>>>(tiles, count, rows);
 }
 
 // Gradients of one training step into w_grad (zeroed here) and the grid gradient; loss (zeroed
-// here) receives the mean relative L2 loss. Raw rows when samples is null. tiles: 32 KB per 128
+// here) receives the mean relative L2 loss. Raw rows when samples is null. tiles: 16 KB per 128
 // rows; gin: 32 floats per row.
 // Sum of the training kernel's per-CTA partial weight gradients, CTA by CTA in a fixed order
 // (so that the gradient does not depend on scheduling).

@@ -351,7 +351,7 @@ struct NrcGrid;
 constexpr uint32_t NRC_WAIT_POLLS = 1u << 22;
 // the bfloat16 operand image of the MLP weights (NRC_WEIGHT_IMAGE_BYTES), rebuilt after every
 // weight update; the query kernel and the training kernel copy it into shared memory
-constexpr uint32_t NRC_WEIGHT_IMAGE_BYTES = 2u * (4u * 8192u + 2048u);
+constexpr uint32_t NRC_WEIGHT_IMAGE_BYTES = 4u * 8192u + 2048u;
 void nrc_tc_weight_image(const float *w, uint8_t *img, cudaStream_t s);
 // ev (optional): two events recorded around the tensor-core kernel alone
 void nrc_tc_forward_raw(const uint8_t *wimg, const float *in, float *out, uint32_t n, uint8_t *tiles,
