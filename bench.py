@@ -825,8 +825,9 @@ def main():
     ms_step = ms_max / args.steps
     value = world * paths * args.steps / (ms_max * 1e-3) / 1e6
 
-    # end to end through the public API with host buffers: render + film download per step
-    host_film = np.empty((H, W, 3), np.float32)
+    # end to end through the public API with host buffers: render + film download per step, into
+    # page-locked host memory (as a caller that reads a film every frame would keep it)
+    host_film = torch.empty((H, W, 3), dtype=torch.float32, pin_memory=True).numpy()
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
