@@ -487,6 +487,8 @@ def bdpt_ao_leg(wl, torch, ctx, res=1024, spp=256, oracle_spp=2048, ao_res=(512,
     out = {"scene": f"glass sphere {sc.num_tris} tris, roughness 0.05, {res}x{res}, subpaths <= 10 vertices",
            "spp": spp, "ms": round(ms, 1), "msamples_s": round(samples / ms / 1e3, 2),
            "closest_hit_rays_per_sample": round(st["segments"] / samples, 3),
+           "kernels_ms": {"closest_hit": round(st["ms_extend"], 1), "vertices_and_connect": round(st["ms_shade"], 1),
+                          "connection_rays": round(st["ms_shadow"], 1), "other": round(st["ms_other"], 1)},
            "connection_rays_per_sample": round(st["shadow_rays"] / samples, 3),
            "relmse_vs_fp64_oracle": rel(img, r64),
            "oracle": f"BDPT in strict math (the reference's estimator, bit-exact per sample), {oracle_spp} spp, "
