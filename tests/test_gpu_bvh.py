@@ -70,6 +70,14 @@ def test_cast_bitexact(ctx, oracle, name, V, I):
     anyr = oracle.cast_bruteforce(g.V, g.I, rays, 1)
     anyg = cast_device(ctx, sc, rays, wl.CAST_ANY)
     assert np.array_equal(anyg["prim"] == wl.INVALID, anyr["prim"] == wl.INVALID)
+    # any hits with a node's children visited far to near (the shadow pass's tunable order)
+    ctx.set_tune(dict(wave_paths=0, extend_ctas_per_sm=0, extend_refill=12, shadow_ctas_per_sm=0,
+                      shadow_refill=12, shadow_far_first=1))
+    try:
+        anyf = cast_device(ctx, sc, rays, wl.CAST_ANY)
+    finally:
+        ctx.set_tune(None)
+    assert np.array_equal(anyf["prim"] == wl.INVALID, anyr["prim"] == wl.INVALID)
     sc.close()
 
 

@@ -272,7 +272,7 @@ def test_tuned_shapes_keep_the_image(ctx):
     imgs = []
     for tune in (None, dict(wave_paths=1 << 12, extend_ctas_per_sm=4, extend_refill=8,
                             shadow_ctas_per_sm=6, shadow_refill=24, extend_postpone=0,
-                            shadow_postpone=32),
+                            shadow_postpone=32, shadow_far_first=1),
                  dict(wave_paths=1 << 13, extend_ctas_per_sm=0, extend_refill=4,
                       shadow_ctas_per_sm=0, shadow_refill=4, extend_postpone=32,
                       shadow_postpone=0)):
@@ -290,6 +290,17 @@ def test_tuned_shapes_keep_the_image(ctx):
     wl.render(ctx, s, sc.camera_struct(), p, film)
     assert np.array_equal(bits(film.download()), bits(imgs[0]))
     film.close()
+    # the bidirectional program's connection rays take the shadow pass's any-hit order
+    bp = wl.render_params(48, 32, 2, strategy=wl.STRATEGY_BDPT, max_depth=6, math=wl.MATH_STRICT)
+    bimgs = []
+    for far in (0, 1):
+        ctx.set_tune(dict(wave_paths=0, extend_ctas_per_sm=0, extend_refill=12, shadow_ctas_per_sm=0,
+                          shadow_refill=12, shadow_far_first=far))
+        film = wl.Film(ctx, 48, 32)
+        wl.render(ctx, s, sc.camera_struct(), bp, film)
+        bimgs.append(film.download())
+        film.close()
+    assert bimgs[0].max() > 0 and np.array_equal(bits(bimgs[0]), bits(bimgs[1]))
     ctx.set_tune(None)
     s.close()
 
