@@ -149,7 +149,7 @@ typedef struct wl_render_params {
     float env[3];           /* constant radiance returned by a miss (reference: 0) */
     uint32_t wave_paths;    /* paths in flight per wave (<= 2^27); 0 = automatic: the context's
                                tuned size, else as many as the render has, up to 2^27 paths
-                               (192 B of queues each) and a quarter of the device memory free
+                               (232 B of queues each) and a quarter of the device memory free
                                at the context's first render. WL_STRATEGY_BDPT: samples per
                                wave, automatic = as many as a quarter of the free device
                                memory holds (about 8.4 KB each at 10 vertices) */
@@ -482,7 +482,7 @@ WL_API int wl_debug_rng(wl_context *ctx, uint32_t rng, uint64_t seed, const uint
 /* ---- rendering without device allocation ------------------------------------------- */
 /* No counterpart in the reference. Same result as wl_render, but the call allocates no device
  * memory: its path queues live in one static device array of WL_NOALLOC_SCRATCH_BYTES
- * (about 12 MiB), which every GPU that loads this library holds until the process exits.
+ * (about 14.5 MiB), which every GPU that loads this library holds until the process exits.
  * It serves callers that must not call cudaMalloc once they are running. Examples are a host
  * that reserves its whole device-memory budget up front, and a real-time frame loop where an
  * allocation's implicit device synchronisation would stall the frame.
@@ -501,7 +501,7 @@ WL_API int wl_debug_rng(wl_context *ctx, uint32_t rng, uint64_t seed, const uint
  *    its own waves, and it restores the caller's current device before returning.
  *  - No render statistics are recorded (wl_render_get_stats keeps the last wl_render's). */
 #define WL_NOALLOC_MAX_PATHS 65536u
-#define WL_NOALLOC_SCRATCH_BYTES (192u * WL_NOALLOC_MAX_PATHS + 512u)
+#define WL_NOALLOC_SCRATCH_BYTES (232u * WL_NOALLOC_MAX_PATHS + 512u)
 WL_API int wl_render_noalloc(wl_context *ctx, wl_scene *scene, const wl_camera *camera,
                              const wl_render_params *params, wl_film *film);
 

@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(AT) k_ao_generate(AoWave w, Queues q) {
     q.ray_o[0][i] = make_float4(w.cam_pos[0], w.cam_pos[1], w.cam_pos[2], w.eps);
     q.ray_d[0][i] = make_float4(dir.x, dir.y, dir.z, 1e30f);
     q.ray_slot[0][i] = i;
-    q.st_rng[i] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
+    q.st_rng[0][i] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
 }
 
 __global__ void __launch_bounds__(AT) k_ao_occlude(AoWave w, DevScene sc, Queues q) {
@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(AT) k_ao_occlude(AoWave w, DevScene sc, Queues
     if (prim != INVALID) {
         float4 ro = q.ray_o[0][i], rd = q.ray_d[0][i];
         v3 dir = f4xyz(rd);
-        uint2 rs = q.st_rng[i];
+        uint2 rs = q.st_rng[0][i];
         uint64_t g = w.base + i;
         Rng rng;
         rng.mode = w.rng;

@@ -164,11 +164,11 @@ DevScene dev_scene(const wl_scene *s) {
 template <class T> size_t al(size_t n) { return ((n * sizeof(T) + 255) / 256) * 256; }
 
 // Bytes of path state and queues per path in flight (ensure_queues).
-constexpr uint64_t QUEUE_BYTES_PER_PATH = 192;
+constexpr uint64_t QUEUE_BYTES_PER_PATH = 232;
 
 // Automatic paths per wave: as many as a render can use, since every wave ends in a tail of
 // small, latency-bound bounce launches (one wave of a 1080p x 64 spp render ran 10 % faster than
-// four). Capped at 2^27 paths (about 26 GB of queues) and at a quarter of the device memory that
+// four). Capped at 2^27 paths (about 31 GB of queues) and at a quarter of the device memory that
 // is free when the context first needs it; fixed from then on.
 uint64_t auto_wave(wl_context *c) {
     if (!c->auto_wave) {
@@ -209,7 +209,7 @@ int ensure_queues(wl_context *c, uint32_t cap) {
         c->q_block = nullptr;
     }
     size_t f4 = al<float4>(cap), u32 = al<uint32_t>(cap), u2 = al<uint2>(cap);
-    size_t total = 4 * f4 + 2 * u32 + f4 + 3 * f4 + u2 + 3 * f4 + 256 + 256;
+    size_t total = 4 * f4 + 2 * u32 + f4 + 5 * f4 + 2 * u2 + 3 * f4 + 256 + 256;
     CK(cudaMalloc(&c->q_block, total));
     char *p = (char *)c->q_block;
     Queues &q = c->q;
@@ -221,10 +221,12 @@ int ensure_queues(wl_context *c, uint32_t cap) {
     q.ray_slot[0] = (uint32_t *)p; p += u32;
     q.ray_slot[1] = (uint32_t *)p; p += u32;
     q.hit = (float4 *)p; p += f4;
-    q.st_thr = (float4 *)p; p += f4;
-    q.st_term = (float4 *)p; p += f4;
+    for (int k = 0; k < 2; k++) {
+        q.st_thr[k] = (float4 *)p; p += f4;
+        q.st_term[k] = (float4 *)p; p += f4;
+        q.st_rng[k] = (uint2 *)p; p += u2;
+    }
     q.st_rad = (float4 *)p; p += f4;
-    q.st_rng = (uint2 *)p; p += u2;
     q.sh_o = (float4 *)p; p += f4;
     q.sh_d = (float4 *)p; p += f4;
     q.sh_l = (float4 *)p; p += f4;

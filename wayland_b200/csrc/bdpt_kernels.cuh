@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(PT) k_bd_eye_gen(WaveParams wp, Queues q, Bdpt
     q.ray_d[0][i] = make_float4(dir.x, dir.y, dir.z, 1e30f);
     q.ray_slot[0][i] = i;
     q.st_rad[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    q.st_rng[i] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
+    q.st_rng[0][i] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
     bw.n_eye[i] = 0;
     bw.n_light[i] = 0;
 }
@@ -211,7 +211,7 @@ __device__ __forceinline__ Rng bd_rng(const WaveParams &wp, const Queues &q, uin
     Rng rng;
     rng.mode = wp.rng;
     rng.pixel = (uint32_t)((wp.base + slot) % wp.npix);
-    uint2 rs = q.st_rng[slot];
+    uint2 rs = q.st_rng[0][slot];
     rng.state = (uint64_t)rs.x | ((uint64_t)rs.y << 32);
     return rng;
 }
@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(PT) k_bd_eye(WaveParams wp, DevScene sc, Queue
                     Rng rng = bd_rng(wp, q, slot);
                     Mat m = load_mat(sc.mats + e.id);
                     ndir = normalize(sample_disney(m, e.ns, e.wi, rng));
-                    q.st_rng[slot] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
+                    q.st_rng[0][slot] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
                     npos = e.pos;
                     push = depth < bw.maxv;
                     // with a radiance cache, the last eye vertex asks the cache for the radiance
@@ -370,7 +370,7 @@ __global__ void __launch_bounds__(PT) k_bd_light_gen(WaveParams wp, DevScene sc,
             l.aux = dir_pdf;
             bd_store(bw.lit, cap, 0, slot, l);
             bw.n_light[slot] = 1;
-            q.st_rng[slot] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
+            q.st_rng[0][slot] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
             push = bw.maxl > 1;
         }
         uint32_t pos = warp_append(push, &q.counters[0]);
@@ -433,7 +433,7 @@ __global__ void __launch_bounds__(PT) k_bd_light(WaveParams wp, DevScene sc, Que
                         Rng rng = bd_rng(wp, q, slot);
                         Mat m = load_mat(sc.mats + v.id);
                         ndir = normalize(sample_disney(m, v.ns, v.wi, rng));
-                        q.st_rng[slot] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
+                        q.st_rng[0][slot] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
                         npos = v.pos;
                         push = true;
                     }

@@ -20,7 +20,7 @@ using namespace wl;
 namespace {
 
 constexpr uint32_t MAX_PATHS = WL_NOALLOC_MAX_PATHS;
-constexpr size_t PER_PATH = 192;  // bytes of queues and path state per path slot
+constexpr size_t PER_PATH = 232;  // bytes of queues and path state per path slot
 static_assert(PER_PATH * MAX_PATHS + 512 == WL_NOALLOC_SCRATCH_BYTES, "scratch layout size");
 
 // The scratch: every GPU that loads this library holds it until the process exits.
@@ -40,10 +40,12 @@ Queues carve(void *base) {
     q.ray_slot[0] = (uint32_t *)p; p += u32;
     q.ray_slot[1] = (uint32_t *)p; p += u32;
     q.hit = (float4 *)p; p += f4;
-    q.st_thr = (float4 *)p; p += f4;
-    q.st_term = (float4 *)p; p += f4;
+    for (int k = 0; k < 2; k++) {
+        q.st_thr[k] = (float4 *)p; p += f4;
+        q.st_term[k] = (float4 *)p; p += f4;
+        q.st_rng[k] = (uint2 *)p; p += u2;
+    }
     q.st_rad = (float4 *)p; p += f4;
-    q.st_rng = (uint2 *)p; p += u2;
     q.sh_o = (float4 *)p; p += f4;
     q.sh_d = (float4 *)p; p += f4;
     q.sh_l = (float4 *)p; p += f4;

@@ -59,10 +59,10 @@ __global__ void __launch_bounds__(PT) k_generate(WaveParams wp, Queues q) {
     q.ray_o[0][i] = make_float4(wp.cam_pos[0], wp.cam_pos[1], wp.cam_pos[2], wp.eps);
     q.ray_d[0][i] = make_float4(dir.x, dir.y, dir.z, 1e30f);
     q.ray_slot[0][i] = i;
-    q.st_thr[i] = make_float4(1.f, 1.f, 1.f, 1.f);
-    q.st_term[i] = make_float4(1.f, 1.f, 1.f, __uint_as_float(0u));
+    q.st_thr[0][i] = make_float4(1.f, 1.f, 1.f, 1.f);
+    q.st_term[0][i] = make_float4(1.f, 1.f, 1.f, __uint_as_float(0u));
     q.st_rad[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    q.st_rng[i] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
+    q.st_rng[0][i] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
 }
 
 __device__ __forceinline__ v3 vtx(const float *V, uint32_t i) {
@@ -126,6 +126,8 @@ struct ShadeOut {
     uint32_t slot = 0;
     float eps = 0.f, sh_tmax = 0.f;
     v3 new_o, new_d, sh_d, ld;
+    float4 thr, term;  // the continuing path's state, stored with its next ray
+    uint2 rng;
 };
 
 // __closesthit__radiance + the NEE block of __raygen__RenderFrame for ray i of queue `in`,
@@ -142,8 +144,8 @@ __device__ __forceinline__ void shade_lane(const WaveParams &wp, const DevScene 
             slot = q.ray_slot[in][i];
             float4 h = q.hit[i];
             float4 ro = q.ray_o[in][i], rd = q.ray_d[in][i];
-            float4 thr4 = q.st_thr[slot], term4 = q.st_term[slot], rad4 = q.st_rad[slot];
-            uint2 rs = q.st_rng[slot];
+            float4 thr4 = q.st_thr[in][i], term4 = q.st_term[in][i], rad4 = q.st_rad[slot];
+            uint2 rs = q.st_rng[in][i];
             v3 thr = f4xyz(thr4), term = f4xyz(term4), rad = f4xyz(rad4);
             float last_pdf = thr4.w;
             uint32_t depth = __float_as_uint(term4.w);
@@ -331,10 +333,10 @@ __device__ __forceinline__ void shade_lane(const WaveParams &wp, const DevScene 
                 }
             }
             (void)alive;
-            q.st_thr[slot] = make_float4(thr.x, thr.y, thr.z, last_pdf);
-            q.st_term[slot] = make_float4(term.x, term.y, term.z, __uint_as_float(depth));
+            o.thr = make_float4(thr.x, thr.y, thr.z, last_pdf);
+            o.term = make_float4(term.x, term.y, term.z, __uint_as_float(depth));
             q.st_rad[slot] = make_float4(rad.x, rad.y, rad.z, 0.f);
-            q.st_rng[slot] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
+            o.rng = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
         }
     }
     o.push_ray = push_ray;
@@ -355,6 +357,9 @@ __device__ __forceinline__ void shade_emit(const Queues &q, int out, bool valid,
         q.ray_o[out][rpos] = make_float4(o.new_o.x, o.new_o.y, o.new_o.z, o.eps);
         q.ray_d[out][rpos] = make_float4(o.new_d.x, o.new_d.y, o.new_d.z, 1e30f);
         q.ray_slot[out][rpos] = o.slot;
+        q.st_thr[out][rpos] = o.thr;
+        q.st_term[out][rpos] = o.term;
+        q.st_rng[out][rpos] = o.rng;
     }
     uint32_t spos = warp_append(o.push_shadow, &q.counters[2]);
     if (o.push_shadow) {
@@ -483,10 +488,10 @@ __global__ void __launch_bounds__(PT) k_generate_batch(BatchView bv, Queues q, u
     q.ray_o[0][i] = make_float4(wp.cam_pos[0], wp.cam_pos[1], wp.cam_pos[2], wp.eps);
     q.ray_d[0][i] = make_float4(dir.x, dir.y, dir.z, 1e30f);
     q.ray_slot[0][i] = i;
-    q.st_thr[i] = make_float4(1.f, 1.f, 1.f, 1.f);
-    q.st_term[i] = make_float4(1.f, 1.f, 1.f, __uint_as_float(0u));
+    q.st_thr[0][i] = make_float4(1.f, 1.f, 1.f, 1.f);
+    q.st_term[0][i] = make_float4(1.f, 1.f, 1.f, __uint_as_float(0u));
     q.st_rad[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    q.st_rng[i] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
+    q.st_rng[0][i] = make_uint2((uint32_t)rng.state, (uint32_t)(rng.state >> 32));
 }
 
 // The shade pass of a batch wave: each ray with its job's scene and parameters.

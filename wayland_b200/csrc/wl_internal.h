@@ -57,18 +57,20 @@ __device__ __forceinline__ uint32_t leaf_prim(const DevScene &sc, uint32_t leaf)
 }
 #endif
 
-// Path-state arrays of one wave (structure of arrays in HBM, indexed by path slot).
+// Path-state arrays of one wave (structure of arrays in HBM).
 struct Queues {
     uint32_t capacity;
     // ray queues A/B: 32-byte rays as two float4, plus the path slot of each entry
     float4 *ray_o[2], *ray_d[2];
     uint32_t *ray_slot[2];
     float4 *hit;             // (t, prim, u, v) for the current queue
-    // per path slot
-    float4 *st_thr;          // throughput.xyz, last bsdf pdf
-    float4 *st_term;         // last trace term (bsdf |cos| / pdf).xyz, depth (bits)
-    float4 *st_rad;          // radiance.xyz
-    uint2 *st_rng;           // random stream state
+    // The path tracer's state moves with its ray: entry i of ray queue A / B has its state at
+    // index i of buffer 0 / 1, so that the shade pass reads and writes it coalesced. The
+    // bidirectional and AO programs index buffer 0 by path slot.
+    float4 *st_thr[2];       // throughput.xyz, last bsdf pdf
+    float4 *st_term[2];      // last trace term (bsdf |cos| / pdf).xyz, depth (bits)
+    uint2 *st_rng[2];        // random stream state
+    float4 *st_rad;          // radiance.xyz, by path slot
     // shadow queue: origin/tmin, dir/tmax, (Ld.xyz, slot)
     float4 *sh_o, *sh_d, *sh_l;
     // counters: [0], [1] ray queue sizes, [2] shadow queue size, [3] segments, [4] shadow rays,
