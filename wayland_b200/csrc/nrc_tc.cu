@@ -295,16 +295,25 @@ __global__ void __launch_bounds__(128 * QC, 1)
 
 // ---------------------------------------------------------------------------------------
 // Training step on the tensor cores: forward, relative-L2 loss, backward and weight gradients
-// of 128 samples per tile, fused in one persistent kernel (one CTA of 256 threads per SM).
-// Thread t owns sample row r = t % 128 and column half h = t / 128 of every 64-wide tile (warp
-// w reads tensor-memory lanes 32 (w % 4) .. + 31). Operands are bfloat16 with FP32
-// accumulation: activations (as in inference), the loss gradient dY and the pre-activation
-// gradients dZ are rounded to bfloat16 where they become MMA operands.
+// of 128 samples per tile, fused in one persistent kernel (one CTA per SM) that keeps two tiles
+// in flight in two slots (shared memory holds no third). Warp 0 is the MMA warp: its lane 0 issues
+// every tensor-core product of both slots, alternating between them in a fixed order, so that
+// while one slot's threads convert accumulators the tensor core runs the other slot's products.
+// Each tile is a chain of ten dependent phases of 77 products in all (M = 128, N = 64, K = 16);
+// with one tile in flight the round trips left the tensor core idle most of the time, with two it
+// is busy for about three quarters of it. Each slot has 8
+// epilogue warps: warp w reads tensor-memory lanes 32 (w % 4) .. + 31, i.e. sample row
+// r = 32 (w % 4) + lane, and column half h of every 64-wide tile. The slots hand off through
+// mbarriers: the epilogue warps arrive on the slot's epilogue barrier when the next product's
+// operand is in shared memory, the MMA warp commits each product to the slot's MMA barrier.
+// Operands are bfloat16 with FP32 accumulation: activations (as in inference), the loss
+// gradient dY and the pre-activation gradients dZ are rounded to bfloat16 where they become MMA
+// operands.
 //   forward   A_{l+1} = relu(A_l W_l^T), out = A_4 W_4^T            (M=128, K=64, N=64 / 16)
 //   backward  dA_4 = dY W_4, dZ_l = dA_{l+1} * [A_{l+1} > 0], dA_l = dZ_l W_l
 //   weights   dW_l += dZ_l^T A_l over the tile's 128 samples (K = 128), accumulated in tensor
-//             memory across all tiles of the CTA (M = 128 with the rows past the 64 (16) outputs
-//             unused), added to the global gradient once at the end
+//             memory across all tiles of both slots (M = 128 with the rows past the 64 (16)
+//             outputs unused), in the MMA warp's fixed issue order, written out once at the end
 //   grid      dA_0[:, 0:32] scattered into the hash grid's gradient
 // Every tile is stored once, K-major as the forward pass reads it (row = sample). The products
 // that contract over samples (dW) or over outputs (dA = dZ W) read the same bytes as MN-major
@@ -312,22 +321,31 @@ __global__ void __launch_bounds__(128 * QC, 1)
 // matrices, 8 consecutive features of one sample are one 16-byte core-matrix row, which is the
 // MN-major core matrix (8 K-rows of 8 contiguous M or N elements) with the feature groups
 // (MN atoms) 128 bytes apart and the sample groups (K atoms) 1024 bytes apart.
-// Shared memory: the forward weight image (W_0..W_4, row = output), the five activation tiles
-// A_0..A_4 (dZ_l overwrites A_{l+1} once dW_{l+1} has read it) and dY.
-// Tensor memory: columns 0-63 forward D, 64-127 backward D, 128 + 64 l the dW_l accumulators.
-constexpr int TR_THREADS = 256;
+// Shared memory: the forward weight image (W_0..W_4, row = output), then per slot the five
+// activation tiles A_0..A_4 (dZ_l overwrites A_{l+1} once dW_{l+1} has read it) and dY.
+// Tensor memory: columns 64 s the slot's accumulator (forward and backward products in turn),
+// 128 + 64 l the dW_l accumulators.
+constexpr uint32_t TR_SLOTS = 2;
+constexpr uint32_t TR_EPI = 256;                             // epilogue threads per slot
+constexpr uint32_t TR_THREADS = 32 + TR_SLOTS * TR_EPI;      // the MMA warp + 16 epilogue warps
+constexpr uint32_t TR_PHASES = 10;                           // products per tile
 constexpr uint32_t TR_TMEM_COLS = 512;
-constexpr uint32_t TS_W = 0;                    // W_0..W_3 (row = output), 8 KB each, then W_4
-constexpr uint32_t TS_A = WI_FWD;               // A_0..A_4, 16 KB each (A_0 as bulk-copied)
-constexpr uint32_t TS_DY = TS_A + 5 * 16384;    // dY, 128 x 16
+constexpr uint32_t TS_W = 0;                                 // W_0..W_3 (row = output), 8 KB each, then W_4
+constexpr uint32_t TS_SLOT = WI_FWD;                         // slot s at TS_SLOT + s * TS_SLOT_BYTES
+constexpr uint32_t TS_DY = 5 * 16384;                        // within a slot: A_0..A_4, then dY (128 x 16)
 // an M=128 MN-major read of dY (16 real rows) or of a dZ tile (64 real rows) spans up to 2 KB
 // more than the 128 x 16 (x 64) data; the rows past the real ones feed unused accumulator rows
-constexpr uint32_t TS_BAR = TS_DY + 4096 + 2048;  // MMA completion
-constexpr uint32_t TS_WBAR = TS_BAR + 8;          // the weights' bulk copy
-constexpr uint32_t TS_LBAR = TS_BAR + 16;         // each tile's bulk copy
-constexpr uint32_t TS_TMEM = TS_BAR + 24;
-constexpr uint32_t TS_BYTES = TS_TMEM + 8;
-static_assert(TS_A % 1024 == 0 && TS_BYTES <= 232448, "training kernel shared-memory layout");
+constexpr uint32_t TS_SLOT_BYTES = TS_DY + 4096 + 2048;
+constexpr uint32_t TS_BAR = TS_SLOT + TR_SLOTS * TS_SLOT_BYTES;
+// mbarriers: the weights' bulk copy, the MMA warp's final commit, then per slot: the input
+// tile's bulk copy, the slot's products (commit), the slot's operands (TR_EPI arrivals)
+constexpr uint32_t TS_NBAR = 2 + 3 * TR_SLOTS;
+constexpr uint32_t TS_TMEM = TS_BAR + 8 * TS_NBAR;
+constexpr uint32_t TS_ABORT = TS_TMEM + 4;                   // set by a thread whose wait gave up
+constexpr uint32_t TS_BYTES = TS_ABORT + 4;
+static_assert(TS_SLOT % 1024 == 0 && TS_SLOT_BYTES % 1024 == 0 && TS_BYTES <= 232448,
+              "training kernel shared-memory layout");
+static_assert(TR_SLOTS * 64 + 5 * 64 <= TR_TMEM_COLS, "training kernel tensor-memory layout");
 
 // K-major tile with 16 columns (core matrices 8 rows x 16 bytes, 8-row groups 256 B apart)
 __device__ __forceinline__ uint32_t kmaj16(uint32_t r, uint32_t k) {
@@ -363,18 +381,29 @@ __device__ __forceinline__ void store8(uint8_t *tile, uint32_t r, uint32_t k0, c
     *reinterpret_cast<uint4 *>(tile + kmaj(r, k0)) = u;
 }
 
-__device__ __forceinline__ bool tc_step(uint32_t bar, uint32_t &phase, uint32_t polls) {
-    bool got = mbar_wait(bar, phase, polls);
-    phase ^= 1u;
-    bool ok = __syncthreads_and(got) != 0;
-    tc_after_sync();
-    return ok;
+// A bounded wait (as mbar_wait) that also gives up once another thread of the CTA has set the
+// abort word, so that one wait that ran out ends the whole CTA's loops without each remaining wait
+// polling to its own limit.
+__device__ __forceinline__ bool mbar_wait_or_abort(uint32_t bar, uint32_t phase, uint32_t polls,
+                                                   const volatile uint32_t *abort) {
+    for (uint32_t it = 0; it < polls; it++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t"
+            ".reg .pred P1;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, P1;\n\t"
+            "}\n"
+            : "=r"(ok)
+            : "r"(bar), "r"(phase)
+            : "memory");
+        if (ok) return true;
+        if (*abort) return false;
+    }
+    return false;
 }
-__device__ __forceinline__ void smem_to_tc() {
-    fence_async_smem();
-    tc_before_sync();
-    __syncthreads();
-    tc_after_sync();
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
 // Encoded inputs in the tensor-core operand layout, one 16 KB K-major tile per 128 rows (row =
@@ -427,21 +456,68 @@ __global__ void __launch_bounds__(256) k_grid_scatter(NrcGrid g, const NrcVertex
     nrc_grid_backward(g, samples[s], g2, l, l + 1u);
 }
 
+// The products of phase p (0..9) of one tile in slot s, issued by the MMA warp's lane 0: p 0..4
+// forward layer p; p 5 dA_4 = dY W_4 and dW_4 += dY^T A_4; p 6..9 layer l = 9 - p, dA_l = dZ_l W_l
+// and dW_l += dZ_l^T A_l. The descriptors are built once per phase as a base plus constant steps (a
+// descriptor's low 14 bits are the address / 16; no shared address here reaches 2^18, so the steps
+// never carry out of the field). wmask: the dW_l accumulators written before (the first product
+// into each starts from zero).
+__device__ __forceinline__ void train_phase(uint32_t p, uint32_t sb, uint32_t sW, uint32_t d, uint32_t dw,
+                                            uint32_t &wmask) {
+    const uint32_t ID64 = idesc(64, 128), ID16 = idesc(16, 128);
+    const uint32_t ID_BMN = idesc_mn(64, 128, false, true), ID_ABMN = idesc_mn(64, 128, true, true);
+    if (p < 5) {
+        const uint64_t a = sdesc(sb + p * 16384u), b = sdesc(sW + p * 8192u);
+        const uint32_t id = p < 4 ? ID64 : ID16;
+#pragma unroll
+        for (uint32_t ks = 0; ks < 4; ks++) mma_bf16(d, a + 16u * ks, b + 16u * ks, id, ks > 0 ? 1u : 0u);
+    } else if (p == 5) {
+        // dA_4 = dY W_4 (W_4 read MN-major: N = its 64 inputs, K = its 16 outputs); dW_4 += dY^T A_4
+        // (dY MN-major: M = its 16 outputs, K = the samples, 8-row groups 256 B apart; A_4 MN-major)
+        const uint64_t y = sdesc_s(sb + TS_DY, 256u, 128u), w = sdesc_s(sW + 4u * 8192u, 128u, 1024u);
+        const uint64_t yt = sdesc_s(sb + TS_DY, 128u, 256u), a4 = mn64(sb + 4u * 16384u, 0);
+        const uint32_t acc = (wmask >> 4) & 1u;
+        mma_bf16(d, y, w, ID_BMN, 0u);
+#pragma unroll
+        for (uint32_t ks = 0; ks < 8; ks++)
+            mma_bf16(dw + 4u * 64u, yt + 32u * ks, a4 + 128u * ks, ID_ABMN, (acc || ks > 0) ? 1u : 0u);
+        wmask |= 16u;
+    } else {
+        const uint32_t l = 9u - p;
+        const uint32_t sZ = sb + (l + 1u) * 16384u;
+        // dA_l = dZ_l W_l: dZ_l K-major, W_l MN-major (N = inputs, K = outputs); dW_l += dZ_l^T A_l:
+        // both MN-major, K = the 128 samples
+        const uint64_t z = sdesc(sZ), wl_ = mn64(sW + l * 8192u, 0);
+        const uint64_t zt = mn64(sZ, 0), al = mn64(sb + l * 16384u, 0);
+        const uint32_t acc = (wmask >> l) & 1u;
+#pragma unroll
+        for (uint32_t ks = 0; ks < 4; ks++) mma_bf16(d, z + 16u * ks, wl_ + 128u * ks, ID_BMN, ks > 0 ? 1u : 0u);
+#pragma unroll
+        for (uint32_t ks = 0; ks < 8; ks++)
+            mma_bf16(dw + 64u * l, zt + 128u * ks, al + 128u * ks, ID_ABMN, (acc || ks > 0) ? 1u : 0u);
+        wmask |= 1u << l;
+    }
+}
+
 // MODE 0: raw rows in[n][64], targets target[n][4]. MODE 1: the collected training samples
 // (count on the device), encoded by k_encode_tiles; the input gradient goes to the hash grid.
+// The CTA's tiles are blockIdx.x + j gridDim.x, j = 0, 1, ...; tile j runs in slot j % 2.
 template <int MODE>
 __global__ void __launch_bounds__(TR_THREADS, 1)
     k_train_tc(const uint8_t *wimg, const NrcVertex *samples, const uint32_t *n_ptr, uint32_t n_fixed,
                const float *target, const uint8_t *tiles, float *gin_out, float *w_part,
                float *loss, uint32_t *err, uint32_t polls) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    const uint32_t tid = threadIdx.x, warp = tid >> 5;
-    const uint32_t r = tid & 127u, h = tid >> 7;
-    const uint32_t bar = smem_u32(smem + TS_BAR), wbar = smem_u32(smem + TS_WBAR), lbar = smem_u32(smem + TS_LBAR);
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TS_BAR);
+    const uint32_t wbar = smem_u32(bars), fbar = smem_u32(bars + 1);
+    volatile uint32_t *abort = reinterpret_cast<volatile uint32_t *>(smem + TS_ABORT);
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(wbar) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(lbar) : "memory");
+        for (uint32_t k = 0; k < TS_NBAR; k++) {
+            const uint32_t count = (k >= 2 && (k - 2) % 3 == 2) ? TR_EPI : 1u;
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bars + k)), "r"(count) : "memory");
+        }
+        *abort = 0u;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         // the weights, one bulk copy of the bfloat16 image (row = output)
         bulk_load(smem_u32(smem + TS_W), wimg, WI_FWD, wbar);
@@ -451,187 +527,222 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
                      "r"(TR_TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
     }
-    smem_to_tc();
+    tc_before_sync();
+    __syncthreads();
+    tc_after_sync();
     const uint32_t tmem = *reinterpret_cast<volatile uint32_t *>(smem + TS_TMEM);
-    const uint32_t lane = ((warp & 3u) * 32u) << 16;
     const uint32_t n = MODE == 1 ? min(*n_ptr, n_fixed) : n_fixed;
-    const float inv = n ? 1.0f / (3.0f * (float)n) : 0.0f;
-    const uint32_t ID64 = idesc(64, 128), ID16 = idesc(16, 128);
-    const uint32_t ID_BMN = idesc_mn(64, 128, false, true), ID_ABMN = idesc_mn(64, 128, true, true);
-    const uint32_t sW = smem_u32(smem + TS_W), sA = smem_u32(smem + TS_A), sDY = smem_u32(smem + TS_DY);
-    uint32_t phase = 0, lphase = 0;
-    bool wok = __syncthreads_and(mbar_wait(wbar, 0, polls)) != 0;
-    bool ok = wok, any = false, lpending = false;
+    const uint32_t ntiles = (n + 127u) / 128u;
+    const uint32_t cnt = blockIdx.x < ntiles ? (ntiles - blockIdx.x + gridDim.x - 1u) / gridDim.x : 0u;
+    bool ok = true;
     float lsum = 0.0f;
-    for (uint32_t tile = blockIdx.x * 128u; tile < n && ok; tile += gridDim.x * 128u) {
-        const uint32_t i = tile + r;
-        const bool valid = i < n;
-        // ---- inputs: the encoded tile (k_encode_tiles), 16 KB in one bulk copy, into A_0
-        float t3[3] = {0.f, 0.f, 0.f};
-        if (tid == 0) bulk_load(sA, tiles + (size_t)(tile / 128u) * 16384u, 16384u, lbar);
-        lpending = true;
-        if (__syncthreads_and(mbar_wait(lbar, lphase, polls)) == 0) {
-            ok = false;
-            break;
-        }
-        lpending = false;
-        lphase ^= 1u;
-        if (valid && h == 0) {
-            if (MODE == 1) {
-                float4 e = samples[i].extra;
-                t3[0] = e.x; t3[1] = e.y; t3[2] = e.z;
-            } else {
-                for (int c = 0; c < 3; c++) t3[c] = target[(size_t)i * 4 + c];
-            }
-        }
-        smem_to_tc();
-        // ---- forward
-        uint32_t mask[4];
-        for (uint32_t l = 0; l < 5 && ok; l++) {
-            const uint32_t sAl = sA + l * 16384u;
-            const uint32_t sB = sW + l * 8192u;  // W_4 follows W_3
-            if (tid == 0) {
+    if (warp == 0) {
+        // ---- the MMA warp
+        if (lane == 0) {
+            const bool wok = mbar_wait_or_abort(wbar, 0, polls, abort);
+            ok = wok;
+            const uint32_t sW = smem_u32(smem + TS_W);
+            uint32_t left[2] = {(cnt + 1u) / 2u * TR_PHASES, cnt / 2u * TR_PHASES};
+            uint32_t ph[2] = {0, 0}, eph[2] = {0, 0}, wmask = 0;
+            while (ok && (left[0] | left[1])) {
 #pragma unroll
-                for (uint32_t ks = 0; ks < 4; ks++)
-                    mma_bf16(tmem, sdesc(sAl + ks * 256u), sdesc(sB + ks * 256u), l < 4 ? ID64 : ID16,
-                             ks > 0 ? 1u : 0u);
-                mma_commit(bar);
-            }
-            ok = tc_step(bar, phase, polls);
-            if (!ok) break;
-            if (l < 4) {
-                float a[32];
-                tmem_ld16(tmem + lane + 32u * h, a);
-                tmem_ld16(tmem + lane + 32u * h + 16u, a + 16);
-                tmem_wait_ld();
-                uint32_t m = 0;
-#pragma unroll
-                for (int k = 0; k < 32; k++) {
-                    a[k] = bf16r(fmaxf(a[k], 0.0f));
-                    m |= (a[k] > 0.0f ? 1u : 0u) << k;
+                for (uint32_t s = 0; s < TR_SLOTS; s++) {
+                    if (!ok) break;
+                    if (left[s] == 0) continue;
+                    if (!mbar_wait_or_abort(smem_u32(bars + 2 + 3 * s + 2), eph[s], polls, abort)) {
+                        ok = false;
+                        break;
+                    }
+                    eph[s] ^= 1u;
+                    tc_after_sync();
+                    train_phase(ph[s], smem_u32(smem + TS_SLOT + s * TS_SLOT_BYTES), sW, tmem + 64u * s, tmem + 128u,
+                                wmask);
+                    mma_commit(smem_u32(bars + 2 + 3 * s + 1));
+                    ph[s] = ph[s] + 1u == TR_PHASES ? 0u : ph[s] + 1u;
+                    left[s]--;
                 }
-                mask[l] = m;
-                uint8_t *next = smem + TS_A + (l + 1) * 16384u;
+            }
+            if (!ok) *abort = 1u;
+            // the final commit arrives once every product issued above has completed (drains them
+            // with the full wait limit, also after a wait gave up)
+            mma_commit(fbar);
+            mbar_wait(fbar, 0);
+            if (!wok) mbar_wait(wbar, 0);
+        }
+        __syncwarp();
+    } else {
+        // ---- the epilogue warps of slot s
+        const uint32_t e = warp - 1u, s = e >> 3, h = (e >> 2) & 1u;
+        const uint32_t r = (warp & 3u) * 32u + lane;
+        const bool leader = tid == 32u + TR_EPI * s;
+        const uint32_t lbar = smem_u32(bars + 2 + 3 * s), mbar = lbar + 8u, ebar = lbar + 16u;
+        uint8_t *sb = smem + TS_SLOT + s * TS_SLOT_BYTES;
+        const uint32_t d = tmem + 64u * s + (((warp & 3u) * 32u) << 16);
+        const float inv = n ? 1.0f / (3.0f * (float)n) : 0.0f;
+        uint32_t lph = 0, mph = 0;
+        bool lpending = false;
+        const uint32_t mine = s == 0 ? (cnt + 1u) / 2u : cnt / 2u;
+        for (uint32_t k = 0; k < mine && ok; k++) {
+            const uint32_t tile = blockIdx.x + (2u * k + s) * gridDim.x;
+            const uint32_t i = tile * 128u + r;
+            const bool valid = i < n;
+            // the encoded inputs (k_encode_tiles), 16 KB in one bulk copy, into A_0; the slot's
+            // previous tile has finished reading A_0 (its last products completed)
+            if (leader) bulk_load(smem_u32(sb), tiles + (size_t)tile * 16384u, 16384u, lbar);
+            lpending = true;
+            float t3[3] = {0.f, 0.f, 0.f};
+            if (valid && h == 0) {
+                if (MODE == 1) {
+                    float4 x = samples[i].extra;
+                    t3[0] = x.x; t3[1] = x.y; t3[2] = x.z;
+                } else {
+                    for (int c = 0; c < 3; c++) t3[c] = target[(size_t)i * 4 + c];
+                }
+            }
+            if (!mbar_wait_or_abort(lbar, lph, polls, abort)) {
+                ok = false;
+                break;
+            }
+            lpending = false;
+            lph ^= 1u;
+            mbar_arrive(ebar);
+            // ---- forward
+            // the activation masks of layers 0..3 (this thread's 32 columns): layer l in the
+            // 32-bit half l % 2 of mlo (l < 2) or mhi
+            uint64_t mlo = 0, mhi = 0;
+#pragma unroll 1
+            for (uint32_t l = 0; l < 5; l++) {
+                if (!mbar_wait_or_abort(mbar, mph, polls, abort)) {
+                    ok = false;
+                    break;
+                }
+                mph ^= 1u;
+                tc_after_sync();
+                if (l < 4) {
+                    float a[32];
+                    tmem_ld16(d + 32u * h, a);
+                    tmem_ld16(d + 32u * h + 16u, a + 16);
+                    tmem_wait_ld();
+                    uint32_t m = 0;
 #pragma unroll
-                for (int c = 0; c < 4; c++) store8(next, r, 32 * h + 8 * c, a + 8 * c);
-            } else if (h == 0) {
-                float o[16], d[16];
-                tmem_ld16(tmem + lane, o);
-                tmem_wait_ld();
+                    for (int c = 0; c < 32; c++) {
+                        a[c] = bf16r(fmaxf(a[c], 0.0f));
+                        m |= (a[c] > 0.0f ? 1u : 0u) << c;
+                    }
+                    if (l < 2) mlo |= (uint64_t)m << (32u * l);
+                    else mhi |= (uint64_t)m << (32u * (l - 2u));
+                    uint8_t *next = sb + (l + 1) * 16384u;
 #pragma unroll
-                for (int c = 0; c < 16; c++) d[c] = 0.0f;
-                if (valid) {
-                    for (int c = 0; c < 3; c++) {
-                        float den = o[c] * o[c] + 0.01f;
-                        float e = o[c] - t3[c];
-                        lsum += e * e / den * inv;
-                        d[c] = 2.0f * e / den * inv;
+                    for (int c = 0; c < 4; c++) store8(next, r, 32 * h + 8 * c, a + 8 * c);
+                } else if (h == 0) {
+                    float o[16], dy[16];
+                    tmem_ld16(d, o);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int c = 0; c < 16; c++) dy[c] = 0.0f;
+                    if (valid) {
+                        for (int c = 0; c < 3; c++) {
+                            float den = o[c] * o[c] + 0.01f;
+                            float ee = o[c] - t3[c];
+                            lsum += ee * ee / den * inv;
+                            dy[c] = 2.0f * ee / den * inv;
+                        }
+                    }
+                    // dY row r: two 16-byte pieces of the 16-column tile
+                    for (int c = 0; c < 2; c++) {
+                        __nv_bfloat162 p0 = __floats2bfloat162_rn(dy[8 * c + 0], dy[8 * c + 1]);
+                        __nv_bfloat162 p1 = __floats2bfloat162_rn(dy[8 * c + 2], dy[8 * c + 3]);
+                        __nv_bfloat162 p2 = __floats2bfloat162_rn(dy[8 * c + 4], dy[8 * c + 5]);
+                        __nv_bfloat162 p3 = __floats2bfloat162_rn(dy[8 * c + 6], dy[8 * c + 7]);
+                        uint4 u;
+                        u.x = *reinterpret_cast<uint32_t *>(&p0);
+                        u.y = *reinterpret_cast<uint32_t *>(&p1);
+                        u.z = *reinterpret_cast<uint32_t *>(&p2);
+                        u.w = *reinterpret_cast<uint32_t *>(&p3);
+                        *reinterpret_cast<uint4 *>(sb + TS_DY + kmaj16(r, 8 * c)) = u;
                     }
                 }
-                // dY row r: two 16-byte pieces of the 16-column tile
-                for (int c = 0; c < 2; c++) {
-                    __nv_bfloat162 p0 = __floats2bfloat162_rn(d[8 * c + 0], d[8 * c + 1]);
-                    __nv_bfloat162 p1 = __floats2bfloat162_rn(d[8 * c + 2], d[8 * c + 3]);
-                    __nv_bfloat162 p2 = __floats2bfloat162_rn(d[8 * c + 4], d[8 * c + 5]);
-                    __nv_bfloat162 p3 = __floats2bfloat162_rn(d[8 * c + 6], d[8 * c + 7]);
-                    uint4 u;
-                    u.x = *reinterpret_cast<uint32_t *>(&p0);
-                    u.y = *reinterpret_cast<uint32_t *>(&p1);
-                    u.z = *reinterpret_cast<uint32_t *>(&p2);
-                    u.w = *reinterpret_cast<uint32_t *>(&p3);
-                    *reinterpret_cast<uint4 *>(smem + TS_DY + kmaj16(r, 8 * c)) = u;
+                fence_async_smem();
+                tc_before_sync();
+                mbar_arrive(ebar);
+            }
+            if (!ok) break;
+            // ---- backward: dZ_l = dA_{l+1} masked by the activation of layer l, into A_{l+1}'s
+            // tile (dW_{l+1} has read A_{l+1})
+#pragma unroll 1
+            for (int l = 3; l >= 0; l--) {
+                if (!mbar_wait_or_abort(mbar, mph, polls, abort)) {
+                    ok = false;
+                    break;
                 }
+                mph ^= 1u;
+                tc_after_sync();
+                float g[32];
+                tmem_ld16(d + 32u * h, g);
+                tmem_ld16(d + 32u * h + 16u, g + 16);
+                tmem_wait_ld();
+                const uint32_t m = (uint32_t)((l < 2 ? mlo : mhi) >> (32u * ((uint32_t)l & 1u)));
+#pragma unroll
+                for (int c = 0; c < 32; c++)
+                    if (!((m >> c) & 1u)) g[c] = 0.0f;
+#pragma unroll
+                for (int c = 0; c < 4; c++) store8(sb + (l + 1) * 16384u, r, 32 * h + 8 * c, g + 8 * c);
+                fence_async_smem();
+                tc_before_sync();
+                mbar_arrive(ebar);
             }
-            smem_to_tc();
-        }
-        if (!ok) break;
-        // ---- backward, output layer: dA_4 = dY W_4 (W_4 read MN-major: N = its 64 inputs,
-        // K = its 16 outputs), dW_4 += dY^T A_4 (dY MN-major: M = its 16 outputs, K = the
-        // samples, 8-row groups 256 B apart; A_4 MN-major)
-        if (tid == 0) {
-            mma_bf16(tmem + 64u, sdesc_s(sDY, 256u, 128u), sdesc_s(sW + 4u * 8192u, 128u, 1024u), ID_BMN, 0u);
-#pragma unroll
-            for (uint32_t ks = 0; ks < 8; ks++)
-                mma_bf16(tmem + 128u + 4u * 64u, sdesc_s(sDY + ks * 512u, 128u, 256u), mn64(sA + 4u * 16384u, ks),
-                         ID_ABMN, (any || ks > 0) ? 1u : 0u);
-            mma_commit(bar);
-        }
-        ok = tc_step(bar, phase, polls);
-        for (int l = 3; l >= 0 && ok; l--) {
-            // dZ_l = dA_{l+1} masked by the activation of layer l, into A_{l+1}'s tile (dW_{l+1}
-            // has read A_{l+1})
-            float d[32];
-            tmem_ld16(tmem + lane + 64u + 32u * h, d);
-            tmem_ld16(tmem + lane + 64u + 32u * h + 16u, d + 16);
-            tmem_wait_ld();
-#pragma unroll
-            for (int k = 0; k < 32; k++)
-                if (!((mask[l] >> k) & 1u)) d[k] = 0.0f;
-            const uint32_t sZ = sA + (uint32_t)(l + 1) * 16384u;
-#pragma unroll
-            for (int c = 0; c < 4; c++) store8(smem + TS_A + (l + 1) * 16384u, r, 32 * h + 8 * c, d + 8 * c);
-            smem_to_tc();
-            if (tid == 0) {
-                // dA_l = dZ_l W_l: dZ_l K-major, W_l MN-major (N = inputs, K = outputs)
-#pragma unroll
-                for (uint32_t ks = 0; ks < 4; ks++)
-                    mma_bf16(tmem + 64u, sdesc(sZ + ks * 256u), mn64(sW + (uint32_t)l * 8192u, ks), ID_BMN,
-                             ks > 0 ? 1u : 0u);
-                // dW_l += dZ_l^T A_l: both MN-major, K = the 128 samples
-#pragma unroll
-                for (uint32_t ks = 0; ks < 8; ks++)
-                    mma_bf16(tmem + 128u + 64u * l, mn64(sZ, ks), mn64(sA + (uint32_t)l * 16384u, ks), ID_ABMN,
-                             (any || ks > 0) ? 1u : 0u);
-                mma_commit(bar);
+            if (!ok) break;
+            // ---- input gradient of the grid features (levels [8h, 8h + 8)), scattered into the
+            // grid by k_grid_scatter
+            if (!mbar_wait_or_abort(mbar, mph, polls, abort)) {
+                ok = false;
+                break;
             }
-            ok = tc_step(bar, phase, polls);
-        }
-        if (!ok) break;
-        // ---- input gradient of the grid features (levels [8h, 8h + 8)), scattered into the grid
-        // by k_grid_scatter
-        {
+            mph ^= 1u;
+            tc_after_sync();
             float gin[16];
-            tmem_ld16(tmem + lane + 64u + 16u * h, gin);
+            tmem_ld16(d + 16u * h, gin);
             tmem_wait_ld();
             if (MODE == 1 && valid) {
                 float4 *o = reinterpret_cast<float4 *>(gin_out + (size_t)i * 32u + 16u * h);
                 for (int c = 0; c < 4; c++) o[c] = make_float4(gin[4 * c], gin[4 * c + 1], gin[4 * c + 2], gin[4 * c + 3]);
             }
+            tc_before_sync();
         }
-        any = true;
-        tc_before_sync();
-        __syncthreads();
-        tc_after_sync();
+        if (!ok) {
+            *abort = 1u;
+            // drain this slot's input copy if one is in flight (its issuer's state is exact)
+            if (leader && lpending) mbar_wait(lbar, lph);
+        }
     }
-    // this CTA's dW_l rows (outputs) r, columns [32h, 32h + 32), into its own partial gradient
-    // (summed over the CTAs in a fixed order by k_wgrad_reduce; zeros when it had no tile)
-    if (r < 64u) {
+    tc_before_sync();
+    const bool all_ok = __syncthreads_and(ok) != 0;
+    tc_after_sync();
+    // this CTA's dW_l rows (outputs) r < 64 (16), column group 16 g .. 16 g + 15 of each layer,
+    // into its own partial gradient (summed over the CTAs in a fixed order by k_wgrad_reduce;
+    // zeros when it had no tile)
+    if (warp > 0 && (warp & 3u) < 2u) {
+        const uint32_t e = warp - 1u, g = 2u * (e >> 3) + ((e >> 2) & 1u);
+        const uint32_t r = (warp & 3u) * 32u + lane;
         float *part = w_part + (size_t)blockIdx.x * NRC_WEIGHTS;
         for (uint32_t l = 0; l < 5; l++) {
-            float a[32];
-            if (ok && any) {
-                tmem_ld16(tmem + lane + 128u + 64u * l + 32u * h, a);
-                tmem_ld16(tmem + lane + 128u + 64u * l + 32u * h + 16u, a + 16);
+            float a[16];
+            if (all_ok && cnt) {
+                tmem_ld16(tmem + 128u + 64u * l + 16u * g + ((r & ~31u) << 16), a);
                 tmem_wait_ld();
             } else {
-                for (int k = 0; k < 32; k++) a[k] = 0.0f;
+                for (int k = 0; k < 16; k++) a[k] = 0.0f;
             }
             const uint32_t rows = l < 4 ? 64u : 16u;
             if (r < rows) {
-                float4 *dst = reinterpret_cast<float4 *>(part + l * 4096u + r * 64u + 32u * h);
-                for (int k = 0; k < 8; k++) dst[k] = make_float4(a[4 * k], a[4 * k + 1], a[4 * k + 2], a[4 * k + 3]);
+                float4 *dst = reinterpret_cast<float4 *>(part + l * 4096u + r * 64u + 16u * g);
+                for (int k = 0; k < 4; k++) dst[k] = make_float4(a[4 * k], a[4 * k + 1], a[4 * k + 2], a[4 * k + 3]);
             }
         }
     }
     for (int off = 16; off > 0; off >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, off);
-    if ((tid & 31u) == 0 && lsum != 0.0f) atomicAdd(loss, lsum);
-    if (!ok) {
-        if (tid == 0) atomicExch(err, 1u);
-        // drain the copies and MMAs still in flight with the full wait limit
-        if (!wok) mbar_wait(wbar, 0);
-        else if (lpending) mbar_wait(lbar, lphase);
-        else mbar_wait(bar, phase ^ 1u);
-    }
+    if (lane == 0 && lsum != 0.0f) atomicAdd(loss, lsum);
+    if (!all_ok && tid == 0) atomicExch(err, 1u);
     tc_before_sync();
     __syncthreads();
     tc_after_sync();
