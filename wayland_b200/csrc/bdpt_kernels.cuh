@@ -50,15 +50,20 @@ __device__ __forceinline__ void bd_store(const BdVerts &V, uint32_t cap, uint32_
     V.e[o] = make_float4(r.tput.x, r.tput.y, r.tput.z, r.aux);
 }
 
-// ComputePdfForward (BDPT.cu:42-50)
-__device__ __forceinline__ float bd_pdf_forward(const DevScene &sc, v3 wi, const BdV &mid,
-                                                const BdV &next) {
-    v3 d = next.pos - mid.pos;
+// ComputePdfForward (BDPT.cu:42-50) on the fields it reads: the pdf of scattering at the middle
+// vertex (position mpos, shading normal mns, material mid) from wi towards the next vertex
+// (npos, nns), as an area density there
+__device__ __forceinline__ float bd_pdf_fwd(const DevScene &sc, v3 wi, v3 mpos, v3 mns, uint32_t mid, v3 npos,
+                                            v3 nns) {
+    v3 d = npos - mpos;
     float dist = length(d);
     d = d / dist;
-    Mat m = load_mat(sc.mats + mid.id);
-    float p = pdf_disney(m, mid.ns, wi, d);
-    return clampf(p, 1e-30f, 1e30f) * fabsf(dot(next.ns, d)) / (dist * dist);
+    Mat m = load_mat(sc.mats + mid);
+    float p = pdf_disney(m, mns, wi, d);
+    return clampf(p, 1e-30f, 1e30f) * fabsf(dot(nns, d)) / (dist * dist);
+}
+__device__ __forceinline__ float bd_pdf_forward(const DevScene &sc, v3 wi, const BdV &mid, const BdV &next) {
+    return bd_pdf_fwd(sc, wi, mid.pos, mid.ns, mid.id, next.pos, next.ns);
 }
 
 // ComputePdfLightDir (BDPT.cu:52-58): PdfCosineHemisphere(d, l.Ns) * |cos at e| / dist^2
@@ -69,84 +74,70 @@ __device__ __forceinline__ float bd_pdf_light_dir(const BdV &l, const BdV &e) {
     return dot(d, l.ns) * RECIP_PI * fabsf(dot(d, e.ns)) / (dist * dist);
 }
 
-// MISweight (BDPT.cu:61-217) with USE_UPT, balance heuristic. lightEnd == -1: the eye path hit
-// a light at eye vertex eyeEnd (whose pdf_light is passed as light_pdf).
-__device__ float bd_mis(const DevScene &sc, const BdptWave &bw, uint32_t slot, int eyeEnd,
-                        int lightEnd, float light_pdf) {
+// MISweight (BDPT.cu:61-217) with USE_UPT, balance heuristic, for the connection of eye vertex
+// eyeEnd (e) and light vertex lightEnd (l), or (lightEnd == -1, e and l unused) for the eye path
+// that hit a light at eye vertex eyeEnd, whose pdf_light is light_pdf.
+// The reference gathers the path's forward pdfs fwd[0 .. S-2] and reverse pdfs inv[0 .. S-1]
+// (S = eyeEnd + lightEnd + 2 strategies) into two arrays and sums the products of their ratios
+// on either side of the current strategy. Here each entry is read where it lies, in the same
+// order and with the same operations: fwd[k] = pdf of eye vertex k + 1 for k < eyeEnd, then the
+// connection's e -> l, l -> ll and the light vertices' pdfs from eyeEnd + lightEnd - k;
+// inv[k] = reverse pdf of eye vertex k + 1 for k < eyeEnd - 1, then e -> ee, l -> e, the light
+// vertices' reverse pdfs, and light_pdf last. The (up to) four pdfs the connection defines go
+// through one call site of the BSDF pdf, which keeps the kernel's code small.
+__device__ float bd_mis(const DevScene &sc, const BdptWave &bw, uint32_t slot, int eyeEnd, int lightEnd,
+                        float light_pdf, const BdV &e, const BdV &l) {
     const uint32_t cap = bw.cap;
     const int strategies = eyeEnd + lightEnd + 2;
-    float fwd[2 * WL_BDPT_MAX_VERTICES], inv[2 * WL_BDPT_MAX_VERTICES];
-    int nf = 0, ni = 0;
-    auto eye_pdfs = [&](int from, int to) {  // eye vertices from..to-1
-        for (int i = from; i < to; ++i) {
-            size_t o = (size_t)i * cap + slot;
-            fwd[nf++] = bw.eye.b[o].w;
-            inv[ni++] = bw.eye.c[o].w;
+    float p_ee = 0.f, p_el = 0.f, p_le = 0.f, p_ll = 0.f;
+    if (lightEnd >= 0) {
+        const v3 d = normalize(l.pos - e.pos);
+#pragma unroll 1
+        for (int r = 0; r < 4; r++) {
+            // r 0: e -> l, 1: l -> e, 2: e -> ee (eyeEnd >= 1), 3: l -> ll (lightEnd >= 1)
+            if (r == 1 && lightEnd == 0) {
+                p_le = bd_pdf_light_dir(l, e);
+                continue;
+            }
+            if ((r == 2 && eyeEnd == 0) || (r == 3 && lightEnd == 0)) continue;
+            const bool at_e = (r & 1) == 0;
+            v3 npos, nns;
+            if (r == 0) {
+                npos = l.pos; nns = l.ns;
+            } else if (r == 1) {
+                npos = e.pos; nns = e.ns;
+            } else {
+                const size_t o = (size_t)(r == 2 ? eyeEnd - 1 : lightEnd - 1) * cap + slot;
+                const float4 pa = r == 2 ? bw.eye.a[o] : bw.lit.a[o];
+                const float4 pb = r == 2 ? bw.eye.b[o] : bw.lit.b[o];
+                npos = f4xyz(pa); nns = f4xyz(pb);
+            }
+            const v3 wi = r == 0 ? e.wi : r == 1 ? l.wi : r == 2 ? d : -d;
+            const float p = bd_pdf_fwd(sc, wi, at_e ? e.pos : l.pos, at_e ? e.ns : l.ns, at_e ? e.id : l.id, npos, nns);
+            if (r == 0) p_el = p;
+            else if (r == 1) p_le = p;
+            else if (r == 2) p_ee = p;
+            else p_ll = p;
         }
-    };
-    auto light_pdfs = [&](int from) {  // light vertices from..0, descending
-        for (int i = from; i >= 0; --i) {
-            size_t o = (size_t)i * cap + slot;
-            fwd[nf++] = bw.lit.b[o].w;
-            inv[ni++] = bw.lit.c[o].w;
-        }
-    };
-    if (lightEnd == -1) {
-        eye_pdfs(1, eyeEnd + 1);
-    } else if (eyeEnd == 0 && lightEnd == 0) {
-        BdV e = bd_load(bw.eye, cap, 0, slot), l = bd_load(bw.lit, cap, 0, slot);
-        fwd[nf++] = bd_pdf_forward(sc, e.wi, e, l);
-        inv[ni++] = bd_pdf_light_dir(l, e);
-    } else if (eyeEnd == 0) {
-        BdV e = bd_load(bw.eye, cap, 0, slot);
-        BdV l = bd_load(bw.lit, cap, lightEnd, slot), ll = bd_load(bw.lit, cap, lightEnd - 1, slot);
-        v3 d = normalize(l.pos - e.pos);
-        float p_el = bd_pdf_forward(sc, e.wi, e, l);
-        float p_le = bd_pdf_forward(sc, l.wi, l, e);
-        float p_ll = bd_pdf_forward(sc, -d, l, ll);
-        fwd[nf++] = p_el;
-        inv[ni++] = p_le;
-        fwd[nf++] = p_ll;
-        inv[ni++] = ll.pdf_inv;
-        light_pdfs(lightEnd - 2);
-    } else if (lightEnd == 0) {
-        BdV ee = bd_load(bw.eye, cap, eyeEnd - 1, slot), e = bd_load(bw.eye, cap, eyeEnd, slot);
-        BdV l = bd_load(bw.lit, cap, 0, slot);
-        v3 d = normalize(l.pos - e.pos);
-        float p_ee = bd_pdf_forward(sc, d, e, ee);
-        float p_el = bd_pdf_forward(sc, e.wi, e, l);
-        float p_le = bd_pdf_light_dir(l, e);
-        eye_pdfs(1, eyeEnd);
-        fwd[nf++] = e.pdf;
-        inv[ni++] = p_ee;
-        fwd[nf++] = p_el;
-        inv[ni++] = p_le;
-    } else {
-        BdV ee = bd_load(bw.eye, cap, eyeEnd - 1, slot), e = bd_load(bw.eye, cap, eyeEnd, slot);
-        BdV l = bd_load(bw.lit, cap, lightEnd, slot), ll = bd_load(bw.lit, cap, lightEnd - 1, slot);
-        v3 d = normalize(l.pos - e.pos);
-        float p_ee = bd_pdf_forward(sc, d, e, ee);
-        float p_el = bd_pdf_forward(sc, e.wi, e, l);
-        float p_le = bd_pdf_forward(sc, l.wi, l, e);
-        float p_ll = bd_pdf_forward(sc, -d, l, ll);
-        eye_pdfs(1, eyeEnd);
-        fwd[nf++] = e.pdf;
-        inv[ni++] = p_ee;
-        fwd[nf++] = p_el;
-        inv[ni++] = p_le;
-        fwd[nf++] = p_ll;
-        inv[ni++] = ll.pdf_inv;
-        light_pdfs(lightEnd - 2);
     }
-    inv[ni++] = light_pdf;
     float den = 1.0f, tmp = 1.0f;
     for (int i = eyeEnd - 1; i >= 0; --i) {
-        tmp *= inv[i + 1] / fwd[i];
+        const int k = i + 1;
+        float iv;
+        if (k < eyeEnd - 1) iv = bw.eye.c[(size_t)(k + 1) * cap + slot].w;
+        else if (k == eyeEnd - 1) iv = lightEnd < 0 ? bw.eye.c[(size_t)eyeEnd * cap + slot].w : p_ee;
+        else iv = lightEnd < 0 ? light_pdf : p_le;
+        tmp *= iv / bw.eye.b[(size_t)(i + 1) * cap + slot].w;
         den += tmp;
     }
     tmp = 1.0f;
     for (int i = eyeEnd + 1; i < strategies; ++i) {
-        tmp *= fwd[i - 1] / inv[i];
+        const int k = i - 1;
+        const float fv = k == eyeEnd ? p_el
+                         : k == eyeEnd + 1 ? p_ll
+                                           : bw.lit.b[(size_t)(eyeEnd + lightEnd - k) * cap + slot].w;
+        const float iv = i == strategies - 1 ? light_pdf : bw.lit.c[(size_t)(eyeEnd + lightEnd - i) * cap + slot].w;
+        tmp *= fv / iv;
         den += tmp;
     }
     float w = 1.0f / den;
@@ -274,7 +265,7 @@ __global__ void __launch_bounds__(PT) k_bd_eye(WaveParams wp, DevScene sc, Queue
                             lp /= tri_area(sc, __float_as_uint(h.y));
                             e.pdf_light = lp;
                             bd_store(bw.eye, cap, v, slot, e);
-                            rad = L * e.tput * bd_mis(sc, bw, slot, (int)v, -1, lp);
+                            rad = L * e.tput * bd_mis(sc, bw, slot, (int)v, -1, lp, e, e);
                         }
                         q.st_rad[slot] = make_float4(rad.x, rad.y, rad.z, 0.f);
                     }
@@ -478,16 +469,23 @@ __global__ void __launch_bounds__(PT) k_bd_connect(WaveParams wp, DevScene sc, Q
                 bool facing = true;
                 if (l_is_light && !sc.lights[l.id & ~BD_LIGHT].two_sided && dot(l.ns, vis) > 0.0f) facing = false;
                 if (facing) {
-                    Mat me = load_mat(sc.mats + e.id);
-                    v3 fe = eval_disney(me, e.ns, e.ng, e.wi, vis, v3(1.f));
-                    v3 cv = e.tput * fe * fabsf(dot(e.ns, vis)) * fabsf(dot(l.ns, vis)) * l.tput / (dist * dist);
-                    if (!l_is_light) {
-                        Mat ml = load_mat(sc.mats + l.id);
-                        cv = cv * eval_disney(ml, l.ns, l.ng, -vis, l.wi, v3(1.f));
+                    // the BSDF at e (e.wi -> vis) and, unless l is on the light, at l (-vis -> l.wi),
+                    // through one call site
+                    v3 fe, fl;
+#pragma unroll 1
+                    for (int r = 0; r < 2; r++) {
+                        if (r == 1 && l_is_light) break;
+                        const v3 f = eval_disney(load_mat(sc.mats + (r == 0 ? e.id : l.id)), r == 0 ? e.ns : l.ns,
+                                                 r == 0 ? e.ng : l.ng, r == 0 ? e.wi : -vis, r == 0 ? vis : l.wi,
+                                                 v3(1.f));
+                        if (r == 0) fe = f;
+                        else fl = f;
                     }
+                    v3 cv = e.tput * fe * fabsf(dot(e.ns, vis)) * fabsf(dot(l.ns, vis)) * l.tput / (dist * dist);
+                    if (!l_is_light) cv = cv * fl;
                     if (cv.x + cv.y + cv.z > 1e-10f) {
                         float lp0 = bw.lit.d[slot].w;  // light vertex pdf_light
-                        val = cv * bd_mis(sc, bw, slot, (int)i, (int)j, lp0);
+                        val = cv * bd_mis(sc, bw, slot, (int)i, (int)j, lp0, e, l);
                         org = e.pos;
                         tmax = dist * (1.0f - wp.eps);
                         push = true;
