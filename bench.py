@@ -460,10 +460,12 @@ def bdpt_ao_leg(wl, torch, ctx, res=1024, spp=256, oracle_spp=2048, ao_res=(512,
     film.close()
     film = wl.Film(ctx, res, res, fp64=True)
     p = wl.render_params(res, res, spp, strategy=wl.STRATEGY_BDPT, max_depth=10)
+    torch.cuda.nvtx.range_push("bdpt")  # the window a profiler can select (--nvtx-include bdpt/)
     e0.record(stream)
     wl.render(ctx, scene, cam, p, film)
     e1.record(stream)
     e1.synchronize()
+    torch.cuda.nvtx.range_pop()
     ms = e0.elapsed_time(e1)
     st = ctx.stats()
     img = film.download64()
@@ -715,6 +717,9 @@ def main():
     ap.add_argument("--no-graph", action="store_true", help="skip the progressive 1-spp launches/graph leg")
     ap.add_argument("--no-cornell", action="store_true", help="skip the Cornell-box configuration leg")
     ap.add_argument("--bdpt-only", action="store_true", help="only the BDPT + AO leg (prints its JSON)")
+    ap.add_argument("--bdpt-res", type=int, default=1024, help="image side of the BDPT leg")
+    ap.add_argument("--bdpt-spp", type=int, default=256, help="samples per pixel of the BDPT leg")
+    ap.add_argument("--bdpt-oracle-spp", type=int, default=2048, help="samples per pixel of its oracle")
     ap.add_argument("--nrc-res", default="1920x1080", help="resolution of the radiance-cache comparison")
     ap.add_argument("--nrc-oracle-spp", type=int, default=8192)
     ap.add_argument("--nrc-budget-s", type=float, default=60.0)
@@ -744,7 +749,8 @@ def main():
     torch.cuda.set_device(local)
     if args.bdpt_only:
         ctx = wl.Context(local)
-        print(json.dumps(bdpt_ao_leg(wl, torch, ctx)), flush=True)
+        print(json.dumps(bdpt_ao_leg(wl, torch, ctx, res=args.bdpt_res, spp=args.bdpt_spp,
+                                     oracle_spp=args.bdpt_oracle_spp)), flush=True)
         ctx.close()
         return 0
     if args.nrc_only:

@@ -64,6 +64,23 @@ def test_gradients_match_oracle(cache):
     assert np.abs(g - ref).max() < 5e-3 * scale, (np.abs(g - ref).max(), scale)
 
 
+@pytest.mark.parametrize("n", [20000, 40000, 65536])
+def test_gradients_many_tiles_per_cta(cache, n):
+    """Batches of 2 to 4 tiles of 128 rows per CTA (the training kernel keeps two in flight and
+    accumulates every tile's weight gradient in tensor memory), with a ragged last tile: the
+    gradient matches the oracle and is the same bit for bit on a second run (fixed order)."""
+    c, _, _ = cache
+    x, t = batch(n, 10 + n)
+    dx, dt = dev(x), dev(t)
+    g = c.gradients(dx.data_ptr(), dt.data_ptr(), n)
+    _, ref = nrc_oracle.gradients(c.weights(), x, t)
+    scale = np.abs(ref).max()
+    assert scale > 0
+    assert np.abs(g - ref).max() < 5e-3 * scale, (np.abs(g - ref).max(), scale)
+    g2 = c.gradients(dx.data_ptr(), dt.data_ptr(), n)
+    assert np.array_equal(g.view(np.uint32), g2.view(np.uint32))
+
+
 def test_training_fits(ctx):
     sc = scenes.cornell_box(16, 16)
     s = wl.Scene(ctx, sc)
