@@ -97,21 +97,12 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v) {
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// write row r (64 values, rounded to bfloat16) of a K-major tile
-__device__ __forceinline__ void store_row(uint8_t *tile, uint32_t r, const float *x) {
-#pragma unroll
-    for (int c = 0; c < 8; c++) {
-        __nv_bfloat162 p0 = __floats2bfloat162_rn(x[8 * c + 0], x[8 * c + 1]);
-        __nv_bfloat162 p1 = __floats2bfloat162_rn(x[8 * c + 2], x[8 * c + 3]);
-        __nv_bfloat162 p2 = __floats2bfloat162_rn(x[8 * c + 4], x[8 * c + 5]);
-        __nv_bfloat162 p3 = __floats2bfloat162_rn(x[8 * c + 6], x[8 * c + 7]);
-        uint4 u;
-        u.x = *reinterpret_cast<uint32_t *>(&p0);
-        u.y = *reinterpret_cast<uint32_t *>(&p1);
-        u.z = *reinterpret_cast<uint32_t *>(&p2);
-        u.w = *reinterpret_cast<uint32_t *>(&p3);
-        *reinterpret_cast<uint4 *>(tile + kmaj(r, 8 * c)) = u;
-    }
+// max(bfloat16(lo), 0), max(bfloat16(hi), 0) as one packed pair (lo in the low half). Rounding
+// keeps the sign, so this is bfloat16(max(x, 0)) up to the sign of a zero, which no later
+// product or mask can see.
+__device__ __forceinline__ uint32_t relu_pack(float lo, float hi) {
+    __nv_bfloat162 p = __hmax2(__floats2bfloat162_rn(lo, hi), __float2bfloat162_rn(0.0f));
+    return *reinterpret_cast<uint32_t *>(&p);
 }
 
 // bfloat16 image of the MLP weights in the tensor-core operand layout, built once per weight
@@ -251,8 +242,14 @@ __global__ void __launch_bounds__(128 * QC, 1)
                 for (int c = 0; c < 4; c++) tmem_ld16(tmem + lane_base + 16u * c, h + 16 * c);
                 tmem_wait_ld();
 #pragma unroll
-                for (int j = 0; j < NRC_HID; j++) h[j] = fmaxf(h[j], 0.0f);
-                store_row(bufs[b], r, h);
+                for (int c = 0; c < 8; c++) {
+                    uint4 u;
+                    u.x = relu_pack(h[8 * c + 0], h[8 * c + 1]);
+                    u.y = relu_pack(h[8 * c + 2], h[8 * c + 3]);
+                    u.z = relu_pack(h[8 * c + 4], h[8 * c + 5]);
+                    u.w = relu_pack(h[8 * c + 6], h[8 * c + 7]);
+                    *reinterpret_cast<uint4 *>(bufs[b] + kmaj(r, 8 * c)) = u;
+                }
                 fence_async_smem();
             } else {
                 float o[16];
@@ -623,17 +620,22 @@ __global__ void __launch_bounds__(TR_THREADS, 1)
                     tmem_ld16(d + 32u * h, a);
                     tmem_ld16(d + 32u * h + 16u, a + 16);
                     tmem_wait_ld();
-                    uint32_t m = 0;
+                    // activations rounded to bfloat16, ReLU on the packed pairs; mask bit c: the
+                    // activation of column 32 h + c is above zero
+                    uint32_t pk[16], m = 0;
 #pragma unroll
-                    for (int c = 0; c < 32; c++) {
-                        a[c] = bf16r(fmaxf(a[c], 0.0f));
-                        m |= (a[c] > 0.0f ? 1u : 0u) << c;
+                    for (int c = 0; c < 16; c++) {
+                        pk[c] = relu_pack(a[2 * c], a[2 * c + 1]);
+                        m |= ((pk[c] & 0x7fffu) != 0u ? 1u : 0u) << (2 * c);
+                        m |= ((pk[c] & 0x7fff0000u) != 0u ? 1u : 0u) << (2 * c + 1);
                     }
                     if (l < 2) mlo |= (uint64_t)m << (32u * l);
                     else mhi |= (uint64_t)m << (32u * (l - 2u));
                     uint8_t *next = sb + (l + 1) * 16384u;
 #pragma unroll
-                    for (int c = 0; c < 4; c++) store8(next, r, 32 * h + 8 * c, a + 8 * c);
+                    for (int c = 0; c < 4; c++)
+                        *reinterpret_cast<uint4 *>(next + kmaj(r, 32 * h + 8 * c)) =
+                            make_uint4(pk[4 * c], pk[4 * c + 1], pk[4 * c + 2], pk[4 * c + 3]);
                 } else if (h == 0) {
                     float o[16], dy[16];
                     tmem_ld16(d, o);
