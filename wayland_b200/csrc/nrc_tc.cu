@@ -218,6 +218,15 @@ __global__ void __launch_bounds__(128 * QC, 1)
             pending[b ^ 1u] = true;
         }
         const uint32_t aA = smem_u32(bufs[b]);
+        // MODE 2: the query's weight and slot and the slot's radiance, loaded now so that their
+        // latency hides behind the five layers (each query has its own path slot, which nothing
+        // else writes during this kernel)
+        const uint32_t qi = t * 128u + r;
+        float4 qe = make_float4(0.f, 0.f, 0.f, 0.f), qv = qe;
+        if (MODE == 2 && qi < n) {
+            qe = q[qi].extra;
+            qv = rad[__float_as_uint(qe.w)];
+        }
         for (int layer = 0; layer < 5; layer++) {
             const uint32_t wB = smem_u32(smem + (layer < 4 ? layer * 8192u : 4 * 8192u));
             const uint32_t id = layer < 4 ? idesc(64, 128) : idesc(16, 128);
@@ -260,13 +269,11 @@ __global__ void __launch_bounds__(128 * QC, 1)
                     if (MODE == 0) {
                         *reinterpret_cast<float4 *>(out + (size_t)i * 4) = make_float4(o[0], o[1], o[2], o[3]);
                     } else {
-                        const float4 e = q[i].extra;
-                        const uint32_t slot = __float_as_uint(e.w);
-                        float4 v = rad[slot];
-                        v.x += e.x * fmaxf(o[0], 0.0f);
-                        v.y += e.y * fmaxf(o[1], 0.0f);
-                        v.z += e.z * fmaxf(o[2], 0.0f);
-                        rad[slot] = v;
+                        float4 v = qv;
+                        v.x += qe.x * fmaxf(o[0], 0.0f);
+                        v.y += qe.y * fmaxf(o[1], 0.0f);
+                        v.z += qe.z * fmaxf(o[2], 0.0f);
+                        rad[__float_as_uint(qe.w)] = v;
                     }
                 }
             }
