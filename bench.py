@@ -324,7 +324,7 @@ def raycast_microbench(wl, torch, ctx, sc, scene, stream, tune=None):
     return out
 
 
-def graph_leg(wl, torch, ctx, sc, scene, stream, repeats=12, frames=4):
+def graph_leg(wl, torch, ctx, sc, scene, stream, repeats=24, frames=4):
     """Progressive rendering, 1 spp per call at 1920x1080 on the benchmark scene: device time per
     call with direct launches and with every wave replayed as one CUDA graph. The two modes
     alternate in blocks of `frames` calls, `repeats` blocks each; the median block time per
