@@ -208,7 +208,7 @@ __device__ __forceinline__ Rng bd_rng(const WaveParams &wp, const Queues &q, uin
 }
 
 // One eye vertex per ray of queue `in` (all at depth `depth`); TraceEyeSubpath's loop body.
-__global__ void __launch_bounds__(PT) k_bd_eye(WaveParams wp, DevScene sc, Queues q, BdptWave bw,
+__global__ void __launch_bounds__(PT, 3) k_bd_eye(WaveParams wp, DevScene sc, Queues q, BdptWave bw,
                                                int in, uint32_t depth) {
     wave_dyn(wp);
     const uint32_t n = q.counters[in];
@@ -374,7 +374,7 @@ __global__ void __launch_bounds__(PT) k_bd_light_gen(WaveParams wp, DevScene sc,
 }
 
 // One light-subpath vertex per ray of queue `in` (all reaching vertex depth - 1).
-__global__ void __launch_bounds__(PT) k_bd_light(WaveParams wp, DevScene sc, Queues q, BdptWave bw,
+__global__ void __launch_bounds__(PT, 3) k_bd_light(WaveParams wp, DevScene sc, Queues q, BdptWave bw,
                                                  int in, uint32_t depth) {
     wave_dyn(wp);
     const uint32_t n = q.counters[in];
@@ -443,7 +443,7 @@ __global__ void __launch_bounds__(PT) k_bd_light(WaveParams wp, DevScene sc, Que
 }
 
 // One thread per connection (EvalContri without its visibility ray + MISweight).
-__global__ void __launch_bounds__(PT) k_bd_connect(WaveParams wp, DevScene sc, Queues q, BdptWave bw) {
+__global__ void __launch_bounds__(PT, 3) k_bd_connect(WaveParams wp, DevScene sc, Queues q, BdptWave bw) {
     const uint32_t total = bw.counters[0];
     const uint32_t stride = gridDim.x * blockDim.x;
     const uint32_t cap = bw.cap;
