@@ -496,6 +496,8 @@ WL_API int wl_debug_rng(wl_context *ctx, uint32_t rng, uint64_t seed, const uint
  *  - All calls on a device share the one array and its contents persist between calls. Calls
  *    whose work overlaps on the GPU (other streams, other threads, other contexts on the same
  *    device) race on it and must not overlap.
+ *  - strategy: the path tracer only (UPT, NEE, MIS); WL_STRATEGY_BDPT, whose subpath vertices
+ *    and connections do not fit the array, is rejected with WL_ERR_INVALID_ARG.
  *  - flags: only WL_RENDER_SORT_MATERIALS; other flags are rejected with WL_ERR_INVALID_ARG.
  *    The render uses the context's launch shapes (wl_autotune / wl_set_tune) but always sizes
  *    its own waves, and it restores the caller's current device before returning.

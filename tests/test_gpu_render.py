@@ -359,6 +359,13 @@ def test_batch_matches_separate_renders(ctx):
             for f, r in zip(gfilms, grefs):
                 assert np.array_equal(bits(f.download()), bits(r))
                 f.close()
+        # batches run the path tracer; a bidirectional job is refused, not rendered another way
+        sc0 = jobs[0][0]
+        bd = wl.render_params(sc0.width, sc0.height, 2, strategy=wl.STRATEGY_BDPT, max_depth=6)
+        bf = wl.Film(ctx, sc0.width, sc0.height)
+        with pytest.raises(wl.WlError, match="INVALID_ARG.*path tracer"):
+            wl.render_batch(ctx, objs[:1], [sc0.camera_struct()], [bd], [bf])
+        bf.close()
         for s in objs:
             s.close()
     finally:

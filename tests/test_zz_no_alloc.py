@@ -78,6 +78,9 @@ def test_noalloc_fast_mode_and_limit(own_ctx):
     for flag in (_abi.RENDER_GRAPH, _abi.RENDER_TRAVERSAL_STATS):
         with pytest.raises(wl.WlError, match="INVALID_ARG.*SORT_MATERIALS"):
             noalloc(ctx, scene, cam, wl.render_params(96, 64, 4, flags=flag), b)
+    # the bidirectional program needs more memory than the static array holds
+    with pytest.raises(wl.WlError, match="INVALID_ARG.*path tracer only"):
+        noalloc(ctx, scene, cam, wl.render_params(96, 64, 4, strategy=wl.STRATEGY_BDPT, max_depth=6), b)
     # the caller's current device is the same after the call
     torch.cuda.set_device(0)
     noalloc(ctx, scene, cam, p, b)

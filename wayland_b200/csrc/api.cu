@@ -2028,7 +2028,8 @@ int noalloc_render_inputs(wl_context *c, wl_scene *s, const wl_camera *cam,
     ARG(p->width == f->f.W && p->height == f->f.H, "film size differs from the render size");
     ARG(p->spp > 0, "spp must be > 0");
     ARG(p->max_depth > 0 && p->max_depth <= 1024, "max_depth out of range");
-    ARG(p->strategy <= WL_STRATEGY_MIS, "bad strategy");
+    ARG(p->strategy <= WL_STRATEGY_MIS,
+        "bad strategy: wl_render_noalloc renders the path tracer only (UPT, NEE or MIS)");
     ARG(p->rng <= WL_RNG_PCG32, "bad rng");
     ARG(p->math <= WL_MATH_STRICT, "bad math mode");
     ARG(p->lights <= WL_LIGHTS_POWER, "bad light selection");
