@@ -56,3 +56,36 @@ def geometries():
     return [("soup", *soup), ("cornell", cb.V, cb.I), ("sphere", sph.V, sph.I),
             ("dup_centroids", dupV, dupI), ("grid", np.array(gv, np.float32), np.array(gi, np.uint32)),
             ("one", *one), ("degenerate", degV, degI)]
+
+
+def degenerate_rays(seed, lo=-1.5, hi=1.5):
+    """Rays a caller can hand to wl_cast_rays by mistake, each kind over several origins: NaN
+    directions (whole or one component), a zero direction, an infinite or NaN origin, an infinite
+    direction component, tmin > tmax, tmin == tmax, and negative tmax. None may hit anything."""
+    rng = np.random.default_rng(seed)
+    kinds = []
+    for _ in range(12):
+        o = rng.uniform(lo, hi, 3)
+        d = rng.normal(size=3)
+        d /= np.linalg.norm(d)
+        nan = float("nan")
+        inf = float("inf")
+        kinds += [
+            (o, (nan, nan, nan), 1e-3, 1e30),
+            (o, (d[0], nan, d[2]), 1e-3, 1e30),
+            (o, (0.0, 0.0, 0.0), 1e-3, 1e30),
+            ((inf, o[1], o[2]), d, 1e-3, 1e30),
+            ((o[0], nan, o[2]), d, 1e-3, 1e30),
+            (o, (d[0], inf, d[2]), 1e-3, 1e30),
+            (o, d, 2.0, 1.0),
+            (o, d, 0.5, 0.5),
+            (o, d, 0.0, -1.0),
+        ]
+    r = np.zeros(len(kinds), _abi.RAY_DTYPE)
+    for i, (o, d, t0, t1) in enumerate(kinds):
+        r["org"][i] = o
+        r["dir"][i] = d
+        r["tmin"][i] = t0
+        r["tmax"][i] = t1
+    return r
+

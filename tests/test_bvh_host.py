@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 
 import pyoracle as po
-from helpers import axis_rays, geometries, random_rays
+from helpers import axis_rays, degenerate_rays, geometries, random_rays
 
 GEOMS = geometries()
 
@@ -117,3 +117,30 @@ def test_batched_traversal_matches(host_bvh, oracle, post, refill, node_steps):
     anyf, _ = host_cast_batched(host_bvh, h, rays, 2, post, refill, node_steps)
     assert np.array_equal(anyf["prim"] == 0xFFFFFFFF, anyr["prim"] == 0xFFFFFFFF)
     host_bvh.hb_destroy(h)
+
+
+def test_degenerate_rays_miss(host_bvh, oracle):
+    """Degenerate rays (NaN or zero directions, infinite or NaN origins, empty [tmin, tmax]) end
+    their traversal and hit nothing, in the single-lane and the batched warp traversal, like the
+    brute force; valid rays in the same batch keep their hits."""
+    from wayland_b200 import scenes
+    sc = scenes.displaced_sphere(subdiv=24)
+    h, V, I = host_build(host_bvh, sc.V, sc.I)
+    bad = degenerate_rays(5)
+    good = random_rays(500, 6, -3.0, 3.0)
+    rays = np.concatenate([good[:250], bad, good[250:]])
+    for mode in (0, 1):
+        ref = oracle.cast_bruteforce(V, I, rays, mode)
+        assert (ref["prim"][250:250 + len(bad)] == 0xFFFFFFFF).all()
+        single, _ = host_cast(host_bvh, h, rays, mode)
+        batched, _ = host_cast_batched(host_bvh, h, rays, mode, 8, 6, 3)
+        for got in (single, batched):
+            assert (got["prim"][250:250 + len(bad)] == 0xFFFFFFFF).all()
+            if mode == 0:
+                assert np.array_equal(got.view(np.uint32).reshape(-1, 4), ref.view(np.uint32).reshape(-1, 4))
+            else:
+                assert np.array_equal(got["prim"] == 0xFFFFFFFF, ref["prim"] == 0xFFFFFFFF)
+    far, _ = host_cast(host_bvh, h, rays, 2)
+    assert (far["prim"][250:250 + len(bad)] == 0xFFFFFFFF).all()
+    host_bvh.hb_destroy(h)
+

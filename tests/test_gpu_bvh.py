@@ -6,7 +6,7 @@ import pytest
 import torch
 
 import wayland_b200 as wl
-from helpers import axis_rays, geometries, random_rays
+from helpers import axis_rays, degenerate_rays, geometries, random_rays
 from wayland_b200 import scenes
 
 pytestmark = pytest.mark.gpu
@@ -86,6 +86,35 @@ def test_empty_scene(ctx):
     sc = wl.Scene(ctx, g)
     h = sc.cast_host(random_rays(100, 1), wl.CAST_CLOSEST)
     assert (h["prim"] == wl.INVALID).all()
+    sc.close()
+
+
+@pytest.mark.parametrize("kind", [wl.BVH_LBVH, wl.BVH_SAH])
+def test_degenerate_rays(ctx, oracle, kind):
+    """wl_cast_rays takes device rays it cannot check on the host: NaN or zero directions,
+    infinite or NaN origins and empty [tmin, tmax] end their traversal and hit nothing (closest
+    and any hit, both any-hit child orders), like the brute force; valid rays in the same batch
+    keep their hits bit for bit."""
+    s = scenes.displaced_sphere(subdiv=24)
+    sc = wl.Scene(ctx, s, bvh_kind=kind)
+    bad = degenerate_rays(5)
+    good = random_rays(500, 6, -3.0, 3.0)
+    rays = np.concatenate([good[:250], bad, good[250:]])
+    sl = slice(250, 250 + len(bad))
+    ref = oracle.cast_bruteforce(s.V, s.I, rays, 0)
+    got = cast_device(ctx, sc, rays, wl.CAST_CLOSEST)
+    assert (got["prim"][sl] == wl.INVALID).all()
+    assert hits_equal(got, ref)
+    anyr = oracle.cast_bruteforce(s.V, s.I, rays, 1)
+    for far in (0, 1):
+        ctx.set_tune(dict(wave_paths=0, extend_ctas_per_sm=0, extend_refill=12, shadow_ctas_per_sm=0,
+                          shadow_refill=12, shadow_far_first=far))
+        try:
+            anyg = cast_device(ctx, sc, rays, wl.CAST_ANY)
+        finally:
+            ctx.set_tune(None)
+        assert (anyg["prim"][sl] == wl.INVALID).all()
+        assert np.array_equal(anyg["prim"] == wl.INVALID, anyr["prim"] == wl.INVALID)
     sc.close()
 
 
